@@ -1,0 +1,355 @@
+"""CPU oracle driver: loads a ParaHPOP run configuration and its environment
+files with independent Python readers, and propagates targets with the C++
+restatement in ``phop_oracle.cpp``.  TEST INFRASTRUCTURE ONLY - used by the
+tests, the smoke check and the benchmark's CPU-baseline leg as the checker.
+
+Readers follow the reference loaders:
+  config + targets    src/common/driver.cpp:72-123
+  .tab                src/common/engine/interface/config/model/sphericalharmonics/Coefficients.h:241-362
+  .brie (layout 1)    third_party/brie/brie/states/metadata/EphUnit.h:55-86, states/EphUnit.h:223-238
+  .brot2 (type 4)     third_party/brie/brie/orientations/metadata/EphUnit.cpp:148-167
+  SW-All              src/common/engine/paraHPOP/model/environment/atmosphere/Nrlmsise00Atmosphere.h:168-235
+  EOP-All             src/common/engine/paraHPOP/model/environment/earthcorrections/EarthCorrections.h:142-177
+  bodies              src/common/engine/interface/config/model/environment/Bodies.h:105-120 (NAIF-id order)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import math
+import os
+import struct
+import subprocess
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "lib" / "liboracle.so"
+
+NAIF = {"Sun": 10, "Moon": 301, "Earth": 399, "MercuryBarycenter": 1, "VenusBarycenter": 2, "MarsBarycenter": 4,
+        "JupiterBarycenter": 5, "SaturnBarycenter": 6, "UranusBarycenter": 7, "NeptuneBarycenter": 8,
+        "PlutoBarycenter": 9}
+F_GRAVITY, F_SHAPE, F_RADIATION, F_ATMOSPHERE, F_OCCULTING = 1, 2, 4, 8, 16
+
+
+def build(force=False):
+    """Compile the oracle library (g++, OpenMP)."""
+    src = HERE / "phop_oracle.cpp"
+    deps = [src, HERE.parent / "parahpop_b200/csrc/nrlmsise00.cuh", HERE.parent / "parahpop_b200/csrc/tides.cuh"]
+    if LIB.exists() and not force and all(LIB.stat().st_mtime >= d.stat().st_mtime for d in deps):
+        return LIB
+    LIB.parent.mkdir(parents=True, exist_ok=True)
+    cmd = ["g++", "-O3", "-march=x86-64-v3", "-std=c++17", "-fopenmp", "-shared", "-fPIC", "-w",
+           str(src), "-o", str(LIB)]
+    subprocess.run(cmd, check=True)
+    return LIB
+
+
+# ---------------------------------------------------------------------------
+# CBOR (RFC 8949) decoder, the subset the .brie/.brot files use
+# ---------------------------------------------------------------------------
+def cbor_loads(buf: bytes):
+    pos = 0
+
+    def head():
+        nonlocal pos
+        b = buf[pos]; pos += 1
+        major, info = b >> 5, b & 31
+        if info < 24:
+            return major, info
+        n = {24: 1, 25: 2, 26: 4, 27: 8}[info]
+        v = int.from_bytes(buf[pos:pos + n], "big"); pos += n
+        if major == 7:
+            return major, (info, v)
+        return major, v
+
+    def item():
+        nonlocal pos
+        major, v = head()
+        if major == 0:
+            return v
+        if major == 1:
+            return -1 - v
+        if major == 2:
+            out = buf[pos:pos + v]; pos += v; return out
+        if major == 3:
+            out = buf[pos:pos + v].decode(); pos += v; return out
+        if major == 4:
+            return [item() for _ in range(v)]
+        if major == 5:
+            d = {}
+            for _ in range(v):
+                k = item(); d[k] = item()
+            return d
+        if major == 6:
+            return item()
+        if major == 7:
+            if isinstance(v, tuple):
+                info, raw = v
+                if info == 27:
+                    return struct.unpack(">d", raw.to_bytes(8, "big"))[0]
+                if info == 26:
+                    return struct.unpack(">f", raw.to_bytes(4, "big"))[0]
+                if info == 25:
+                    return float(np.frombuffer(raw.to_bytes(2, "big"), dtype=">f2")[0])
+            return {20: False, 21: True, 22: None}.get(v)
+        raise ValueError("bad CBOR")
+
+    return item()
+
+
+# ---------------------------------------------------------------------------
+class _Env(C.Structure):
+    _fields_ = [
+        ("sh_degree", C.c_int), ("sh_order", C.c_int), ("sh_normalized", C.c_int),
+        ("sh_R", C.c_double), ("sh_GM", C.c_double),
+        ("sh_C", C.POINTER(C.c_double)), ("sh_S", C.POINTER(C.c_double)),
+        ("nbodies", C.c_int), ("body_id", C.POINTER(C.c_int)), ("body_gm", C.POINTER(C.c_double)),
+        ("body_radius", C.POINTER(C.c_double)), ("body_flags", C.POINTER(C.c_int)),
+        ("flattening", C.c_double), ("au", C.c_double),
+        ("neph", C.c_int), ("eph_target", C.POINTER(C.c_int)), ("eph_center", C.POINTER(C.c_int)),
+        ("eph_nint", C.POINTER(C.c_int)), ("eph_pdeg", C.POINTER(C.c_int)), ("eph_offset", C.POINTER(C.c_int64)),
+        ("eph_data", C.POINTER(C.c_double)),
+        ("has_rot", C.c_int), ("rot_nnut", C.c_int), ("rot_nerp", C.c_int), ("rot_data", C.POINTER(C.c_double)),
+        ("has_nrl", C.c_int), ("nrl_ndays", C.c_int), ("nrl_start_mjd", C.c_double), ("nrl_hcutoff", C.c_double),
+        ("nrl_density_scale", C.c_double), ("nrl_weather", C.POINTER(C.c_double)),
+        ("solid", C.c_int), ("ocean", C.c_int), ("relativity", C.c_int), ("zero_tide", C.c_int),
+        ("eop_n", C.c_int), ("eop_first_mjd", C.c_double), ("eop", C.POINTER(C.c_double)),
+    ]
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def calendar_mjd(y, m, d):
+    a = (14 - m) // 12
+    yy = y + 4800 - a
+    mm = m + 12 * a - 3
+    jdn = d + (153 * mm + 2) // 5 + 365 * yy + yy // 4 - yy // 100 + yy // 400 - 32045
+    return float(jdn) - 2400001.0
+
+
+@dataclass
+class Environment:
+    cfg: dict
+    keep: list
+    env: _Env
+    duration: float
+    step: float
+    max_steps: int
+    threads: int
+
+
+def load_environment(config_path) -> Environment:
+    config_path = Path(config_path).resolve()
+    cfg = json.loads(config_path.read_text())
+    base = config_path.parent
+    envc = cfg["model"]["environment"]
+    P = lambda p: (base / p).resolve()
+    keep = []
+    e = _Env()
+
+    def hold(a):
+        keep.append(a); return a
+
+    # constants
+    consts = json.loads(P(envc["constants"]).read_text())
+    au = next(c["AU"] for c in consts if "AU" in c)
+    byid = {c["NAIFID"]: c for c in consts if "NAIFID" in c}
+    e.au = au
+    # bodies (sorted by NAIF id, Bodies.h:105-120)
+    rows = []
+    flattening = 0.0
+    shape = None
+    atm = None
+    for name, bc in envc["bodies"].items():
+        nid = NAIF[name]
+        flags = 0
+        g = bc.get("gravity", False)
+        if g:
+            flags |= F_GRAVITY
+            if isinstance(g, dict) and "shape" in g:
+                flags |= F_SHAPE
+                shape = g["shape"]
+        if bc.get("radiation"):
+            flags |= F_RADIATION
+        if "atmosphere" in bc:
+            flags |= F_ATMOSPHERE
+            atm = bc["atmosphere"]["nrlmsise00"]
+        if bc.get("occulting"):
+            flags |= F_OCCULTING
+        if name == "Earth":
+            flattening = bc.get("flattening", 0.0)
+        gm = bc.get("gm", byid.get(nid, {}).get("GM", 0.0))
+        radius = byid.get(nid, {}).get("R", 0.0)
+        rows.append((nid, gm, radius, flags))
+    rows.sort()
+    e.nbodies = len(rows)
+    e.body_id = _ip(hold(np.array([r[0] for r in rows], dtype=np.int32)))
+    e.body_gm = _dp(hold(np.array([r[1] for r in rows], dtype=np.float64)))
+    e.body_radius = _dp(hold(np.array([r[2] for r in rows], dtype=np.float64)))
+    e.body_flags = _ip(hold(np.array([r[3] for r in rows], dtype=np.int32)))
+    e.flattening = flattening
+    # geopotential
+    if shape is not None:
+        lines = [l for l in P(shape["file"]).read_text().splitlines() if l.strip()]
+        hdr = [float(x) for x in lines[0].split(",")]
+        N = int(shape.get("degree", hdr[3]))
+        M = int(shape.get("order", hdr[4]))
+        half = (N + 2) * (N + 3) // 2  # storage for maxDeg+1 as the loader allocates
+        Cc = np.zeros(half); Ss = np.zeros(half)
+        for l in lines[1:]:
+            v = [float(x) for x in l.split(",")]
+            n, m = int(v[0]), int(v[1])
+            if n > N or m > M:
+                continue
+            Cc[n * (n + 1) // 2 + m] = v[2]
+            if m > 0:
+                Ss[n * (n + 1) // 2 + m] = v[3]
+        e.sh_degree, e.sh_order, e.sh_normalized = N, M, int(hdr[5])
+        e.sh_R, e.sh_GM = hdr[0], hdr[1]
+        e.sh_C = _dp(hold(Cc)); e.sh_S = _dp(hold(Ss))
+    # ephemeris
+    units = []
+    for f in envc.get("ephemeris", []):
+        j = cbor_loads(P(f).read_bytes())
+        assert j["layout"] == 1, "only layout 1 is read by the oracle"
+        units += j["core"]
+    off = np.zeros(len(units), dtype=np.int64)
+    data = []
+    o = 0
+    for k, u in enumerate(units):
+        off[k] = o
+        data += list(u["data"])
+        o += len(u["data"])
+    e.neph = len(units)
+    e.eph_target = _ip(hold(np.array([u["metadata"]["target"] for u in units], dtype=np.int32)))
+    e.eph_center = _ip(hold(np.array([u["metadata"]["center"] for u in units], dtype=np.int32)))
+    e.eph_nint = _ip(hold(np.array([u["metadata"]["nintervals"] for u in units], dtype=np.int32)))
+    e.eph_pdeg = _ip(hold(np.array([u["metadata"]["pdeg"] for u in units], dtype=np.int32)))
+    e.eph_offset = hold(off).ctypes.data_as(C.POINTER(C.c_int64))
+    e.eph_data = _dp(hold(np.array(data, dtype=np.float64)))
+    # orientation
+    for f in envc.get("orientations", []):
+        j = cbor_loads(P(f).read_bytes())
+        for u in j["core"]:
+            if u["metadata"]["unit_type"] == 4:
+                e.has_rot = 1
+                e.rot_nnut = u["metadata"]["n_nodes_nut"]
+                e.rot_nerp = u["metadata"]["n_nodes_erp"]
+                e.rot_data = _dp(hold(np.array(u["data"], dtype=np.float64)))
+    # atmosphere
+    if atm is not None:
+        recs = []
+        for line in P(atm["spaceWeatherFile"]).read_text().splitlines():
+            t = line.split()
+            if len(t) < 33:
+                continue
+            try:
+                y, mo, d = int(t[0]), int(t[1]), int(t[2])
+                ap = [int(x) for x in t[14:22]]
+                avg = int(t[22])
+                adj, adjc, obs, obsc = float(t[26]), float(t[28]), float(t[30]), float(t[31])
+            except ValueError:
+                continue
+            recs.append((calendar_mjd(y, mo, d), obs, obsc, adj, adjc, avg, ap))
+        s0 = atm.get("coverageStartMjdUtc", -1.0)
+        s1 = atm.get("coverageEndMjdUtc", -1.0)
+        ks = math.floor(s0) - 4.0 if s0 >= 0 else recs[0][0]
+        ke = math.floor(s1) + 1.0 if s1 >= 0 else recs[-1][0]
+        sel = [r for r in recs if ks <= r[0] <= ke]
+        W = np.zeros((13, len(sel)))
+        for i, r in enumerate(sel):
+            W[0, i], W[1, i], W[2, i], W[3, i], W[4, i] = r[1], r[2], r[3], r[4], r[5]
+            W[5:13, i] = r[6]
+        e.has_nrl = 1
+        e.nrl_ndays = len(sel)
+        e.nrl_start_mjd = sel[0][0]
+        e.nrl_hcutoff = atm.get("hCutoff", 1000.0)
+        e.nrl_density_scale = atm.get("densityScale", 1.0)
+        e.nrl_weather = _dp(hold(np.ascontiguousarray(W.reshape(-1))))
+    # Earth corrections
+    ec = envc.get("earthCorrections")
+    if ec:
+        e.solid = int(bool(ec.get("solidEarthTides", False)))
+        e.ocean = int(bool(ec.get("oceanTides", False)))
+        e.relativity = int(bool(ec.get("relativity", False)))
+        e.zero_tide = int(ec.get("tideSystem", "zero_tide") == "zero_tide")
+        if e.solid or e.ocean:
+            rows = []
+            for line in P(ec["eopFile"]).read_text().splitlines():
+                t = line.split()
+                if len(t) < 13:
+                    continue
+                rows.append((float(t[3]), float(t[4]), float(t[5]), float(t[6]), float(t[12])))
+            E = np.array(rows)
+            e.eop_n = len(rows)
+            e.eop_first_mjd = E[0, 0]
+            e.eop = _dp(hold(np.ascontiguousarray(E[:, 1:].T.reshape(-1))))
+    ex = cfg["execution"]
+    return Environment(cfg, keep, e, float(cfg["run"]["duration_seconds"]),
+                       float(ex["integration"]["initialStepSize"]), int(ex["integration"]["maxNumSteps"]),
+                       int(ex.get("maxThreads", 1)))
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = C.CDLL(str(build()))
+        _lib.oracle_propagate.restype = C.c_int
+        _lib.oracle_propagate.argtypes = [C.POINTER(_Env), C.c_int64] + [C.POINTER(C.c_double)] * 9 + \
+            [C.c_int64, C.POINTER(C.c_double), C.c_int]
+        _lib.oracle_nrl_density.restype = C.c_double
+        _lib.oracle_nrl_density.argtypes = [C.c_int] + [C.c_double] * 8 + [C.POINTER(C.c_double)]
+    return _lib
+
+
+def propagate(environment: Environment, targets: dict, duration=None, step=None, threads=None, max_steps=None):
+    """Propagate every target of a reference-schema targets document; returns
+    (ids, final_epochs_mjd2000, final_states (n, 6)).  Per-target
+    ``duration_seconds`` / ``step_seconds`` override the run values."""
+    t = targets["targets"]
+    n = len(t)
+    ids = np.array([x["id"] for x in t])
+    ep = np.array([x["epoch_mjd2000_tdb"] for x in t], dtype=np.float64)
+    st = np.ascontiguousarray(np.array([x["state_km_km_s"] for x in t], dtype=np.float64))
+    g = lambda k: np.array([x[k] for x in t], dtype=np.float64)
+    mass, ad, asrp, cd, cr = g("mass_kg"), g("drag_area_m2"), g("srp_area_m2"), g("cd"), g("cr")
+    dur0 = environment.duration if duration is None else duration
+    stp0 = environment.step if step is None else step
+    dur = np.array([x.get("duration_seconds", dur0) for x in t], dtype=np.float64)
+    stp = np.array([x.get("step_seconds", stp0) for x in t], dtype=np.float64)
+    out_ep = np.zeros(n)
+    ms = environment.max_steps if max_steps is None else max_steps
+    th = threads if threads is not None else (os.cpu_count() or 1)
+    rc = lib().oracle_propagate(C.byref(environment.env), n, _dp(ep), _dp(st), _dp(mass), _dp(ad), _dp(asrp),
+                                _dp(cd), _dp(cr), _dp(dur), _dp(stp), ms, _dp(out_ep), th)
+    if rc:
+        raise RuntimeError("A target stopped without reaching the requested end of simulation.")
+    return ids, out_ep, st
+
+
+def nrl_density(doy, sec, alt, glat, glong, lst, f107A, f107, ap, ap_a):
+    a = np.ascontiguousarray(np.asarray(ap_a, dtype=np.float64))
+    return lib().oracle_nrl_density(int(doy), sec, alt, glat, glong, lst, f107A, f107, ap, _dp(a))
+
+
+def read_final_states(directory):
+    """Parse a final_states.csv written by the reference or by this package."""
+    import csv
+    with open(Path(directory) / "final_states.csv") as fh:
+        rows = list(csv.DictReader(fh))
+    ids = np.array([int(r["id"]) for r in rows])
+    ep = np.array([float(r["epoch_mjd2000_tdb"]) for r in rows])
+    st = np.array([[float(r[k]) for k in ("x_km", "y_km", "z_km", "vx_km_s", "vy_km_s", "vz_km_s")] for r in rows])
+    return ids, ep, st
