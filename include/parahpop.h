@@ -1,0 +1,102 @@
+/*
+ * parahpop-b200 C ABI: the drop-in boundary of the B200 propagation backend.
+ *
+ * Shared library: parahpop_b200/lib/libparahpop_engine.so
+ * Command line:   parahpop_b200/bin/parahpop_gpu CONFIG.json TARGETS.json OUTPUT_DIRECTORY
+ *
+ * Conventions: plain C types only; every call returns 0 on success and 1 on
+ * failure (the reference driver's exit codes); the failure text is available
+ * from phop_last_error().  The library owns device memory; callers own every
+ * host buffer they pass.  One context holds one loaded model configuration
+ * resident on one GPU and is used by one host thread at a time.
+ *
+ * Units and frames are the reference's: states in km and km/s in Earth-centred
+ * ICRF-aligned axes, epochs in MJD2000 TDB days, areas in m^2, masses in kg.
+ */
+#ifndef PARAHPOP_B200_H
+#define PARAHPOP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct phop_context phop_context;
+
+/* Replaces the reference export of the same name and signature
+ * (src/common/engine/paraHPOP/util/log.cu:26-38): 0 silences informational
+ * output, higher values enable it. */
+void paraHPOP_setLogLevel(int level);
+
+/* The reference command-line driver, in process: argument and JSON checks,
+ * environment load, propagation, final_states.csv / summary.json /
+ * configuration_resolved.json outputs, "ParaHPOP: <message>" on stderr and
+ * exit status 0/1.  Replaces int paraHPOP::run(int, char**, const char*)
+ * (include/paraHPOP/driver.h:3, src/common/driver.cpp:57-186); `backend` is
+ * reported in summary.json ("device" for parahpop_gpu). */
+int paraHPOP_run(int argc, char** argv, const char* backend);
+
+/* Loads the configuration file's "model" section and its environment files
+ * and makes them resident on `device` (the reference's
+ * interface::config::Model + Environment::load + model upload,
+ * src/common/driver.cpp:132-135, PH/run.h:5-13).  Relative data paths are
+ * resolved against the configuration file's directory. */
+int phop_create(const char* config_json_path, int device, phop_context** out);
+
+void phop_destroy(phop_context* ctx);
+
+/* Text of the last failure on `ctx` (or of the last failed phop_create when
+ * ctx is NULL).  Valid until the next call on the same context. */
+const char* phop_last_error(const phop_context* ctx);
+
+/* Run parameters read from the configuration (run.duration_seconds,
+ * execution.integration.initialStepSize / maxNumSteps). */
+int phop_run_parameters(const phop_context* ctx, double* duration_s, double* step_s, int64_t* max_steps);
+
+/* Propagates n objects (the reference's device Propagator::run,
+ * src/common/engine/paraHPOP/propagators/device/Propagator.h:33-66, with the
+ * driver's target conversion, src/common/driver.cpp:97-123).
+ *   states: n x 6 row-major; duration_s / step_s: per-object arrays, or NULL
+ *   for the configuration's values (the reference accepts only one of each).
+ * Outputs: final epochs (n) and states (n x 6).  Fails, like the reference,
+ * when an object would need more than the configured maxNumSteps. */
+int phop_propagate(phop_context* ctx, int64_t n, const double* epoch_mjd2000_tdb, const double* states,
+                   const double* mass_kg, const double* drag_area_m2, const double* srp_area_m2, const double* cd,
+                   const double* cr, const double* duration_s, const double* step_s, double* out_epoch_mjd2000_tdb,
+                   double* out_states);
+
+/* Same propagation with the state already resident in device memory:
+ * d_states_soa is a device array of 6*n doubles (x[n], y[n], z[n], vx[n],
+ * vy[n], vz[n]) updated in place; every object shares epoch, duration and
+ * step.  Other arrays are host arrays.  No counterpart in the reference
+ * (which always copies from host); it lets a caller keep batches in HBM. */
+int phop_propagate_device(phop_context* ctx, int64_t n, double* d_states_soa, double epoch_mjd2000_tdb,
+                          const double* mass_kg, const double* drag_area_m2, const double* srp_area_m2,
+                          const double* cd, const double* cr, double duration_s, double step_s,
+                          double* out_epoch_mjd2000_tdb);
+
+/* Execution options (no reference counterpart; the reference hard-codes its
+ * launch shapes):
+ *   "lanes"    lanes per object, 0 = autotuned, else 1, 2, 4, 8 or 16
+ *   "split"    0 = plain FP64, 1 = split precision (FP32 for geopotential
+ *              degrees n > 8, FP64 elsewhere)
+ *   "threads"  threads per CTA (multiple of 32, <= 256) */
+int phop_set_option(phop_context* ctx, const char* key, double value);
+
+typedef struct {
+    double kernel_ms;        /* step kernel time of the last call, CUDA events */
+    double records_ms;       /* epoch-record kernel time of the last call */
+    double total_ms;         /* whole call including host<->device copies */
+    int64_t object_steps;    /* sum over objects of RKF78 steps taken */
+    int64_t launches;        /* kernels launched by the last call */
+    int lanes, ctas, threads, split, shared_grid, tile_in_smem;
+} phop_stats;
+
+int phop_last_stats(const phop_context* ctx, phop_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PARAHPOP_B200_H */

@@ -1,0 +1,159 @@
+"""Python binding of the C ABI in ``include/parahpop.h`` (ctypes over the
+in-tree ``libparahpop_engine.so``).
+
+The operator surface mirrors the reference's: a run configuration (the JSON
+schema of ``example/config/*.json``) plus targets in the reference's target
+schema, propagated by the B200 backend to final epochs and states.  There is
+no CPU path: the library needs a CUDA device and fails loudly without one.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libparahpop_engine.so"
+CLI_PATH = PKG / "bin" / "parahpop_gpu"
+
+_lib = None
+
+
+class PhopStats(C.Structure):
+    _fields_ = [("kernel_ms", C.c_double), ("records_ms", C.c_double), ("total_ms", C.c_double),
+                ("object_steps", C.c_int64), ("launches", C.c_int64), ("lanes", C.c_int), ("ctas", C.c_int),
+                ("threads", C.c_int), ("split", C.c_int), ("shared_grid", C.c_int), ("tile_in_smem", C.c_int)]
+
+
+def library() -> C.CDLL:
+    """Load the engine library (built by ``parahpop_b200.build``)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: run `python -m parahpop_b200.build` first")
+        lib = C.CDLL(str(LIB_PATH))
+        D = C.POINTER(C.c_double)
+        lib.phop_create.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]
+        lib.phop_create.restype = C.c_int
+        lib.phop_destroy.argtypes = [C.c_void_p]
+        lib.phop_last_error.argtypes = [C.c_void_p]
+        lib.phop_last_error.restype = C.c_char_p
+        lib.phop_run_parameters.argtypes = [C.c_void_p, D, D, C.POINTER(C.c_int64)]
+        lib.phop_propagate.argtypes = [C.c_void_p, C.c_int64] + [D] * 11
+        lib.phop_propagate.restype = C.c_int
+        lib.phop_propagate_device.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_double] + [D] * 5 + \
+            [C.c_double, C.c_double, D]
+        lib.phop_propagate_device.restype = C.c_int
+        lib.phop_set_option.argtypes = [C.c_void_p, C.c_char_p, C.c_double]
+        lib.phop_last_stats.argtypes = [C.c_void_p, C.POINTER(PhopStats)]
+        lib.paraHPOP_run.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.c_char_p]
+        lib.paraHPOP_setLogLevel.argtypes = [C.c_int]
+        _lib = lib
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class PhopError(RuntimeError):
+    pass
+
+
+class Propagator:
+    """One loaded configuration, resident on one GPU (``phop_create``)."""
+
+    def __init__(self, config_path, device: int = 0, lanes: int | None = None, split: bool = False,
+                 threads: int | None = None):
+        lib = library()
+        h = C.c_void_p()
+        if lib.phop_create(str(config_path).encode(), device, C.byref(h)) != 0:
+            raise PhopError(lib.phop_last_error(None).decode())
+        self._h = h
+        d, s, m = C.c_double(), C.c_double(), C.c_int64()
+        lib.phop_run_parameters(h, C.byref(d), C.byref(s), C.byref(m))
+        self.duration, self.step, self.max_steps = d.value, s.value, m.value
+        if lanes is not None:
+            self.set_option("lanes", lanes)
+        if split:
+            self.set_option("split", 1)
+        if threads is not None:
+            self.set_option("threads", threads)
+
+    def set_option(self, key: str, value: float):
+        if library().phop_set_option(self._h, key.encode(), float(value)) != 0:
+            raise PhopError(library().phop_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            library().phop_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def propagate(self, epochs, states, mass, drag_area, srp_area, cd, cr, duration=None, step=None):
+        """Propagate arrays of targets; returns (final_epochs, final_states)."""
+        n = len(epochs)
+        f = lambda a: np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+        ep, st, ma, ad, asr, cdd, crr = map(f, (epochs, states, mass, drag_area, srp_area, cd, cr))
+        st = st.reshape(n, 6)
+        dur = None if duration is None else f(np.broadcast_to(duration, (n,)))
+        stp = None if step is None else f(np.broadcast_to(step, (n,)))
+        out_e = np.zeros(n)
+        out_s = np.zeros((n, 6))
+        rc = library().phop_propagate(self._h, n, _dp(ep), _dp(st), _dp(ma), _dp(ad), _dp(asr), _dp(cdd), _dp(crr),
+                                      _dp(dur) if dur is not None else None, _dp(stp) if stp is not None else None,
+                                      _dp(out_e), _dp(out_s))
+        if rc != 0:
+            raise PhopError(library().phop_last_error(self._h).decode())
+        return out_e, out_s
+
+    def propagate_targets(self, targets: dict, use_target_times=True):
+        """Propagate a reference-schema targets document (dict)."""
+        t = targets["targets"]
+        g = lambda k: np.array([x[k] for x in t], dtype=np.float64)
+        dur = step = None
+        if use_target_times and any("duration_seconds" in x for x in t):
+            dur = np.array([x.get("duration_seconds", self.duration) for x in t])
+        if use_target_times and any("step_seconds" in x for x in t):
+            step = np.array([x.get("step_seconds", self.step) for x in t])
+        return self.propagate(g("epoch_mjd2000_tdb"), np.array([x["state_km_km_s"] for x in t]), g("mass_kg"),
+                              g("drag_area_m2"), g("srp_area_m2"), g("cd"), g("cr"), dur, step)
+
+    def propagate_device(self, d_state_ptr: int, n: int, epoch: float, mass, drag_area, srp_area, cd, cr,
+                         duration: float, step: float) -> float:
+        """Propagate an SoA state already in device memory (6*n doubles) in place."""
+        f = lambda a: np.ascontiguousarray(np.broadcast_to(np.asarray(a, dtype=np.float64), (n,)))
+        ma, ad, asr, cdd, crr = map(f, (mass, drag_area, srp_area, cd, cr))
+        out = C.c_double()
+        rc = library().phop_propagate_device(self._h, n, C.c_void_p(d_state_ptr), epoch, _dp(ma), _dp(ad), _dp(asr),
+                                             _dp(cdd), _dp(crr), duration, step, C.byref(out))
+        if rc != 0:
+            raise PhopError(library().phop_last_error(self._h).decode())
+        return out.value
+
+    def stats(self) -> dict:
+        s = PhopStats()
+        library().phop_last_stats(self._h, C.byref(s))
+        return {k: getattr(s, k) for k, _ in PhopStats._fields_}
+
+
+def run(config, targets, output, backend="device") -> int:
+    """In-process equivalent of ``parahpop_gpu CONFIG TARGETS OUTPUT``."""
+    argv = [b"parahpop_gpu", str(config).encode(), str(targets).encode(), str(output).encode()]
+    arr = (C.c_char_p * len(argv))(*argv)
+    return library().paraHPOP_run(len(argv), arr, backend.encode())
+
+
+def run_cli(config, targets, output, env=None) -> subprocess.CompletedProcess:
+    """Run the ``parahpop_gpu`` executable."""
+    return subprocess.run([str(CLI_PATH), str(config), str(targets), str(output)], stdout=subprocess.PIPE,
+                          stderr=subprocess.PIPE, text=True, env=env)

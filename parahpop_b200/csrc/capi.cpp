@@ -1,0 +1,411 @@
+// C ABI and the command-line driver of the B200 backend.
+//
+// The driver restates src/common/driver.cpp:57-186: the same arguments,
+// validation order, error texts, exit codes and output files.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <filesystem>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <limits>
+#include <memory>
+#include <set>
+#include <string>
+
+#include "../../include/parahpop.h"
+#include "engine.hpp"
+
+namespace fs = std::filesystem;
+using phop::Value;
+
+static int g_logLevel = 1;
+static thread_local std::string g_createError;
+
+struct phop_context {
+    std::unique_ptr<phop::Engine> engine;
+    Value config;
+    double duration = 0.0, step = 0.0;
+    int64_t maxSteps = 0;
+    phop::RunOptions opt;
+    phop::RunStats stats;
+    std::string error;
+};
+
+namespace {
+
+// Resolve only the configuration fields documented as paths (driver.cpp:41-55).
+void resolvePaths(Value& v, const fs::path& base, const std::string& key = "") {
+    const bool pathField = key == "file" || key == "spaceWeatherFile" || key == "eopFile" || key == "constants"
+        || key == "ephemeris" || key == "orientations";
+    if (v.isString() && pathField) {
+        fs::path p(v.asString());
+        if (p.is_relative()) p = base / p;
+        p = fs::absolute(p).lexically_normal();
+        if (!fs::is_regular_file(p)) throw std::runtime_error("Required data file not found: " + p.string());
+        v = Value::string(p.string());
+    } else if (v.isObject()) {
+        for (auto& kv : v.members()) resolvePaths(kv.second, base, kv.first);
+    } else if (v.isArray()) {
+        for (auto& item : v.items()) resolvePaths(item, base, key);
+    }
+}
+
+void checkKeys(const Value& v, std::initializer_list<const char*> allowed, const char* context) {
+    if (!v.isObject()) throw std::runtime_error(std::string(context) + " must be an object.");
+    for (const auto& kv : v.members()) {
+        bool found = false;
+        for (const char* k : allowed) found |= kv.first == k;
+        if (!found) throw std::runtime_error(std::string("Unsupported ") + context + " option: " + kv.first);
+    }
+}
+
+// JSON objects written the way the reference's JSON library writes them:
+// keys in sorted order.
+Value sortedCopy(const Value& v) {
+    if (v.isObject()) {
+        Value out = Value::object();
+        std::vector<std::pair<std::string, Value>> m(v.members());
+        std::sort(m.begin(), m.end(), [](auto& a, auto& b) { return a.first < b.first; });
+        for (auto& kv : m) out.set(kv.first, sortedCopy(kv.second));
+        return out;
+    }
+    if (v.isArray()) {
+        Value out = Value::array();
+        for (auto& x : v.items()) out.push(sortedCopy(x));
+        return out;
+    }
+    return v;
+}
+
+struct LoadedConfig {
+    Value config;
+    double duration = 0, step = 0;
+    int64_t maxSteps = 0;
+    int threads = 1;
+};
+
+LoadedConfig readConfig(const fs::path& configPath, const char* backend) {
+    LoadedConfig lc;
+    Value config = phop::parseJson(phop::readTextFile(configPath.string()));
+    checkKeys(config, {"run", "execution", "model"}, "configuration");
+    checkKeys(config.at("run"), {"duration_seconds"}, "run");
+    checkKeys(config.at("execution"), {"maxThreads", "integration"}, "execution");
+    checkKeys(config.at("execution").at("integration"), {"initialStepSize", "maxNumSteps"}, "integration");
+    const int64_t maxSteps = config.at("execution").at("integration").at("maxNumSteps").asInt();
+    const int64_t threads = config.at("execution").find("maxThreads") ? config.at("execution").at("maxThreads").asInt() : 1;
+    if (maxSteps <= 0 || threads <= 0) throw std::runtime_error("maxNumSteps and maxThreads must be positive integers.");
+    const double duration = config.at("run").at("duration_seconds").asDouble();
+    config.erase("run");
+    if (!(duration > 0) || !std::isfinite(duration)) throw std::runtime_error("duration_seconds must be finite and positive.");
+    config.find("execution")->set("on", Value::string(backend));
+    const double step = config.at("execution").at("integration").at("initialStepSize").asDouble();
+    if (!(step > 0) || !std::isfinite(step)) throw std::runtime_error("initialStepSize must be finite and positive.");
+    resolvePaths(config, configPath.parent_path());
+    lc.config = config;
+    lc.duration = duration;
+    lc.step = step;
+    lc.maxSteps = maxSteps;
+    lc.threads = (int)threads;
+    return lc;
+}
+
+}  // namespace
+
+extern "C" {
+
+void paraHPOP_setLogLevel(int level) { g_logLevel = level; }
+
+int phop_create(const char* configPath, int device, phop_context** out) {
+    try {
+        if (!configPath || !out) throw std::runtime_error("phop_create: null argument");
+        *out = nullptr;
+        const fs::path cp = fs::absolute(configPath);
+        LoadedConfig lc = readConfig(cp, "device");
+        int count = 0;
+        const cudaError_t st = cudaGetDeviceCount(&count);
+        if (st != cudaSuccess || count == 0)
+            throw std::runtime_error(std::string("No usable CUDA device: ") + cudaGetErrorString(st));
+        phop::HostEnvironment env;
+        phop::loadEnvironment(lc.config.at("model"), env);
+        auto ctx = std::make_unique<phop_context>();
+        ctx->engine = std::make_unique<phop::Engine>(env, device);
+        ctx->config = lc.config;
+        ctx->duration = lc.duration;
+        ctx->step = lc.step;
+        ctx->maxSteps = lc.maxSteps;
+        *out = ctx.release();
+        return 0;
+    } catch (const std::exception& e) {
+        g_createError = e.what();
+        return 1;
+    }
+}
+
+void phop_destroy(phop_context* ctx) { delete ctx; }
+
+const char* phop_last_error(const phop_context* ctx) { return ctx ? ctx->error.c_str() : g_createError.c_str(); }
+
+int phop_run_parameters(const phop_context* ctx, double* duration, double* step, int64_t* maxSteps) {
+    if (!ctx) return 1;
+    if (duration) *duration = ctx->duration;
+    if (step) *step = ctx->step;
+    if (maxSteps) *maxSteps = ctx->maxSteps;
+    return 0;
+}
+
+int phop_set_option(phop_context* ctx, const char* key, double value) {
+    if (!ctx || !key) return 1;
+    const std::string k(key);
+    if (k == "lanes") {
+        const int L = (int)value;
+        if (L != 0 && L != 1 && L != 2 && L != 4 && L != 8 && L != 16) {
+            ctx->error = "lanes must be 0, 1, 2, 4, 8 or 16";
+            return 1;
+        }
+        ctx->opt.lanes = L;
+    } else if (k == "split") {
+        ctx->opt.split = value != 0.0;
+    } else if (k == "threads") {
+        const int t = (int)value;
+        if (t < 32 || t > 256 || t % 32) {
+            ctx->error = "threads must be a multiple of 32 in [32, 256]";
+            return 1;
+        }
+        ctx->opt.threads = t;
+    } else if (k == "ctas_per_sm") {
+        ctx->opt.ctasPerSm = (int)value;
+    } else {
+        ctx->error = "Unknown option: " + k;
+        return 1;
+    }
+    return 0;
+}
+
+int phop_propagate(phop_context* ctx, int64_t n, const double* epoch, const double* states, const double* mass,
+                   const double* dragArea, const double* srpArea, const double* cd, const double* cr,
+                   const double* duration, const double* step, double* outEpoch, double* outStates) {
+    if (!ctx) return 1;
+    try {
+        if (n <= 0) throw std::runtime_error("targets must be a nonempty array.");
+        phop::TargetSet t;
+        t.ids.resize(n);
+        t.epoch.assign(epoch, epoch + n);
+        t.state.assign(states, states + 6 * n);
+        t.mass.assign(mass, mass + n);
+        t.dragArea.assign(dragArea, dragArea + n);
+        t.srpArea.assign(srpArea, srpArea + n);
+        t.cd.assign(cd, cd + n);
+        t.cr.assign(cr, cr + n);
+        t.duration = duration ? std::vector<double>(duration, duration + n) : std::vector<double>(n, ctx->duration);
+        t.step = step ? std::vector<double>(step, step + n) : std::vector<double>(n, ctx->step);
+        for (int64_t i = 0; i < n; ++i) {
+            for (int k = 0; k < 6; ++k)
+                if (!std::isfinite(t.state[6 * i + k])) throw std::runtime_error("State contains a nonfinite value.");
+            if (!std::isfinite(t.epoch[i]) || !std::isfinite(t.mass[i]) || !std::isfinite(t.dragArea[i])
+                || !std::isfinite(t.srpArea[i]) || !std::isfinite(t.cd[i]) || !std::isfinite(t.cr[i])
+                || t.mass[i] <= 0 || t.dragArea[i] <= 0 || t.srpArea[i] < 0 || t.cd[i] < 0 || t.cr[i] < 0)
+                throw std::runtime_error("Invalid target epoch or physical parameter.");
+            if (!(t.duration[i] > 0) || !std::isfinite(t.duration[i]))
+                throw std::runtime_error("duration_seconds must be finite and positive.");
+            if (!(t.step[i] > 0) || !std::isfinite(t.step[i]))
+                throw std::runtime_error("initialStepSize must be finite and positive.");
+        }
+        double lo = INFINITY, hi = -INFINITY;
+        for (int64_t i = 0; i < n; ++i) {
+            lo = std::min(lo, t.epoch[i]);
+            hi = std::max(hi, t.epoch[i] + t.duration[i] / 86400.0);
+        }
+        ctx->engine->assertCoverage(lo, hi);
+        std::vector<double> oe, os;
+        ctx->stats = phop::RunStats{};
+        ctx->engine->propagate(t, ctx->maxSteps, ctx->opt, oe, os, &ctx->stats);
+        std::copy(oe.begin(), oe.end(), outEpoch);
+        std::copy(os.begin(), os.end(), outStates);
+        return 0;
+    } catch (const std::exception& e) {
+        ctx->error = e.what();
+        return 1;
+    }
+}
+
+int phop_propagate_device(phop_context* ctx, int64_t n, double* dState, double epoch, const double* mass,
+                          const double* dragArea, const double* srpArea, const double* cd, const double* cr,
+                          double duration, double step, double* outEpoch) {
+    if (!ctx) return 1;
+    try {
+        if (n <= 0) throw std::runtime_error("targets must be a nonempty array.");
+        std::vector<double> bc(n), ams(n), ep(n, epoch);
+        for (int64_t i = 0; i < n; ++i) {
+            if (!(mass[i] > 0) || !(dragArea[i] > 0) || srpArea[i] < 0 || cd[i] < 0 || cr[i] < 0)
+                throw std::runtime_error("Invalid target epoch or physical parameter.");
+            const double area = dragArea[i] * 1e-6;
+            const double crf = cr[i] * srpArea[i] / dragArea[i];
+            ams[i] = crf * area / mass[i];
+            bc[i] = cd[i] * area / mass[i];
+        }
+        ctx->engine->assertCoverage(epoch, epoch + duration / 86400.0);
+        std::vector<double> oe;
+        ctx->stats = phop::RunStats{};
+        ctx->engine->propagateResident(n, dState, ep.data(), bc.data(), ams.data(), duration, step, ctx->maxSteps,
+                                       ctx->opt, oe, &ctx->stats);
+        if (outEpoch) *outEpoch = oe.empty() ? 0.0 : oe[0];
+        return 0;
+    } catch (const std::exception& e) {
+        ctx->error = e.what();
+        return 1;
+    }
+}
+
+int phop_last_stats(const phop_context* ctx, phop_stats* out) {
+    if (!ctx || !out) return 1;
+    out->kernel_ms = ctx->stats.kernelMs;
+    out->records_ms = ctx->stats.recordsMs;
+    out->total_ms = ctx->stats.totalMs;
+    out->object_steps = ctx->stats.objectSteps;
+    out->launches = ctx->stats.launches;
+    out->lanes = ctx->stats.lanes;
+    out->ctas = ctx->stats.ctas;
+    out->threads = ctx->stats.threads;
+    out->split = ctx->stats.split;
+    out->shared_grid = ctx->stats.sharedGrid;
+    out->tile_in_smem = ctx->stats.tileInSmem;
+    return 0;
+}
+
+int paraHPOP_run(int argc, char** argv, const char* backend) {
+    try {
+        if (argc == 2 && std::string(argv[1]) == "--help") {
+            std::cout << "Usage: " << argv[0] << " CONFIG.json TARGETS.json OUTPUT_DIRECTORY\n"
+                      << "Backend: " << backend << "; integrator: RKF78 fixed step\n";
+            return 0;
+        }
+        if (argc != 4) throw std::runtime_error("Expected CONFIG.json TARGETS.json OUTPUT_DIRECTORY (or --help).");
+        const fs::path configPath = fs::absolute(argv[1]);
+        const fs::path inputPath = fs::absolute(argv[2]);
+        const fs::path outputPath = fs::absolute(argv[3]);
+        for (const char* f : {"final_states.csv", "summary.json", "configuration_resolved.json"})
+            if (fs::exists(outputPath / f))
+                throw std::runtime_error("Output exists; use a new directory: " + outputPath.string());
+        LoadedConfig lc = readConfig(configPath, backend);
+        const Value input = phop::parseJson(phop::readTextFile(inputPath.string()));
+        const Value& targets = input.at("targets");
+        if (!targets.isArray() || targets.size() == 0) throw std::runtime_error("targets must be a nonempty array.");
+        if (targets.size() > (size_t)std::numeric_limits<int32_t>::max())
+            throw std::runtime_error("Too many targets for the engine index type.");
+        const int64_t n = (int64_t)targets.size();
+        phop::TargetSet t;
+        std::set<int64_t> ids;
+        double earliest = INFINITY, latest = -INFINITY;
+        for (int64_t i = 0; i < n; ++i) {
+            const Value& tg = targets[i];
+            const int64_t id = tg.at("id").asInt();
+            if (!ids.insert(id).second) throw std::runtime_error("Target IDs must be unique.");
+            const Value& st = tg.at("state_km_km_s");
+            if (!st.isArray() || st.size() != 6) throw std::runtime_error("state_km_km_s must hold six numbers.");
+            for (int k = 0; k < 6; ++k) {
+                const double x = st[k].asDouble();
+                if (!std::isfinite(x)) throw std::runtime_error("State contains a nonfinite value.");
+                t.state.push_back(x);
+            }
+            const double epoch = tg.at("epoch_mjd2000_tdb").asDouble();
+            const double mass = tg.at("mass_kg").asDouble();
+            const double area = tg.at("drag_area_m2").asDouble();
+            const double srp = tg.at("srp_area_m2").asDouble();
+            const double cd = tg.at("cd").asDouble();
+            const double cr = tg.at("cr").asDouble();
+            if (!std::isfinite(epoch) || !std::isfinite(mass) || !std::isfinite(area) || !std::isfinite(srp)
+                || !std::isfinite(cd) || !std::isfinite(cr) || mass <= 0 || area <= 0 || srp < 0 || cd < 0 || cr < 0)
+                throw std::runtime_error("Invalid target epoch or physical parameter.");
+            // per-target duration / step: extension for mixed populations
+            const double dur = tg.numberOr("duration_seconds", lc.duration);
+            const double stp = tg.numberOr("step_seconds", lc.step);
+            if (!(dur > 0) || !std::isfinite(dur)) throw std::runtime_error("duration_seconds must be finite and positive.");
+            if (!(stp > 0) || !std::isfinite(stp)) throw std::runtime_error("initialStepSize must be finite and positive.");
+            t.ids.push_back(id);
+            t.epoch.push_back(epoch);
+            t.mass.push_back(mass);
+            t.dragArea.push_back(area);
+            t.srpArea.push_back(srp);
+            t.cd.push_back(cd);
+            t.cr.push_back(cr);
+            t.duration.push_back(dur);
+            t.step.push_back(stp);
+            earliest = std::min(earliest, epoch);
+            latest = std::max(latest, epoch + dur / 86400.0);
+        }
+        if (std::string(backend) == "device") {
+            int count = 0;
+            const cudaError_t status = cudaGetDeviceCount(&count);
+            if (status != cudaSuccess || count == 0)
+                throw std::runtime_error(std::string("No usable CUDA device: ") + cudaGetErrorString(status));
+        }
+        const auto environmentStart = std::chrono::steady_clock::now();
+        phop::HostEnvironment env;
+        phop::loadEnvironment(lc.config.at("model"), env);
+        phop::Engine engine(env, 0);
+        engine.assertCoverage(earliest, latest);
+        const auto integrationStart = std::chrono::steady_clock::now();
+        std::vector<double> finalEpoch, finalState;
+        phop::RunOptions opt;
+        if (const char* s = std::getenv("PARAHPOP_B200_SPLIT")) opt.split = std::atoi(s) != 0;
+        if (const char* s = std::getenv("PARAHPOP_B200_LANES")) opt.lanes = std::atoi(s);
+        engine.propagate(t, lc.maxSteps, opt, finalEpoch, finalState, nullptr);
+        {
+            const cudaError_t status = cudaDeviceSynchronize();
+            if (status != cudaSuccess) throw std::runtime_error(cudaGetErrorString(status));
+        }
+        const auto integrationEnd = std::chrono::steady_clock::now();
+        double maxEpochError = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            const double expected = t.epoch[i] + t.duration[i] / 86400.0;
+            const double err = std::abs(finalEpoch[i] - expected) * 86400.0;
+            if (!std::isfinite(err) || err > 1e-4) throw std::runtime_error("A target did not reach its requested end epoch.");
+            maxEpochError = std::max(maxEpochError, err);
+            for (int k = 0; k < 6; ++k)
+                if (!std::isfinite(finalState[6 * i + k])) throw std::runtime_error("Nonfinite final state.");
+        }
+        fs::create_directories(outputPath);
+        std::ofstream csv(outputPath / "final_states.csv");
+        csv << "id,epoch_mjd2000_tdb,x_km,y_km,z_km,vx_km_s,vy_km_s,vz_km_s\n" << std::setprecision(17);
+        for (int64_t i = 0; i < n; ++i) {
+            csv << t.ids[i] << ',' << finalEpoch[i];
+            for (int k = 0; k < 6; ++k) csv << ',' << finalState[6 * i + k];
+            csv << '\n';
+        }
+        csv.close();
+        if (!csv) throw std::runtime_error("Failed to write final_states.csv.");
+        Value summary = Value::object();
+        summary.set("backend", Value::string(backend));
+        summary.set("targets", Value::integer(n));
+        summary.set("integrator", Value::string("RKF78 fixed step"));
+        summary.set("initial_step_seconds", Value::real(lc.step));
+        summary.set("duration_seconds", Value::real(lc.duration));
+        summary.set("environment_seconds",
+                    Value::real(std::chrono::duration<double>(integrationStart - environmentStart).count()));
+        summary.set("propagation_seconds",
+                    Value::real(std::chrono::duration<double>(integrationEnd - integrationStart).count()));
+        summary.set("max_end_epoch_error_seconds", Value::real(maxEpochError));
+        summary.set("validation_passed", Value::boolean(true));
+        std::ofstream resolved(outputPath / "configuration_resolved.json");
+        resolved << sortedCopy(lc.config).dump(2) << '\n';
+        resolved.close();
+        if (!resolved) throw std::runtime_error("Failed to write resolved configuration.");
+        const std::string sj = sortedCopy(summary).dump(2);
+        std::ofstream ss(outputPath / "summary.json");
+        ss << sj << '\n';
+        ss.close();
+        if (!ss) throw std::runtime_error("Failed to write summary.");
+        std::cout << sj << '\n';
+        return 0;
+    } catch (const std::exception& e) {
+        std::cerr << "ParaHPOP: " << e.what() << '\n';
+        return 1;
+    }
+}
+
+}  // extern "C"

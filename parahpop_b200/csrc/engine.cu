@@ -1,0 +1,868 @@
+// Host engine: environment loading (reference file formats and validation),
+// device residency, coefficient-tile construction and kernel launches.
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <sstream>
+#include <stdexcept>
+
+#include "engine.hpp"
+
+namespace phop {
+
+static double mjdToEtHost(double mjd) { return std::fma(mjd, 86400.0, -43200.0); }
+static double etToMjdHost(double et) { return std::fma(et, 1.0 / 86400.0, 0.5); }
+
+#define PHOP_CUDA(call)                                                                                    \
+    do {                                                                                                   \
+        cudaError_t e_ = (call);                                                                           \
+        if (e_ != cudaSuccess) throw std::runtime_error(std::string("CUDA error: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+// ---- naming (IF/naming/points/Registry.h, NAIF ids) ------------------------------------------------
+static int naifId(const std::string& name) {
+    static const std::map<std::string, int> ids = {
+        {"Sun", 10}, {"Moon", 301}, {"Earth", 399}, {"MercuryBarycenter", 1}, {"VenusBarycenter", 2},
+        {"EarthMoonBarycenter", 3}, {"MarsBarycenter", 4}, {"JupiterBarycenter", 5}, {"SaturnBarycenter", 6},
+        {"UranusBarycenter", 7}, {"NeptuneBarycenter", 8}, {"PlutoBarycenter", 9}};
+    auto it = ids.find(name);
+    if (it == ids.end()) throw std::runtime_error("Unknown body name: " + name);
+    return it->second;
+}
+
+// ---- loaders ------------------------------------------------------------------------------------------
+static void loadConstants(const std::string& path, HostEnvironment& env) {
+    const Value c = parseJson(readTextFile(path));
+    if (!c.isArray()) throw std::runtime_error("Constants file must hold a JSON array: " + path);
+    for (const Value& item : c.items()) {
+        if (const Value* au = item.find("AU")) env.au = au->asDouble();
+        if (const Value* id = item.find("NAIFID")) {
+            const int nid = (int)id->asInt();
+            if (const Value* gm = item.find("GM")) env.constGm[nid] = gm->asDouble();
+            if (const Value* r = item.find("R")) env.constRadius[nid] = r->asDouble();
+        }
+    }
+    if (env.au <= 0) throw std::runtime_error("Constants file lacks AU: " + path);
+}
+
+// PDS-SHA table (Coefficients.h:241-362)
+static void loadShTable(const Value& shape, HostEnvironment& env) {
+    const std::string path = shape.at("file").asString();
+    const std::string delimStr = shape.find("delimiter") ? shape.at("delimiter").asString() : std::string(",");
+    const char delim = delimStr.empty() ? ',' : delimStr[0];
+    const int headerLines = shape.find("headerLines") ? (int)shape.at("headerLines").asInt() : 0;
+    const int reqDeg = shape.find("degree") ? (int)shape.at("degree").asInt() : -1;
+    const int reqOrd = shape.find("order") ? (int)shape.at("order").asInt() : -1;
+    std::istringstream in(readTextFile(path));
+    std::string line;
+    std::vector<std::vector<double>> rows;
+    int skip = headerLines;
+    while (std::getline(in, line)) {
+        if (skip > 0) {
+            --skip;
+            continue;
+        }
+        std::vector<double> row;
+        std::string tok;
+        std::istringstream ls(line);
+        bool any = false;
+        while (std::getline(ls, tok, delim)) {
+            size_t a = tok.find_first_not_of(" \t\r");
+            if (a == std::string::npos) continue;
+            row.push_back(std::stod(tok.substr(a)));
+            any = true;
+        }
+        if (any) rows.push_back(row);
+    }
+    if (rows.empty()) throw std::runtime_error("No coefficients found in file: " + path);
+    const auto& h = rows.front();
+    if (h.size() != 8)
+        throw std::runtime_error("Invalid PDS-SHA header in file: " + path + " - Expected 8 values, found "
+                                 + std::to_string(h.size()));
+    const int maxDegH = (int)h[3], maxOrdH = (int)h[4], norm = (int)h[5];
+    if (reqDeg != -1 && reqDeg > maxDegH)
+        throw std::runtime_error("Requested maximum degree " + std::to_string(reqDeg)
+                                 + " exceeds available maximum degree " + std::to_string(maxDegH) + " in file: " + path);
+    if (reqOrd != -1 && reqOrd > maxOrdH)
+        throw std::runtime_error("Requested maximum order " + std::to_string(reqOrd)
+                                 + " exceeds available maximum order " + std::to_string(maxOrdH) + " in file: " + path);
+    if (norm != 0 && norm != 1) throw std::runtime_error("Unsupported normalization flag in file: " + path);
+    if (h[6] != 0.0 || h[7] != 0.0) throw std::runtime_error("Non-zero latitude/longitude offsets are not supported.");
+    env.shDegree = reqDeg == -1 ? maxDegH : reqDeg;
+    env.shOrder = reqOrd == -1 ? maxOrdH : reqOrd;
+    if (env.shOrder > env.shDegree) env.shOrder = env.shDegree;
+    if (env.shDegree <= 0) throw std::runtime_error("Maximum degree must be > 0");
+    env.shNormalized = norm;
+    env.shR = h[0];
+    env.shGM = h[1];
+    const size_t tri = (size_t)(env.shDegree + 1) * (env.shDegree + 2) / 2;
+    env.shC.assign(tri, 0.0);
+    env.shS.assign(tri, 0.0);
+    for (size_t i = 1; i < rows.size(); ++i) {
+        const auto& r = rows[i];
+        if (r.size() != 4 && r.size() != 6)
+            throw std::runtime_error("Invalid coefficient row in file: " + path + " - Expected 6 values, found "
+                                     + std::to_string(r.size()));
+        const int n = (int)r[0], m = (int)r[1];
+        if (n <= 0) throw std::runtime_error("Invalid degree 0 coefficient found in file: " + path);
+        if (m > n) throw std::runtime_error("Invalid order " + std::to_string(m) + " for degree " + std::to_string(n)
+                                            + " found in file: " + path);
+        if (m == 0 && r[3] != 0.0) throw std::runtime_error("Invalid non-zero Sn0 coefficient found in file: " + path);
+        if (n > env.shDegree || m > env.shOrder) continue;
+        env.shC[(size_t)n * (n + 1) / 2 + m] = r[2];
+        if (m > 0) env.shS[(size_t)n * (n + 1) / 2 + m] = r[3];
+    }
+    env.hasShape = true;
+}
+
+static const Value& cborCore(const Value& root, const std::string& path) {
+    const Value* layout = root.find("layout");
+    if (!layout) throw std::runtime_error("Unknown BRIE layout type: " + path);
+    if (layout->asInt() != 1)
+        throw std::runtime_error("BRIE layout " + std::to_string(layout->asInt()) + " is not supported: " + path);
+    return root.at("core");
+}
+
+static void loadEphemeris(const std::string& path, HostEnvironment& env) {
+    const Value root = parseCbor(readBinaryFile(path));
+    const Value& core = cborCore(root, path);
+    for (const Value& u : core.items()) {
+        const Value& md = u.at("metadata");
+        if (md.at("frame").asInt() != 1) throw std::runtime_error("Ephemeris units must use the ICRF frame (1): " + path);
+        if (md.at("dtype").asInt() != 2)
+            throw std::runtime_error("Only Type-2 Chebyshev position units are supported: " + path);
+        EphUnitHost e;
+        e.target = (int)md.at("target").asInt();
+        e.center = (int)md.at("center").asInt();
+        e.nint = (int)md.at("nintervals").asInt();
+        e.pdeg = (int)md.at("pdeg").asInt();
+        e.startEpoch = md.at("startEpoch").asDouble();
+        e.finalEpoch = md.at("finalEpoch").asDouble();
+        const Value& d = u.at("data");
+        e.data.resize(d.size());
+        for (size_t k = 0; k < d.size(); ++k) e.data[k] = d[k].asDouble();
+        if (e.data.size() != (size_t)(1 + e.nint + 3 * (e.pdeg + 1) * e.nint))
+            throw std::runtime_error("Ephemeris unit size mismatch for target " + std::to_string(e.target));
+        env.eph.push_back(std::move(e));
+    }
+}
+
+static void loadOrientation(const std::string& path, HostEnvironment& env) {
+    const Value root = parseCbor(readBinaryFile(path));
+    const Value& core = cborCore(root, path);
+    for (const Value& u : core.items()) {
+        const Value& md = u.at("metadata");
+        const int type = (int)md.at("unit_type").asInt();
+        if (type != 4)
+            throw std::runtime_error("Orientation unit type " + std::to_string(type) + " is not supported: " + path);
+        if (md.at("lag_order_nut").asInt() != 5 || md.at("lag_order_erp").asInt() != 3)
+            throw std::runtime_error("IERS2000 units must use Lagrange orders 5 (nutation) and 3 (ERP): " + path);
+        env.hasRot = true;
+        env.rotNnut = (int)md.at("n_nodes_nut").asInt();
+        env.rotNerp = (int)md.at("n_nodes_erp").asInt();
+        env.rotStart = md.at("startEpoch").asDouble();
+        env.rotFinal = md.at("finalEpoch").asDouble();
+        const Value& d = u.at("data");
+        env.rotData.resize(d.size());
+        for (size_t k = 0; k < d.size(); ++k) env.rotData[k] = d[k].asDouble();
+        if (env.rotData.size() != (size_t)(3 * env.rotNnut + 6 * env.rotNerp + 4))
+            throw std::runtime_error("IERS2000 unit size mismatch: " + path);
+    }
+}
+
+static double calendarMjd(int year, int month, int day) {
+    const int a = (14 - month) / 12;
+    const int y = year + 4800 - a;
+    const int m = month + 12 * a - 3;
+    const long jdn = day + (153 * m + 2) / 5 + 365L * y + y / 4 - y / 100 + y / 400 - 32045;
+    return (double)jdn - 2400001.0;
+}
+
+// CelesTrak SW-All (Nrlmsise00Atmosphere.h:168-235)
+static void loadSpaceWeather(const Value& nrl, HostEnvironment& env) {
+    const std::string path = nrl.at("spaceWeatherFile").asString();
+    const double reqStart = nrl.numberOr("coverageStartMjdUtc", -1.0);
+    const double reqEnd = nrl.numberOr("coverageEndMjdUtc", -1.0);
+    env.nrlHcutoff = nrl.numberOr("hCutoff", 1000.0);
+    env.nrlDensityScale = nrl.numberOr("densityScale", 1.0);
+    for (const auto& kv : nrl.members()) {
+        std::string k = kv.first;
+        std::transform(k.begin(), k.end(), k.begin(), ::tolower);
+        if (k != "spaceweatherfile" && k != "coveragestartmjdutc" && k != "coverageendmjdutc" && k != "hcutoff"
+            && k != "densityscale")
+            throw std::runtime_error("Invalid NRLMSISE-00 atmosphere field: '" + kv.first
+                                     + "'. Valid fields are: [spaceWeatherFile, coverageStartMjdUtc, "
+                                       "coverageEndMjdUtc, hCutoff, densityScale].");
+    }
+    if (!(env.nrlHcutoff > 0.0)) throw std::runtime_error("NRLMSISE-00 hCutoff must be positive.");
+    if (!(env.nrlDensityScale > 0.0)) throw std::runtime_error("NRLMSISE-00 densityScale must be positive.");
+    struct Rec {
+        double mjd, obs, obsc, adj, adjc, avg;
+        int ap[8];
+    };
+    std::vector<Rec> all;
+    std::istringstream in(readTextFile(path));
+    std::string line;
+    while (std::getline(in, line)) {
+        std::istringstream ls(line);
+        int y, mo, d, bsrn, nd, kp[8], sumKp, c9, isn, q, avg;
+        double cp, adj, adjc, adjl, obs, obsc, obsl;
+        Rec r{};
+        if (!(ls >> y >> mo >> d >> bsrn >> nd)) continue;
+        bool ok = true;
+        for (int& v : kp) ok = ok && (bool)(ls >> v);
+        ok = ok && (bool)(ls >> sumKp);
+        for (int& v : r.ap) ok = ok && (bool)(ls >> v);
+        ok = ok && (bool)(ls >> avg >> cp >> c9 >> isn >> adj >> q >> adjc >> adjl >> obs >> obsc >> obsl);
+        if (!ok) continue;
+        r.mjd = calendarMjd(y, mo, d);
+        r.obs = obs;
+        r.obsc = obsc;
+        r.adj = adj;
+        r.adjc = adjc;
+        r.avg = avg;
+        all.push_back(r);
+    }
+    if (all.empty()) throw std::runtime_error("No CelesTrak SW-All records found in: " + path);
+    const double keepStart = reqStart >= 0.0 ? std::floor(reqStart) - 4.0 : all.front().mjd;
+    const double keepEnd = reqEnd >= 0.0 ? std::floor(reqEnd) + 1.0 : all.back().mjd;
+    std::vector<Rec> sel;
+    for (const Rec& r : all)
+        if (r.mjd >= keepStart && r.mjd <= keepEnd) sel.push_back(r);
+    if (sel.size() < 5)
+        throw std::runtime_error(
+            "NRLMSISE-00 weather coverage is missing or too short; at least four look-back days plus the "
+            "propagation day are required.");
+    for (size_t i = 1; i < sel.size(); ++i)
+        if (sel[i].mjd != sel[i - 1].mjd + 1.0)
+            throw std::runtime_error("NRLMSISE-00 space-weather records must be consecutive days.");
+    const int n = (int)sel.size();
+    env.nrlNdays = n;
+    env.nrlStartMjd = sel.front().mjd;
+    env.nrlWeather.assign((size_t)13 * n, 0.0);
+    for (int i = 0; i < n; ++i) {
+        env.nrlWeather[0 * n + i] = sel[i].obs;
+        env.nrlWeather[1 * n + i] = sel[i].obsc;
+        env.nrlWeather[2 * n + i] = sel[i].adj;
+        env.nrlWeather[3 * n + i] = sel[i].adjc;
+        env.nrlWeather[4 * n + i] = sel[i].avg;
+        for (int k = 0; k < 8; ++k) env.nrlWeather[(size_t)(5 + k) * n + i] = sel[i].ap[k];
+    }
+    env.hasNrl = true;
+}
+
+// HPOP EOP-All (earthcorrections/EarthCorrections.h:142-177)
+static void loadEop(const std::string& path, HostEnvironment& env) {
+    std::istringstream in(readTextFile(path));
+    std::string line;
+    std::vector<std::array<double, 5>> rec;
+    while (std::getline(in, line)) {
+        std::istringstream row(line);
+        int y, mo, d;
+        double mjd, xp, yp, dut, lod, dpsi, deps, dx, dy, dat;
+        if (!(row >> y >> mo >> d >> mjd >> xp >> yp >> dut >> lod >> dpsi >> deps >> dx >> dy >> dat)) continue;
+        if (!(y >= 1960 && mo >= 1 && mo <= 12 && d >= 1 && d <= 31 && std::isfinite(mjd) && std::isfinite(xp)
+              && std::isfinite(yp) && std::isfinite(dut) && std::isfinite(dat) && mjd == std::floor(mjd)))
+            throw std::runtime_error("Invalid Earth-tide EOP record in: " + path);
+        if (!rec.empty() && mjd != rec.back()[0] + 1.0)
+            throw std::runtime_error("Earth-tide EOP records must be sorted, unique, consecutive days: " + path);
+        rec.push_back({mjd, xp, yp, dut, dat});
+    }
+    if (rec.size() < 2) throw std::runtime_error("Earth tides require at least two HPOP EOP-All records in: " + path);
+    const int n = (int)rec.size();
+    env.eopN = n;
+    env.eopFirstMjd = rec.front()[0];
+    env.eop.assign((size_t)4 * n, 0.0);
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < 4; ++k) env.eop[(size_t)k * n + i] = rec[i][k + 1];
+}
+
+void loadEnvironment(const Value& model, HostEnvironment& env) {
+    const Value& e = model.at("environment");
+    for (const auto& kv : e.members()) {
+        const std::string& k = kv.first;
+        if (k != "bodies" && k != "ephemeris" && k != "orientations" && k != "constants" && k != "preferSSB"
+            && k != "earthCorrections")
+            throw std::runtime_error("Unsupported environment option: " + k);
+    }
+    loadConstants(e.at("constants").asString(), env);
+    const Value& bodies = e.at("bodies");
+    if (!bodies.isObject() || bodies.size() == 0) throw std::runtime_error("model.environment.bodies must be a nonempty object.");
+    const Value* atmosphere = nullptr;
+    for (const auto& kv : bodies.members()) {
+        HostEnvironment::Body b;
+        b.name = kv.first;
+        b.id = naifId(kv.first);
+        const Value& c = kv.second;
+        for (const auto& f : c.members()) {
+            const std::string& k = f.first;
+            if (k == "gravity") {
+                if (f.second.isBool()) {
+                    if (f.second.asBool()) b.flags |= kGravity;
+                } else if (f.second.isObject()) {
+                    b.flags |= kGravity;
+                    if (const Value* sh = f.second.find("shape")) {
+                        if (b.id != 399) throw std::runtime_error("Spherical-harmonic gravity is supported for the Earth only.");
+                        b.flags |= kShape;
+                        loadShTable(*sh, env);
+                    }
+                } else {
+                    throw std::runtime_error("Body gravity must be a boolean or an object: " + b.name);
+                }
+            } else if (k == "radiation") {
+                if (f.second.asBool()) {
+                    if (b.id != 10) throw std::runtime_error("Radiation pressure is supported for the Sun only.");
+                    b.flags |= kRadiation;
+                }
+            } else if (k == "occulting") {
+                if (f.second.asBool()) b.flags |= kOcculting;
+            } else if (k == "atmosphere") {
+                if (b.id != 399) throw std::runtime_error("Atmospheric drag is supported for the Earth only.");
+                const Value* nrl = f.second.find("nrlmsise00");
+                if (!nrl) throw std::runtime_error("Only the nrlmsise00 atmosphere is supported by this backend.");
+                b.flags |= kAtmosphere;
+                atmosphere = nrl;
+            } else if (k == "flattening") {
+                if (b.id == 399) env.flattening = f.second.asDouble();
+            } else if (k == "gm") {
+                b.gm = f.second.asDouble();
+            } else if (k == "oblateness") {
+                if (f.second.isBool() ? f.second.asBool() : true)
+                    throw std::runtime_error("The oblateness (J2) model is not supported by this backend.");
+            } else {
+                throw std::runtime_error("Unsupported body option for " + b.name + ": " + k);
+            }
+        }
+        if (b.gm == 0.0) {
+            auto it = env.constGm.find(b.id);
+            if (it != env.constGm.end()) b.gm = it->second;
+            else if (b.flags & kGravity) throw std::runtime_error("No gravitational parameter for body " + b.name);
+        }
+        auto r = env.constRadius.find(b.id);
+        b.radius = r != env.constRadius.end() ? r->second : 0.0;
+        env.bodies.push_back(b);
+    }
+    std::sort(env.bodies.begin(), env.bodies.end(), [](auto& a, auto& b) { return a.id < b.id; });
+    if (env.bodies.size() > (size_t)kMaxBodies) throw std::runtime_error("Too many bodies for this backend.");
+    bool haveEarth = false;
+    for (auto& b : env.bodies) haveEarth |= b.id == 399;
+    if (!haveEarth) throw std::runtime_error("The Earth (center of integration) must be configured.");
+    if (const Value* eph = e.find("ephemeris"))
+        for (const Value& p : eph->items()) loadEphemeris(p.asString(), env);
+    if (const Value* ori = e.find("orientations"))
+        for (const Value& p : ori->items()) loadOrientation(p.asString(), env);
+    if (atmosphere) loadSpaceWeather(*atmosphere, env);
+    if (const Value* ec = e.find("earthCorrections")) {
+        env.solid = ec->find("solidEarthTides") && ec->at("solidEarthTides").asBool();
+        env.ocean = ec->find("oceanTides") && ec->at("oceanTides").asBool();
+        env.relativity = ec->find("relativity") && ec->at("relativity").asBool();
+        const std::string sys = ec->find("tideSystem") ? ec->at("tideSystem").asString() : std::string("zero_tide");
+        if (sys != "zero_tide" && sys != "tide_free") throw std::runtime_error("tideSystem must be zero_tide or tide_free.");
+        env.zeroTide = sys == "zero_tide";
+        if (env.solid || env.ocean) loadEop(ec->at("eopFile").asString(), env);
+    }
+    if ((env.hasShape || env.hasNrl || env.solid || env.ocean) && !env.hasRot)
+        throw std::runtime_error("An Earth orientation (IERS2000) unit is required for the configured forces.");
+}
+
+// ---- engine --------------------------------------------------------------------------------------------
+static int unitIndex(const HostEnvironment& env, int target) {
+    for (size_t u = 0; u < env.eph.size(); ++u)
+        if (env.eph[u].target == target) return (int)u;
+    return -1;
+}
+
+// ephemeris units giving body - center through the common ancestor of their chains
+static void chainUnits(const HostEnvironment& env, int body, int center, int plus[kMaxChain], int minus[kMaxChain]) {
+    for (int k = 0; k < kMaxChain; ++k) plus[k] = minus[k] = -1;
+    if (body == center) return;
+    auto path = [&](int b) {
+        std::vector<int> p;
+        while (true) {
+            p.push_back(b);
+            if (b == 0) break;
+            const int u = unitIndex(env, b);
+            if (u < 0) throw std::runtime_error("Ephemeris does not cover body " + std::to_string(b));
+            b = env.eph[u].center;
+            if (p.size() > 8) throw std::runtime_error("Ephemeris chain too long");
+        }
+        return p;
+    };
+    const auto pb = path(body), pc = path(center);
+    int common = 0;
+    for (int x : pb)
+        if (std::find(pc.begin(), pc.end(), x) != pc.end()) {
+            common = x;
+            break;
+        }
+    int np = 0, nm = 0;
+    for (int x : pb) {
+        if (x == common) break;
+        if (np >= kMaxChain) throw std::runtime_error("Ephemeris chain too long");
+        plus[np++] = unitIndex(env, x);
+    }
+    for (int x : pc) {
+        if (x == common) break;
+        if (nm >= kMaxChain) throw std::runtime_error("Ephemeris chain too long");
+        minus[nm++] = unitIndex(env, x);
+    }
+}
+
+template <typename T>
+static T* upload(std::vector<void*>& owned, const std::vector<T>& v) {
+    if (v.empty()) return nullptr;
+    T* d = nullptr;
+    PHOP_CUDA(cudaMalloc(&d, v.size() * sizeof(T)));
+    owned.push_back(d);
+    PHOP_CUDA(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return d;
+}
+
+static double factorA(int n, int m, bool norm) {
+    const double nn = n, mm = m;
+    return norm ? std::sqrt(((2.0 * nn - 1.0) * (2.0 * nn + 1.0)) / ((nn - mm) * (nn + mm))) : (2.0 * nn - 1.0) / (nn - mm);
+}
+static double factorB(int n, int m, bool norm) {
+    const double nn = n, mm = m;
+    return norm ? std::sqrt(((2.0 * nn + 1.0) * (nn + mm - 1.0) * (nn - mm - 1.0)) / ((2.0 * nn - 3.0) * (nn + mm) * (nn - mm)))
+                : (nn + mm - 1.0) / (nn - mm);
+}
+static double factorC(int m, bool norm) {
+    if (norm) return m == 1 ? std::sqrt(3.0) : (m == 0 ? 1.0 : std::sqrt((2.0 * m + 1.0) / (2.0 * m)));
+    return (m == 1 || m == 0) ? 1.0 : (2.0 * m - 1.0);
+}
+
+Engine::Engine(const HostEnvironment& env, int device) : host_(env), device_(device) {
+    PHOP_CUDA(cudaSetDevice(device_));
+    PHOP_CUDA(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_));
+    PHOP_CUDA(cudaDeviceGetAttribute(&maxSmem_, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
+    uploadEnvironment();
+}
+
+Engine::~Engine() {
+    cudaSetDevice(device_);
+    for (void* p : owned_) cudaFree(p);
+    for (auto& kv : scratch_) cudaFree(kv.second.first);
+    for (auto& kv : tiles_) {
+        cudaFree(kv.second.dTile);
+        cudaFree(kv.second.dBlocks);
+    }
+}
+
+void Engine::uploadEnvironment() {
+    const HostEnvironment& h = host_;
+    DevEnv& e = denv_;
+    std::memset(&e, 0, sizeof e);
+    e.shDegree = h.hasShape ? h.shDegree : 0;
+    e.shOrder = h.hasShape ? h.shOrder : 0;
+    e.shNormalized = h.shNormalized;
+    e.shR = h.shR;
+    e.shGM = h.shGM;
+    // tide coefficients are defined with the tide model's GM and radius
+    for (int n = 0; n <= 6; ++n)
+        e.tideScale[n] = h.hasShape ? (tides::Consts::muEarth * 1e-9 / h.shGM) * std::pow(tides::Consts::radius * 1e-3 / h.shR, (double)n) : 0.0;
+    if (h.hasShape) {
+        e.shC = upload(owned_, h.shC);
+        e.shS = upload(owned_, h.shS);
+        LowTable low{};
+        for (int n = 0; n <= kLowDeg + 1 && n <= h.shDegree; ++n)
+            for (int m = 0; m <= n && m <= h.shOrder; ++m) {
+                const int ti = n * (n + 1) / 2 + m;
+                if (n <= kLowDeg) {
+                    low.C[ti] = h.shC[ti];
+                    low.S[ti] = h.shS[ti];
+                }
+                if (n > m) {
+                    low.a[ti] = factorA(n, m, h.shNormalized);
+                    low.b[ti] = factorB(n, m, h.shNormalized);
+                }
+            }
+        std::vector<LowTable> lv(1, low);
+        dLow_ = upload(owned_, lv);
+        std::vector<double> diag((size_t)h.shOrder + 2, 0.0);
+        for (int m = 0; m <= h.shOrder + 1; ++m) diag[m] = factorC(m, h.shNormalized);
+        dDiag_ = upload(owned_, diag);
+    }
+    e.nbodies = (int)h.bodies.size();
+    e.sunIndex = e.moonIndex = e.earthIndex = -1;
+    int anyOcc = 0;
+    for (int b = 0; b < e.nbodies; ++b) {
+        const auto& B = h.bodies[b];
+        e.bodyId[b] = B.id;
+        e.bodyFlags[b] = B.flags;
+        e.bodyGm[b] = B.gm;
+        e.bodyRadius[b] = B.radius;
+        if (B.id == 10) e.sunIndex = b;
+        if (B.id == 301) e.moonIndex = b;
+        if (B.id == 399) e.earthIndex = b;
+        if ((B.flags & kOcculting) && B.id != 10) anyOcc = 1;
+        chainUnits(h, B.id, 399, e.chainPlus[b], e.chainMinus[b]);
+    }
+    e.anyOcculter = anyOcc;
+    e.earthRadius = h.bodies[e.earthIndex].radius;
+    e.flattening = h.flattening;
+    e.au = h.au;
+    if (h.solid || h.ocean) {
+        chainUnits(h, 10, 399, e.sunUnitsPlus, e.sunUnitsMinus);
+        chainUnits(h, 301, 399, e.moonUnitsPlus, e.moonUnitsMinus);
+    }
+    e.neph = (int)h.eph.size();
+    std::vector<int> nint, pdeg;
+    std::vector<int64_t> off;
+    std::vector<double> data;
+    for (const auto& u : h.eph) {
+        nint.push_back(u.nint);
+        pdeg.push_back(u.pdeg);
+        off.push_back((int64_t)data.size());
+        data.insert(data.end(), u.data.begin(), u.data.end());
+    }
+    e.ephNint = upload(owned_, nint);
+    e.ephPdeg = upload(owned_, pdeg);
+    e.ephOffset = upload(owned_, off);
+    e.ephData = upload(owned_, data);
+    e.hasRot = h.hasRot;
+    e.rotNnut = h.rotNnut;
+    e.rotNerp = h.rotNerp;
+    e.rotData = upload(owned_, h.rotData);
+    e.hasNrl = h.hasNrl;
+    e.nrlNdays = h.nrlNdays;
+    e.nrlStartMjd = h.nrlStartMjd;
+    e.nrlHcutoff = h.nrlHcutoff;
+    e.nrlDensityScale = h.nrlDensityScale;
+    e.nrlWeather = upload(owned_, h.nrlWeather);
+    e.solid = h.solid;
+    e.ocean = h.ocean;
+    e.relativity = h.relativity;
+    e.zeroTide = h.zeroTide;
+    e.eopN = h.eopN;
+    e.eopFirstMjd = h.eopFirstMjd;
+    e.eop = upload(owned_, h.eop);
+}
+
+// Lane-interleaved coefficient tile for the n > 8 part (layout in propagate.cuh)
+const Engine::Tile& Engine::tileFor(int L, bool split) {
+    const int key = L * 2 + (split ? 1 : 0);
+    auto it = tiles_.find(key);
+    if (it != tiles_.end()) return it->second;
+    const HostEnvironment& h = host_;
+    const int N = h.shDegree, M = h.shOrder;
+    const bool norm = h.shNormalized != 0;
+    const int nb = h.hasShape ? (M + 1 + L - 1) / L : 0;
+    std::vector<int2> blocks(nb > 0 ? nb : 1, int2{0, 0});
+    std::vector<TileD> entries;
+    for (int b = 0; b < nb; ++b) {
+        const int n0b = std::max(b * L, kLowDeg + 1);
+        const int len = std::max(0, N - n0b + 1);
+        blocks[b] = int2{(int)entries.size(), len};
+        const size_t base = entries.size();
+        entries.resize(base + (size_t)len * L, TileD{0, 0, 0, 0, 0, 0});
+        for (int j = 0; j < L; ++j) {
+            const int m = b * L + j;
+            if (m > M) continue;
+            const int n0 = std::max(m, kLowDeg + 1);
+            for (int i = 0; i < len; ++i) {
+                const int n = n0 + i;
+                if (n > N) break;
+                TileD& t = entries[base + (size_t)i * L + j];
+                const size_t ti = (size_t)n * (n + 1) / 2 + m;
+                t.c = h.shC[ti];
+                t.s = m > 0 ? h.shS[ti] : 0.0;
+                t.cp = (double)(n + 1) * t.c;
+                t.sp = (double)(n + 1) * t.s;
+                if (n + 1 <= N) {
+                    t.a = factorA(n + 1, m, norm);
+                    t.b = factorB(n + 1, m, norm);
+                }
+            }
+        }
+    }
+    Tile tile;
+    tile.nblocks = nb;
+    std::vector<unsigned char> bytes;
+    if (split) {
+        std::vector<TileF> f(entries.size());
+        for (size_t k = 0; k < entries.size(); ++k)
+            f[k] = TileF{(float)entries[k].c, (float)entries[k].s, (float)entries[k].cp, (float)entries[k].sp,
+                         (float)entries[k].a, (float)entries[k].b, 0.f, 0.f};
+        bytes.resize(f.size() * sizeof(TileF));
+        std::memcpy(bytes.data(), f.data(), bytes.size());
+    } else {
+        bytes.resize(entries.size() * sizeof(TileD));
+        std::memcpy(bytes.data(), entries.data(), bytes.size());
+    }
+    bytes.resize((bytes.size() + 15) / 16 * 16 + 16, 0);
+    tile.bytes = (int)bytes.size();
+    PHOP_CUDA(cudaMalloc(&tile.dTile, bytes.size()));
+    PHOP_CUDA(cudaMemcpy(tile.dTile, bytes.data(), bytes.size(), cudaMemcpyHostToDevice));
+    PHOP_CUDA(cudaMalloc(&tile.dBlocks, blocks.size() * sizeof(int2)));
+    PHOP_CUDA(cudaMemcpy(tile.dBlocks, blocks.data(), blocks.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    return tiles_.emplace(key, tile).first->second;
+}
+
+void* Engine::scratch(const std::string& name, size_t bytes) {
+    auto it = scratch_.find(name);
+    if (it != scratch_.end() && it->second.second >= bytes) return it->second.first;
+    if (it != scratch_.end()) {
+        cudaFree(it->second.first);
+        scratch_.erase(it);
+    }
+    void* p = nullptr;
+    PHOP_CUDA(cudaMalloc(&p, bytes > 0 ? bytes : 16));
+    scratch_[name] = {p, bytes};
+    return p;
+}
+
+int Engine::autoLanes(int64_t n) const {
+    // enough threads for ~16 resident warps per SM, at most 16 lanes per object
+    const double want = (double)sms_ * 512.0 / (double)std::max<int64_t>(n, 1);
+    int L = 1;
+    while (L < 16 && L < want) L *= 2;
+    return L;
+}
+
+void Engine::assertCoverage(double loMjd, double hiMjd) const {
+    const double lo = mjdToEtHost(loMjd), hi = mjdToEtHost(hiMjd);
+    for (const auto& u : host_.eph)
+        if (lo < u.startEpoch || hi > u.finalEpoch)
+            throw std::runtime_error("Ephemeris coverage is insufficient for the requested epochs (target "
+                                     + std::to_string(u.target) + ").");
+    if (host_.hasRot && (lo < host_.rotStart || hi > host_.rotFinal))
+        throw std::runtime_error("Earth orientation coverage is insufficient for the requested epochs.");
+}
+
+void Engine::runKernel(int64_t n, double* dState, const double* dBc, const double* dAms, bool shared, int nsteps,
+                       const std::vector<double>& t0, const std::vector<double>& dt, double* dCur, double* dEnd,
+                       double* dDt, double* dStep, int* dUnfinished, const int64_t* dOrder, int64_t maxSteps,
+                       const RunOptions& opt, RunStats* stats, cudaStream_t stream) {
+    const int L = opt.lanes > 0 ? opt.lanes : autoLanes(n);
+    if (L != 1 && L != 2 && L != 4 && L != 8 && L != 16) throw std::runtime_error("lanes must be 1, 2, 4, 8 or 16");
+    const Tile& tile = tileFor(L, opt.split);
+    StepParams p{};
+    p.env = denv_;
+    p.n = n;
+    p.state = dState;
+    p.bc = dBc;
+    p.ams = dAms;
+    p.tile = tile.dTile;
+    p.tileBytes = tile.bytes;
+    p.blocks = tile.dBlocks;
+    p.nblocks = tile.nblocks;
+    p.low = dLow_;
+    p.diagC = dDiag_;
+    const int threadsReq = opt.threads > 0 ? opt.threads : 256;
+    const int kBytes = 13 * ((6 + L - 1) / L) * threadsReq * 8;
+    p.useSmemTile = (tile.bytes + kBytes + 1024 <= maxSmem_) ? 1 : 0;
+    p.maxSteps = maxSteps;
+    p.order = dOrder;
+    p.cur = dCur;
+    p.end = dEnd;
+    p.dt = dDt;
+    p.step = dStep;
+    p.unfinished = dUnfinished;
+    EpochRecord* dRec = nullptr;
+    cudaEvent_t e0, e1, e2;
+    PHOP_CUDA(cudaEventCreate(&e0));
+    PHOP_CUDA(cudaEventCreate(&e1));
+    PHOP_CUDA(cudaEventCreate(&e2));
+    int64_t launches = 0;
+    PHOP_CUDA(cudaEventRecord(e0, stream));
+    if (shared) {
+        std::vector<double> stageT((size_t)nsteps * 13);
+        for (int k = 0; k < nsteps; ++k)
+            for (int s = 0; s < 13; ++s) {
+                static const double c[12] = {2. / 27, 1. / 9, 1. / 6, 5. / 12, 1. / 2, 5. / 6, 1. / 6, 2. / 3, 1. / 3, 1.0, 0, 1.0};
+                stageT[(size_t)k * 13 + s] = s == 0 ? t0[k] : std::fma(dt[k], c[s - 1], t0[k]);
+            }
+        double* dStage = (double*)scratch("stageT", stageT.size() * sizeof(double));
+        dRec = (EpochRecord*)scratch("records", stageT.size() * sizeof(EpochRecord));
+        double* dT0 = (double*)scratch("t0", (size_t)nsteps * sizeof(double));
+        double* dDtv = (double*)scratch("dt", (size_t)nsteps * sizeof(double));
+        PHOP_CUDA(cudaMemcpyAsync(dStage, stageT.data(), stageT.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+        PHOP_CUDA(cudaMemcpyAsync(dT0, t0.data(), t0.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+        PHOP_CUDA(cudaMemcpyAsync(dDtv, dt.data(), dt.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+        launchEpochRecords(denv_, dStage, (int)stageT.size(), dRec, stream);
+        PHOP_CUDA(cudaGetLastError());
+        ++launches;
+        p.nsteps = nsteps;
+        p.stepT0 = dT0;
+        p.stepDt = dDtv;
+        p.records = dRec;
+    }
+    int* dCtl = (int*)scratch("ctl", 2 * sizeof(int));
+    PHOP_CUDA(cudaMemsetAsync(dCtl, 0, 2 * sizeof(int), stream));
+    p.workCounter = dCtl;
+    p.errorFlag = dCtl + 1;
+    PHOP_CUDA(cudaEventRecord(e1, stream));
+    const int threads = opt.threads > 0 ? opt.threads : 256;
+    const int smem = propagateSmemBytes(p, L, threads);
+    int perSm = opt.ctasPerSm > 0 ? opt.ctasPerSm : propagateMaxCtasPerSm(L, opt.split, shared, threads, smem);
+    if (perSm <= 0) perSm = 1;
+    const int64_t groups = (n + (32 / L) - 1) / (32 / L);
+    const int64_t warpsPerCta = threads / 32;
+    const int64_t need = (groups + warpsPerCta - 1) / warpsPerCta;
+    const int ctas = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms_ * perSm, need));
+    PHOP_CUDA(launchPropagate(p, L, opt.split, shared, ctas, threads, stream));
+    ++launches;
+    PHOP_CUDA(cudaEventRecord(e2, stream));
+    PHOP_CUDA(cudaEventSynchronize(e2));
+    int err = 0;
+    PHOP_CUDA(cudaMemcpy(&err, dCtl + 1, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) throw std::runtime_error("Propagation kernel reported error " + std::to_string(err) + ".");
+    if (stats) {
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, e0, e1);
+        cudaEventElapsedTime(&b, e1, e2);
+        stats->recordsMs += a;
+        stats->kernelMs += b;
+        stats->launches += launches;
+        stats->lanes = L;
+        stats->ctas = ctas;
+        stats->threads = threads;
+        stats->split = opt.split;
+        stats->sharedGrid = shared;
+        stats->tileInSmem = p.useSmemTile != 0;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+}
+
+// time grid of one object (FixedStep.h:7-37): step start epochs and sizes
+static int buildGrid(double epochMjd, double duration, double step, int64_t maxSteps, std::vector<double>& t0,
+                     std::vector<double>& dt, double& finalEt) {
+    const double start = mjdToEtHost(epochMjd);
+    const double end = mjdToEtHost(epochMjd + duration / 86400.0);
+    const double span = end - start;
+    if (!(span > 0) || !std::isfinite(span))
+        throw std::runtime_error("Duration/step cannot be represented by the integration time/index types.");
+    double cur = start, d = std::min(step, span);
+    t0.clear();
+    dt.clear();
+    bool done = false;
+    for (int64_t k = 0; k < maxSteps && !done; ++k) {
+        t0.push_back(cur);
+        dt.push_back(d);
+        cur += d;
+        const double rem = end - cur;
+        done = rem <= 0;
+        d = done ? 0 : std::min(step, rem);
+    }
+    finalEt = cur;
+    return done ? 1 : 0;
+}
+
+void Engine::propagate(const TargetSet& t, int64_t maxSteps, const RunOptions& opt, std::vector<double>& outEpoch,
+                       std::vector<double>& outState, RunStats* stats, cudaStream_t stream) {
+    PHOP_CUDA(cudaSetDevice(device_));
+    const int64_t n = (int64_t)t.size();
+    if (n == 0) throw std::runtime_error("targets must be a nonempty array.");
+    cudaEvent_t a0, a1;
+    PHOP_CUDA(cudaEventCreate(&a0));
+    PHOP_CUDA(cudaEventCreate(&a1));
+    PHOP_CUDA(cudaEventRecord(a0, stream));
+    std::vector<double> soa((size_t)6 * n), bc(n), ams(n);
+    for (int64_t i = 0; i < n; ++i) {
+        for (int d = 0; d < 6; ++d) soa[(size_t)d * n + i] = t.state[(size_t)6 * i + d];
+        // driver.cpp:118-120 then PrivateAccelerations.h:41-42
+        const double area = t.dragArea[i] * 1e-6;
+        const double crf = t.cr[i] * t.srpArea[i] / t.dragArea[i];
+        ams[i] = crf * area / t.mass[i];
+        bc[i] = t.cd[i] * area / t.mass[i];
+    }
+    double* dState = (double*)scratch("state", soa.size() * sizeof(double));
+    double* dBc = (double*)scratch("bc", (size_t)n * sizeof(double));
+    double* dAms = (double*)scratch("ams", (size_t)n * sizeof(double));
+    PHOP_CUDA(cudaMemcpyAsync(dState, soa.data(), soa.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+    PHOP_CUDA(cudaMemcpyAsync(dBc, bc.data(), bc.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+    PHOP_CUDA(cudaMemcpyAsync(dAms, ams.data(), ams.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+    bool uniform = true;
+    for (int64_t i = 1; i < n && uniform; ++i)
+        uniform = t.epoch[i] == t.epoch[0] && t.duration[i] == t.duration[0] && t.step[i] == t.step[0];
+    outEpoch.assign(n, 0.0);
+    RunStats local;
+    RunStats* st = stats ? stats : &local;
+    if (uniform) {
+        std::vector<double> t0, dt;
+        double finalEt = 0.0;
+        if (!buildGrid(t.epoch[0], t.duration[0], t.step[0], maxSteps, t0, dt, finalEt))
+            throw std::runtime_error("A target stopped without reaching the requested end of simulation.");
+        runKernel(n, dState, dBc, dAms, true, (int)t0.size(), t0, dt, nullptr, nullptr, nullptr, nullptr, nullptr,
+                  nullptr, maxSteps, opt, st, stream);
+        std::fill(outEpoch.begin(), outEpoch.end(), etToMjdHost(finalEt));
+        st->objectSteps += n * (int64_t)t0.size();
+    } else {
+        std::vector<double> cur(n), end(n), dtv(n), stp(n);
+        std::vector<int64_t> cost(n), order(n);
+        for (int64_t i = 0; i < n; ++i) {
+            cur[i] = mjdToEtHost(t.epoch[i]);
+            end[i] = mjdToEtHost(t.epoch[i] + t.duration[i] / 86400.0);
+            const double span = end[i] - cur[i];
+            if (!(span > 0) || !std::isfinite(span))
+                throw std::runtime_error("Duration/step cannot be represented by the integration time/index types.");
+            dtv[i] = std::min(t.step[i], span);
+            stp[i] = t.step[i];
+            cost[i] = (int64_t)std::ceil(span / t.step[i]);
+            st->objectSteps += cost[i];
+        }
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cost[a] > cost[b]; });
+        double* dCur = (double*)scratch("cur", (size_t)n * 8);
+        double* dEnd = (double*)scratch("end", (size_t)n * 8);
+        double* dDt = (double*)scratch("dtv", (size_t)n * 8);
+        double* dStep = (double*)scratch("step", (size_t)n * 8);
+        int* dUnf = (int*)scratch("unfinished", (size_t)n * 4);
+        int64_t* dOrder = (int64_t*)scratch("order", (size_t)n * 8);
+        PHOP_CUDA(cudaMemcpyAsync(dCur, cur.data(), n * 8, cudaMemcpyHostToDevice, stream));
+        PHOP_CUDA(cudaMemcpyAsync(dEnd, end.data(), n * 8, cudaMemcpyHostToDevice, stream));
+        PHOP_CUDA(cudaMemcpyAsync(dDt, dtv.data(), n * 8, cudaMemcpyHostToDevice, stream));
+        PHOP_CUDA(cudaMemcpyAsync(dStep, stp.data(), n * 8, cudaMemcpyHostToDevice, stream));
+        PHOP_CUDA(cudaMemcpyAsync(dOrder, order.data(), n * 8, cudaMemcpyHostToDevice, stream));
+        runKernel(n, dState, dBc, dAms, false, 0, {}, {}, dCur, dEnd, dDt, dStep, dUnf, dOrder, maxSteps, opt, st,
+                  stream);
+        std::vector<int> unf(n);
+        PHOP_CUDA(cudaMemcpy(cur.data(), dCur, n * 8, cudaMemcpyDeviceToHost));
+        PHOP_CUDA(cudaMemcpy(unf.data(), dUnf, n * 4, cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < n; ++i) {
+            if (unf[i]) throw std::runtime_error("A target stopped without reaching the requested end of simulation.");
+            outEpoch[i] = etToMjdHost(cur[i]);
+        }
+    }
+    PHOP_CUDA(cudaMemcpyAsync(soa.data(), dState, soa.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    PHOP_CUDA(cudaEventRecord(a1, stream));
+    PHOP_CUDA(cudaEventSynchronize(a1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a0, a1);
+    st->totalMs += ms;
+    cudaEventDestroy(a0);
+    cudaEventDestroy(a1);
+    outState.assign((size_t)6 * n, 0.0);
+    for (int64_t i = 0; i < n; ++i)
+        for (int d = 0; d < 6; ++d) outState[(size_t)6 * i + d] = soa[(size_t)d * n + i];
+}
+
+void Engine::propagateResident(int64_t n, double* dState, const double* epochMjd, const double* bc, const double* ams,
+                               double duration, double step, int64_t maxSteps, const RunOptions& opt,
+                               std::vector<double>& outEpochMjd, RunStats* stats, cudaStream_t stream) {
+    PHOP_CUDA(cudaSetDevice(device_));
+    for (int64_t i = 1; i < n; ++i)
+        if (epochMjd[i] != epochMjd[0])
+            throw std::runtime_error("The resident entry point needs one common epoch.");
+    std::vector<double> t0, dt;
+    double finalEt = 0;
+    if (!buildGrid(epochMjd[0], duration, step, maxSteps, t0, dt, finalEt))
+        throw std::runtime_error("A target stopped without reaching the requested end of simulation.");
+    double* dBc = (double*)scratch("bc", (size_t)n * 8);
+    double* dAms = (double*)scratch("ams", (size_t)n * 8);
+    PHOP_CUDA(cudaMemcpyAsync(dBc, bc, (size_t)n * 8, cudaMemcpyHostToDevice, stream));
+    PHOP_CUDA(cudaMemcpyAsync(dAms, ams, (size_t)n * 8, cudaMemcpyHostToDevice, stream));
+    RunStats local;
+    RunStats* st = stats ? stats : &local;
+    runKernel(n, dState, dBc, dAms, true, (int)t0.size(), t0, dt, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+              maxSteps, opt, st, stream);
+    st->objectSteps += n * (int64_t)t0.size();
+    outEpochMjd.assign(n, etToMjdHost(finalEt));
+}
+
+}  // namespace phop

@@ -1,0 +1,156 @@
+// Host engine: loads a ParaHPOP model configuration and its environment files,
+// keeps the environment resident on one GPU and propagates batches of objects
+// through the fused kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "device_env.cuh"
+#include "propagate.cuh"
+#include "value.hpp"
+
+namespace phop {
+
+struct EphUnitHost {
+    int target, center, nint, pdeg;
+    double startEpoch, finalEpoch;
+    std::vector<double> data;
+};
+
+// Everything read from the environment files, in host memory.
+struct HostEnvironment {
+    // constants
+    double au = 0.0;
+    std::map<int, double> constGm, constRadius;
+    // bodies sorted by NAIF id
+    struct Body {
+        std::string name;
+        int id = 0;
+        int flags = 0;
+        double gm = 0.0, radius = 0.0;
+    };
+    std::vector<Body> bodies;
+    double flattening = 0.0;
+    // geopotential
+    bool hasShape = false;
+    int shDegree = 0, shOrder = 0, shNormalized = 1;
+    double shR = 0.0, shGM = 0.0;
+    std::vector<double> shC, shS;  // triangle n(n+1)/2+m, n <= shDegree
+    // ephemeris
+    std::vector<EphUnitHost> eph;
+    // orientation (IERS2000 unit)
+    bool hasRot = false;
+    int rotNnut = 0, rotNerp = 0;
+    double rotStart = 0.0, rotFinal = 0.0;
+    std::vector<double> rotData;
+    // NRLMSISE-00
+    bool hasNrl = false;
+    double nrlStartMjd = 0.0, nrlHcutoff = 1000.0, nrlDensityScale = 1.0;
+    std::vector<double> nrlWeather;  // 13 x ndays
+    int nrlNdays = 0;
+    // Earth corrections
+    bool solid = false, ocean = false, relativity = false, zeroTide = true;
+    double eopFirstMjd = 0.0;
+    std::vector<double> eop;  // 4 x n
+    int eopN = 0;
+};
+
+// Loads the environment of a `model` configuration object (the reference's
+// interface::config::Model input); relative paths must already be resolved.
+void loadEnvironment(const Value& model, HostEnvironment& env);
+
+// Per-object inputs in the reference's target schema (driver.cpp:97-123).
+struct TargetSet {
+    std::vector<int64_t> ids;
+    std::vector<double> epoch;     // MJD2000 TDB
+    std::vector<double> state;     // n x 6, km and km/s
+    std::vector<double> mass, dragArea, srpArea, cd, cr;
+    std::vector<double> duration;  // s, per object
+    std::vector<double> step;      // s, per object
+    size_t size() const { return ids.size(); }
+};
+
+struct RunStats {
+    double kernelMs = 0.0;         // step kernel, CUDA events
+    double recordsMs = 0.0;        // epoch-record kernel
+    double totalMs = 0.0;          // whole propagate call incl. copies
+    int64_t objectSteps = 0;       // sum over objects of steps taken
+    int64_t launches = 0;          // kernels launched by this call
+    int lanes = 0;
+    int ctas = 0;
+    int threads = 0;
+    bool split = false;
+    bool sharedGrid = false;
+    bool tileInSmem = false;
+};
+
+struct RunOptions {
+    int lanes = 0;     // 0: autotuned
+    int threads = 256;
+    bool split = false;
+    int ctasPerSm = 0; // 0: occupancy
+};
+
+class Engine {
+public:
+    Engine(const HostEnvironment& env, int device);
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    const HostEnvironment& environment() const { return host_; }
+
+    // Checks that ephemeris / orientation / EOP data cover [loMjd, hiMjd].
+    void assertCoverage(double loMjd, double hiMjd) const;
+
+    // Propagates `t` in place: final MJD2000 epochs and states (n x 6).
+    // Per-object duration / step.  Throws on error.
+    void propagate(const TargetSet& t, int64_t maxSteps, const RunOptions& opt, std::vector<double>& outEpoch,
+                   std::vector<double>& outState, RunStats* stats, cudaStream_t stream = 0);
+
+    // Device-resident variant: `state` is an SoA device array (6 x n) updated in
+    // place; other inputs are host arrays.  Used for timing with inputs held
+    // in HBM.
+    void propagateResident(int64_t n, double* dState, const double* epochMjd, const double* bc, const double* ams,
+                           double duration, double step, int64_t maxSteps, const RunOptions& opt,
+                           std::vector<double>& outEpochMjd, RunStats* stats, cudaStream_t stream = 0);
+
+    int device() const { return device_; }
+    int smCount() const { return sms_; }
+    int autoLanes(int64_t n) const;
+
+    // internal
+    struct Tile {
+        void* dTile = nullptr;
+        int2* dBlocks = nullptr;
+        int bytes = 0;
+        int nblocks = 0;
+    };
+
+private:
+    const Tile& tileFor(int lanes, bool split);
+    void uploadEnvironment();
+    void* scratch(const std::string& name, size_t bytes);
+    void runKernel(int64_t n, double* dState, const double* dBc, const double* dAms, bool shared, int nsteps,
+                   const std::vector<double>& t0, const std::vector<double>& dt, double* dCur, double* dEnd,
+                   double* dDt, double* dStep, int* dUnfinished, const int64_t* dOrder, int64_t maxSteps,
+                   const RunOptions& opt, RunStats* stats, cudaStream_t stream);
+
+    HostEnvironment host_;
+    int device_ = 0;
+    int sms_ = 0;
+    int maxSmem_ = 0;
+    DevEnv denv_{};
+    std::vector<void*> owned_;
+    std::map<std::string, std::pair<void*, size_t>> scratch_;
+    std::map<int, Tile> tiles_;
+    LowTable* dLow_ = nullptr;
+    double* dDiag_ = nullptr;
+};
+
+}  // namespace phop

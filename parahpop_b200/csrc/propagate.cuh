@@ -1,0 +1,106 @@
+// Fused batched RKF78 propagation kernels for sm_100a.
+//
+// One persistent kernel advances object groups through all their fixed steps:
+// the 13 RKF78 stages, the full force model and the 8th-order update run in
+// registers, so the per-step HBM traffic is the state read at the start and
+// written at the end of the whole propagation.
+//
+// Work split (autotuned):  L lanes (1, 2, 4, 8 or 16) cooperate on one object,
+// a warp holds 32/L objects.
+//   * RK state: lane j of a group owns the state components d with d % L == j,
+//     keeps y_d and the 13 stage derivatives k_s[d] in registers, forms the
+//     stage state for its components in the reference's order
+//     (parm/integrate/rk/host/Step.h:33-84) and the 8th-order update in stage
+//     order (Step.h:86-104), and broadcasts components by warp shuffle.
+//   * Spherical harmonics: orders m are processed in blocks of L columns, lane
+//     j taking m = bL + j.  Every lane advances the diagonal P_mm, dP_mm,
+//     cos/sin(m lambda) and alpha^m with the reference's recurrences
+//     (LegendreRecursor.h:202-208, PseudoPhasor.h:58-64), so the column start
+//     values are the reference's.  The n <= 8 part of each column (with the
+//     epoch's tide deltas folded into n <= 6) is always FP64; the n > 8 part
+//     runs in the tile type T (double, or float for split precision) from a
+//     lane-interleaved coefficient tile that a TMA bulk copy stages into
+//     shared memory, so the L lanes of a group read one contiguous line per
+//     term and the groups of a warp share it by broadcast.  Per column the
+//     sums  sum (n+1) c Pt, sum (n+1) s Pt, sum c dPt, sum s dPt, sum c Pt,
+//     sum s Pt  (Pt = alpha^n P) are accumulated and the phasor applied once,
+//     which is algebraically the reference's per-term phase product
+//     (DegreeLoop.h:83-112).  Partial accelerations are folded across the
+//     group by xor shuffles.
+//   * Everything else (third bodies, SRP with shadow, NRLMSISE-00 drag,
+//     relativity) is evaluated by every lane of the group on the broadcast
+//     stage state.
+//
+// Time grid: batches whose objects share epoch, step and duration read the
+// per-step start / step size and the per-stage EpochRecord from tables made
+// before the launch; mixed batches keep per-object time and evaluate the
+// epoch record inline, mirroring FixedStep.h:30-37 per object.
+#pragma once
+#include <stdint.h>
+
+#include "device_env.cuh"
+
+namespace phop {
+
+constexpr int kLowDeg = 8;                          // n <= 8 stays FP64
+constexpr int kLowTri = (kLowDeg + 2) * (kLowDeg + 3) / 2;  // factor triangle up to n = 9
+
+// coefficient tile entry for the n > 8 part: c, s, (n+1)c, (n+1)s and the
+// recursion factors a, b of the step n -> n+1
+struct __align__(16) TileD {
+    double c, s, cp, sp, a, b;
+};
+struct __align__(16) TileF {
+    float c, s, cp, sp, a, b, pad0, pad1;
+};
+template <typename T> struct TileOf;
+template <> struct TileOf<double> { using type = TileD; };
+template <> struct TileOf<float> { using type = TileF; };
+
+// low-degree FP64 table (n <= 8 coefficients, factors to n = 9, diagonal c_m)
+struct LowTable {
+    double C[kLowTri];
+    double S[kLowTri];
+    double a[kLowTri];
+    double b[kLowTri];
+};
+
+struct StepParams {
+    DevEnv env;
+    int64_t n;          // objects
+    double* state;      // SoA: x[n], y[n], z[n], vx[n], vy[n], vz[n]
+    const double* bc;   // cd * area / mass  (km^2 / kg)
+    const double* ams;  // cr * area / mass
+    // shared time grid
+    int nsteps;
+    const double* stepT0;
+    const double* stepDt;
+    const EpochRecord* records;  // [nsteps][13]
+    // per-object time (mixed batches)
+    double* cur;
+    const double* end;
+    double* dt;
+    const double* step;
+    int64_t maxSteps;
+    int* unfinished;        // per object: 1 if it did not reach its end
+    const int64_t* order;   // processing order of objects (nullable)
+    // geopotential
+    const void* tile;       // tile entries in global memory
+    int tileBytes;          // multiple of 16
+    const int2* blocks;     // per block: entry offset, length
+    int nblocks;
+    const LowTable* low;
+    const double* diagC;    // c_m, m = 0..M
+    int useSmemTile;
+    // scheduling and errors
+    int* workCounter;
+    int* errorFlag;
+};
+
+void launchEpochRecords(const DevEnv& env, const double* epochs, int count, EpochRecord* out, cudaStream_t stream);
+cudaError_t launchPropagate(const StepParams& p, int lanes, bool split, bool shared, int ctas, int threads,
+                            cudaStream_t stream);
+int propagateSmemBytes(const StepParams& p, int lanes, int threads);
+int propagateMaxCtasPerSm(int lanes, bool split, bool shared, int threads, int smem);
+
+}  // namespace phop

@@ -1,0 +1,549 @@
+// Kernel bodies shared by the per-precision translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "nrlmsise00.cuh"
+#include "propagate.cuh"
+
+namespace phop {
+
+
+// ---- RKF78 tableau (parm/integrate/rk/coefs/tableau.h:24-48) ----------------------------
+__host__ __device__ constexpr double rkA(int s, int j) {
+    // s = stage - 1 (row), j = column; rows list the nonzero Fehlberg coefficients
+    return s == 0 ? (j == 0 ? 2. / 27 : 0)
+         : s == 1 ? (j == 0 ? 1. / 36 : j == 1 ? 1. / 12 : 0)
+         : s == 2 ? (j == 0 ? 1. / 24 : j == 2 ? 1. / 8 : 0)
+         : s == 3 ? (j == 0 ? 5. / 12 : j == 2 ? -25. / 16 : j == 3 ? 25. / 16 : 0)
+         : s == 4 ? (j == 0 ? 1. / 20 : j == 3 ? 1. / 4 : j == 4 ? 1. / 5 : 0)
+         : s == 5 ? (j == 0 ? -25. / 108 : j == 3 ? 125. / 108 : j == 4 ? -65. / 27 : j == 5 ? 125. / 54 : 0)
+         : s == 6 ? (j == 0 ? 31. / 300 : j == 4 ? 61. / 225 : j == 5 ? -2. / 9 : j == 6 ? 13. / 900 : 0)
+         : s == 7 ? (j == 0 ? 2.0 : j == 3 ? -53. / 6 : j == 4 ? 704. / 45 : j == 5 ? -107. / 9
+                    : j == 6 ? 67. / 90 : j == 7 ? 3.0 : 0)
+         : s == 8 ? (j == 0 ? -91. / 108 : j == 3 ? 23. / 108 : j == 4 ? -976. / 135 : j == 5 ? 311. / 54
+                    : j == 6 ? -19. / 60 : j == 7 ? 17. / 6 : j == 8 ? -1. / 12 : 0)
+         : s == 9 ? (j == 0 ? 2383. / 4100 : j == 3 ? -341. / 164 : j == 4 ? 4496. / 1025 : j == 5 ? -301. / 82
+                    : j == 6 ? 2133. / 4100 : j == 7 ? 45. / 82 : j == 8 ? 45. / 164 : j == 9 ? 18. / 41 : 0)
+         : s == 10 ? (j == 0 ? 3. / 205 : j == 5 ? -6. / 41 : j == 6 ? -3. / 205 : j == 7 ? -3. / 41
+                     : j == 8 ? 3. / 41 : j == 9 ? 6. / 41 : 0)
+         : s == 11 ? (j == 0 ? -1777. / 4100 : j == 3 ? -341. / 164 : j == 4 ? 4496. / 1025 : j == 5 ? -289. / 82
+                     : j == 6 ? 2193. / 4100 : j == 7 ? 51. / 82 : j == 8 ? 33. / 164 : j == 9 ? 12. / 41
+                     : j == 11 ? 1.0 : 0)
+         : 0;
+}
+__host__ __device__ constexpr double rkC(int s) {
+    return s == 0 ? 2. / 27 : s == 1 ? 1. / 9 : s == 2 ? 1. / 6 : s == 3 ? 5. / 12 : s == 4 ? 1. / 2
+         : s == 5 ? 5. / 6 : s == 6 ? 1. / 6 : s == 7 ? 2. / 3 : s == 8 ? 1. / 3 : s == 9 ? 1.0
+         : s == 10 ? 0 : 1.0;
+}
+__host__ __device__ constexpr double rkB(int s) {
+    return s == 5 ? 34. / 105 : s == 6 ? 9. / 35 : s == 7 ? 9. / 35 : s == 8 ? 9. / 280 : s == 9 ? 9. / 280
+         : s == 11 ? 41. / 840 : s == 12 ? 41. / 840 : 0;
+}
+
+// ---- RK stage storage ------------------------------------------------------------------------
+// Lane j of a group owns state components d = j + c*L (c < CPL).  The stage
+// derivatives live in shared memory, [stage][component slot][thread], so that
+// consecutive threads hit consecutive banks.
+static __constant__ double c_rkA[12][12] = {
+    {2. / 27, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0},
+    {1. / 36, 1. / 12, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0},
+    {1. / 24, 0, 1. / 8, 0, 0, 0, 0, 0, 0, 0, 0, 0},
+    {5. / 12, 0, -25. / 16, 25. / 16, 0, 0, 0, 0, 0, 0, 0, 0},
+    {1. / 20, 0, 0, 1. / 4, 1. / 5, 0, 0, 0, 0, 0, 0, 0},
+    {-25. / 108, 0, 0, 125. / 108, -65. / 27, 125. / 54, 0, 0, 0, 0, 0, 0},
+    {31. / 300, 0, 0, 0, 61. / 225, -2. / 9, 13. / 900, 0, 0, 0, 0, 0},
+    {2.0, 0, 0, -53. / 6, 704. / 45, -107. / 9, 67. / 90, 3.0, 0, 0, 0, 0},
+    {-91. / 108, 0, 0, 23. / 108, -976. / 135, 311. / 54, -19. / 60, 17. / 6, -1. / 12, 0, 0, 0},
+    {2383. / 4100, 0, 0, -341. / 164, 4496. / 1025, -301. / 82, 2133. / 4100, 45. / 82, 45. / 164, 18. / 41, 0, 0},
+    {3. / 205, 0, 0, 0, 0, -6. / 41, -3. / 205, -3. / 41, 3. / 41, 6. / 41, 0, 0},
+    {-1777. / 4100, 0, 0, -341. / 164, 4496. / 1025, -289. / 82, 2193. / 4100, 51. / 82, 33. / 164, 12. / 41, 0, 1.0}};
+
+template <int CPL>
+struct StageStore {
+    double* base;  // shared memory, 13 * CPL * blockDim doubles
+    int stride;    // blockDim.x
+    __device__ __forceinline__ double& at(int s, int c) const {
+        return base[((s * CPL) + c) * stride + threadIdx.x];
+    }
+};
+
+// y_s = y + sum_j (dt a_sj) k_j in stage order (Step.h:33-84)
+template <int CPL>
+static __device__ __forceinline__ void combine(int s, const double (&y)[CPL], const StageStore<CPL>& k, double dt,
+                                        double (&ys)[CPL]) {
+#pragma unroll
+    for (int c = 0; c < CPL; ++c) ys[c] = y[c];
+    for (int jj = 0; jj < s; ++jj) {
+        const double a = c_rkA[s - 1][jj];
+        if (a != 0.0) {
+            const double coef = dt * a;
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) ys[c] = fma(coef, k.at(jj, c), ys[c]);
+        }
+    }
+}
+
+// y += sum_s (dt b_s) k_s in stage order (Step.h:86-104)
+template <int CPL>
+static __device__ __forceinline__ void finalUpdate(double (&y)[CPL], const StageStore<CPL>& k, double dt, bool apply) {
+    double yn[CPL];
+#pragma unroll
+    for (int c = 0; c < CPL; ++c) yn[c] = y[c];
+#pragma unroll
+    for (int s = 0; s < 13; ++s)
+        if (rkB(s) != 0.0) {
+            const double cb = dt * rkB(s);
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) yn[c] = fma(cb, k.at(s, c), yn[c]);
+        }
+    if (apply) {
+#pragma unroll
+        for (int c = 0; c < CPL; ++c) y[c] = yn[c];
+    }
+}
+
+// ---- spherical harmonics, lane-split over orders --------------------------------------------
+template <int L, typename T>
+static __device__ __forceinline__ void shAccel(const StepParams& p, const typename TileOf<T>::type* __restrict__ tile,
+                                        const double* __restrict__ dC, const double* __restrict__ dS, double x,
+                                        double y, double z, double out[3]) {
+    using Tile = typename TileOf<T>::type;
+    const int j = (int)(threadIdx.x % L);
+    const int N = p.env.shDegree, M = p.env.shOrder;
+    const LowTable* __restrict__ low = p.low;
+    const double* __restrict__ diagC = p.diagC;
+    const double rn = sqrt(x * x + y * y + z * z);
+    const double rho = sqrt(x * x + y * y);
+    const double sinPhi = z / rn, cosPhi = rho / rn;
+    const double sinL = rho > 1e-14 ? y / rho : 0.0;
+    const double cosL = rho > 1e-14 ? x / rho : 1.0;
+    const double alpha = p.env.shR / rn;
+    const double invCos = cosPhi == 0.0 ? 0.0 : 1.0 / cosPhi;
+    // diagonal state (reference recurrences) for this lane's first column
+    double Pmm = 1.0, dPmm = 0.0, cML = 1.0, sML = 0.0, am = 1.0;
+    int m = 0;
+    auto advance = [&]() {
+        const double ns = cosL * sML + sinL * cML;
+        const double nc = cosL * cML - sinL * sML;
+        sML = ns;
+        cML = nc;
+        const double cm = diagC[m + 1];
+        const double nP = cm * cosPhi * Pmm;
+        const double ndP = cm * (cosPhi * dPmm - sinPhi * Pmm);
+        Pmm = nP;
+        dPmm = ndP;
+        am *= alpha;
+        ++m;
+    };
+    for (int t = 0; t < j; ++t)
+        if (m < M) advance();
+    const T u = T(alpha * sinPhi), v = T(alpha * cosPhi), a2 = T(alpha * alpha);
+    double ar = 0.0, aphi = 0.0, alam = 0.0;
+    const int nblocks = p.nblocks;
+    for (int b = 0; b < nblocks; ++b) {
+        const int mcol = b * L + j;
+        const bool act = mcol <= M;
+        double SA0 = 0, SA1 = 0, SA2 = 0, SA3 = 0, SA4 = 0, SA5 = 0;
+        T P = T(0), P1 = T(0), dP = T(0), dP1 = T(0);
+        if (act && mcol <= kLowDeg) {
+            // n = mcol .. 8 in FP64 with the epoch's tide deltas (n <= 6)
+            double Pn = Pmm, Pn1 = 0.0, dPn = dPmm, dPn1 = 0.0, an = am, anPrev = am;
+            const int nEnd = N < kLowDeg ? N : kLowDeg;
+            for (int n = mcol; n <= nEnd; ++n) {
+                const int ti = n * (n + 1) / 2 + mcol;
+                double c = low->C[ti], s = low->S[ti];
+                if (n <= 6) {
+                    c += dC[ti];
+                    s += dS[ti];
+                }
+                if (mcol == 0) s = 0.0;
+                const double q = an * Pn, qd = an * dPn, np1 = (double)(n + 1);
+                SA0 = fma(np1 * c, q, SA0);
+                SA1 = fma(np1 * s, q, SA1);
+                SA2 = fma(c, qd, SA2);
+                SA3 = fma(s, qd, SA3);
+                SA4 = fma(c, q, SA4);
+                SA5 = fma(s, q, SA5);
+                if (n < N) {
+                    const int tn = (n + 1) * (n + 2) / 2 + mcol;
+                    const double fa = low->a[tn], fb = low->b[tn];
+                    const double P2 = Pn1;
+                    Pn1 = Pn;
+                    Pn = fa * sinPhi * Pn1 - fb * P2;
+                    const double dP2 = dPn1;
+                    dPn1 = dPn;
+                    dPn = fa * (sinPhi * dPn1 + cosPhi * Pn1) - fb * dP2;
+                    anPrev = an;
+                    an *= alpha;
+                }
+            }
+            P = T(an * Pn);
+            P1 = T(anPrev * Pn1);
+            dP = T(an * dPn);
+            dP1 = T(anPrev * dPn1);
+        } else if (act) {
+            P = T(am * Pmm);
+            dP = T(am * dPmm);
+        }
+        // n > 8 part from the lane-interleaved tile
+        const int2 blk = p.blocks[b];
+        T Scc = T(0), Ssc = T(0), Sdc = T(0), Sds = T(0), Spc = T(0), Sps = T(0);
+        const Tile* tp = tile + blk.x + j;
+        for (int i = 0; i < blk.y; ++i, tp += L) {
+            const Tile e = *tp;
+            Scc = fma(T(e.cp), P, Scc);
+            Ssc = fma(T(e.sp), P, Ssc);
+            Spc = fma(T(e.c), P, Spc);
+            Sps = fma(T(e.s), P, Sps);
+            Sdc = fma(T(e.c), dP, Sdc);
+            Sds = fma(T(e.s), dP, Sds);
+            const T Pn = fma(T(e.a), u * P, -T(e.b) * (a2 * P1));
+            const T dPn = fma(T(e.a), fma(u, dP, v * P), -T(e.b) * (a2 * dP1));
+            P1 = P;
+            P = Pn;
+            dP1 = dP;
+            dP = dPn;
+        }
+        if (act) {
+            const double cc = SA0 + (double)Scc, sc = SA1 + (double)Ssc;
+            const double dc = SA2 + (double)Sdc, ds = SA3 + (double)Sds;
+            const double pc = SA4 + (double)Spc, ps = SA5 + (double)Sps;
+            ar -= cML * cc + sML * sc;
+            aphi += cML * dc + sML * ds;
+            alam -= ((double)mcol * invCos) * (sML * pc - cML * ps);
+        }
+        for (int t = 0; t < L; ++t)
+            if (m < M) advance();
+    }
+#pragma unroll
+    for (int off = L / 2; off > 0; off >>= 1) {
+        ar += __shfl_xor_sync(0xffffffffu, ar, off);
+        aphi += __shfl_xor_sync(0xffffffffu, aphi, off);
+        alam += __shfl_xor_sync(0xffffffffu, alam, off);
+    }
+    if (cosPhi == 0.0 && M >= 1) {
+        // exact pole: the m = 1 longitudinal term takes its analytical limit
+        // (DegreeLoop.h:98-103, Coefficients.h:123-131)
+        double an = alpha;
+        for (int n = 1; n <= N; ++n) {
+            const int ti = n * (n + 1) / 2 + 1;
+            double s = p.env.shS[ti];
+            if (n <= 6) s += dS[ti];
+            const double sign = sinPhi > 0.0 ? 1.0 : ((n & 1) ? 1.0 : -1.0);
+            double lim = 0.5 * (double)n * (n + 1.0);
+            if (p.env.shNormalized) lim *= sqrt(2.0 * (2.0 * n + 1.0) / ((double)n * (n + 1.0)));
+            // S~ = c sin(l) - s cos(l) with sin(l) = 0, cos(l) = 1 at the pole
+            alam -= an * (sign * lim) * (-s);
+            an *= alpha;
+        }
+    }
+    const double g = p.env.shGM / (rn * rn);
+    ar *= g;
+    aphi *= g;
+    alam *= g;
+    out[0] = cosPhi * cosL * ar - sinPhi * cosL * aphi - sinL * alam;
+    out[1] = cosPhi * sinL * ar - sinPhi * sinL * aphi + cosL * alam;
+    out[2] = sinPhi * ar + cosPhi * aphi;
+}
+
+// ---- the remaining forces ------------------------------------------------------------------
+static __device__ __forceinline__ double shadowFactor(const double rS[3], const double rB[3], double RSun, double RBody) {
+    const double s2 = rS[0] * rS[0] + rS[1] * rS[1] + rS[2] * rS[2];
+    const double b2 = rB[0] * rB[0] + rB[1] * rB[1] + rB[2] * rB[2];
+    const double sb = rS[0] * rB[0] + rS[1] * rB[1] + rS[2] * rB[2];
+    const double iS = 1.0 / sqrt(s2), iB = 1.0 / sqrt(b2);
+    if (b2 <= RBody * RBody) return 0.0;
+    const double a = asin(fmin(fmax(RSun * iS, 0.0), 1.0));
+    const double b = asin(fmin(fmax(RBody * iB, 0.0), 1.0));
+    const double c = acos(fmin(fmax(sb * iS * iB, -1.0), 1.0));
+    if (c >= a + b) return 1.0;
+    if (c <= fabs(b - a)) return b >= a ? 0.0 : 1.0 - (b * b) / (a * a);
+    const double a2 = a * a, bb = b * b, c2 = c * c;
+    const double x = (c2 + a2 - bb) / (2.0 * c);
+    const double yv = sqrt(fmax(a2 - x * x, 0.0));
+    const double al = acos(fmin(fmax(x / a, -1.0), 1.0));
+    const double be = acos(fmin(fmax((c - x) / b, -1.0), 1.0));
+    return 1.0 - (a2 * al + bb * be - c * yv) / (a2 * 3.14159265358979323846);
+}
+
+static __device__ __noinline__ double nrlDensity(const DevEnv& e, const EpochRecord& r, const double f[3]) {
+    // geodetic latitude / longitude / altitude (Nrlmsise00.cu:243-266)
+    const double rho2 = f[0] * f[0] + f[1] * f[1];
+    if (!(rho2 + f[2] * f[2] > 0.0)) return NAN;
+    const double radius = e.earthRadius;
+    const double e2 = e.flattening * (2.0 - e.flattening);
+    double dz = e2 * f[2], zdz = f[2] + dz, nn = radius, nh = 0.0;
+    for (int it = 0; it < 20; ++it) {
+        zdz = f[2] + dz;
+        nh = sqrt(rho2 + zdz * zdz);
+        const double sp = zdz / nh;
+        nn = radius / sqrt(1.0 - e2 * sp * sp);
+        const double next = nn * e2 * sp;
+        if (fabs(dz - next) < 1.0e-12 * radius) {
+            dz = next;
+            break;
+        }
+        dz = next;
+    }
+    zdz = f[2] + dz;
+    nh = sqrt(rho2 + zdz * zdz);
+    const double lon = atan2(f[1], f[0]);
+    const double lat = atan2(zdz, sqrt(rho2));
+    const double alt = nh - nn;
+    if (!(isfinite(lat) && isfinite(lon) && isfinite(alt))) return NAN;
+    if (alt > e.nrlHcutoff) return 0.0;
+    if (!r.nrlValid) return NAN;
+    const double kRad = 57.2957795130823208768;
+    nrl::Input<double> in;
+    in.doy = r.nrlDoy;
+    in.sec = r.nrlSec;
+    in.alt = alt;
+    in.g_lat = lat * kRad;
+    in.g_long = lon * kRad;
+    in.lst = wrapHours(r.nrlGast + lon * kRad / 15.0);
+    in.f107A = r.nrlF107a;
+    in.f107 = r.nrlF107;
+    in.ap = r.nrlAp;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) in.ap_a[k] = r.nrlApa[k];
+    const double rhoSi = nrl::density<double>(in);
+    if (!isfinite(rhoSi) || rhoSi < 0.0) return NAN;
+    return (rhoSi * 1.0e9) * e.nrlDensityScale;
+}
+
+// full right-hand side acceleration (km/s^2); every lane of the group calls it
+template <int L, typename T>
+static __device__ __forceinline__ void accelerations(const StepParams& p, const typename TileOf<T>::type* tile,
+                                              const EpochRecord& r, const double pos[3], const double vel[3],
+                                              double bc, double ams, double acc[3]) {
+    const DevEnv& e = p.env;
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    for (int bi = 0; bi < e.nbodies; ++bi) {
+        const int fl = e.bodyFlags[bi];
+        const bool isEarth = (bi == e.earthIndex);
+        if (fl & kGravity) {
+            const double gm = e.bodyGm[bi];
+            if (isEarth) {
+                const double rr = sqrt(pos[0] * pos[0] + pos[1] * pos[1] + pos[2] * pos[2]);
+                const double f = -gm * (1.0 / (rr * rr * rr));
+                ax += f * pos[0];
+                ay += f * pos[1];
+                az += f * pos[2];
+            } else {
+                const double* rb = r.body[bi];
+                const double d0 = pos[0] - rb[0], d1 = pos[1] - rb[1], d2 = pos[2] - rb[2];
+                const double rd = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+                const double rbn = sqrt(rb[0] * rb[0] + rb[1] * rb[1] + rb[2] * rb[2]);
+                const double f1 = -gm * (1.0 / (rd * rd * rd));
+                const double f2 = -gm * (1.0 / (rbn * rbn * rbn));
+                ax += f1 * d0 + f2 * rb[0];
+                ay += f1 * d1 + f2 * rb[1];
+                az += f1 * d2 + f2 * rb[2];
+            }
+        }
+        if (fl & kShape) {
+            const double* R = r.R;
+            const double bx = R[0] * pos[0] + R[1] * pos[1] + R[2] * pos[2];
+            const double by = R[3] * pos[0] + R[4] * pos[1] + R[5] * pos[2];
+            const double bz = R[6] * pos[0] + R[7] * pos[1] + R[8] * pos[2];
+            double a[3];
+            shAccel<L, T>(p, tile, r.dC, r.dS, bx, by, bz, a);
+            ax += R[0] * a[0] + R[3] * a[1] + R[6] * a[2];
+            ay += R[1] * a[0] + R[4] * a[1] + R[7] * a[2];
+            az += R[2] * a[0] + R[5] * a[1] + R[8] * a[2];
+        }
+        if (fl & kRadiation) {
+            const double* rb = r.body[bi];
+            const double dp[3] = {pos[0] - rb[0], pos[1] - rb[1], pos[2] - rb[2]};
+            const double rd = sqrt(dp[0] * dp[0] + dp[1] * dp[1] + dp[2] * dp[2]);
+            double occ = 1.0;
+            if (e.anyOcculter) {
+                for (int oj = 0; oj < e.nbodies; ++oj) {
+                    if (!(e.bodyFlags[oj] & kOcculting) || oj == e.sunIndex) continue;
+                    const double* op = r.body[oj];
+                    const double rB[3] = {pos[0] - op[0], pos[1] - op[1], pos[2] - op[2]};
+                    occ *= shadowFactor(dp, rB, e.bodyRadius[bi], e.bodyRadius[oj]);
+                }
+            }
+            const double f = occ * ((e.au * e.au * 4.56e-3 * ams) * (1.0 / (rd * rd * rd)));
+            ax += f * dp[0];
+            ay += f * dp[1];
+            az += f * dp[2];
+        }
+        if ((fl & kAtmosphere) && e.hasNrl) {
+            const double* R = r.R;
+            const double fx[3] = {R[0] * pos[0] + R[1] * pos[1] + R[2] * pos[2],
+                                  R[3] * pos[0] + R[4] * pos[1] + R[5] * pos[2],
+                                  R[6] * pos[0] + R[7] * pos[1] + R[8] * pos[2]};
+            const double rho = nrlDensity(e, r, fx);
+            const double* w = r.w;
+            const double vr0 = vel[0] - (w[1] * pos[2] - w[2] * pos[1]);
+            const double vr1 = vel[1] - (w[2] * pos[0] - w[0] * pos[2]);
+            const double vr2 = vel[2] - (w[0] * pos[1] - w[1] * pos[0]);
+            const double f = -0.5 * rho * bc * sqrt(vr0 * vr0 + vr1 * vr1 + vr2 * vr2);
+            ax += f * vr0;
+            ay += f * vr1;
+            az += f * vr2;
+        }
+    }
+    if (e.relativity) {
+        const double mu = tides::Consts::muEarth, c = tides::Consts::c;
+        const double r0 = 1000.0 * pos[0], r1 = 1000.0 * pos[1], r2 = 1000.0 * pos[2];
+        const double v0 = 1000.0 * vel[0], v1 = 1000.0 * vel[1], v2 = 1000.0 * vel[2];
+        const double rr = sqrt(r0 * r0 + r1 * r1 + r2 * r2);
+        const double vv = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+        const double rv = r0 * v0 + r1 * v1 + r2 * v2;
+        const double f = mu / (c * c * (rr * rr * rr));
+        const double g = 4.0 * mu / rr - vv * vv;
+        ax += 1.0e-3 * (f * (g * r0 + 4.0 * rv * v0));
+        ay += 1.0e-3 * (f * (g * r1 + 4.0 * rv * v1));
+        az += 1.0e-3 * (f * (g * r2 + 4.0 * rv * v2));
+    }
+    acc[0] = ax;
+    acc[1] = ay;
+    acc[2] = az;
+}
+
+// ---- TMA bulk staging of the coefficient tile --------------------------------------------------
+static __device__ __forceinline__ bool stageTile(void* dst, const void* src, int bytes, int* errorFlag) {
+    __shared__ __align__(8) uint64_t bar;
+    const uint32_t barAddr = (uint32_t)__cvta_generic_to_shared(&bar);
+    const uint32_t dstAddr = (uint32_t)__cvta_generic_to_shared(dst);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barAddr));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(barAddr), "r"(bytes) : "memory");
+        const int chunk = 32768;
+        for (int off = 0; off < bytes; off += chunk) {
+            const int sz = (bytes - off) < chunk ? (bytes - off) : chunk;
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    dstAddr + off),
+                "l"((const char*)src + off), "r"(sz), "r"(barAddr)
+                : "memory");
+        }
+    }
+    __syncthreads();
+    // bounded wait on phase 0
+    uint32_t done = 0;
+    for (long it = 0; it < (1L << 24) && !done; ++it) {
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(done)
+            : "r"(barAddr), "r"(0)
+            : "memory");
+    }
+    if (!done) {
+        if (threadIdx.x == 0) atomicExch(errorFlag, 2);
+        return false;
+    }
+    return true;
+}
+
+// ---- the persistent step kernel ----------------------------------------------------------------
+static __device__ __noinline__ void epochRecordOutOfLine(const DevEnv& env, double et, EpochRecord& r) {
+    evalEpochRecord(env, et, r);
+}
+
+template <int L, typename T, bool SHARED_GRID>
+__global__ void __launch_bounds__(256, 2) propagateKernel(const __grid_constant__ StepParams p) {
+    using Tile = typename TileOf<T>::type;
+    constexpr int CPL = (6 + L - 1) / L;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const Tile* tile = (const Tile*)p.tile;
+    int kOffset = 0;
+    if (p.useSmemTile) {
+        if (!stageTile(smem, p.tile, p.tileBytes, p.errorFlag)) return;
+        tile = (const Tile*)smem;
+        kOffset = p.tileBytes;
+    }
+    StageStore<CPL> kst{(double*)(smem + kOffset), (int)blockDim.x};
+    const int lane = (int)(threadIdx.x & 31);
+    const int j = lane % L;
+    const int g = lane / L;
+    constexpr int groups = 32 / L;
+    const int groupBase = lane - j;
+    for (;;) {
+        int64_t base = 0;
+        if (lane == 0) base = (int64_t)atomicAdd(p.workCounter, groups);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= p.n) break;
+        const int64_t slot = base + g;
+        const bool valid = slot < p.n;
+        const int64_t sidx = valid ? slot : p.n - 1;
+        const int64_t oi = p.order ? p.order[sidx] : sidx;
+        double y[CPL];
+#pragma unroll
+        for (int c = 0; c < CPL; ++c) {
+            const int d = j + c * L;
+            y[c] = d < 6 ? p.state[(int64_t)d * p.n + oi] : 0.0;
+        }
+        const double bc = p.bc[oi], ams = p.ams[oi];
+        double cur = 0.0, dtv = 0.0, endv = 0.0, stepv = 0.0;
+        bool done = false;
+        if (!SHARED_GRID) {
+            cur = p.cur[oi];
+            dtv = p.dt[oi];
+            endv = p.end[oi];
+            stepv = p.step[oi];
+            done = !valid;
+        }
+        const int64_t nsteps = SHARED_GRID ? (int64_t)p.nsteps : p.maxSteps;
+        for (int64_t kstep = 0; kstep < nsteps; ++kstep) {
+            if (!SHARED_GRID) {
+                if (!__any_sync(0xffffffffu, !done)) break;
+            }
+            const double t0 = SHARED_GRID ? p.stepT0[kstep] : cur;
+            const double dt = SHARED_GRID ? p.stepDt[kstep] : dtv;
+            for (int s = 0; s < 13; ++s) {
+                double ys[CPL];
+                combine<CPL>(s, y, kst, dt, ys);
+                double st[6];
+#pragma unroll
+                for (int d = 0; d < 6; ++d) {
+                    const double own = ys[(d / L) < CPL ? (d / L) : 0];
+                    st[d] = (L == 1) ? ys[d < CPL ? d : 0] : __shfl_sync(0xffffffffu, own, groupBase + d % L);
+                }
+                double acc[3];
+                if (SHARED_GRID) {
+                    const EpochRecord& rec = p.records[kstep * 13 + s];
+                    accelerations<L, T>(p, tile, rec, st, st + 3, bc, ams, acc);
+                } else {
+                    EpochRecord rec;
+                    const double ts = s == 0 ? t0 : t0 + dt * rkC(s - 1);
+                    epochRecordOutOfLine(p.env, ts, rec);
+                    accelerations<L, T>(p, tile, rec, st, st + 3, bc, ams, acc);
+                }
+#pragma unroll
+                for (int c = 0; c < CPL; ++c) {
+                    const int d = j + c * L;
+                    kst.at(s, c) = d < 3 ? st[d + 3] : (d < 6 ? acc[d - 3] : 0.0);
+                }
+            }
+            finalUpdate<CPL>(y, kst, dt, SHARED_GRID || !done);
+            if (!SHARED_GRID && !done) {
+                // FixedStep.h:30-37
+                cur += dtv;
+                const double rem = endv - cur;
+                done = rem <= 0;
+                dtv = done ? 0.0 : fmin(stepv, rem);
+            }
+        }
+        if (valid) {
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) {
+                const int d = j + c * L;
+                if (d < 6) p.state[(int64_t)d * p.n + oi] = y[c];
+            }
+            if (!SHARED_GRID && j == 0) {
+                p.cur[oi] = cur;
+                p.dt[oi] = dtv;
+                p.unfinished[oi] = done ? 0 : 1;
+            }
+        }
+    }
+}
+
+}  // namespace phop
