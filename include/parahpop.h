@@ -81,7 +81,7 @@ int phop_propagate_device(phop_context* ctx, int64_t n, double* d_states_soa, do
  *   "lanes"    lanes per object, 0 = autotuned, else 1, 2, 4, 8 or 16
  *   "split"    0 = plain FP64, 1 = split precision (FP32 for geopotential
  *              degrees n > 8, FP64 elsewhere)
- *   "threads"  threads per CTA (multiple of 32, <= 256) */
+ *   "threads"  threads per CTA (multiple of 32, <= 512) */
 int phop_set_option(phop_context* ctx, const char* key, double value);
 
 typedef struct {
@@ -94,6 +94,12 @@ typedef struct {
 } phop_stats;
 
 int phop_last_stats(const phop_context* ctx, phop_stats* out);
+
+/* Measured FMA throughput of `device` in TFLOP/s (2 FLOP per FMA), FP64 and
+ * FP32: the roofline denominators for the step kernel, which is bound by the
+ * FP64 / FP32 pipes rather than by HBM or the tensor cores.  No reference
+ * counterpart (the reference reports no roofline). */
+int phop_fma_peak(int device, double* fp64_tflops, double* fp32_tflops);
 
 #ifdef __cplusplus
 }

@@ -52,6 +52,7 @@ def library() -> C.CDLL:
         lib.phop_last_stats.argtypes = [C.c_void_p, C.POINTER(PhopStats)]
         lib.paraHPOP_run.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.c_char_p]
         lib.paraHPOP_setLogLevel.argtypes = [C.c_int]
+        lib.phop_fma_peak.argtypes = [C.c_int, D, D]
         _lib = lib
     return _lib
 
@@ -144,6 +145,14 @@ class Propagator:
         s = PhopStats()
         library().phop_last_stats(self._h, C.byref(s))
         return {k: getattr(s, k) for k, _ in PhopStats._fields_}
+
+
+def fma_peak(device: int = 0) -> tuple[float, float]:
+    """Measured (FP64, FP32) FMA throughput in TFLOP/s on `device`."""
+    a, b = C.c_double(), C.c_double()
+    if library().phop_fma_peak(device, C.byref(a), C.byref(b)) != 0:
+        raise PhopError("FMA peak measurement failed")
+    return a.value, b.value
 
 
 def run(config, targets, output, backend="device") -> int:

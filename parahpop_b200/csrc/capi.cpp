@@ -172,8 +172,8 @@ int phop_set_option(phop_context* ctx, const char* key, double value) {
         ctx->opt.split = value != 0.0;
     } else if (k == "threads") {
         const int t = (int)value;
-        if (t < 32 || t > 256 || t % 32) {
-            ctx->error = "threads must be a multiple of 32 in [32, 256]";
+        if (t < 32 || t > 512 || t % 32) {
+            ctx->error = "threads must be a multiple of 32 in [32, 512]";
             return 1;
         }
         ctx->opt.threads = t;

@@ -20,6 +20,7 @@
 #include <math.h>
 #include <stdint.h>
 
+#include "nrl_fast.cuh"
 #include "tides.cuh"
 
 namespace phop {
@@ -64,6 +65,7 @@ struct DevEnv {
     int hasNrl, nrlNdays;
     double nrlStartMjd, nrlHcutoff, nrlDensityScale;
     const double* nrlWeather;  // 13 x ndays component-major
+    const nrlf::NrlEpochBlock* nrlBlocks;  // per (UTC day record, 3-hour ap slot): index record * 8 + slot
     // Earth corrections
     int solid, ocean, relativity, zeroTide;
     int eopN;
@@ -77,9 +79,8 @@ struct EpochRecord {
     double body[kMaxBodies][3];  // body positions relative to the Earth, km
     double dC[kTideTri];         // tide coefficient deltas, field units
     double dS[kTideTri];
-    double nrlSec, nrlGast, nrlF107, nrlF107a, nrlAp;
-    double nrlApa[7];
-    int nrlDoy, nrlValid, tideValid, pad;
+    double nrlSec, nrlGast;      // UTC seconds of day, apparent sidereal time (h)
+    int nrlBlock, nrlValid, tideValid, pad;
 };
 
 #if defined(__CUDACC__)
@@ -343,56 +344,18 @@ static __device__ double gastHours(double mjdUtc) {
 
 static __device__ void nrlEpoch(const DevEnv& e, double et, EpochRecord& r) {
     const double mjdUtc = etToMjdUtc(et);
-    // weather record (Nrlmsise00.cu:207-235), adjusted flux
+    // weather record and 3-hour slot (Nrlmsise00.cu:207-214)
     const int rec = (int)floor(mjdUtc - e.nrlStartMjd);
     r.nrlValid = (rec >= 3 && rec < e.nrlNdays);
-    const int recc = r.nrlValid ? rec : 3;
     int slot = (int)floor((mjdUtc - floor(mjdUtc)) * 8.0);
     slot = slot < 0 ? 0 : (slot > 7 ? 7 : slot);
-    const double* W = e.nrlWeather;
-    const int nd = e.nrlNdays;
-    auto at = [&](int comp, int rr) { return W[(int64_t)comp * nd + rr]; };
-    auto lag = [&](int l) {
-        const int hh = 24 + slot - l;
-        return at(5 + hh % 8, recc - 3 + hh / 8);
-    };
-    r.nrlF107 = at(2, recc - 1);
-    r.nrlF107a = at(3, recc);
-    r.nrlAp = at(4, recc);
-    r.nrlApa[0] = r.nrlAp;
-    r.nrlApa[1] = at(5 + slot, recc);
-    r.nrlApa[2] = lag(1);
-    r.nrlApa[3] = lag(2);
-    r.nrlApa[4] = lag(3);
-    double a5 = 0.0, a6 = 0.0;
-    for (int d = 4; d <= 11; ++d) a5 += lag(d);
-    for (int d = 12; d <= 19; ++d) a6 += lag(d);
-    r.nrlApa[5] = a5 / 8.0;
-    r.nrlApa[6] = a6 / 8.0;
-    // calendar date, day of year, seconds of day (Nrlmsise00.cu:113-145)
-    const long a = (long)floor(mjdUtc + 2400001.0);
-    long b = 0, c = 0;
-    if (a < 2299161) c = a + 1524;
-    else {
-        b = (long)((a - 1867216.25) / 36524.25);
-        c = a + b - b / 4 + 1525;
-    }
-    const long dd = (long)((c - 122.1) / 365.25);
-    const long ee = 365 * dd + dd / 4;
-    const long ff = (long)((c - ee) / 30.6001);
-    const int day = (int)(c - ee - (long)(30.6001 * ff));
-    const int month = (int)(ff - 1 - 12 * (ff / 14));
-    const int year = (int)(dd - 4715 - (7 + month) / 10);
+    r.nrlBlock = r.nrlValid ? rec * 8 + slot : 0;
+    // seconds of day as calendarDate forms them (Nrlmsise00.cu:113-130)
     double sod = (mjdUtc - floor(mjdUtc)) * 86400.0;
     if (sod < 0.0) sod += 86400.0;
     const int hour = (int)(sod / 3600.0);
     const int minute = (int)((sod - hour * 3600.0) / 60.0);
     const double second = sod - hour * 3600.0 - minute * 60.0;
-    int mdays[12] = {31, 28, 31, 30, 31, 30, 31, 31, 30, 31, 30, 31};
-    if ((year % 4 == 0 && year % 100 != 0) || year % 400 == 0) mdays[1] = 29;
-    int doy = day;
-    for (int m = 1; m < month; ++m) doy += mdays[m - 1];
-    r.nrlDoy = doy;
     r.nrlSec = hour * 3600.0 + minute * 60.0 + second;
     r.nrlGast = gastHours(mjdUtc);
 }

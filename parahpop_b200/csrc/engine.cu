@@ -532,6 +532,57 @@ void Engine::uploadEnvironment() {
     e.nrlHcutoff = h.nrlHcutoff;
     e.nrlDensityScale = h.nrlDensityScale;
     e.nrlWeather = upload(owned_, h.nrlWeather);
+    if (h.hasNrl) {
+        // NRLMSISE-00 (UTC day, 3-hour slot) blocks: the weather record and ap
+        // history exactly as Nrlmsise00.cu:207-235 fills them, then the
+        // day/slot-only parts of the model (nrl_fast.cuh)
+        const int nd = h.nrlNdays;
+        std::vector<nrlf::NrlEpochBlock> blocks((size_t)nd * 8);
+        const double* W = h.nrlWeather.data();
+        auto at = [&](int comp, int rec) { return W[(size_t)comp * nd + rec]; };
+        for (int rec = 0; rec < nd; ++rec)
+            for (int slot = 0; slot < 8; ++slot) {
+                nrlf::NrlEpochBlock& b = blocks[(size_t)rec * 8 + slot];
+                std::memset(&b, 0, sizeof b);
+                if (rec < 3) continue;
+                auto lag = [&](int l) {
+                    const int hh = 24 + slot - l;
+                    return at(5 + hh % 8, rec - 3 + hh / 8);
+                };
+                double apa[7];
+                apa[0] = at(4, rec);
+                apa[1] = at(5 + slot, rec);
+                apa[2] = lag(1);
+                apa[3] = lag(2);
+                apa[4] = lag(3);
+                apa[5] = apa[6] = 0.0;
+                for (int d = 4; d <= 11; ++d) apa[5] += lag(d);
+                for (int d = 12; d <= 19; ++d) apa[6] += lag(d);
+                apa[5] /= 8.0;
+                apa[6] /= 8.0;
+                // day of year of the record's UTC date (calendarDate, Nrlmsise00.cu:113-130)
+                const double mjd = h.nrlStartMjd + rec;
+                const long a = (long)std::floor(mjd + 2400001.0);
+                long bb = 0, c = 0;
+                if (a < 2299161) c = a + 1524;
+                else {
+                    bb = (long)((a - 1867216.25) / 36524.25);
+                    c = a + bb - bb / 4 + 1525;
+                }
+                const long dd = (long)((c - 122.1) / 365.25);
+                const long ee = 365 * dd + dd / 4;
+                const long ff = (long)((c - ee) / 30.6001);
+                const int day = (int)(c - ee - (long)(30.6001 * ff));
+                const int month = (int)(ff - 1 - 12 * (ff / 14));
+                const int year = (int)(dd - 4715 - (7 + month) / 10);
+                int mdays[12] = {31, 28, 31, 30, 31, 30, 31, 31, 30, 31, 30, 31};
+                if ((year % 4 == 0 && year % 100 != 0) || year % 400 == 0) mdays[1] = 29;
+                int doy = day;
+                for (int m = 1; m < month; ++m) doy += mdays[m - 1];
+                nrlf::nrlSlotBlock(doy, at(2, rec - 1), at(3, rec), apa, b);
+            }
+        e.nrlBlocks = upload(owned_, blocks);
+    }
     e.solid = h.solid;
     e.ocean = h.ocean;
     e.relativity = h.relativity;
@@ -651,9 +702,18 @@ void Engine::runKernel(int64_t n, double* dState, const double* dBc, const doubl
     p.nblocks = tile.nblocks;
     p.low = dLow_;
     p.diagC = dDiag_;
-    const int threadsReq = opt.threads > 0 ? opt.threads : 256;
-    const int kBytes = 13 * ((6 + L - 1) / L) * threadsReq * 8;
-    p.useSmemTile = (tile.bytes + kBytes + 1024 <= maxSmem_) ? 1 : 0;
+    // shared memory per CTA: the coefficient tile (when it fits) plus the
+    // stage derivatives, 13 x ceil(6/L) doubles per thread
+    const int threadsReq = opt.threads > 0 ? opt.threads : 512;
+    const int kPerThread = 13 * ((6 + L - 1) / L) * 8;
+    int threads = threadsReq;
+    if (tile.bytes + 1024 + 64 * kPerThread <= maxSmem_) {
+        p.useSmemTile = 1;
+        threads = std::min(threadsReq, (maxSmem_ - tile.bytes - 1024) / kPerThread / 32 * 32);
+    } else {
+        p.useSmemTile = 0;
+        threads = std::min(threadsReq, (maxSmem_ - 1024) / kPerThread / 32 * 32);
+    }
     p.maxSteps = maxSteps;
     p.order = dOrder;
     p.cur = dCur;
@@ -695,7 +755,6 @@ void Engine::runKernel(int64_t n, double* dState, const double* dBc, const doubl
     p.workCounter = dCtl;
     p.errorFlag = dCtl + 1;
     PHOP_CUDA(cudaEventRecord(e1, stream));
-    const int threads = opt.threads > 0 ? opt.threads : 256;
     const int smem = propagateSmemBytes(p, L, threads);
     int perSm = opt.ctasPerSm > 0 ? opt.ctasPerSm : propagateMaxCtasPerSm(L, opt.split, shared, threads, smem);
     if (perSm <= 0) perSm = 1;

@@ -91,7 +91,7 @@ struct RunStats {
 
 struct RunOptions {
     int lanes = 0;     // 0: autotuned
-    int threads = 256;
+    int threads = 512;
     bool split = false;
     int ctasPerSm = 0; // 0: occupancy
 };

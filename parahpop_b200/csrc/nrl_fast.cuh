@@ -1,0 +1,532 @@
+// NRLMSISE-00 total mass density for the step kernel, split into an
+// epoch-only part and a per-object part.
+//
+// Same model and call sequence as nrlmsise00.cuh (gtd7d, switch 9 = -1), but
+// every sub-expression that depends only on the UTC day and the 3-hour ap
+// slot (day-of-year phases cd32/cd18/cd14/cd39, the F10.7 terms t[0], f1, f2,
+// the six 3-hour-ap responses g0 of Eq. A24d) is evaluated once per (day,
+// slot) into an NrlEpochBlock when the environment is loaded, and the
+// per-object part evaluates only what depends on the seconds of day,
+// latitude, longitude, local time and altitude.  Differences of angles are
+// expanded with precomputed table constants (cos(x - p) = cos x cos p +
+// sin x sin p) and integer powers are products; results agree with the
+// straight restatement to rounding (checked against it by the tests).
+//
+// T is the arithmetic type of the per-object part (double, or float in
+// split precision); the epoch block is always double.
+#pragma once
+#include <math.h>
+
+#include "nrlmsise00.cuh"
+
+namespace phop {
+namespace nrlf {
+
+using namespace ::phop::nrl;  // coefficient tables
+
+constexpr int kGlobeTables = 11;  // pt, ps, pd[0..8]
+constexpr int kGlobSTables = 14;  // ptl[0..3], pma[0..9]
+
+struct NrlGlobeEpoch {
+    double cd32, cd18, cd14, cd39;
+    double t0, f1, f2;            // F10.7 terms of globe7
+    double g0[6];                 // Eq. A24d responses to ap[1..6]
+    double c131, s131, c97, s97, c136, s136;  // table phase constants
+    double c71, s71, c58, s58, c79, s79;      // cos / sin (sr p[k]) for the seconds-of-day phases
+};
+
+struct NrlGlobSEpoch {
+    double cd32, cd18, cd14, cd39;
+    double lonA;  // p80 cos(dr(doy-p81)) + p85 cos(2dr(doy-p86))  (multiplies plg[0][1])
+    double lonB;  // p83 cos(dr(doy-p84)) + p87 cos(2dr(doy-p88))
+};
+
+struct NrlEpochBlock {
+    NrlGlobeEpoch ge[kGlobeTables];
+    NrlGlobSEpoch gs[kGlobSTables];
+    double dfa;
+    double f107A;
+    int doy;
+    int valid;
+};
+
+#if defined(__CUDACC__)
+
+// table order of the globe7 calls: pt, ps, pd[0..8]
+__host__ __device__ __forceinline__ const double* globeTable(int k) {
+    return k == 0 ? NRLT(pt) : k == 1 ? NRLT(ps) : NRLT(pd) + 150 * (k - 2);
+}
+__host__ __device__ __forceinline__ const double* globSTable(int k) {
+    return k < 4 ? NRLT(ptl) + 100 * k : NRLT(pma) + 100 * (k - 4);
+}
+
+// (day, ap slot) part: day of year, F10.7 of the previous day, 81-day mean,
+// ap history (as Nrlmsise00.cu:207-235 fills them).
+__host__ __device__ inline void nrlSlotBlock(int doy, double f107, double f107A, const double apa[7],
+                                             NrlEpochBlock& b) {
+    const double dr = 1.72142E-2, sr = 7.2722E-5;
+    const double df = f107 - f107A;
+    const double dfa = f107A - 150.0;
+    b.dfa = dfa;
+    b.f107A = f107A;
+    b.doy = doy;
+    b.valid = 1;
+    const double dd = (double)doy;
+    for (int k = 0; k < kGlobeTables; ++k) {
+        const double* p = globeTable(k);
+        NrlGlobeEpoch& g = b.ge[k];
+        g.cd32 = cos(dr * (dd - p[31]));
+        g.cd18 = cos(2.0 * dr * (dd - p[17]));
+        g.cd14 = cos(dr * (dd - p[13]));
+        g.cd39 = cos(2.0 * dr * (dd - p[38]));
+        g.t0 = p[19] * df * (1.0 + p[59] * dfa) + p[20] * df * df + p[21] * dfa + p[29] * (dfa * dfa);
+        g.f1 = 1.0 + (p[47] * dfa + p[19] * df + p[20] * df * df);
+        g.f2 = 1.0 + (p[49] * dfa + p[19] * df + p[20] * df * df);
+        g.c71 = cos(sr * p[71]);
+        g.s71 = sin(sr * p[71]);
+        g.c58 = cos(sr * p[58]);
+        g.s58 = sin(sr * p[58]);
+        g.c79 = cos(sr * p[79]);
+        g.s79 = sin(sr * p[79]);
+        for (int i = 0; i < 6; ++i) g.g0[i] = nrl::Model<double>::g0(apa[i + 1], p);
+        g.c131 = cos(0.2618 * p[131]);
+        g.s131 = sin(0.2618 * p[131]);
+        g.c97 = cos(1.74533E-2 * p[97]);
+        g.s97 = sin(1.74533E-2 * p[97]);
+        g.c136 = cos(1.74533E-2 * p[136]);
+        g.s136 = sin(1.74533E-2 * p[136]);
+    }
+    for (int k = 0; k < kGlobSTables; ++k) {
+        const double* p = globSTable(k);
+        NrlGlobSEpoch& g = b.gs[k];
+        g.cd32 = cos(dr * (dd - p[31]));
+        g.cd18 = cos(2.0 * dr * (dd - p[17]));
+        g.cd14 = cos(dr * (dd - p[13]));
+        g.cd39 = cos(2.0 * dr * (dd - p[38]));
+        g.lonA = p[80] * cos(dr * (dd - p[81])) + p[85] * cos(2.0 * dr * (dd - p[86]));
+        g.lonB = p[83] * cos(dr * (dd - p[84])) + p[87] * cos(2.0 * dr * (dd - p[88]));
+    }
+}
+
+// Per-object part.  Returns the gtd7d total mass density in kg/m^3.
+template <typename T>
+struct Fast {
+    const NrlEpochBlock& eb;
+    T gsurf, re;
+    T plg[4][9];
+    T ctloc, stloc, c2tloc, s2tloc, s3tloc, c3tloc;
+    T cgl, sgl, c2gl, s2gl;  // cos / sin of (dgtr * g_long) and of twice it
+    T glat, absLat, gLong;
+    T csec, ssec;  // cos / sin (sr * seconds of day)
+    T apt0;
+    T meso_tn1[5], meso_tgn1[2];
+    T dm28;
+
+    __device__ __forceinline__ Fast(const NrlEpochBlock& b, double sec) : eb(b) {
+        double sc, cc;
+        sincos(7.2722E-5 * sec, &sc, &cc);
+        csec = T(cc);
+        ssec = T(sc);
+    }
+
+    __device__ __forceinline__ T zeta(T zz, T zl) const { return ((zz - zl) * (re + zl) / (re + zz)); }
+
+    __device__ __forceinline__ void basis(T lat, T lst) {
+        const T dgtr = T(1.74533E-2), hr = T(0.2618);
+        T c, s;
+        sincos(lat * dgtr, &c, &s);  // c = sin(lat), s = cos(lat)
+        const T c2 = c * c, c4 = c2 * c2, s2 = s * s;
+        plg[0][1] = c;
+        plg[0][2] = T(0.5) * (T(3.0) * c2 - T(1.0));
+        plg[0][3] = T(0.5) * (T(5.0) * c * c2 - T(3.0) * c);
+        plg[0][4] = (T(35.0) * c4 - T(30.0) * c2 + T(3.0)) / T(8.0);
+        plg[0][5] = (T(63.0) * c2 * c2 * c - T(70.0) * c2 * c + T(15.0) * c) / T(8.0);
+        plg[0][6] = (T(11.0) * c * plg[0][5] - T(5.0) * plg[0][4]) / T(6.0);
+        plg[1][1] = s;
+        plg[1][2] = T(3.0) * c * s;
+        plg[1][3] = T(1.5) * (T(5.0) * c2 - T(1.0)) * s;
+        plg[1][4] = T(2.5) * (T(7.0) * c2 * c - T(3.0) * c) * s;
+        plg[1][5] = T(1.875) * (T(21.0) * c4 - T(14.0) * c2 + T(1.0)) * s;
+        plg[1][6] = (T(11.0) * c * plg[1][5] - T(6.0) * plg[1][4]) / T(5.0);
+        plg[2][2] = T(3.0) * s2;
+        plg[2][3] = T(15.0) * s2 * c;
+        plg[2][4] = T(7.5) * (T(7.0) * c2 - T(1.0)) * s2;
+        plg[2][5] = T(3.0) * c * plg[2][4] - T(2.0) * plg[2][3];
+        plg[2][6] = (T(11.0) * c * plg[2][5] - T(7.0) * plg[2][4]) / T(4.0);
+        plg[2][7] = (T(13.0) * c * plg[2][6] - T(8.0) * plg[2][5]) / T(5.0);
+        plg[3][3] = T(15.0) * s2 * s;
+        plg[3][4] = T(105.0) * s2 * s * c;
+        plg[3][5] = (T(9.0) * c * plg[3][4] - T(7.) * plg[3][3]) / T(2.0);
+        plg[3][6] = (T(11.0) * c * plg[3][5] - T(8.) * plg[3][4]) / T(3.0);
+        sincos(hr * lst, &stloc, &ctloc);
+        sincos(T(2.0) * hr * lst, &s2tloc, &c2tloc);
+        sincos(T(3.0) * hr * lst, &s3tloc, &c3tloc);
+        sincos(dgtr * gLong, &sgl, &cgl);
+        sincos(T(2.0) * dgtr * gLong, &s2gl, &c2gl);
+    }
+
+    // G(L), upper thermosphere; table k of the globe7 sequence
+    __device__ T globe7(int k) {
+        const double* p = globeTable(k);
+        const NrlGlobeEpoch& g = eb.ge[k];
+        const T hr = T(0.2618), dgtr = T(1.74533E-2);
+        const T dfa = T(eb.dfa);
+        const T cd32 = T(g.cd32), cd18 = T(g.cd18), cd14 = T(g.cd14), cd39 = T(g.cd39);
+        const T f1 = T(g.f1), f2 = T(g.f2);
+        T tinf = T(p[30]) + T(g.t0);
+        tinf += (T(p[1]) * plg[0][2] + T(p[2]) * plg[0][4] + T(p[22]) * plg[0][6]) + (T(p[14]) * plg[0][2]) * dfa
+            + T(p[26]) * plg[0][1];
+        tinf += T(p[18]) * cd32;
+        tinf += (T(p[15]) + T(p[16]) * plg[0][2]) * cd18;
+        tinf += f1 * (T(p[9]) * plg[0][1] + T(p[10]) * plg[0][3]) * cd14;
+        tinf += T(p[37]) * plg[0][1] * cd39;
+        {
+            const T t71 = (T(p[11]) * plg[1][2]) * cd14;
+            const T t72 = (T(p[12]) * plg[1][2]) * cd14;
+            tinf += f2 * ((T(p[3]) * plg[1][1] + T(p[4]) * plg[1][3] + T(p[27]) * plg[1][5] + t71) * ctloc
+                          + (T(p[6]) * plg[1][1] + T(p[7]) * plg[1][3] + T(p[28]) * plg[1][5] + t72) * stloc);
+        }
+        {
+            const T t81 = (T(p[23]) * plg[2][3] + T(p[35]) * plg[2][5]) * cd14;
+            const T t82 = (T(p[33]) * plg[2][3] + T(p[36]) * plg[2][5]) * cd14;
+            tinf += f2 * ((T(p[5]) * plg[2][2] + T(p[41]) * plg[2][4] + t81) * c2tloc
+                          + (T(p[8]) * plg[2][2] + T(p[42]) * plg[2][4] + t82) * s2tloc);
+        }
+        tinf += f2 * ((T(p[39]) * plg[3][3] + (T(p[93]) * plg[3][4] + T(p[46]) * plg[3][6]) * cd14) * s3tloc
+                      + (T(p[40]) * plg[3][3] + (T(p[94]) * plg[3][4] + T(p[48]) * plg[3][6]) * cd14) * c3tloc);
+        if (p[51] != 0) {
+            T exp1 = exp(T(-10800.0) * fabs(T(p[51])) / (T(1.0) + T(p[138]) * (T(45.0) - absLat)));
+            if (exp1 > T(0.99999)) exp1 = T(0.99999);
+            // sg0 (Eq. A24a) with the epoch's g0 responses
+            const T e2 = exp1 * exp1, e3 = e2 * exp1, e4 = e2 * e2, e8 = e4 * e4, e12 = e8 * e4;
+            const T e19 = e12 * e4 * e3;
+            const T sumex = T(1.0) + (T(1.0) - e19) / (T(1.0) - exp1) * sqrt(exp1);
+            apt0 = (T(g.g0[0]) + (T(g.g0[1]) * exp1 + T(g.g0[2]) * e2 + T(g.g0[3]) * e3
+                                  + (T(g.g0[4]) * e4 + T(g.g0[5]) * e12) * (T(1.0) - e8) / (T(1.0) - exp1)))
+                / sumex;
+            const T c131 = T(g.c131), s131 = T(g.s131);
+            tinf += apt0 * (T(p[50]) + T(p[96]) * plg[0][2] + T(p[54]) * plg[0][4]
+                            + (T(p[125]) * plg[0][1] + T(p[126]) * plg[0][3] + T(p[127]) * plg[0][5]) * cd14
+                            + (T(p[128]) * plg[1][1] + T(p[129]) * plg[1][3] + T(p[130]) * plg[1][5])
+                                * (ctloc * c131 + stloc * s131));
+        }
+        // longitudinal
+        tinf += (T(1.0) + T(p[80]) * dfa)
+            * ((T(p[64]) * plg[1][2] + T(p[65]) * plg[1][4] + T(p[66]) * plg[1][6] + T(p[103]) * plg[1][1]
+                + T(p[104]) * plg[1][3] + T(p[105]) * plg[1][5]
+                + (T(p[109]) * plg[1][1] + T(p[110]) * plg[1][3] + T(p[111]) * plg[1][5]) * cd14)
+                   * cgl
+               + (T(p[90]) * plg[1][2] + T(p[91]) * plg[1][4] + T(p[92]) * plg[1][6] + T(p[106]) * plg[1][1]
+                  + T(p[107]) * plg[1][3] + T(p[108]) * plg[1][5]
+                  + (T(p[112]) * plg[1][1] + T(p[113]) * plg[1][3] + T(p[114]) * plg[1][5]) * cd14)
+                   * sgl);
+        // ut and mixed ut / longitude
+        tinf += (T(1.0) + T(p[95]) * plg[0][1]) * (T(1.0) + T(p[81]) * dfa) * (T(1.0) + T(p[119]) * plg[0][1] * cd14)
+            * ((T(p[68]) * plg[0][1] + T(p[69]) * plg[0][3] + T(p[70]) * plg[0][5])
+               * (csec * T(g.c71) + ssec * T(g.s71)));
+        {
+            // cos(sr (sec - p79) + 2 dgtr g_long)
+            const T c79 = csec * T(g.c79) + ssec * T(g.s79), s79 = ssec * T(g.c79) - csec * T(g.s79);
+            tinf += (T(p[76]) * plg[2][3] + T(p[77]) * plg[2][5] + T(p[78]) * plg[2][7]) * (c79 * c2gl - s79 * s2gl)
+                * (T(1.0) + T(p[137]) * dfa);
+        }
+        if (p[51] != 0) {
+            const T c97 = T(g.c97), s97 = T(g.s97);
+            const T c136 = T(g.c136), s136 = T(g.s136);
+            tinf += apt0 * (T(1.) + T(p[132]) * plg[0][1])
+                    * ((T(p[52]) * plg[1][2] + T(p[98]) * plg[1][4] + T(p[67]) * plg[1][6]) * (cgl * c97 + sgl * s97))
+                + apt0 * (T(p[133]) * plg[1][1] + T(p[134]) * plg[1][3] + T(p[135]) * plg[1][5]) * cd14
+                    * (cgl * c136 + sgl * s136)
+                + apt0 * (T(p[55]) * plg[0][1] + T(p[56]) * plg[0][3] + T(p[57]) * plg[0][5])
+                    * (csec * T(g.c58) + ssec * T(g.s58));
+        }
+        (void)hr;
+        (void)dgtr;
+        return tinf;
+    }
+
+    __device__ T glob7s(int k) const {
+        const double* p = globSTable(k);
+        const NrlGlobSEpoch& g = eb.gs[k];
+        const T dfa = T(eb.dfa);
+        T tt = T(p[21]) * dfa;
+        tt += T(p[1]) * plg[0][2] + T(p[2]) * plg[0][4] + T(p[22]) * plg[0][6] + T(p[26]) * plg[0][1]
+            + T(p[14]) * plg[0][3] + T(p[59]) * plg[0][5];
+        tt += (T(p[18]) + T(p[47]) * plg[0][2] + T(p[29]) * plg[0][4]) * T(g.cd32);
+        tt += (T(p[15]) + T(p[16]) * plg[0][2] + T(p[30]) * plg[0][4]) * T(g.cd18);
+        tt += (T(p[9]) * plg[0][1] + T(p[10]) * plg[0][3] + T(p[20]) * plg[0][5]) * T(g.cd14);
+        tt += (T(p[37]) * plg[0][1]) * T(g.cd39);
+        {
+            const T t71 = T(p[11]) * plg[1][2] * T(g.cd14);
+            const T t72 = T(p[12]) * plg[1][2] * T(g.cd14);
+            tt += ((T(p[3]) * plg[1][1] + T(p[4]) * plg[1][3] + t71) * ctloc
+                   + (T(p[6]) * plg[1][1] + T(p[7]) * plg[1][3] + t72) * stloc);
+        }
+        {
+            const T t81 = (T(p[23]) * plg[2][3] + T(p[35]) * plg[2][5]) * T(g.cd14);
+            const T t82 = (T(p[33]) * plg[2][3] + T(p[36]) * plg[2][5]) * T(g.cd14);
+            tt += ((T(p[5]) * plg[2][2] + T(p[41]) * plg[2][4] + t81) * c2tloc
+                   + (T(p[8]) * plg[2][2] + T(p[42]) * plg[2][4] + t82) * s2tloc);
+        }
+        tt += T(p[39]) * plg[3][3] * s3tloc + T(p[40]) * plg[3][3] * c3tloc;
+        tt += (T(p[50]) * apt0 + T(p[96]) * plg[0][2] * apt0);
+        tt += (T(1.0) + plg[0][1] * T(g.lonA) + T(g.lonB))
+            * ((T(p[64]) * plg[1][2] + T(p[65]) * plg[1][4] + T(p[66]) * plg[1][6] + T(p[74]) * plg[1][1]
+                + T(p[75]) * plg[1][3] + T(p[76]) * plg[1][5]) * cgl
+               + (T(p[90]) * plg[1][2] + T(p[91]) * plg[1][4] + T(p[92]) * plg[1][6] + T(p[77]) * plg[1][1]
+                  + T(p[78]) * plg[1][3] + T(p[79]) * plg[1][5]) * sgl);
+        return tt;
+    }
+
+    __device__ T densu(T alt, T dlb, T tinf, T tlb, T xm, T alpha, T* tz, T zlb, T s2, const T* zn1) {
+        const T rgas = T(831.4);
+        T xs[5], ys[5], y2out[5];
+        T x = T(0), z1 = T(0), t1 = T(0), zgdif = T(0);
+        const int mn1 = 5;
+        const T za = zn1[0];
+        T z = (alt > za) ? alt : za;
+        const T zg2 = zeta(z, zlb);
+        const T tt = tinf - (tinf - tlb) * exp(-s2 * zg2);
+        const T ta = tt;
+        *tz = tt;
+        T densu_temp = *tz;
+        if (alt < za) {
+            const T q = (re + zlb) / (re + za);
+            meso_tgn1[0] = (tinf - ta) * s2 * (q * q);
+            meso_tn1[0] = ta;
+            z = (alt > zn1[mn1 - 1]) ? alt : zn1[mn1 - 1];
+            z1 = zn1[0];
+            const T z2 = zn1[mn1 - 1];
+            t1 = meso_tn1[0];
+            const T t2 = meso_tn1[mn1 - 1];
+            const T zg = zeta(z, z1);
+            zgdif = zeta(z2, z1);
+            for (int k = 0; k < mn1; k++) {
+                xs[k] = zeta(zn1[k], z1) / zgdif;
+                ys[k] = T(1.0) / meso_tn1[k];
+            }
+            const T r2 = (re + z2) / (re + z1);
+            const T yd1 = -meso_tgn1[0] / (t1 * t1) * zgdif;
+            const T yd2 = -meso_tgn1[1] / (t2 * t2) * zgdif * (r2 * r2);
+            nrl::Model<T>::spline(xs, ys, mn1, yd1, yd2, y2out);
+            x = zg / zgdif;
+            const T y = nrl::Model<T>::splint(xs, ys, y2out, mn1, x);
+            *tz = T(1.0) / y;
+            densu_temp = *tz;
+        }
+        if (xm == T(0)) return densu_temp;
+        const T g1 = T(1.0) + zlb / re;
+        T glb = gsurf / (g1 * g1);
+        const T gamma = xm * glb / (s2 * rgas * tinf);
+        T expl = exp(-s2 * gamma * zg2);
+        if (expl > T(50.0)) expl = T(50.0);
+        if (tt <= T(0)) expl = T(50.0);
+        densu_temp = dlb * pow((tlb / tt), ((T(1.0) + alpha + gamma))) * expl;
+        if (alt >= za) return densu_temp;
+        const T g2 = T(1.0) + z1 / re;
+        glb = gsurf / (g2 * g2);
+        const T gamm = xm * glb * zgdif / rgas;
+        const T yi = nrl::Model<T>::splini(xs, ys, y2out, mn1, x);
+        expl = gamm * yi;
+        if (expl > T(50.0)) expl = T(50.0);
+        if (*tz <= T(0)) expl = T(50.0);
+        return densu_temp * pow((t1 / *tz), (T(1.0) + alpha)) * exp(-expl);
+    }
+
+    // thermosphere (alt >= 72.5 km): number densities d[0..8] (m^-3)
+    __device__ void gts7(T alt, T* d) {
+        T zn1[5] = {T(NRL_PDL(1)[15]), T(110.0), T(100.0), T(90.0), T(72.5)};
+        const T za = zn1[0];
+        for (int j = 0; j < 9; j++) d[j] = T(0);
+        const T z = alt;
+        T dummyT;
+        const T tinf = (z > za) ? T(NRL_PTM(0)) * T(NRL_PT[0]) * (T(1.0) + globe7(0)) : T(NRL_PTM(0)) * T(NRL_PT[0]);
+        const T g0v = (z > zn1[4]) ? T(NRL_PTM(3)) * T(NRL_PS[0]) * (T(1.0) + globe7(1)) : T(NRL_PTM(3)) * T(NRL_PS[0]);
+        const T tlb = T(NRL_PTM(1)) * (T(1.0) + globe7(5)) * T(NRL_PD(3)[0]);
+        const T s = g0v / (tinf - tlb);
+        const T ptl30 = T(NRL_PTM(4)) * T(NRL_PTL(3)[0]);
+        if (z < T(300.0)) {
+            meso_tn1[1] = T(NRL_PTM(6)) * T(NRL_PTL(0)[0]) / (T(1.0) - glob7s(0));
+            meso_tn1[2] = T(NRL_PTM(2)) * T(NRL_PTL(1)[0]) / (T(1.0) - glob7s(1));
+            meso_tn1[3] = T(NRL_PTM(7)) * T(NRL_PTL(2)[0]) / (T(1.0) - glob7s(2));
+            meso_tn1[4] = ptl30 / (T(1.0) - glob7s(3));
+            meso_tgn1[1] = T(NRL_PTM(8)) * T(NRL_PMA(8)[0]) * (T(1.0) + glob7s(4 + 8)) * meso_tn1[4] * meso_tn1[4]
+                / (ptl30 * ptl30);
+        } else {
+            meso_tn1[1] = T(NRL_PTM(6)) * T(NRL_PTL(0)[0]);
+            meso_tn1[2] = T(NRL_PTM(2)) * T(NRL_PTL(1)[0]);
+            meso_tn1[3] = T(NRL_PTM(7)) * T(NRL_PTL(2)[0]);
+            meso_tn1[4] = ptl30;
+            meso_tgn1[1] = T(NRL_PTM(8)) * T(NRL_PMA(8)[0]) * meso_tn1[4] * meso_tn1[4] / (ptl30 * ptl30);
+        }
+        const T zlb = T(NRL_PTM(5));
+        const T xmm = T(NRL_PDM(2, 4));
+        // N2
+        const T g28 = globe7(4);
+        // sin(dgtr glat) = plg[0][1]; cos(dr (doy - pt[13])) is the pt table's cd14
+        const T zhf = T(NRL_PDL(1)[24]) * (T(1.0) + T(NRL_PDL(0)[24]) * plg[0][1] * T(eb.ge[0].cd14));
+        const T db28 = T(NRL_PDM(2, 0)) * exp(g28) * T(NRL_PD(2)[0]);
+        d[2] = densu(z, db28, tinf, tlb, T(28.0), T(0.0), &dummyT, zlb, s, zn1);
+        const T zhm28 = T(NRL_PDM(2, 3)) * T(NRL_PDL(1)[5]);
+        T b28 = T(0.0);
+        if (!(z > T(450.0) && z >= za))
+            b28 = densu(T(NRL_PDM(2, 2)) * zhf, db28, tinf, tlb, T(28.0) - xmm, T(-1.0), &dummyT, zlb, s, zn1);
+        if (z <= T(160.0)) {
+            dm28 = densu(z, b28, tinf, tlb, xmm, T(0.0), &dummyT, zlb, s, zn1);
+            d[2] = nrl::Model<T>::dnet(d[2], dm28, zhm28, xmm, T(28.0));
+        }
+        // He
+        const T db04 = T(NRL_PDM(0, 0)) * exp(globe7(2)) * T(NRL_PD(0)[0]);
+        d[0] = densu(z, db04, tinf, tlb, T(4.), T(-0.38), &dummyT, zlb, s, zn1);
+        if (z < T(200.0)) {
+            const T b04 = densu(T(NRL_PDM(0, 2)), db04, tinf, tlb, T(4.) - xmm, T(-1.38), &dummyT, zlb, s, zn1);
+            const T dm04 = densu(z, b04, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1);
+            d[0] = nrl::Model<T>::dnet(d[0], dm04, zhm28, xmm, T(4.));
+            const T rl = log(b28 * T(NRL_PDM(0, 1)) / b04);
+            d[0] = d[0] * nrl::Model<T>::ccor(z, rl, T(NRL_PDM(0, 5)) * T(NRL_PDL(1)[1]), T(NRL_PDM(0, 4)) * T(NRL_PDL(1)[0]));
+        }
+        // O
+        const T db16 = T(NRL_PDM(1, 0)) * exp(globe7(3)) * T(NRL_PD(1)[0]);
+        d[1] = densu(z, db16, tinf, tlb, T(16.), T(0.0), &dummyT, zlb, s, zn1);
+        if (z <= T(300.0)) {
+            const T b16 = densu(T(NRL_PDM(1, 2)), db16, tinf, tlb, T(16.0) - xmm, T(-1.0), &dummyT, zlb, s, zn1);
+            const T dm16 = densu(z, b16, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1);
+            d[1] = nrl::Model<T>::dnet(d[1], dm16, zhm28, xmm, T(16.));
+            const T rl = T(NRL_PDM(1, 1)) * T(NRL_PDL(1)[16]) * (T(1.0) + T(NRL_PDL(0)[23]) * (T(eb.f107A) - T(150.0)));
+            d[1] = d[1] * nrl::Model<T>::ccor2(z, rl, T(NRL_PDM(1, 5)) * T(NRL_PDL(1)[3]),
+                                               T(NRL_PDM(1, 4)) * T(NRL_PDL(1)[2]), T(NRL_PDM(1, 5)) * T(NRL_PDL(1)[4]));
+            d[1] = d[1] * nrl::Model<T>::ccor(z, T(NRL_PDM(1, 3)) * T(NRL_PDL(1)[14]),
+                                              T(NRL_PDM(1, 7)) * T(NRL_PDL(1)[13]), T(NRL_PDM(1, 6)) * T(NRL_PDL(1)[12]));
+        }
+        // O2
+        const T db32 = T(NRL_PDM(3, 0)) * exp(globe7(6)) * T(NRL_PD(4)[0]);
+        d[3] = densu(z, db32, tinf, tlb, T(32.), T(0.0), &dummyT, zlb, s, zn1);
+        if (z <= T(250.0)) {
+            const T b32 = densu(T(NRL_PDM(3, 2)), db32, tinf, tlb, T(32.) - xmm, T(-1.), &dummyT, zlb, s, zn1);
+            const T dm32 = densu(z, b32, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1);
+            d[3] = nrl::Model<T>::dnet(d[3], dm32, zhm28, xmm, T(32.));
+            const T rl = log(b28 * T(NRL_PDM(3, 1)) / b32);
+            d[3] = d[3] * nrl::Model<T>::ccor(z, rl, T(NRL_PDM(3, 5)) * T(NRL_PDL(1)[7]), T(NRL_PDM(3, 4)) * T(NRL_PDL(1)[6]));
+        }
+        {
+            const T rc32 = T(NRL_PDM(3, 3)) * T(NRL_PDL(1)[23]) * (T(1.) + T(NRL_PDL(0)[23]) * (T(eb.f107A) - T(150.)));
+            d[3] = d[3] * nrl::Model<T>::ccor2(z, rc32, T(NRL_PDM(3, 7)) * T(NRL_PDL(1)[22]),
+                                               T(NRL_PDM(3, 6)) * T(NRL_PDL(1)[21]), T(NRL_PDM(3, 7)) * T(NRL_PDL(0)[22]));
+        }
+        // Ar
+        const T db40 = T(NRL_PDM(4, 0)) * exp(globe7(7)) * T(NRL_PD(5)[0]);
+        d[4] = densu(z, db40, tinf, tlb, T(40.), T(0.17), &dummyT, zlb, s, zn1);
+        if (z <= T(240.0)) {
+            const T b40 = densu(T(NRL_PDM(4, 2)), db40, tinf, tlb, T(40.) - xmm, T(-0.83), &dummyT, zlb, s, zn1);
+            const T dm40 = densu(z, b40, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1);
+            d[4] = nrl::Model<T>::dnet(d[4], dm40, zhm28, xmm, T(40.));
+            const T rl = log(b28 * T(NRL_PDM(4, 1)) / b40);
+            d[4] = d[4] * nrl::Model<T>::ccor(z, rl, T(NRL_PDM(4, 5)) * T(NRL_PDL(1)[9]), T(NRL_PDM(4, 4)) * T(NRL_PDL(1)[8]));
+        }
+        // H
+        const T db01 = T(NRL_PDM(5, 0)) * exp(globe7(8)) * T(NRL_PD(6)[0]);
+        d[6] = densu(z, db01, tinf, tlb, T(1.), T(-0.38), &dummyT, zlb, s, zn1);
+        if (z <= T(320.0)) {
+            const T b01 = densu(T(NRL_PDM(5, 2)), db01, tinf, tlb, T(1.) - xmm, T(-1.38), &dummyT, zlb, s, zn1);
+            const T dm01 = densu(z, b01, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1);
+            d[6] = nrl::Model<T>::dnet(d[6], dm01, zhm28, xmm, T(1.));
+            const T rl = log(b28 * T(NRL_PDM(5, 1)) * fabs(T(NRL_PDL(1)[17])) / b01);
+            d[6] = d[6] * nrl::Model<T>::ccor(z, rl, T(NRL_PDM(5, 5)) * T(NRL_PDL(1)[11]), T(NRL_PDM(5, 4)) * T(NRL_PDL(1)[10]));
+            d[6] = d[6] * nrl::Model<T>::ccor(z, T(NRL_PDM(5, 3)) * T(NRL_PDL(1)[20]),
+                                              T(NRL_PDM(5, 7)) * T(NRL_PDL(1)[19]), T(NRL_PDM(5, 6)) * T(NRL_PDL(1)[18]));
+        }
+        // N
+        const T db14 = T(NRL_PDM(6, 0)) * exp(globe7(9)) * T(NRL_PD(7)[0]);
+        d[7] = densu(z, db14, tinf, tlb, T(14.), T(0.0), &dummyT, zlb, s, zn1);
+        if (z <= T(450.0)) {
+            const T b14 = densu(T(NRL_PDM(6, 2)), db14, tinf, tlb, T(14.) - xmm, T(-1.), &dummyT, zlb, s, zn1);
+            const T dm14 = densu(z, b14, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1);
+            d[7] = nrl::Model<T>::dnet(d[7], dm14, zhm28, xmm, T(14.));
+            const T rl = log(b28 * T(NRL_PDM(6, 1)) * fabs(T(NRL_PDL(0)[2])) / b14);
+            d[7] = d[7] * nrl::Model<T>::ccor(z, rl, T(NRL_PDM(6, 5)) * T(NRL_PDL(0)[1]), T(NRL_PDM(6, 4)) * T(NRL_PDL(0)[0]));
+            d[7] = d[7] * nrl::Model<T>::ccor(z, T(NRL_PDM(6, 3)) * T(NRL_PDL(0)[5]),
+                                              T(NRL_PDM(6, 7)) * T(NRL_PDL(0)[4]), T(NRL_PDM(6, 6)) * T(NRL_PDL(0)[3]));
+        }
+        // anomalous O
+        const T db16h = T(NRL_PDM(7, 0)) * exp(globe7(10)) * T(NRL_PD(8)[0]);
+        const T tho = T(NRL_PDM(7, 9)) * T(NRL_PDL(0)[6]);
+        const T dd = densu(z, db16h, tho, tho, T(16.), T(0.0), &dummyT, zlb, s, zn1);
+        const T zsht = T(NRL_PDM(7, 5)), zmho = T(NRL_PDM(7, 4));
+        const T gz = T(1.0) + zmho / re;
+        const T zsho = T(831.4) * tho / ((gsurf / (gz * gz)) * T(16.0));
+        d[8] = dd * exp(-zsht / zsho * (exp(-(z - zmho) / zsht) - T(1.)));
+        for (int i = 0; i < 9; i++) d[i] = d[i] * T(1.0E6);
+    }
+
+    // gtd7 + gtd7d total mass density (kg/m^3)
+    __device__ T density(T lat, T lon, T alt, T lst) {
+        glat = lat;
+        absLat = fabs(lat);
+        gLong = lon;
+        apt0 = T(0);
+        dm28 = T(0);
+        meso_tn1[0] = T(0);
+        meso_tgn1[0] = T(0);
+        // glatf
+        const T c2 = cos(T(2.0) * T(1.74533E-2) * lat);
+        gsurf = T(980.616) * (T(1.0) - T(0.0026373) * c2);
+        re = T(2.0) * gsurf / (T(3.085462E-6) + T(2.27E-9) * c2) * T(1.0E-5);
+        basis(lat, lst);
+        T d[9];
+        const T zn2top = T(72.5);
+        gts7(alt > zn2top ? alt : zn2top, d);
+        if (!(alt >= zn2top)) return lowerAtmosphere(alt, d);
+        return (T(1.66E-24) * (T(4.0) * d[0] + T(16.0) * d[1] + T(28.0) * d[2] + T(32.0) * d[3] + T(40.0) * d[4]
+                               + d[6] + T(14.0) * d[7] + T(16.0) * d[8]))
+            / T(1000);
+    }
+
+    // below 72.5 km (not reached in orbit, kept for completeness)
+    __device__ __noinline__ T lowerAtmosphere(T alt, const T* d) {
+        nrl::Model<T> m;
+        m.gsurf = gsurf;
+        m.re = re;
+        const T zn3[5] = {T(32.5), T(20.0), T(15.0), T(10.0), T(0.0)};
+        const T zn2[4] = {T(72.5), T(55.0), T(45.0), T(32.5)};
+        T tn2[4], tgn2[2], tn3[5] = {0, 0, 0, 0, 0}, tgn3[2] = {0, 0};
+        tgn2[0] = meso_tgn1[1];
+        tn2[0] = meso_tn1[4];
+        tn2[1] = T(NRL_PMA(0)[0]) * T(NRL_PAVGM(0)) / (T(1.0) - glob7s(4 + 0));
+        tn2[2] = T(NRL_PMA(1)[0]) * T(NRL_PAVGM(1)) / (T(1.0) - glob7s(4 + 1));
+        tn2[3] = T(NRL_PMA(2)[0]) * T(NRL_PAVGM(2)) / (T(1.0) - glob7s(4 + 2));
+        const T q2 = T(NRL_PMA(2)[0]) * T(NRL_PAVGM(2));
+        tgn2[1] = T(NRL_PAVGM(8)) * T(NRL_PMA(9)[0]) * (T(1.0) + glob7s(4 + 9)) * tn2[3] * tn2[3] / (q2 * q2);
+        tn3[0] = tn2[3];
+        if (alt <= zn3[0]) {
+            tgn3[0] = tgn2[1];
+            tn3[1] = T(NRL_PMA(3)[0]) * T(NRL_PAVGM(3)) / (T(1.0) - glob7s(4 + 3));
+            tn3[2] = T(NRL_PMA(4)[0]) * T(NRL_PAVGM(4)) / (T(1.0) - glob7s(4 + 4));
+            tn3[3] = T(NRL_PMA(5)[0]) * T(NRL_PAVGM(5)) / (T(1.0) - glob7s(4 + 5));
+            tn3[4] = T(NRL_PMA(6)[0]) * T(NRL_PAVGM(6)) / (T(1.0) - glob7s(4 + 6));
+            const T q6 = T(NRL_PMA(6)[0]) * T(NRL_PAVGM(6));
+            tgn3[1] = T(NRL_PMA(7)[0]) * T(NRL_PAVGM(7)) * (T(1.0) + glob7s(4 + 7)) * tn3[4] * tn3[4] / (q6 * q6);
+        }
+        const T zmix = T(62.5);
+        T dmc = T(0);
+        if (alt > zmix) dmc = T(1.0) - (zn2[0] - alt) / (zn2[0] - zmix);
+        const T dm28m = dm28 * T(1.0E6);
+        const T xmm = T(NRL_PDM(2, 4));
+        T tz = T(0);
+        const T dz28 = d[2];
+        T o[9];
+        T dmr = d[2] / dm28m - T(1.0);
+        o[2] = m.densm(alt, dm28m, xmm, &tz, 5, zn3, tn3, tgn3, 4, zn2, tn2, tgn2) * (T(1.0) + dmr * dmc);
+        dmr = d[0] / (dz28 * T(NRL_PDM(0, 1))) - T(1.0);
+        o[0] = o[2] * T(NRL_PDM(0, 1)) * (T(1.0) + dmr * dmc);
+        dmr = d[3] / (dz28 * T(NRL_PDM(3, 1))) - T(1.0);
+        o[3] = o[2] * T(NRL_PDM(3, 1)) * (T(1.0) + dmr * dmc);
+        dmr = d[4] / (dz28 * T(NRL_PDM(4, 1))) - T(1.0);
+        o[4] = o[2] * T(NRL_PDM(4, 1)) * (T(1.0) + dmr * dmc);
+        return (T(1.66E-24) * (T(4.0) * o[0] + T(28.0) * o[2] + T(32.0) * o[3] + T(40.0) * o[4])) / T(1000);
+    }
+};
+
+#endif  // __CUDACC__
+
+}  // namespace nrlf
+}  // namespace phop

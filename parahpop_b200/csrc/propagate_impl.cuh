@@ -296,19 +296,9 @@ static __device__ __noinline__ double nrlDensity(const DevEnv& e, const EpochRec
     if (alt > e.nrlHcutoff) return 0.0;
     if (!r.nrlValid) return NAN;
     const double kRad = 57.2957795130823208768;
-    nrl::Input<double> in;
-    in.doy = r.nrlDoy;
-    in.sec = r.nrlSec;
-    in.alt = alt;
-    in.g_lat = lat * kRad;
-    in.g_long = lon * kRad;
-    in.lst = wrapHours(r.nrlGast + lon * kRad / 15.0);
-    in.f107A = r.nrlF107a;
-    in.f107 = r.nrlF107;
-    in.ap = r.nrlAp;
-#pragma unroll
-    for (int k = 0; k < 7; ++k) in.ap_a[k] = r.nrlApa[k];
-    const double rhoSi = nrl::density<double>(in);
+    nrlf::Fast<double> model(e.nrlBlocks[r.nrlBlock], r.nrlSec);
+    const double lst = wrapHours(r.nrlGast + lon * kRad / 15.0);
+    const double rhoSi = model.density(lat * kRad, lon * kRad, alt, lst);
     if (!isfinite(rhoSi) || rhoSi < 0.0) return NAN;
     return (rhoSi * 1.0e9) * e.nrlDensityScale;
 }
@@ -448,7 +438,7 @@ static __device__ __noinline__ void epochRecordOutOfLine(const DevEnv& env, doub
 }
 
 template <int L, typename T, bool SHARED_GRID>
-__global__ void __launch_bounds__(256, 2) propagateKernel(const __grid_constant__ StepParams p) {
+__global__ void __launch_bounds__(512, 1) propagateKernel(const __grid_constant__ StepParams p) {
     using Tile = typename TileOf<T>::type;
     constexpr int CPL = (6 + L - 1) / L;
     extern __shared__ __align__(128) unsigned char smem[];

@@ -186,6 +186,53 @@ def _loguniform(rng, lo, hi, n):
     return np.exp(rng.uniform(math.log(lo), math.log(hi), n))
 
 
+# Rough thermosphere (F10.7 = 150) for screening decay: (altitude km, density
+# kg/m^3, scale height km).  Only used to keep objects that would re-enter
+# during the run out of the population: the reference driver rejects a run in
+# which any object ends non-finite ("Nonfinite final state").
+_ATM = [(150, 2.0e-9, 22), (200, 2.8e-10, 37), (250, 7.2e-11, 45), (300, 2.4e-11, 53), (350, 9.5e-12, 53),
+        (400, 4.0e-12, 58), (450, 1.8e-12, 60), (500, 8.5e-13, 63), (600, 2.2e-13, 71), (700, 6.5e-14, 88),
+        (800, 2.2e-14, 124), (900, 9.5e-15, 181), (1000, 5.0e-15, 268)]
+
+
+def _density(h):
+    h = np.asarray(h, dtype=float)
+    out = np.zeros_like(h)
+    for k in range(len(_ATM)):
+        lo = _ATM[k][0]
+        hi = _ATM[k + 1][0] if k + 1 < len(_ATM) else 1e9
+        m = (h >= lo) & (h < hi)
+        out[m] = _ATM[k][1] * np.exp(-(h[m] - lo) / _ATM[k][2])
+    out[h < _ATM[0][0]] = _ATM[0][1]
+    return out
+
+
+def decay_km(a_km, e, cd, area_m2, mass_kg, duration_s):
+    """Semi-major-axis decay estimate (km) over ``duration_s`` at perigee density."""
+    hp = a_km * (1 - e) - R_EARTH
+    B = cd * area_m2 / mass_kg
+    a = a_km * 1e3
+    per_rev = 2 * np.pi * B * _density(hp) * a * a
+    revs = duration_s / (2 * np.pi * np.sqrt(a ** 3 / (MU_ELEMENTS * 1e9)))
+    return per_rev * revs * 1e-3
+
+
+def _screen_decay(rng, a, e, mass, area, srp, cd, duration, limit_km=25.0):
+    """Redraw mass and areas of objects whose decay over ``duration`` would
+    exceed ``limit_km`` (they would re-enter and end non-finite)."""
+    for _ in range(100):
+        bad = decay_km(a, e, cd, area, mass, duration) > limit_km
+        if not bad.any():
+            break
+        k = int(bad.sum())
+        mass[bad] = _loguniform(rng, 100.0, 8000.0, k)
+        area[bad] = _loguniform(rng, 1.0, 50.0, k)
+        srp[bad] = _loguniform(rng, 1.0, 50.0, k)
+    bad = decay_km(a, e, cd, area, mass, duration) > limit_km
+    mass[bad], area[bad] = 8000.0, 1.0
+    return mass, area, srp
+
+
 def population_central(n=1024, seed=0):
     """Central-gravity population: a = R + U(300,1200) km, e ~ U(0,0.01)."""
     rng = np.random.default_rng(seed)
@@ -199,8 +246,10 @@ def population_central(n=1024, seed=0):
                       seed=seed, note=f"central LEO population, n={n}, seed={seed}")
 
 
-def population_leo(n=10000, seed=1, alt=(300.0, 2000.0)):
-    """Full-force LEO population with log-uniform mass and areas."""
+def population_leo(n=10000, seed=1, alt=(300.0, 2000.0), screen_duration=86400.0):
+    """Full-force LEO population with log-uniform mass and areas; objects that
+    would decay more than 25 km within ``screen_duration`` get new mass and
+    areas (see ``_screen_decay``)."""
     rng = np.random.default_rng(seed)
     a = R_EARTH + rng.uniform(alt[0], alt[1], n)
     e = rng.uniform(0.0, 0.01, n)
@@ -212,6 +261,8 @@ def population_leo(n=10000, seed=1, alt=(300.0, 2000.0)):
     mass = _loguniform(rng, 100.0, 8000.0, n)
     ad = _loguniform(rng, 1.0, 50.0, n)
     asrp = _loguniform(rng, 1.0, 50.0, n)
+    if screen_duration:
+        mass, ad, asrp = _screen_decay(rng, a, e, mass, ad, asrp, np.full(n, 2.2), screen_duration)
     return Population(np.arange(1, n + 1), np.full(n, EPOCH0), st, mass, ad, asrp,
                       np.full(n, 2.2), np.full(n, 1.3), seed=seed,
                       note=f"full-force LEO population, n={n}, seed={seed}")
@@ -237,6 +288,7 @@ def population_mixed(n=1000000, seed=3):
     asrp = _loguniform(rng, 1.0, 50.0, n)
     epochs = EPOCH0 + rng.uniform(-10.0, 10.0, n)
     dur = _loguniform(rng, 3600.0, 7 * 86400.0, n)
+    mass, ad, asrp = _screen_decay(rng, a, e, mass, ad, asrp, np.full(n, 2.2), dur)
     return Population(np.arange(1, n + 1), epochs, st, mass, ad, asrp, np.full(n, 2.2), np.full(n, 1.3),
                       duration=dur, step=step, seed=seed,
                       note=f"mixed LEO/MEO/GEO population, n={n}, seed={seed}")
