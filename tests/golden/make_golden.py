@@ -1,0 +1,184 @@
+"""Generate the golden fixtures in tests/golden/ from the reference itself.
+
+Runs where the reference sources are available and built into oracle/_ref
+(``make -f oracle/Makefile.ref -j8 all kat``):
+
+* ``propagation_<case>.json`` - final states written by the reference CPU
+  backend (oracle/_ref/bin/parahpop_cpu, built from the reference sources) for
+  seeded synthetic environments and targets.  The cases follow the reference's
+  own validation script (scripts/validate.py): full force 600 s, central
+  600 s, final-step shortening at 65 s and 5 s, per-object epochs / masses,
+  33 objects across a block boundary, central-gravity invariants; plus the
+  benchmark configurations' shapes at small sizes.
+* ``nrlmsise00_kat.json`` - NRLMSISE-00 densities from the reference model
+  sources (oracle/_ref/ref_kat) on an input grid.
+* ``tides_kat.json`` - solid / ocean tide coefficient sets and the tide and
+  relativity accelerations from the reference's HpopCorrections.h.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+from parahpop_b200 import synthetic as S  # noqa: E402
+
+GOLD = Path(__file__).resolve().parent
+REF_CPU = ROOT / "oracle" / "_ref" / "bin" / "parahpop_cpu"
+REF_KAT = ROOT / "oracle" / "_ref" / "ref_kat"
+SHIM = ROOT / "oracle" / "_ref" / "libnodrv_shim.so"
+
+
+def env_hash(d: Path) -> str:
+    h = hashlib.sha256()
+    for name in ("gravity.tab", "bodies.brie", "earth.brot2", "SW-All.txt", "EOP-All.txt", "constants.json"):
+        h.update((d / name).read_bytes())
+    return h.hexdigest()
+
+
+def run_reference(env_dir: Path, cfg: dict, targets: dict) -> dict:
+    (env_dir / "config.json").write_text(json.dumps(cfg, indent=1))
+    (env_dir / "targets.json").write_text(json.dumps(targets))
+    out = env_dir / "ref_out"
+    shutil.rmtree(out, ignore_errors=True)
+    env = dict(os.environ, OMP_DYNAMIC="FALSE")
+    try:
+        import ctypes
+        ctypes.CDLL("libcuda.so.1")
+    except OSError:
+        env["LD_PRELOAD"] = str(SHIM)
+    r = subprocess.run([str(REF_CPU), "config.json", "targets.json", "ref_out"], cwd=env_dir, env=env,
+                       capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(r.stderr)
+    rows = (out / "final_states.csv").read_text().splitlines()[1:]
+    ids, ep, st = [], [], []
+    for row in rows:
+        v = row.split(",")
+        ids.append(int(v[0]))
+        ep.append(float(v[1]))
+        st.append([float(x) for x in v[2:8]])
+    return {"ids": ids, "epochs": ep, "states": st, "summary": json.loads((out / "summary.json").read_text())}
+
+
+CASES = {
+    # name: (population factory, duration, step, config kwargs, env spec kwargs)
+    "full_600s": (lambda: S.population_leo(8, 1), 600.0, 60.0, {}, {}),
+    "central_600s": (lambda: S.population_central(32, 0), 600.0, 60.0, {"force": "central"}, {}),
+    "full_65s_endpoint": (lambda: S.population_leo(4, 2), 65.0, 60.0, {}, {}),
+    "full_5s_endpoint": (lambda: S.population_leo(4, 2), 5.0, 60.0, {}, {}),
+    "batch_33": (lambda: S.population_leo(33, 5), 1800.0, 60.0, {}, {}),
+    "full_1h": (lambda: S.population_leo(16, 9), 3600.0, 60.0, {}, {}),
+    "deg120_1h": (lambda: S.population_leo(8, 10), 3600.0, 60.0, {"degree": 120}, {"degree": 120}),
+    "zonal_2h": (lambda: S.population_leo(8, 11), 7200.0, 60.0, {"degree": 6}, {"degree": 6, "zonal_only": True}),
+    "central_1d": (lambda: S.population_central(16, 4), 86400.0, 60.0, {"force": "central"}, {}),
+}
+
+
+def per_object_epochs():
+    """Per-object epochs and masses in one run (validate.py batch_4)."""
+    p = S.population_leo(4, 12)
+    p.epochs = p.epochs + np.array([0.0, 0.25, 0.5, 1.25])
+    p.mass = np.array([500.0, 1000.0, 2000.0, 4000.0])
+    return p
+
+
+CASES["batch_4_epochs"] = (per_object_epochs, 1800.0, 60.0, {"threads": 2}, {})
+
+
+def make_propagation_goldens(only=None):
+    for name, (pop_fn, dur, step, ckw, ekw) in CASES.items():
+        if only and name not in only:
+            continue
+        spec = S.EnvSpec(**ekw)
+        with tempfile.TemporaryDirectory() as td:
+            d = S.write_environment(Path(td), spec)
+            pop = pop_fn()
+            ckw2 = dict(ckw)
+            threads = ckw2.pop("threads", 1)
+            cfg = S.make_config(d, dur, step, max_steps=100000, threads=threads, **ckw2)
+            tg = pop.targets_json()
+            res = run_reference(d, cfg, tg)
+            out = {"case": name, "env_spec": {k: v for k, v in spec.__dict__.items()}, "env_sha256": env_hash(d),
+                   "config": cfg, "targets": tg, "reference": res,
+                   "generator": "tests/golden/make_golden.py via oracle/_ref/bin/parahpop_cpu"}
+            (GOLD / f"propagation_{name}.json").write_text(json.dumps(out))
+            print(name, "ok", res["summary"]["propagation_seconds"])
+
+
+def make_nrl_kat():
+    rng = np.random.default_rng(21)
+    lines, inputs = [], []
+    alts = [0.0, 10.0, 25.0, 40.0, 60.0, 70.0, 80.0, 95.0, 110.0, 130.0, 160.0, 200.0, 250.0, 300.0, 350.0,
+            400.0, 450.0, 500.0, 600.0, 800.0, 1000.0]
+    for alt in alts:
+        for _ in range(6):
+            doy = int(rng.integers(1, 366))
+            sec = float(rng.uniform(0, 86400))
+            lat = float(rng.uniform(-89, 89))
+            lon = float(rng.uniform(-180, 180))
+            lst = float(rng.uniform(0, 24))
+            f107a = float(rng.uniform(70, 250))
+            f107 = float(rng.uniform(70, 300))
+            ap = [float(x) for x in rng.choice([0, 3, 7, 15, 27, 48, 80, 132, 207], 7)]
+            v = [doy, sec, alt, lat, lon, lst, f107a, f107, ap[0]] + ap
+            inputs.append(v)
+            lines.append("nrl " + " ".join(repr(float(x)) for x in v))
+    r = subprocess.run([str(REF_KAT)], input="\n".join(lines) + "\n", capture_output=True, text=True, check=True)
+    outs = [json.loads(l) for l in r.stdout.splitlines()]
+    (GOLD / "nrlmsise00_kat.json").write_text(json.dumps({
+        "fields": "doy sec alt g_lat g_long lst f107A f107 ap ap_a[0..6]",
+        "inputs": inputs, "rho_kg_m3": [o["rho"] for o in outs],
+        "generator": "tests/golden/make_golden.py via oracle/_ref/ref_kat (reference Nrlmsise00Model.inl)"}))
+    print("nrl kat", len(outs))
+
+
+def make_tide_kat():
+    rng = np.random.default_rng(22)
+    lines, inputs = [], []
+    for _ in range(12):
+        r = rng.normal(size=3)
+        r = r / np.linalg.norm(r) * rng.uniform(6.7e6, 8.5e6)
+        v = rng.normal(size=3) * 4000.0
+        sun = rng.normal(size=3)
+        sun = sun / np.linalg.norm(sun) * 1.496e11
+        moon = rng.normal(size=3)
+        moon = moon / np.linalg.norm(moon) * 3.844e8
+        a, b, c = rng.uniform(0, 2 * np.pi, 3)
+        Rz = lambda t: np.array([[np.cos(t), np.sin(t), 0], [-np.sin(t), np.cos(t), 0], [0, 0, 1]])
+        Rx = lambda t: np.array([[1, 0, 0], [0, np.cos(t), np.sin(t)], [0, -np.sin(t), np.cos(t)]])
+        E = (Rz(a) @ Rx(1e-3 * b) @ Rz(c)).reshape(-1)
+        mjd = float(rng.uniform(55000, 60000))
+        ut1 = float(rng.uniform(-0.9, 0.9))
+        tt = 32.184 + float(rng.integers(33, 38))
+        xp, yp = float(rng.uniform(-0.3, 0.3)), float(rng.uniform(0.1, 0.6))
+        vals = list(r) + list(v) + list(sun) + list(moon) + list(E) + [mjd, ut1, tt, xp, yp]
+        inputs.append([float(x) for x in vals])
+        lines.append("tide " + " ".join(repr(float(x)) for x in vals))
+    res = subprocess.run([str(REF_KAT)], input="\n".join(lines) + "\n", capture_output=True, text=True, check=True)
+    outs = [json.loads(l) for l in res.stdout.splitlines()]
+    (GOLD / "tides_kat.json").write_text(json.dumps({
+        "fields": "r[3] v[3] sun[3] moon[3] (m, m/s) E[9] mjdUtc ut1Utc ttUtc xp yp (arcsec)",
+        "inputs": inputs, "outputs": outs,
+        "generator": "tests/golden/make_golden.py via oracle/_ref/ref_kat (reference HpopCorrections.h)"}))
+    print("tide kat", len(outs))
+
+
+if __name__ == "__main__":
+    only = sys.argv[1:]
+    if not only or "nrl" in only:
+        make_nrl_kat()
+    if not only or "tides" in only:
+        make_tide_kat()
+    make_propagation_goldens([x for x in only if x not in ("nrl", "tides")] or None)

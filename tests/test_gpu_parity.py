@@ -1,0 +1,165 @@
+"""B200 parity: the CUDA path (through the C ABI) against the reference's own
+outputs (golden fixtures) and against the CPU oracle.
+
+Tolerances: the reference's CPU/GPU acceptance, 1 mm in position and
+1e-6 m/s in velocity (example/compare.py:7-8), for the plain FP64 path;
+1 cm in position for split precision (FP32 for geopotential degrees n > 8).
+"""
+import json
+
+import numpy as np
+import pytest
+
+from conftest import golden_names
+from oracle import oracle as O
+from parahpop_b200 import api, synthetic as S
+
+pytestmark = pytest.mark.gpu
+
+POS_TOL_M = 1e-3
+VEL_TOL_M_S = 1e-6
+SPLIT_POS_TOL_M = 1e-2
+
+
+def errors(states, ref):
+    dpos = np.linalg.norm(states[:, :3] - ref[:, :3], axis=1) * 1e3
+    dvel = np.linalg.norm(states[:, 3:] - ref[:, 3:], axis=1) * 1e3
+    return dpos.max(), dvel.max()
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_matches_reference(golden, name):
+    case = golden(name)
+    p = api.Propagator(case.config_path)
+    ep, st = p.propagate_targets(case.targets)
+    dpos, dvel = errors(st, case.ref_states)
+    assert dpos <= POS_TOL_M and dvel <= VEL_TOL_M_S, (dpos, dvel)
+    assert np.abs(ep - case.ref_epochs).max() * 86400.0 <= 1e-4
+    p.close()
+
+
+@pytest.mark.parametrize("lanes", [1, 2, 4, 8, 16])
+@pytest.mark.parametrize("name", ["full_1h", "batch_33"])
+def test_every_lane_split_matches(golden, name, lanes):
+    case = golden(name)
+    p = api.Propagator(case.config_path, lanes=lanes)
+    ep, st = p.propagate_targets(case.targets)
+    assert p.stats()["lanes"] == lanes
+    dpos, dvel = errors(st, case.ref_states)
+    assert dpos <= POS_TOL_M and dvel <= VEL_TOL_M_S, (dpos, dvel)
+
+
+@pytest.mark.parametrize("name", ["full_1h", "deg120_1h"])
+def test_split_precision_within_1cm(golden, name):
+    case = golden(name)
+    p = api.Propagator(case.config_path, split=True)
+    ep, st = p.propagate_targets(case.targets)
+    assert p.stats()["split"] == 1
+    dpos, _ = errors(st, case.ref_states)
+    assert dpos <= SPLIT_POS_TOL_M, dpos
+
+
+def test_mixed_population_matches_oracle(tmp_path):
+    """Per-object epochs, durations and steps in one persistent launch."""
+    d = S.write_environment(tmp_path)
+    pop = S.population_mixed(40, seed=31)
+    pop.duration = np.minimum(pop.duration, 6 * 3600.0)
+    cfg = S.make_config(d, 3600.0, 60.0, max_steps=10 ** 6)
+    (d / "config.json").write_text(json.dumps(cfg))
+    tg = pop.targets_json()
+    p = api.Propagator(d / "config.json")
+    ep, st = p.propagate_targets(tg)
+    assert p.stats()["shared_grid"] == 0
+    env = O.load_environment(d / "config.json")
+    _, oep, ost = O.propagate(env, tg)
+    dpos, dvel = errors(st, ost)
+    assert dpos <= POS_TOL_M and dvel <= VEL_TOL_M_S, (dpos, dvel)
+    np.testing.assert_allclose(ep, oep, rtol=0, atol=1e-4 / 86400.0)
+
+
+def test_command_line_end_to_end(golden):
+    case = golden("full_600s")
+    out = case.dir / "cli_out"
+    r = api.run_cli(case.config_path, case.targets_path, out)
+    assert r.returncode == 0, r.stderr
+    lines = (out / "final_states.csv").read_text().splitlines()
+    assert lines[0] == "id,epoch_mjd2000_tdb,x_km,y_km,z_km,vx_km_s,vy_km_s,vz_km_s"
+    _, ep, st = O.read_final_states(out)
+    dpos, dvel = errors(st, case.ref_states)
+    assert dpos <= POS_TOL_M and dvel <= VEL_TOL_M_S
+    summary = json.loads((out / "summary.json").read_text())
+    assert summary["backend"] == "device" and summary["validation_passed"] is True
+    assert set(summary) == {"backend", "targets", "integrator", "initial_step_seconds", "duration_seconds",
+                            "environment_seconds", "propagation_seconds", "max_end_epoch_error_seconds",
+                            "validation_passed"}
+    resolved = json.loads((out / "configuration_resolved.json").read_text())
+    assert "run" not in resolved and resolved["execution"]["on"] == "device"
+    # refuses to overwrite
+    r2 = api.run_cli(case.config_path, case.targets_path, out)
+    assert r2.returncode == 1 and "Output exists" in r2.stderr
+
+
+def test_insufficient_max_steps_is_an_error(golden):
+    case = golden("full_600s")
+    cfg = json.loads(case.config_path.read_text())
+    cfg["execution"]["integration"]["maxNumSteps"] = 5
+    p2 = case.dir / "c_short.json"
+    p2.write_text(json.dumps(cfg))
+    r = api.run_cli(p2, case.targets_path, case.dir / "o_short")
+    assert r.returncode == 1
+    assert "A target stopped without reaching the requested end of simulation." in r.stderr
+
+
+def test_device_resident_path_equals_host_path(golden):
+    case = golden("full_600s")
+    import torch
+    p = api.Propagator(case.config_path)
+    t = case.targets["targets"]
+    st0 = np.array([x["state_km_km_s"] for x in t])
+    g = lambda k: np.array([x[k] for x in t])
+    ep_h, st_h = p.propagate(g("epoch_mjd2000_tdb"), st0, g("mass_kg"), g("drag_area_m2"), g("srp_area_m2"),
+                             g("cd"), g("cr"))
+    dev = torch.from_numpy(np.ascontiguousarray(st0.T).reshape(-1).copy()).cuda()
+    ep_d = p.propagate_device(dev.data_ptr(), len(t), float(t[0]["epoch_mjd2000_tdb"]), g("mass_kg"),
+                              g("drag_area_m2"), g("srp_area_m2"), g("cd"), g("cr"), p.duration, p.step)
+    st_d = dev.cpu().numpy().reshape(6, -1).T
+    np.testing.assert_array_equal(st_d, st_h)
+    assert ep_d == ep_h[0]
+
+
+def test_central_invariants(golden):
+    case = golden("central_1d")
+    p = api.Propagator(case.config_path)
+    _, st = p.propagate_targets(case.targets)
+    s0 = np.array([t["state_km_km_s"] for t in case.targets["targets"]])
+    mu = 398600.4415
+    e0 = 0.5 * (s0[:, 3:] ** 2).sum(1) - mu / np.linalg.norm(s0[:, :3], axis=1)
+    e1 = 0.5 * (st[:, 3:] ** 2).sum(1) - mu / np.linalg.norm(st[:, :3], axis=1)
+    h0 = np.linalg.norm(np.cross(s0[:, :3], s0[:, 3:]), axis=1)
+    h1 = np.linalg.norm(np.cross(st[:, :3], st[:, 3:]), axis=1)
+    assert np.abs((e1 - e0) / e0).max() < 1e-9
+    assert np.abs((h1 - h0) / h0).max() < 1e-9
+
+
+def test_benchmark_size_properties(tmp_path):
+    """10^4 objects (the benchmark batch) over 30 min: a seeded sample agrees
+    with the oracle, repeated runs are bit-identical, and split precision stays
+    within 1 cm of FP64 for every object."""
+    d = S.write_environment(tmp_path)
+    cfg = S.make_config(d, 1800.0, 60.0, max_steps=10 ** 6)
+    (d / "config.json").write_text(json.dumps(cfg))
+    pop = S.population_leo(10000, 1)
+    args = (pop.epochs, pop.states, pop.mass, pop.drag_area, pop.srp_area, pop.cd, pop.cr)
+    p = api.Propagator(d / "config.json")
+    ep1, st1 = p.propagate(*args)
+    ep2, st2 = p.propagate(*args)
+    np.testing.assert_array_equal(st1, st2)
+    ps = api.Propagator(d / "config.json", split=True)
+    _, st3 = ps.propagate(*args)
+    assert np.linalg.norm(st3[:, :3] - st1[:, :3], axis=1).max() * 1e3 <= SPLIT_POS_TOL_M
+    sample = np.random.default_rng(5).choice(10000, 24, replace=False)
+    sub = pop.subset(sample)
+    env = O.load_environment(d / "config.json")
+    _, _, ost = O.propagate(env, sub.targets_json())
+    dpos, dvel = errors(st1[sample], ost)
+    assert dpos <= POS_TOL_M and dvel <= VEL_TOL_M_S, (dpos, dvel)
