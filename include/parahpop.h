@@ -76,6 +76,24 @@ int phop_propagate_device(phop_context* ctx, int64_t n, double* d_states_soa, do
                           const double* cd, const double* cr, double duration_s, double step_s,
                           double* out_epoch_mjd2000_tdb);
 
+/* Allocation-free form of phop_propagate_device, for callers that cannot
+ * call cudaMalloc while they propagate (inside a stream capture that must not
+ * allocate, under a fixed memory budget, or as a plug-in in a process whose
+ * allocator it does not own).  No counterpart in the reference.  Scratch
+ * comes from one 4 MiB device array built into the library, held on every
+ * GPU that loads it until the process exits; the call allocates nothing.
+ * The caller passes device arrays: d_states_soa (6*n doubles, updated in
+ * place), d_bc = cd * area / mass and d_ams = cr_eff * area / mass (area in
+ * km^2, cr_eff = cr * srp_area / drag_area, n doubles each).  Limits: at most
+ * 256 fixed steps per call and a coefficient tile of at most 512 KiB
+ * (degree/order 120 in FP64); larger requests fail with an error.  All calls
+ * share the array, so calls whose GPU work overlaps race on it: order them.
+ * The first call on a device resolves the array's address and should come
+ * before any stream capture. */
+int phop_propagate_device_noalloc(phop_context* ctx, int64_t n, double* d_states_soa, const double* d_bc,
+                                  const double* d_ams, double epoch_mjd2000_tdb, double duration_s, double step_s,
+                                  double* out_epoch_mjd2000_tdb);
+
 /* Execution options (no reference counterpart; the reference hard-codes its
  * launch shapes):
  *   "lanes"    lanes per object, 0 = autotuned, else 1, 2, 4, 8 or 16

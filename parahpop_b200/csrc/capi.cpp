@@ -261,6 +261,23 @@ int phop_propagate_device(phop_context* ctx, int64_t n, double* dState, double e
     }
 }
 
+int phop_propagate_device_noalloc(phop_context* ctx, int64_t n, double* dState, const double* dBc,
+                                  const double* dAms, double epoch, double duration, double step, double* outEpoch) {
+    if (!ctx) return 1;
+    try {
+        if (n <= 0) throw std::runtime_error("targets must be a nonempty array.");
+        if (!dState || !dBc || !dAms) throw std::runtime_error("device arrays must not be null");
+        if (!(duration > 0) || !std::isfinite(duration)) throw std::runtime_error("duration_seconds must be finite and positive.");
+        if (!(step > 0) || !std::isfinite(step)) throw std::runtime_error("initialStepSize must be finite and positive.");
+        ctx->engine->assertCoverage(epoch, epoch + duration / 86400.0);
+        ctx->engine->propagateNoAlloc(n, dState, dBc, dAms, epoch, duration, step, ctx->maxSteps, ctx->opt, outEpoch);
+        return 0;
+    } catch (const std::exception& e) {
+        ctx->error = e.what();
+        return 1;
+    }
+}
+
 int phop_last_stats(const phop_context* ctx, phop_stats* out) {
     if (!ctx || !out) return 1;
     out->kernel_ms = ctx->stats.kernelMs;

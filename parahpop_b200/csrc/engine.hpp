@@ -124,7 +124,18 @@ public:
     int smCount() const { return sms_; }
     int autoLanes(int64_t n) const;
 
+    // Allocation-free variant of propagateResident (noalloc.cu): scratch comes
+    // from a file-scope device array; dBc / dAms are device arrays.
+    void propagateNoAlloc(int64_t n, double* dState, const double* dBc, const double* dAms, double epochMjd,
+                          double duration, double step, int64_t maxSteps, const RunOptions& opt,
+                          double* outEpochMjd, cudaStream_t stream = 0);
+
     // internal
+    struct HostTile {
+        std::vector<unsigned char> bytes;
+        std::vector<int2> blocks;
+        int nblocks = 0;
+    };
     struct Tile {
         void* dTile = nullptr;
         int2* dBlocks = nullptr;
@@ -134,6 +145,7 @@ public:
 
 private:
     const Tile& tileFor(int lanes, bool split);
+    const HostTile& hostTileFor(int lanes, bool split);
     void uploadEnvironment();
     void* scratch(const std::string& name, size_t bytes);
     void runKernel(int64_t n, double* dState, const double* dBc, const double* dAms, bool shared, int nsteps,
@@ -149,6 +161,7 @@ private:
     std::vector<void*> owned_;
     std::map<std::string, std::pair<void*, size_t>> scratch_;
     std::map<int, Tile> tiles_;
+    std::map<int, HostTile> hostTiles_;
     LowTable* dLow_ = nullptr;
     double* dDiag_ = nullptr;
 };
