@@ -99,8 +99,57 @@ int phop_propagate_device_noalloc(phop_context* ctx, int64_t n, double* d_states
  *   "lanes"    lanes per object, 0 = autotuned, else 1, 2, 4, 8 or 16
  *   "split"    0 = plain FP64, 1 = split precision (FP32 for geopotential
  *              degrees n > 8, FP64 elsewhere)
- *   "threads"  threads per CTA (multiple of 32, <= 512) */
+ *   "threads"  threads per CTA (multiple of 32, <= 512)
+ *   "ctas_per_sm"  resident CTAs per SM, 0 = from occupancy
+ *   "ordered"  1 (default) = hand objects to warps in order of geocentric
+ *              radius, 0 = in input order; results are identical either way */
 int phop_set_option(phop_context* ctx, const char* key, double value);
+
+/* ---- serving loop (no counterpart in the reference, whose driver propagates
+ * one batch per process) ----------------------------------------------------
+ * A server keeps a device-resident pool of `capacity` object slots (132 bytes
+ * of HBM each: the admission budget) on the context's GPU.  Submitted
+ * requests queue until their objects fit the pool, then join the running
+ * batch: each phop_server_step() call admits what fits, launches the step
+ * kernel once over every unfinished object of every admitted request for as
+ * many fixed steps as fit `slice_ms`, and retires finished requests (their
+ * results wait for phop_server_take).  Requests carry per-object epochs,
+ * durations and steps; an object's results are bit-identical whichever other
+ * requests share its slices.  The server uses its context exclusively while
+ * it exists (no phop_propagate* calls on the same context meanwhile) and the
+ * context's options ("lanes", "split", "ordered") at creation; without an
+ * explicit "lanes" it uses 2.  Failures of a request (maxNumSteps exceeded)
+ * are reported by phop_server_take. */
+typedef struct phop_server phop_server;
+
+typedef struct {
+    int64_t queued, running;      /* requests waiting / admitted now */
+    int64_t done, failed;         /* requests finished / failed since creation */
+    int64_t active_objects;       /* unfinished objects in the pool */
+    int64_t launches;             /* kernels launched by the server */
+    int64_t rounds;               /* phop_server_step calls */
+    int64_t object_steps;         /* object-steps of finished requests */
+    double busy_ms;               /* step-kernel time, CUDA events */
+    int lanes;
+} phop_server_stats;
+
+int phop_server_create(phop_context* ctx, int64_t capacity, double slice_ms, phop_server** out);
+void phop_server_destroy(phop_server* server);
+const char* phop_server_last_error(const phop_server* server);
+/* Same arrays and checks as phop_propagate; returns a request id. */
+int phop_server_submit(phop_server* server, int64_t n, const double* epoch_mjd2000_tdb, const double* states,
+                       const double* mass_kg, const double* drag_area_m2, const double* srp_area_m2, const double* cd,
+                       const double* cr, const double* duration_s, const double* step_s, int64_t* request_id);
+/* One scheduling round; *finished = requests finished or failed in it. */
+int phop_server_step(phop_server* server, int64_t* finished);
+/* 0 queued, 1 running, 2 done, 3 failed */
+int phop_server_status(const phop_server* server, int64_t request_id, int* state);
+/* Results of a finished request (epochs n, states n x 6), its latency from
+ * submission to completion and its time in the queue, in ms; forgets the
+ * request.  Returns 1 with the request's error for a failed request. */
+int phop_server_take(phop_server* server, int64_t request_id, double* out_epoch_mjd2000_tdb, double* out_states,
+                     double* latency_ms, double* queue_ms);
+int phop_server_get_stats(const phop_server* server, phop_server_stats* out);
 
 typedef struct {
     double kernel_ms;        /* step kernel time of the last call, CUDA events */

@@ -53,8 +53,23 @@ def library() -> C.CDLL:
         lib.paraHPOP_run.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.c_char_p]
         lib.paraHPOP_setLogLevel.argtypes = [C.c_int]
         lib.phop_fma_peak.argtypes = [C.c_int, D, D]
+        lib.phop_server_create.argtypes = [C.c_void_p, C.c_int64, C.c_double, C.POINTER(C.c_void_p)]
+        lib.phop_server_destroy.argtypes = [C.c_void_p]
+        lib.phop_server_last_error.argtypes = [C.c_void_p]
+        lib.phop_server_last_error.restype = C.c_char_p
+        lib.phop_server_submit.argtypes = [C.c_void_p, C.c_int64] + [D] * 9 + [C.POINTER(C.c_int64)]
+        lib.phop_server_step.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+        lib.phop_server_status.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_int)]
+        lib.phop_server_take.argtypes = [C.c_void_p, C.c_int64, D, D, D, D]
+        lib.phop_server_get_stats.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
         _lib = lib
     return _lib
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("queued", C.c_int64), ("running", C.c_int64), ("done", C.c_int64), ("failed", C.c_int64),
+                ("active_objects", C.c_int64), ("launches", C.c_int64), ("rounds", C.c_int64),
+                ("object_steps", C.c_int64), ("busy_ms", C.c_double), ("lanes", C.c_int)]
 
 
 def _dp(a):
@@ -145,6 +160,95 @@ class Propagator:
         s = PhopStats()
         library().phop_last_stats(self._h, C.byref(s))
         return {k: getattr(s, k) for k, _ in PhopStats._fields_}
+
+
+class Server:
+    """Serving loop over one Propagator (``phop_server_*``): queued requests
+    are admitted into a device-resident pool of ``capacity`` objects and
+    advanced together in slices of about ``slice_ms``."""
+
+    QUEUED, RUNNING, DONE, FAILED = 0, 1, 2, 3
+
+    def __init__(self, propagator: Propagator, capacity: int, slice_ms: float = 20.0):
+        h = C.c_void_p()
+        if library().phop_server_create(propagator._h, int(capacity), float(slice_ms), C.byref(h)) != 0:
+            raise PhopError(library().phop_last_error(propagator._h).decode())
+        self._h = h
+        self._prop = propagator
+        self._sizes = {}
+
+    def _err(self):
+        return PhopError(library().phop_server_last_error(self._h).decode())
+
+    def submit(self, epochs, states, mass, drag_area, srp_area, cd, cr, duration=None, step=None) -> int:
+        n = len(epochs)
+        f = lambda a: np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+        ep, st, ma, ad, asr, cdd, crr = map(f, (epochs, states, mass, drag_area, srp_area, cd, cr))
+        st = st.reshape(n, 6)
+        dur = None if duration is None else f(np.broadcast_to(duration, (n,)))
+        stp = None if step is None else f(np.broadcast_to(step, (n,)))
+        rid = C.c_int64()
+        rc = library().phop_server_submit(self._h, n, _dp(ep), _dp(st), _dp(ma), _dp(ad), _dp(asr), _dp(cdd),
+                                          _dp(crr), _dp(dur) if dur is not None else None,
+                                          _dp(stp) if stp is not None else None, C.byref(rid))
+        if rc != 0:
+            raise self._err()
+        self._sizes[rid.value] = n
+        return rid.value
+
+    def submit_targets(self, targets: dict) -> int:
+        t = targets["targets"]
+        g = lambda k: np.array([x[k] for x in t], dtype=np.float64)
+        dur = np.array([x.get("duration_seconds", self._prop.duration) for x in t])
+        step = np.array([x.get("step_seconds", self._prop.step) for x in t])
+        return self.submit(g("epoch_mjd2000_tdb"), np.array([x["state_km_km_s"] for x in t]), g("mass_kg"),
+                           g("drag_area_m2"), g("srp_area_m2"), g("cd"), g("cr"), dur, step)
+
+    def step(self) -> int:
+        f = C.c_int64()
+        if library().phop_server_step(self._h, C.byref(f)) != 0:
+            raise self._err()
+        return f.value
+
+    def status(self, rid: int) -> int:
+        s = C.c_int()
+        if library().phop_server_status(self._h, rid, C.byref(s)) != 0:
+            raise self._err()
+        return s.value
+
+    def take(self, rid: int):
+        """(final_epochs, final_states, latency_ms, queue_ms) of a finished request."""
+        n = self._sizes.pop(rid)
+        ep = np.zeros(n)
+        st = np.zeros((n, 6))
+        lat, q = C.c_double(), C.c_double()
+        if library().phop_server_take(self._h, rid, _dp(ep), _dp(st), C.byref(lat), C.byref(q)) != 0:
+            raise self._err()
+        return ep, st, lat.value, q.value
+
+    def run_until_idle(self, max_rounds: int = 10 ** 7):
+        for _ in range(max_rounds):
+            self.step()
+            s = self.stats()
+            if s["queued"] == 0 and s["running"] == 0:
+                return
+        raise PhopError("server did not become idle")
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        library().phop_server_get_stats(self._h, C.byref(s))
+        return {k: getattr(s, k) for k, _ in ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            library().phop_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def fma_peak(device: int = 0) -> tuple[float, float]:

@@ -19,6 +19,7 @@
 
 #include "../../include/parahpop.h"
 #include "engine.hpp"
+#include "server.hpp"
 
 namespace fs = std::filesystem;
 using phop::Value;
@@ -179,6 +180,8 @@ int phop_set_option(phop_context* ctx, const char* key, double value) {
         ctx->opt.threads = t;
     } else if (k == "ctas_per_sm") {
         ctx->opt.ctasPerSm = (int)value;
+    } else if (k == "ordered") {
+        ctx->opt.ordered = value != 0.0;
     } else {
         ctx->error = "Unknown option: " + k;
         return 1;
@@ -186,41 +189,60 @@ int phop_set_option(phop_context* ctx, const char* key, double value) {
     return 0;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Target arrays in the reference's target schema, checked as the driver
+// checks them (driver.cpp:97-129).
+phop::TargetSet makeTargets(const phop_context* ctx, int64_t n, const double* epoch, const double* states,
+                            const double* mass, const double* dragArea, const double* srpArea, const double* cd,
+                            const double* cr, const double* duration, const double* step) {
+    if (n <= 0) throw std::runtime_error("targets must be a nonempty array.");
+    if (!epoch || !states || !mass || !dragArea || !srpArea || !cd || !cr)
+        throw std::runtime_error("target arrays must not be null");
+    phop::TargetSet t;
+    t.ids.resize(n);
+    t.epoch.assign(epoch, epoch + n);
+    t.state.assign(states, states + 6 * n);
+    t.mass.assign(mass, mass + n);
+    t.dragArea.assign(dragArea, dragArea + n);
+    t.srpArea.assign(srpArea, srpArea + n);
+    t.cd.assign(cd, cd + n);
+    t.cr.assign(cr, cr + n);
+    t.duration = duration ? std::vector<double>(duration, duration + n) : std::vector<double>(n, ctx->duration);
+    t.step = step ? std::vector<double>(step, step + n) : std::vector<double>(n, ctx->step);
+    for (int64_t i = 0; i < n; ++i) {
+        for (int k = 0; k < 6; ++k)
+            if (!std::isfinite(t.state[6 * i + k])) throw std::runtime_error("State contains a nonfinite value.");
+        if (!std::isfinite(t.epoch[i]) || !std::isfinite(t.mass[i]) || !std::isfinite(t.dragArea[i])
+            || !std::isfinite(t.srpArea[i]) || !std::isfinite(t.cd[i]) || !std::isfinite(t.cr[i])
+            || t.mass[i] <= 0 || t.dragArea[i] <= 0 || t.srpArea[i] < 0 || t.cd[i] < 0 || t.cr[i] < 0)
+            throw std::runtime_error("Invalid target epoch or physical parameter.");
+        if (!(t.duration[i] > 0) || !std::isfinite(t.duration[i]))
+            throw std::runtime_error("duration_seconds must be finite and positive.");
+        if (!(t.step[i] > 0) || !std::isfinite(t.step[i]))
+            throw std::runtime_error("initialStepSize must be finite and positive.");
+    }
+    double lo = INFINITY, hi = -INFINITY;
+    for (int64_t i = 0; i < n; ++i) {
+        lo = std::min(lo, t.epoch[i]);
+        hi = std::max(hi, t.epoch[i] + t.duration[i] / 86400.0);
+    }
+    ctx->engine->assertCoverage(lo, hi);
+    return t;
+}
+
+}  // namespace
+
+extern "C" {
+
 int phop_propagate(phop_context* ctx, int64_t n, const double* epoch, const double* states, const double* mass,
                    const double* dragArea, const double* srpArea, const double* cd, const double* cr,
                    const double* duration, const double* step, double* outEpoch, double* outStates) {
     if (!ctx) return 1;
     try {
-        if (n <= 0) throw std::runtime_error("targets must be a nonempty array.");
-        phop::TargetSet t;
-        t.ids.resize(n);
-        t.epoch.assign(epoch, epoch + n);
-        t.state.assign(states, states + 6 * n);
-        t.mass.assign(mass, mass + n);
-        t.dragArea.assign(dragArea, dragArea + n);
-        t.srpArea.assign(srpArea, srpArea + n);
-        t.cd.assign(cd, cd + n);
-        t.cr.assign(cr, cr + n);
-        t.duration = duration ? std::vector<double>(duration, duration + n) : std::vector<double>(n, ctx->duration);
-        t.step = step ? std::vector<double>(step, step + n) : std::vector<double>(n, ctx->step);
-        for (int64_t i = 0; i < n; ++i) {
-            for (int k = 0; k < 6; ++k)
-                if (!std::isfinite(t.state[6 * i + k])) throw std::runtime_error("State contains a nonfinite value.");
-            if (!std::isfinite(t.epoch[i]) || !std::isfinite(t.mass[i]) || !std::isfinite(t.dragArea[i])
-                || !std::isfinite(t.srpArea[i]) || !std::isfinite(t.cd[i]) || !std::isfinite(t.cr[i])
-                || t.mass[i] <= 0 || t.dragArea[i] <= 0 || t.srpArea[i] < 0 || t.cd[i] < 0 || t.cr[i] < 0)
-                throw std::runtime_error("Invalid target epoch or physical parameter.");
-            if (!(t.duration[i] > 0) || !std::isfinite(t.duration[i]))
-                throw std::runtime_error("duration_seconds must be finite and positive.");
-            if (!(t.step[i] > 0) || !std::isfinite(t.step[i]))
-                throw std::runtime_error("initialStepSize must be finite and positive.");
-        }
-        double lo = INFINITY, hi = -INFINITY;
-        for (int64_t i = 0; i < n; ++i) {
-            lo = std::min(lo, t.epoch[i]);
-            hi = std::max(hi, t.epoch[i] + t.duration[i] / 86400.0);
-        }
-        ctx->engine->assertCoverage(lo, hi);
+        const phop::TargetSet t = makeTargets(ctx, n, epoch, states, mass, dragArea, srpArea, cd, cr, duration, step);
         std::vector<double> oe, os;
         ctx->stats = phop::RunStats{};
         ctx->engine->propagate(t, ctx->maxSteps, ctx->opt, oe, os, &ctx->stats);
@@ -276,6 +298,102 @@ int phop_propagate_device_noalloc(phop_context* ctx, int64_t n, double* dState, 
         ctx->error = e.what();
         return 1;
     }
+}
+
+// ---- serving loop ----------------------------------------------------------------------------------
+}  // extern "C"
+
+struct phop_server {
+    phop_context* ctx = nullptr;
+    std::unique_ptr<phop::Server> server;
+    std::string error;
+};
+
+extern "C" {
+
+int phop_server_create(phop_context* ctx, int64_t capacity, double sliceMs, phop_server** out) {
+    if (!ctx || !out) return 1;
+    try {
+        *out = nullptr;
+        auto s = std::make_unique<phop_server>();
+        s->ctx = ctx;
+        s->server = std::make_unique<phop::Server>(*ctx->engine, ctx->opt, capacity, sliceMs, ctx->maxSteps);
+        *out = s.release();
+        return 0;
+    } catch (const std::exception& e) {
+        ctx->error = e.what();
+        return 1;
+    }
+}
+
+void phop_server_destroy(phop_server* s) { delete s; }
+
+const char* phop_server_last_error(const phop_server* s) { return s ? s->error.c_str() : ""; }
+
+int phop_server_submit(phop_server* s, int64_t n, const double* epoch, const double* states, const double* mass,
+                       const double* dragArea, const double* srpArea, const double* cd, const double* cr,
+                       const double* duration, const double* step, int64_t* requestId) {
+    if (!s) return 1;
+    try {
+        const phop::TargetSet t = makeTargets(s->ctx, n, epoch, states, mass, dragArea, srpArea, cd, cr, duration, step);
+        const int64_t id = s->server->submit(t);
+        if (requestId) *requestId = id;
+        return 0;
+    } catch (const std::exception& e) {
+        s->error = e.what();
+        return 1;
+    }
+}
+
+int phop_server_step(phop_server* s, int64_t* finished) {
+    if (!s) return 1;
+    try {
+        const int f = s->server->step();
+        if (finished) *finished = f;
+        return 0;
+    } catch (const std::exception& e) {
+        s->error = e.what();
+        return 1;
+    }
+}
+
+int phop_server_status(const phop_server* s, int64_t requestId, int* state) {
+    if (!s || !state) return 1;
+    try {
+        *state = (int)s->server->status(requestId);
+        return 0;
+    } catch (const std::exception& e) {
+        const_cast<phop_server*>(s)->error = e.what();
+        return 1;
+    }
+}
+
+int phop_server_take(phop_server* s, int64_t requestId, double* outEpoch, double* outStates, double* latencyMs,
+                     double* queueMs) {
+    if (!s) return 1;
+    try {
+        s->server->take(requestId, outEpoch, outStates, latencyMs, queueMs);
+        return 0;
+    } catch (const std::exception& e) {
+        s->error = e.what();
+        return 1;
+    }
+}
+
+int phop_server_get_stats(const phop_server* s, phop_server_stats* out) {
+    if (!s || !out) return 1;
+    const phop::Server::Stats st = s->server->stats();
+    out->queued = st.queued;
+    out->running = st.running;
+    out->done = st.done;
+    out->failed = st.failed;
+    out->active_objects = st.activeObjects;
+    out->launches = st.launches;
+    out->rounds = st.rounds;
+    out->object_steps = st.objectSteps;
+    out->busy_ms = st.busyMs;
+    out->lanes = st.lanes;
+    return 0;
 }
 
 int phop_last_stats(const phop_context* ctx, phop_stats* out) {

@@ -8,6 +8,8 @@
 #include <sstream>
 #include <stdexcept>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "engine.hpp"
 
 namespace phop {
@@ -683,25 +685,68 @@ void Engine::assertCoverage(double loMjd, double hiMjd) const {
         throw std::runtime_error("Earth orientation coverage is insufficient for the requested epochs.");
 }
 
-void Engine::runKernel(int64_t n, double* dState, const double* dBc, const double* dAms, bool shared, int nsteps,
-                       const std::vector<double>& t0, const std::vector<double>& dt, double* dCur, double* dEnd,
-                       double* dDt, double* dStep, int* dUnfinished, const int64_t* dOrder, int64_t maxSteps,
-                       const RunOptions& opt, RunStats* stats, cudaStream_t stream) {
-    const int L = opt.lanes > 0 ? opt.lanes : autoLanes(n);
+// ---- scheduling ---------------------------------------------------------------------------------
+// Objects whose altitudes are close take the same branches through the
+// NRLMSISE-00 model (lower / upper thermosphere, cut-off), so the work queue
+// hands them out in order of geocentric radius: warps stay converged and the
+// results do not depend on the order (objects never interact).
+__global__ void radiusKeysKernel(const double* __restrict__ state, int64_t stride, const int64_t* __restrict__ slots,
+                                 int64_t n, uint32_t* __restrict__ keys, int64_t* __restrict__ idx) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t o = slots ? slots[i] : i;
+    const double x = state[o], y = state[stride + o], z = state[2 * stride + o];
+    const float r2 = (float)(x * x + y * y + z * z);
+    keys[i] = isfinite(r2) ? __float_as_uint(r2) : 0xffffffffu;  // non-negative floats order as integers
+    idx[i] = o;
+}
+
+const int64_t* Engine::orderByRadius(int64_t n, const double* dState, cudaStream_t stream, int64_t* launches,
+                                     int64_t stride, const int64_t* slots) {
+    if (n > INT32_MAX) throw std::runtime_error("too many objects for one batch");
+    uint32_t* keys = (uint32_t*)scratch("orderKeys", (size_t)n * 4);
+    uint32_t* keysOut = (uint32_t*)scratch("orderKeysOut", (size_t)n * 4);
+    int64_t* idx = (int64_t*)scratch("orderIdx", (size_t)n * 8);
+    int64_t* order = (int64_t*)scratch("order", (size_t)n * 8);
+    radiusKeysKernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(dState, stride ? stride : n, slots, n, keys, idx);
+    PHOP_CUDA(cudaGetLastError());
+    size_t temp = 0;
+    PHOP_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, keys, keysOut, idx, order, (int)n, 0, 32, stream));
+    void* dTemp = scratch("orderTemp", temp);
+    PHOP_CUDA(cub::DeviceRadixSort::SortPairs(dTemp, temp, keys, keysOut, idx, order, (int)n, 0, 32, stream));
+    if (launches) *launches += 1 + 6;  // key kernel + CUB histogram, scan and four one-sweep passes (32-bit keys)
+    return order;
+}
+
+// Epoch records at TDB seconds k * 30 for every k whose 4-point stencil an
+// epoch in [lo, hi] can reach, for the per-object time path.
+void Engine::buildRecordGrid(double lo, double hi, TimeGrid& g, cudaStream_t stream, int64_t* launches) {
+    const double H = kRecordGridSeconds;
+    const int64_t kLo = (int64_t)std::floor(lo / H) - 1;
+    const int64_t kHi = (int64_t)std::ceil(hi / H) + 2;
+    const int64_t G = kHi - kLo + 1;
+    if (G > (int64_t)1 << 26) throw std::runtime_error("the batch spans too long a time interval");
+    std::vector<double> ts(G);
+    for (int64_t k = 0; k < G; ++k) ts[k] = (double)(kLo + k) * H;
+    double* dT = (double*)scratch("gridT", (size_t)G * 8);
+    EpochRecord* dRec = (EpochRecord*)scratch("gridRecords", (size_t)G * sizeof(EpochRecord));
+    PHOP_CUDA(cudaMemcpyAsync(dT, ts.data(), (size_t)G * 8, cudaMemcpyHostToDevice, stream));
+    launchEpochRecords(denv_, dT, (int)G, dRec, stream);
+    PHOP_CUDA(cudaGetLastError());
+    if (launches) *launches += 1;
+    g.grid = dRec;
+    g.gridH = H;
+    g.gridBase = kLo;
+    g.gridN = (int)G;
+}
+
+Engine::LaunchShape Engine::launchStep(StepParams p, int L, const RunOptions& opt, bool shared, cudaStream_t stream) {
     if (L != 1 && L != 2 && L != 4 && L != 8 && L != 16) throw std::runtime_error("lanes must be 1, 2, 4, 8 or 16");
     const Tile& tile = tileFor(L, opt.split);
-    StepParams p{};
-    p.env = denv_;
-    p.n = n;
-    p.state = dState;
-    p.bc = dBc;
-    p.ams = dAms;
     p.tile = tile.dTile;
     p.tileBytes = tile.bytes;
     p.blocks = tile.dBlocks;
     p.nblocks = tile.nblocks;
-    p.low = dLow_;
-    p.diagC = dDiag_;
     // shared memory per CTA: the coefficient tile (when it fits) plus the
     // stage derivatives, 13 x ceil(6/L) doubles per thread
     const int threadsReq = opt.threads > 0 ? opt.threads : 512;
@@ -714,34 +759,133 @@ void Engine::runKernel(int64_t n, double* dState, const double* dBc, const doubl
         p.useSmemTile = 0;
         threads = std::min(threadsReq, (maxSmem_ - 1024) / kPerThread / 32 * 32);
     }
+    PHOP_CUDA(cudaMemsetAsync(p.workCounter, 0, 2 * sizeof(int), stream));
+    int perSm = opt.ctasPerSm > 0 ? opt.ctasPerSm
+                                  : propagateMaxCtasPerSm(L, opt.split, shared, threads, propagateSmemBytes(p, L, threads));
+    if (perSm <= 0) perSm = 1;
+    // one warp per group of 32 / L objects; when every group fits one wave,
+    // spread the warps evenly over all SMs instead of filling CTAs first
+    const int64_t warpsNeeded = (p.n + (32 / L) - 1) / (32 / L);
+    const int64_t slots = (int64_t)sms_ * perSm;
+    if (warpsNeeded <= slots * (threads / 32)) {
+        const int64_t warpsPerCta = (warpsNeeded + slots - 1) / slots;
+        threads = (int)std::min<int64_t>(threads, std::max<int64_t>(1, warpsPerCta) * 32);
+    }
+    const int64_t warpsPerCta = threads / 32;
+    const int64_t need = (warpsNeeded + warpsPerCta - 1) / warpsPerCta;
+    LaunchShape shape;
+    shape.lanes = L;
+    shape.threads = threads;
+    shape.ctas = (int)std::max<int64_t>(1, std::min<int64_t>(slots, need));
+    shape.smemTile = p.useSmemTile != 0;
+    PHOP_CUDA(launchPropagate(p, L, opt.split, shared, shape.ctas, threads, stream));
+    return shape;
+}
+
+// Project autotuner for the lane split.  The first batch of each class
+// (log2 of the batch size, time-grid mode, precision) times a two-step probe
+// of every lane count on scratch copies of the inputs and keeps the fastest;
+// later batches of the class reuse the choice.
+int Engine::tunedLanes(const StepParams& base, const RunOptions& opt, bool shared, cudaStream_t stream,
+                       int64_t* launches) {
+    int bucket = 0;
+    while (bucket < 40 && (int64_t(1) << bucket) < base.n) ++bucket;
+    const int key = bucket * 4 + (shared ? 2 : 0) + (opt.split ? 1 : 0);
+    auto it = tuned_.find(key);
+    if (it != tuned_.end()) return it->second;
+    if (base.stride != 0 && base.stride != base.n) return autoLanes(base.n);  // pools pin their lane count
+    const int64_t n = base.n;
+    StepParams p = base;
+    double* st = (double*)scratch("probeState", (size_t)6 * n * 8);
+    p.state = st;
+    if (shared) {
+        p.nsteps = std::min(p.nsteps, 2);
+    } else {
+        p.maxSteps = 2;
+        p.cur = (double*)scratch("probeCur", (size_t)n * 8);
+        p.dt = (double*)scratch("probeDt", (size_t)n * 8);
+        p.unfinished = (int*)scratch("probeUnf", (size_t)n * 4);
+    }
+    cudaEvent_t e0, e1;
+    PHOP_CUDA(cudaEventCreate(&e0));
+    PHOP_CUDA(cudaEventCreate(&e1));
+    int best = autoLanes(n);
+    float bestMs = 1e30f;
+    for (int L : {1, 2, 4, 8, 16}) {
+        if (L >= 8 && n >= (int64_t)sms_ * 512 * 4) continue;  // enough objects to fill the GPU with narrow groups
+        // an untimed launch first (module loading, attribute set-up), then the timed probe
+        float ms = 0.f;
+        for (int rep = 0; rep < 2; ++rep) {
+            PHOP_CUDA(cudaMemcpyAsync(st, base.state, (size_t)6 * n * 8, cudaMemcpyDeviceToDevice, stream));
+            if (!shared) {
+                PHOP_CUDA(cudaMemcpyAsync(p.cur, base.cur, (size_t)n * 8, cudaMemcpyDeviceToDevice, stream));
+                PHOP_CUDA(cudaMemcpyAsync(p.dt, base.dt, (size_t)n * 8, cudaMemcpyDeviceToDevice, stream));
+            }
+            PHOP_CUDA(cudaEventRecord(e0, stream));
+            launchStep(p, L, opt, shared, stream);
+            PHOP_CUDA(cudaEventRecord(e1, stream));
+            PHOP_CUDA(cudaEventSynchronize(e1));
+            if (launches) ++*launches;
+            PHOP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        }
+        int err = 0;
+        PHOP_CUDA(cudaMemcpy(&err, p.errorFlag, sizeof(int), cudaMemcpyDeviceToHost));
+        if (err) throw std::runtime_error("Propagation kernel reported error " + std::to_string(err) + ".");
+        if (ms < bestMs) {
+            bestMs = ms;
+            best = L;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    tuned_[key] = best;
+    return best;
+}
+
+void Engine::runKernel(int64_t n, double* dState, const double* dBc, const double* dAms, const TimeGrid& g,
+                       const int64_t* dOrder, int64_t maxSteps, const RunOptions& opt, RunStats* stats,
+                       cudaStream_t stream, int64_t launchesBefore) {
+    StepParams p{};
+    p.env = denv_;
+    p.n = n;
+    p.state = dState;
+    p.bc = dBc;
+    p.ams = dAms;
+    p.low = dLow_;
+    p.diagC = dDiag_;
     p.maxSteps = maxSteps;
     p.order = dOrder;
-    p.cur = dCur;
-    p.end = dEnd;
-    p.dt = dDt;
-    p.step = dStep;
-    p.unfinished = dUnfinished;
-    EpochRecord* dRec = nullptr;
+    p.cur = g.cur;
+    p.end = g.end;
+    p.dt = g.dt1;
+    p.step = g.step;
+    p.unfinished = g.unfinished;
+    p.grid = g.grid;
+    p.gridH = g.gridH;
+    p.gridBase = g.gridBase;
+    p.gridN = g.gridN;
+    p.stride = g.stride;
+    const bool shared = g.shared;
     cudaEvent_t e0, e1, e2;
     PHOP_CUDA(cudaEventCreate(&e0));
     PHOP_CUDA(cudaEventCreate(&e1));
     PHOP_CUDA(cudaEventCreate(&e2));
-    int64_t launches = 0;
+    int64_t launches = launchesBefore;
     PHOP_CUDA(cudaEventRecord(e0, stream));
     if (shared) {
+        const int nsteps = (int)g.t0.size();
         std::vector<double> stageT((size_t)nsteps * 13);
+        static const double c[12] = {2. / 27, 1. / 9, 1. / 6, 5. / 12, 1. / 2, 5. / 6, 1. / 6, 2. / 3, 1. / 3, 1.0, 0, 1.0};
         for (int k = 0; k < nsteps; ++k)
-            for (int s = 0; s < 13; ++s) {
-                static const double c[12] = {2. / 27, 1. / 9, 1. / 6, 5. / 12, 1. / 2, 5. / 6, 1. / 6, 2. / 3, 1. / 3, 1.0, 0, 1.0};
-                stageT[(size_t)k * 13 + s] = s == 0 ? t0[k] : std::fma(dt[k], c[s - 1], t0[k]);
-            }
+            for (int s = 0; s < 13; ++s)
+                stageT[(size_t)k * 13 + s] = s == 0 ? g.t0[k] : std::fma(g.dt[k], c[s - 1], g.t0[k]);
         double* dStage = (double*)scratch("stageT", stageT.size() * sizeof(double));
-        dRec = (EpochRecord*)scratch("records", stageT.size() * sizeof(EpochRecord));
+        EpochRecord* dRec = (EpochRecord*)scratch("records", stageT.size() * sizeof(EpochRecord));
         double* dT0 = (double*)scratch("t0", (size_t)nsteps * sizeof(double));
         double* dDtv = (double*)scratch("dt", (size_t)nsteps * sizeof(double));
         PHOP_CUDA(cudaMemcpyAsync(dStage, stageT.data(), stageT.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
-        PHOP_CUDA(cudaMemcpyAsync(dT0, t0.data(), t0.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
-        PHOP_CUDA(cudaMemcpyAsync(dDtv, dt.data(), dt.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+        PHOP_CUDA(cudaMemcpyAsync(dT0, g.t0.data(), (size_t)nsteps * sizeof(double), cudaMemcpyHostToDevice, stream));
+        PHOP_CUDA(cudaMemcpyAsync(dDtv, g.dt.data(), (size_t)nsteps * sizeof(double), cudaMemcpyHostToDevice, stream));
         launchEpochRecords(denv_, dStage, (int)stageT.size(), dRec, stream);
         PHOP_CUDA(cudaGetLastError());
         ++launches;
@@ -751,18 +895,12 @@ void Engine::runKernel(int64_t n, double* dState, const double* dBc, const doubl
         p.records = dRec;
     }
     int* dCtl = (int*)scratch("ctl", 2 * sizeof(int));
-    PHOP_CUDA(cudaMemsetAsync(dCtl, 0, 2 * sizeof(int), stream));
     p.workCounter = dCtl;
     p.errorFlag = dCtl + 1;
+    PHOP_CUDA(cudaMemsetAsync(dCtl, 0, 2 * sizeof(int), stream));
+    const int L = opt.lanes > 0 ? opt.lanes : tunedLanes(p, opt, shared, stream, &launches);
     PHOP_CUDA(cudaEventRecord(e1, stream));
-    const int smem = propagateSmemBytes(p, L, threads);
-    int perSm = opt.ctasPerSm > 0 ? opt.ctasPerSm : propagateMaxCtasPerSm(L, opt.split, shared, threads, smem);
-    if (perSm <= 0) perSm = 1;
-    const int64_t groups = (n + (32 / L) - 1) / (32 / L);
-    const int64_t warpsPerCta = threads / 32;
-    const int64_t need = (groups + warpsPerCta - 1) / warpsPerCta;
-    const int ctas = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms_ * perSm, need));
-    PHOP_CUDA(launchPropagate(p, L, opt.split, shared, ctas, threads, stream));
+    const LaunchShape shape = launchStep(p, L, opt, shared, stream);
     ++launches;
     PHOP_CUDA(cudaEventRecord(e2, stream));
     PHOP_CUDA(cudaEventSynchronize(e2));
@@ -776,12 +914,12 @@ void Engine::runKernel(int64_t n, double* dState, const double* dBc, const doubl
         stats->recordsMs += a;
         stats->kernelMs += b;
         stats->launches += launches;
-        stats->lanes = L;
-        stats->ctas = ctas;
-        stats->threads = threads;
+        stats->lanes = shape.lanes;
+        stats->ctas = shape.ctas;
+        stats->threads = shape.threads;
         stats->split = opt.split;
         stats->sharedGrid = shared;
-        stats->tileInSmem = p.useSmemTile != 0;
+        stats->tileInSmem = shape.smemTile;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -847,10 +985,15 @@ void Engine::propagate(const TargetSet& t, int64_t maxSteps, const RunOptions& o
         double finalEt = 0.0;
         if (!buildGrid(t.epoch[0], t.duration[0], t.step[0], maxSteps, t0, dt, finalEt))
             throw std::runtime_error("A target stopped without reaching the requested end of simulation.");
-        runKernel(n, dState, dBc, dAms, true, (int)t0.size(), t0, dt, nullptr, nullptr, nullptr, nullptr, nullptr,
-                  nullptr, maxSteps, opt, st, stream);
+        TimeGrid g;
+        g.shared = true;
+        g.t0 = std::move(t0);
+        g.dt = std::move(dt);
+        int64_t launches = 0;
+        const int64_t* dOrder = opt.ordered ? orderByRadius(n, dState, stream, &launches) : nullptr;
+        runKernel(n, dState, dBc, dAms, g, dOrder, maxSteps, opt, st, stream, launches);
         std::fill(outEpoch.begin(), outEpoch.end(), etToMjdHost(finalEt));
-        st->objectSteps += n * (int64_t)t0.size();
+        st->objectSteps += n * (int64_t)g.t0.size();
     } else {
         std::vector<double> cur(n), end(n), dtv(n), stp(n);
         std::vector<int64_t> cost(n), order(n);
@@ -865,8 +1008,25 @@ void Engine::propagate(const TargetSet& t, int64_t maxSteps, const RunOptions& o
             cost[i] = (int64_t)std::ceil(span / t.step[i]);
             st->objectSteps += cost[i];
         }
+        // longest objects first (in buckets of 2^(1/16) in step count), then
+        // by geocentric radius inside a bucket
+        std::vector<int> bucket(n);
+        std::vector<float> radius(n);
+        for (int64_t i = 0; i < n; ++i) {
+            bucket[i] = (int)std::floor(16.0 * std::log2((double)std::max<int64_t>(cost[i], 1)));
+            const double* x = &t.state[(size_t)6 * i];
+            radius[i] = (float)(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+        }
         std::iota(order.begin(), order.end(), 0);
-        std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cost[a] > cost[b]; });
+        std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
+            if (bucket[a] != bucket[b]) return bucket[a] > bucket[b];
+            return opt.ordered && radius[a] < radius[b];
+        });
+        double lo = cur[0], hi = end[0];
+        for (int64_t i = 1; i < n; ++i) {
+            lo = std::min(lo, cur[i]);
+            hi = std::max(hi, end[i]);
+        }
         double* dCur = (double*)scratch("cur", (size_t)n * 8);
         double* dEnd = (double*)scratch("end", (size_t)n * 8);
         double* dDt = (double*)scratch("dtv", (size_t)n * 8);
@@ -878,8 +1038,16 @@ void Engine::propagate(const TargetSet& t, int64_t maxSteps, const RunOptions& o
         PHOP_CUDA(cudaMemcpyAsync(dDt, dtv.data(), n * 8, cudaMemcpyHostToDevice, stream));
         PHOP_CUDA(cudaMemcpyAsync(dStep, stp.data(), n * 8, cudaMemcpyHostToDevice, stream));
         PHOP_CUDA(cudaMemcpyAsync(dOrder, order.data(), n * 8, cudaMemcpyHostToDevice, stream));
-        runKernel(n, dState, dBc, dAms, false, 0, {}, {}, dCur, dEnd, dDt, dStep, dUnf, dOrder, maxSteps, opt, st,
-                  stream);
+        TimeGrid g;
+        g.shared = false;
+        g.cur = dCur;
+        g.end = dEnd;
+        g.dt1 = dDt;
+        g.step = dStep;
+        g.unfinished = dUnf;
+        int64_t launches = 0;
+        buildRecordGrid(lo, hi, g, stream, &launches);
+        runKernel(n, dState, dBc, dAms, g, dOrder, maxSteps, opt, st, stream, launches);
         std::vector<int> unf(n);
         PHOP_CUDA(cudaMemcpy(cur.data(), dCur, n * 8, cudaMemcpyDeviceToHost));
         PHOP_CUDA(cudaMemcpy(unf.data(), dUnf, n * 4, cudaMemcpyDeviceToHost));
@@ -918,9 +1086,15 @@ void Engine::propagateResident(int64_t n, double* dState, const double* epochMjd
     PHOP_CUDA(cudaMemcpyAsync(dAms, ams, (size_t)n * 8, cudaMemcpyHostToDevice, stream));
     RunStats local;
     RunStats* st = stats ? stats : &local;
-    runKernel(n, dState, dBc, dAms, true, (int)t0.size(), t0, dt, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
-              maxSteps, opt, st, stream);
-    st->objectSteps += n * (int64_t)t0.size();
+    const int64_t nsteps = (int64_t)t0.size();
+    TimeGrid g;
+    g.shared = true;
+    g.t0 = std::move(t0);
+    g.dt = std::move(dt);
+    int64_t launches = 0;
+    const int64_t* dOrder = opt.ordered ? orderByRadius(n, dState, stream, &launches) : nullptr;
+    runKernel(n, dState, dBc, dAms, g, dOrder, maxSteps, opt, st, stream, launches);
+    st->objectSteps += n * nsteps;
     outEpochMjd.assign(n, etToMjdHost(finalEt));
 }
 

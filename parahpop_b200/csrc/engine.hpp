@@ -16,6 +16,9 @@
 
 namespace phop {
 
+// spacing of the epoch-record grid of mixed batches (TDB seconds)
+constexpr double kRecordGridSeconds = 30.0;
+
 struct EphUnitHost {
     int target, center, nint, pdeg;
     double startEpoch, finalEpoch;
@@ -94,6 +97,7 @@ struct RunOptions {
     int threads = 512;
     bool split = false;
     int ctasPerSm = 0; // 0: occupancy
+    bool ordered = true;  // process objects in order of geocentric radius
 };
 
 class Engine {
@@ -143,15 +147,42 @@ public:
         int nblocks = 0;
     };
 
+    // Launch geometry of one step-kernel launch.
+    struct LaunchShape {
+        int lanes = 0, threads = 0, ctas = 0;
+        bool smemTile = false;
+    };
+    // Per-batch time description handed to the step kernel.
+    struct TimeGrid {
+        bool shared = false;
+        // shared grid: per-step start epochs and sizes
+        std::vector<double> t0, dt;
+        // per-object time (device arrays) and the batch's record grid
+        double *cur = nullptr, *end = nullptr, *dt1 = nullptr, *step = nullptr;
+        int* unfinished = nullptr;
+        const EpochRecord* grid = nullptr;
+        double gridH = 0.0;
+        int64_t gridBase = 0;
+        int gridN = 0;
+        int64_t stride = 0;  // SoA stride of the state (0: n)
+    };
+
 private:
+    friend class Server;
     const Tile& tileFor(int lanes, bool split);
     const HostTile& hostTileFor(int lanes, bool split);
     void uploadEnvironment();
     void* scratch(const std::string& name, size_t bytes);
-    void runKernel(int64_t n, double* dState, const double* dBc, const double* dAms, bool shared, int nsteps,
-                   const std::vector<double>& t0, const std::vector<double>& dt, double* dCur, double* dEnd,
-                   double* dDt, double* dStep, int* dUnfinished, const int64_t* dOrder, int64_t maxSteps,
-                   const RunOptions& opt, RunStats* stats, cudaStream_t stream);
+    // device order of objects by increasing geocentric radius (SoA state of
+    // stride `stride`); `slots` (nullable) lists the objects to order
+    const int64_t* orderByRadius(int64_t n, const double* dState, cudaStream_t stream, int64_t* launches,
+                                 int64_t stride = 0, const int64_t* slots = nullptr);
+    void buildRecordGrid(double lo, double hi, TimeGrid& g, cudaStream_t stream, int64_t* launches);
+    LaunchShape launchStep(StepParams p, int lanes, const RunOptions& opt, bool shared, cudaStream_t stream);
+    int tunedLanes(const StepParams& base, const RunOptions& opt, bool shared, cudaStream_t stream, int64_t* launches);
+    void runKernel(int64_t n, double* dState, const double* dBc, const double* dAms, const TimeGrid& g,
+                   const int64_t* dOrder, int64_t maxSteps, const RunOptions& opt, RunStats* stats,
+                   cudaStream_t stream, int64_t launchesBefore);
 
     HostEnvironment host_;
     int device_ = 0;
@@ -164,6 +195,7 @@ private:
     std::map<int, HostTile> hostTiles_;
     LowTable* dLow_ = nullptr;
     double* dDiag_ = nullptr;
+    std::map<int, int> tuned_;  // autotuned lane count per batch class
 };
 
 }  // namespace phop

@@ -1,14 +1,15 @@
 // Fused batched RKF78 propagation kernels for sm_100a.
 //
 // One persistent kernel advances object groups through all their fixed steps:
-// the 13 RKF78 stages, the full force model and the 8th-order update run in
-// registers, so the per-step HBM traffic is the state read at the start and
-// written at the end of the whole propagation.
+// the 13 RKF78 stages, the full force model and the 8th-order update run on
+// chip (registers and shared memory), so the only per-object HBM traffic is the
+// state read at the start and written at the end of the whole propagation.
 //
 // Work split (autotuned):  L lanes (1, 2, 4, 8 or 16) cooperate on one object,
 // a warp holds 32/L objects.
 //   * RK state: lane j of a group owns the state components d with d % L == j,
-//     keeps y_d and the 13 stage derivatives k_s[d] in registers, forms the
+//     keeps y_d in registers and the 13 stage derivatives k_s[d] in shared
+//     memory ([stage][component][thread], conflict-free), forms the
 //     stage state for its components in the reference's order
 //     (parm/integrate/rk/host/Step.h:33-84) and the 8th-order update in stage
 //     order (Step.h:86-104), and broadcasts components by warp shuffle.
@@ -33,8 +34,11 @@
 //
 // Time grid: batches whose objects share epoch, step and duration read the
 // per-step start / step size and the per-stage EpochRecord from tables made
-// before the launch; mixed batches keep per-object time and evaluate the
-// epoch record inline, mirroring FixedStep.h:30-37 per object.
+// before the launch; mixed batches keep per-object time (FixedStep.h:30-37
+// per object) and form each stage's record by 4-point Lagrange interpolation
+// in an epoch-record grid of at most 30 s spacing that spans the batch, with
+// the NRLMSISE-00 time inputs (seconds of day, sidereal time, weather slot)
+// evaluated exactly at the stage epoch.
 #pragma once
 #include <stdint.h>
 
@@ -84,6 +88,15 @@ struct StepParams {
     int64_t maxSteps;
     int* unfinished;        // per object: 1 if it did not reach its end
     const int64_t* order;   // processing order of objects (nullable)
+    // epoch-record grid of a mixed batch (nullable): grid[k] holds the record
+    // at TDB seconds (gridBase + k) * gridH, k < gridN.  The grid is anchored
+    // at multiples of gridH, so an object's interpolated records do not depend
+    // on which other objects share its batch.
+    const EpochRecord* grid;
+    double gridH;
+    int64_t gridBase;
+    int gridN;
+    int64_t stride;  // SoA stride of `state` (0: n); object pools use their capacity
     // geopotential
     const void* tile;       // tile entries in global memory
     int tileBytes;          // multiple of 16

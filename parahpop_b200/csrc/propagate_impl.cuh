@@ -1,6 +1,7 @@
 // Kernel bodies shared by the per-precision translation units.
 #pragma once
 #include <cuda_runtime.h>
+#include <stddef.h>
 #include <stdint.h>
 
 #include "nrlmsise00.cuh"
@@ -437,6 +438,57 @@ static __device__ __noinline__ void epochRecordOutOfLine(const DevEnv& env, doub
     evalEpochRecord(env, et, r);
 }
 
+// Stage record of a mixed batch: 4-point Lagrange interpolation in the
+// batch's record grid (rotation, angular velocity, body positions, tide
+// deltas; a 30 s spacing keeps the interpolation error of the rotation below
+// 1e-12 relative), with the NRLMSISE-00 time inputs evaluated exactly.
+static __device__ __noinline__ void epochRecordFromGrid(const StepParams& p, double et, EpochRecord& r) {
+    // stencil k0 - 1 .. k0 + 2 around the absolute grid index k0 = floor(et / H);
+    // q depends on et alone, so the weights are the same in every batch
+    const double u = et / p.gridH;
+    const double kf = floor(u);
+    int64_t i0 = (int64_t)kf - 1 - p.gridBase;
+    i0 = i0 < 0 ? 0 : (i0 > p.gridN - 4 ? p.gridN - 4 : i0);
+    const double q = u - kf + 1.0;
+    double w[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        double num = 1.0, den = 1.0;
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+            if (m != j) {
+                num *= q - (double)m;
+                den *= (double)(j - m);
+            }
+        w[j] = num / den;
+    }
+    const EpochRecord* g = p.grid + i0;
+    auto interp = [&](const double* f0, size_t off) {
+        const double* b = f0 + off;
+        constexpr size_t stride = sizeof(EpochRecord) / sizeof(double);
+        return w[0] * b[0] + w[1] * b[stride] + w[2] * b[2 * stride] + w[3] * b[3 * stride];
+    };
+    const double* f0 = (const double*)g;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) r.R[i] = interp(f0, offsetof(EpochRecord, R) / 8 + i);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) r.w[i] = interp(f0, offsetof(EpochRecord, w) / 8 + i);
+    for (int b = 0; b < p.env.nbodies; ++b)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) r.body[b][i] = interp(f0, offsetof(EpochRecord, body) / 8 + 3 * b + i);
+    r.tideValid = g[0].tideValid & g[1].tideValid & g[2].tideValid & g[3].tideValid;
+    if (p.env.solid || p.env.ocean) {
+        for (int k = 0; k < kTideTri; ++k) {
+            r.dC[k] = interp(f0, offsetof(EpochRecord, dC) / 8 + k);
+            r.dS[k] = interp(f0, offsetof(EpochRecord, dS) / 8 + k);
+        }
+    } else {
+        for (int k = 0; k < kTideTri; ++k) r.dC[k] = r.dS[k] = 0.0;
+    }
+    if (p.env.hasNrl) nrlEpoch(p.env, et, r);
+    else r.nrlValid = 0;
+}
+
 template <int L, typename T, bool SHARED_GRID>
 __global__ void __launch_bounds__(512, 1) propagateKernel(const __grid_constant__ StepParams p) {
     using Tile = typename TileOf<T>::type;
@@ -464,11 +516,12 @@ __global__ void __launch_bounds__(512, 1) propagateKernel(const __grid_constant_
         const bool valid = slot < p.n;
         const int64_t sidx = valid ? slot : p.n - 1;
         const int64_t oi = p.order ? p.order[sidx] : sidx;
+        const int64_t stride = p.stride ? p.stride : p.n;
         double y[CPL];
 #pragma unroll
         for (int c = 0; c < CPL; ++c) {
             const int d = j + c * L;
-            y[c] = d < 6 ? p.state[(int64_t)d * p.n + oi] : 0.0;
+            y[c] = d < 6 ? p.state[(int64_t)d * stride + oi] : 0.0;
         }
         const double bc = p.bc[oi], ams = p.ams[oi];
         double cur = 0.0, dtv = 0.0, endv = 0.0, stepv = 0.0;
@@ -503,7 +556,8 @@ __global__ void __launch_bounds__(512, 1) propagateKernel(const __grid_constant_
                 } else {
                     EpochRecord rec;
                     const double ts = s == 0 ? t0 : t0 + dt * rkC(s - 1);
-                    epochRecordOutOfLine(p.env, ts, rec);
+                    if (p.grid) epochRecordFromGrid(p, ts, rec);
+                    else epochRecordOutOfLine(p.env, ts, rec);
                     accelerations<L, T>(p, tile, rec, st, st + 3, bc, ams, acc);
                 }
 #pragma unroll
@@ -525,7 +579,7 @@ __global__ void __launch_bounds__(512, 1) propagateKernel(const __grid_constant_
 #pragma unroll
             for (int c = 0; c < CPL; ++c) {
                 const int d = j + c * L;
-                if (d < 6) p.state[(int64_t)d * p.n + oi] = y[c];
+                if (d < 6) p.state[(int64_t)d * stride + oi] = y[c];
             }
             if (!SHARED_GRID && j == 0) {
                 p.cur[oi] = cur;
