@@ -102,7 +102,10 @@ int phop_propagate_device_noalloc(phop_context* ctx, int64_t n, double* d_states
  *   "threads"  threads per CTA (multiple of 32, <= 512)
  *   "ctas_per_sm"  resident CTAs per SM, 0 = from occupancy
  *   "ordered"  1 (default) = hand objects to warps in order of geocentric
- *              radius, 0 = in input order; results are identical either way */
+ *              radius, 0 = in input order; results are identical either way
+ *   "graph"    1 (default) = launch the step as a CUDA graph cached by its
+ *              launch parameters (replayed for repeated batches), 0 = plain
+ *              launches */
 int phop_set_option(phop_context* ctx, const char* key, double value);
 
 /* ---- serving loop (no counterpart in the reference, whose driver propagates

@@ -182,6 +182,8 @@ int phop_set_option(phop_context* ctx, const char* key, double value) {
         ctx->opt.ctasPerSm = (int)value;
     } else if (k == "ordered") {
         ctx->opt.ordered = value != 0.0;
+    } else if (k == "graph") {
+        ctx->opt.graph = value != 0.0;
     } else {
         ctx->error = "Unknown option: " + k;
         return 1;

@@ -98,6 +98,7 @@ struct RunOptions {
     bool split = false;
     int ctasPerSm = 0; // 0: occupancy
     bool ordered = true;  // process objects in order of geocentric radius
+    bool graph = true;    // launch the step as a cached CUDA graph
 };
 
 class Engine {
@@ -143,6 +144,7 @@ public:
     struct Tile {
         void* dTile = nullptr;
         int2* dBlocks = nullptr;
+        double2* dDiagStep = nullptr;
         int bytes = 0;
         int nblocks = 0;
     };
@@ -179,6 +181,17 @@ private:
                                  int64_t stride = 0, const int64_t* slots = nullptr);
     void buildRecordGrid(double lo, double hi, TimeGrid& g, cudaStream_t stream, int64_t* launches);
     LaunchShape launchStep(StepParams p, int lanes, const RunOptions& opt, bool shared, cudaStream_t stream);
+    LaunchShape prepareStep(StepParams& p, int lanes, const RunOptions& opt, bool shared);
+    void enqueueStep(const StepParams& p, const LaunchShape& shape, const RunOptions& opt, bool shared,
+                     cudaStream_t stream);
+    void launchStepGraph(const StepParams& p, const LaunchShape& shape, const RunOptions& opt, bool shared,
+                         cudaStream_t stream);
+    struct GraphEntry {
+        unsigned char params[sizeof(StepParams)];
+        int lanes = 0, threads = 0, ctas = 0, flags = 0;
+        cudaGraphExec_t exec = nullptr;
+    };
+    std::vector<GraphEntry> graphs_;
     int tunedLanes(const StepParams& base, const RunOptions& opt, bool shared, cudaStream_t stream, int64_t* launches);
     void runKernel(int64_t n, double* dState, const double* dBc, const double* dAms, const TimeGrid& g,
                    const int64_t* dOrder, int64_t maxSteps, const RunOptions& opt, RunStats* stats,
@@ -196,6 +209,7 @@ private:
     LowTable* dLow_ = nullptr;
     double* dDiag_ = nullptr;
     std::map<int, int> tuned_;  // autotuned lane count per batch class
+    std::map<int64_t, int> occupancy_;  // resident CTAs per SM by launch configuration
 };
 
 }  // namespace phop

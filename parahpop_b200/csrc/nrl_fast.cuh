@@ -52,9 +52,27 @@ struct NrlEpochBlock {
 
 #if defined(__CUDACC__)
 
+// Global-memory copies of the coefficient tables, read through L1 where the
+// lanes of a warp evaluate different tables at once (constant-bank reads
+// serialise on distinct addresses).
+#define PHOP_NRL_TABLE(name, count) static __device__ const double gdev_##name[count]
+#include "tables/nrlmsise00_coeffs.inc"
+#undef PHOP_NRL_TABLE
+
 // table order of the globe7 calls: pt, ps, pd[0..8]
 __host__ __device__ __forceinline__ const double* globeTable(int k) {
     return k == 0 ? NRLT(pt) : k == 1 ? NRLT(ps) : NRLT(pd) + 150 * (k - 2);
+}
+__device__ __forceinline__ const double* globeTableGlobal(int k) {
+    return k == 0 ? gdev_nrl_pt : k == 1 ? gdev_nrl_ps : gdev_nrl_pd + 150 * (k - 2);
+}
+
+// The globe7 evaluations of one gts7 call in task order: tinf (pt), g0 (ps),
+// tlb (pd[3]), then N2, He, O, O2, Ar, H, N and anomalous O (pd[2], pd[0],
+// pd[1], pd[4] .. pd[8]).
+constexpr int kGlobeTasks = 11;
+__host__ __device__ __forceinline__ int globeTaskTable(int t) {
+    return t == 0 ? 0 : t == 1 ? 1 : t == 2 ? 5 : t == 3 ? 4 : t == 4 ? 2 : t == 5 ? 3 : t;
 }
 __host__ __device__ __forceinline__ const double* globSTable(int k) {
     return k < 4 ? NRLT(ptl) + 100 * k : NRLT(pma) + 100 * (k - 4);
@@ -158,16 +176,22 @@ struct Fast {
         plg[3][4] = T(105.0) * s2 * s * c;
         plg[3][5] = (T(9.0) * c * plg[3][4] - T(7.) * plg[3][3]) / T(2.0);
         plg[3][6] = (T(11.0) * c * plg[3][5] - T(8.) * plg[3][4]) / T(3.0);
+        // multiples of the local-time and longitude angles by the double- and
+        // triple-angle identities (one sincos each)
         sincos(hr * lst, &stloc, &ctloc);
-        sincos(T(2.0) * hr * lst, &s2tloc, &c2tloc);
-        sincos(T(3.0) * hr * lst, &s3tloc, &c3tloc);
+        s2tloc = T(2.0) * stloc * ctloc;
+        c2tloc = (ctloc - stloc) * (ctloc + stloc);
+        s3tloc = stloc * (T(3.0) - T(4.0) * stloc * stloc);
+        c3tloc = ctloc * (T(4.0) * ctloc * ctloc - T(3.0));
         sincos(dgtr * gLong, &sgl, &cgl);
-        sincos(T(2.0) * dgtr * gLong, &s2gl, &c2gl);
+        s2gl = T(2.0) * sgl * cgl;
+        c2gl = (cgl - sgl) * (cgl + sgl);
     }
 
     // G(L), upper thermosphere; table k of the globe7 sequence
-    __device__ T globe7(int k) {
-        const double* p = globeTable(k);
+    __device__ __forceinline__ T globe7(int k) { return globe7At(k, globeTable(k)); }
+
+    __device__ __forceinline__ T globe7At(int k, const double* __restrict__ p) {
         const NrlGlobeEpoch& g = eb.ge[k];
         const T hr = T(0.2618), dgtr = T(1.74533E-2);
         const T dfa = T(eb.dfa);
@@ -333,19 +357,71 @@ struct Fast {
         return densu_temp * pow((t1 / *tz), (T(1.0) + alpha)) * exp(-expl);
     }
 
-    // thermosphere (alt >= 72.5 km): number densities d[0..8] (m^-3)
-    __device__ void gts7(T alt, T* d) {
+    // The 11 globe7 values of one gts7 call (task order above), with the ap
+    // response apt0 left by the pd[3] table (used by the mesosphere glob7s
+    // terms) and by the last table (used below 72.5 km).  L lanes of a group
+    // share the tables round-robin and exchange the values by shuffles; the
+    // tables are then read from global memory, since the lanes read
+    // different ones.
+    template <int L>
+    __device__ __forceinline__ void globeTasks(T (&G)[kGlobeTasks], T& aptTlb, T& aptLast, int j, int groupBase) {
+        if (L == 1) {
+#pragma unroll 1
+            for (int t = 0; t < kGlobeTasks; ++t) {
+                G[t] = globe7(globeTaskTable(t));
+                if (t == 2) aptTlb = apt0;
+            }
+            aptLast = apt0;
+            return;
+        }
+        // the group's lanes only: groups of a warp may leave the density
+        // evaluation at different points (altitude cut-off), a group never splits
+        const unsigned mask = ((1u << L) - 1u) << groupBase;
+        // apt0 after task t in the sequential order: the value set by the last
+        // table up to t whose ap term is present (p[51] != 0)
+        T aptSeq = apt0;
+#pragma unroll
+        for (int r = 0; r < (kGlobeTasks + L - 1) / L; ++r) {
+            const int t = r * L + j;
+            T v = T(0), a = T(0);
+            if (t < kGlobeTasks) {
+                const int k = globeTaskTable(t);
+                v = globe7At(k, globeTableGlobal(k));
+                a = apt0;
+            }
+#pragma unroll
+            for (int jj = 0; jj < L; ++jj) {
+                const int tt = r * L + jj;
+                if (tt < kGlobeTasks) {
+                    G[tt] = __shfl_sync(mask, v, groupBase + jj);
+                    const T at = __shfl_sync(mask, a, groupBase + jj);
+                    if (globeTable(globeTaskTable(tt))[51] != 0.0) aptSeq = at;
+                    if (tt == 2) aptTlb = aptSeq;
+                }
+            }
+        }
+        aptLast = aptSeq;
+    }
+
+    // thermosphere (alt >= 72.5 km): number densities d[0..8] (m^-3), from
+    // the globe7 values G (task order).  Above za the main density of each
+    // species, densu(z, dlb, tinf, tlb, xm, alpha) with dlb = pdm exp(g) pd,
+    // is formed as pdm pd exp(g + (1 + alpha + gamma) ln(tlb/tt) - s gamma zg2):
+    // the temperature profile tt and its logarithm are shared by the
+    // species, and one exponential replaces exp, pow and exp.
+    __device__ void gts7(T alt, const T (&G)[kGlobeTasks], T aptTlb, T* d) {
         T zn1[5] = {T(NRL_PDL(1)[15]), T(110.0), T(100.0), T(90.0), T(72.5)};
         const T za = zn1[0];
         for (int j = 0; j < 9; j++) d[j] = T(0);
         const T z = alt;
         T dummyT;
-        const T tinf = (z > za) ? T(NRL_PTM(0)) * T(NRL_PT[0]) * (T(1.0) + globe7(0)) : T(NRL_PTM(0)) * T(NRL_PT[0]);
-        const T g0v = (z > zn1[4]) ? T(NRL_PTM(3)) * T(NRL_PS[0]) * (T(1.0) + globe7(1)) : T(NRL_PTM(3)) * T(NRL_PS[0]);
-        const T tlb = T(NRL_PTM(1)) * (T(1.0) + globe7(5)) * T(NRL_PD(3)[0]);
+        const T tinf = (z > za) ? T(NRL_PTM(0)) * T(NRL_PT[0]) * (T(1.0) + G[0]) : T(NRL_PTM(0)) * T(NRL_PT[0]);
+        const T g0v = (z > zn1[4]) ? T(NRL_PTM(3)) * T(NRL_PS[0]) * (T(1.0) + G[1]) : T(NRL_PTM(3)) * T(NRL_PS[0]);
+        const T tlb = T(NRL_PTM(1)) * (T(1.0) + G[2]) * T(NRL_PD(3)[0]);
         const T s = g0v / (tinf - tlb);
         const T ptl30 = T(NRL_PTM(4)) * T(NRL_PTL(3)[0]);
         if (z < T(300.0)) {
+            apt0 = aptTlb;
             meso_tn1[1] = T(NRL_PTM(6)) * T(NRL_PTL(0)[0]) / (T(1.0) - glob7s(0));
             meso_tn1[2] = T(NRL_PTM(2)) * T(NRL_PTL(1)[0]) / (T(1.0) - glob7s(1));
             meso_tn1[3] = T(NRL_PTM(7)) * T(NRL_PTL(2)[0]) / (T(1.0) - glob7s(2));
@@ -361,24 +437,41 @@ struct Fast {
         }
         const T zlb = T(NRL_PTM(5));
         const T xmm = T(NRL_PDM(2, 4));
+        // shared temperature profile of the main species densities (densu, z >= za)
+        const T rgas = T(831.4);
+        const T zg2 = zeta(z >= za ? z : za, zlb);
+        const T tt = tinf - (tinf - tlb) * exp(-s * zg2);
+        const bool direct = z >= za && tt > T(0);
+        T lnX = T(0), kGamma = T(0);
+        if (direct) {
+            lnX = log(tlb / tt);
+            const T g1 = T(1.0) + zlb / re;
+            kGamma = (gsurf / (g1 * g1)) / (s * rgas * tinf);  // gamma = xm * kGamma
+        }
+        auto mainDensity = [&](T g, T pdm0, T pd0, T xm, T alpha) -> T {
+            if (direct) {
+                const T gamma = xm * kGamma;
+                return pdm0 * pd0 * exp(g + (T(1.0) + alpha + gamma) * lnX - s * gamma * zg2);
+            }
+            return densu(z, pdm0 * exp(g) * pd0, tinf, tlb, xm, alpha, &dummyT, zlb, s, zn1);
+        };
         // N2
-        const T g28 = globe7(4);
-        // sin(dgtr glat) = plg[0][1]; cos(dr (doy - pt[13])) is the pt table's cd14
         const T zhf = T(NRL_PDL(1)[24]) * (T(1.0) + T(NRL_PDL(0)[24]) * plg[0][1] * T(eb.ge[0].cd14));
-        const T db28 = T(NRL_PDM(2, 0)) * exp(g28) * T(NRL_PD(2)[0]);
-        d[2] = densu(z, db28, tinf, tlb, T(28.0), T(0.0), &dummyT, zlb, s, zn1);
+        d[2] = mainDensity(G[3], T(NRL_PDM(2, 0)), T(NRL_PD(2)[0]), T(28.0), T(0.0));
         const T zhm28 = T(NRL_PDM(2, 3)) * T(NRL_PDL(1)[5]);
         T b28 = T(0.0);
-        if (!(z > T(450.0) && z >= za))
+        if (!(z > T(450.0) && z >= za)) {
+            const T db28 = T(NRL_PDM(2, 0)) * exp(G[3]) * T(NRL_PD(2)[0]);
             b28 = densu(T(NRL_PDM(2, 2)) * zhf, db28, tinf, tlb, T(28.0) - xmm, T(-1.0), &dummyT, zlb, s, zn1);
+        }
         if (z <= T(160.0)) {
             dm28 = densu(z, b28, tinf, tlb, xmm, T(0.0), &dummyT, zlb, s, zn1);
             d[2] = nrl::Model<T>::dnet(d[2], dm28, zhm28, xmm, T(28.0));
         }
         // He
-        const T db04 = T(NRL_PDM(0, 0)) * exp(globe7(2)) * T(NRL_PD(0)[0]);
-        d[0] = densu(z, db04, tinf, tlb, T(4.), T(-0.38), &dummyT, zlb, s, zn1);
+        d[0] = mainDensity(G[4], T(NRL_PDM(0, 0)), T(NRL_PD(0)[0]), T(4.), T(-0.38));
         if (z < T(200.0)) {
+            const T db04 = T(NRL_PDM(0, 0)) * exp(G[4]) * T(NRL_PD(0)[0]);
             const T b04 = densu(T(NRL_PDM(0, 2)), db04, tinf, tlb, T(4.) - xmm, T(-1.38), &dummyT, zlb, s, zn1);
             const T dm04 = densu(z, b04, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1);
             d[0] = nrl::Model<T>::dnet(d[0], dm04, zhm28, xmm, T(4.));
@@ -386,9 +479,9 @@ struct Fast {
             d[0] = d[0] * nrl::Model<T>::ccor(z, rl, T(NRL_PDM(0, 5)) * T(NRL_PDL(1)[1]), T(NRL_PDM(0, 4)) * T(NRL_PDL(1)[0]));
         }
         // O
-        const T db16 = T(NRL_PDM(1, 0)) * exp(globe7(3)) * T(NRL_PD(1)[0]);
-        d[1] = densu(z, db16, tinf, tlb, T(16.), T(0.0), &dummyT, zlb, s, zn1);
+        d[1] = mainDensity(G[5], T(NRL_PDM(1, 0)), T(NRL_PD(1)[0]), T(16.), T(0.0));
         if (z <= T(300.0)) {
+            const T db16 = T(NRL_PDM(1, 0)) * exp(G[5]) * T(NRL_PD(1)[0]);
             const T b16 = densu(T(NRL_PDM(1, 2)), db16, tinf, tlb, T(16.0) - xmm, T(-1.0), &dummyT, zlb, s, zn1);
             const T dm16 = densu(z, b16, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1);
             d[1] = nrl::Model<T>::dnet(d[1], dm16, zhm28, xmm, T(16.));
@@ -399,9 +492,9 @@ struct Fast {
                                               T(NRL_PDM(1, 7)) * T(NRL_PDL(1)[13]), T(NRL_PDM(1, 6)) * T(NRL_PDL(1)[12]));
         }
         // O2
-        const T db32 = T(NRL_PDM(3, 0)) * exp(globe7(6)) * T(NRL_PD(4)[0]);
-        d[3] = densu(z, db32, tinf, tlb, T(32.), T(0.0), &dummyT, zlb, s, zn1);
+        d[3] = mainDensity(G[6], T(NRL_PDM(3, 0)), T(NRL_PD(4)[0]), T(32.), T(0.0));
         if (z <= T(250.0)) {
+            const T db32 = T(NRL_PDM(3, 0)) * exp(G[6]) * T(NRL_PD(4)[0]);
             const T b32 = densu(T(NRL_PDM(3, 2)), db32, tinf, tlb, T(32.) - xmm, T(-1.), &dummyT, zlb, s, zn1);
             const T dm32 = densu(z, b32, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1);
             d[3] = nrl::Model<T>::dnet(d[3], dm32, zhm28, xmm, T(32.));
@@ -414,9 +507,9 @@ struct Fast {
                                                T(NRL_PDM(3, 6)) * T(NRL_PDL(1)[21]), T(NRL_PDM(3, 7)) * T(NRL_PDL(0)[22]));
         }
         // Ar
-        const T db40 = T(NRL_PDM(4, 0)) * exp(globe7(7)) * T(NRL_PD(5)[0]);
-        d[4] = densu(z, db40, tinf, tlb, T(40.), T(0.17), &dummyT, zlb, s, zn1);
+        d[4] = mainDensity(G[7], T(NRL_PDM(4, 0)), T(NRL_PD(5)[0]), T(40.), T(0.17));
         if (z <= T(240.0)) {
+            const T db40 = T(NRL_PDM(4, 0)) * exp(G[7]) * T(NRL_PD(5)[0]);
             const T b40 = densu(T(NRL_PDM(4, 2)), db40, tinf, tlb, T(40.) - xmm, T(-0.83), &dummyT, zlb, s, zn1);
             const T dm40 = densu(z, b40, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1);
             d[4] = nrl::Model<T>::dnet(d[4], dm40, zhm28, xmm, T(40.));
@@ -424,9 +517,9 @@ struct Fast {
             d[4] = d[4] * nrl::Model<T>::ccor(z, rl, T(NRL_PDM(4, 5)) * T(NRL_PDL(1)[9]), T(NRL_PDM(4, 4)) * T(NRL_PDL(1)[8]));
         }
         // H
-        const T db01 = T(NRL_PDM(5, 0)) * exp(globe7(8)) * T(NRL_PD(6)[0]);
-        d[6] = densu(z, db01, tinf, tlb, T(1.), T(-0.38), &dummyT, zlb, s, zn1);
+        d[6] = mainDensity(G[8], T(NRL_PDM(5, 0)), T(NRL_PD(6)[0]), T(1.), T(-0.38));
         if (z <= T(320.0)) {
+            const T db01 = T(NRL_PDM(5, 0)) * exp(G[8]) * T(NRL_PD(6)[0]);
             const T b01 = densu(T(NRL_PDM(5, 2)), db01, tinf, tlb, T(1.) - xmm, T(-1.38), &dummyT, zlb, s, zn1);
             const T dm01 = densu(z, b01, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1);
             d[6] = nrl::Model<T>::dnet(d[6], dm01, zhm28, xmm, T(1.));
@@ -436,9 +529,9 @@ struct Fast {
                                               T(NRL_PDM(5, 7)) * T(NRL_PDL(1)[19]), T(NRL_PDM(5, 6)) * T(NRL_PDL(1)[18]));
         }
         // N
-        const T db14 = T(NRL_PDM(6, 0)) * exp(globe7(9)) * T(NRL_PD(7)[0]);
-        d[7] = densu(z, db14, tinf, tlb, T(14.), T(0.0), &dummyT, zlb, s, zn1);
+        d[7] = mainDensity(G[9], T(NRL_PDM(6, 0)), T(NRL_PD(7)[0]), T(14.), T(0.0));
         if (z <= T(450.0)) {
+            const T db14 = T(NRL_PDM(6, 0)) * exp(G[9]) * T(NRL_PD(7)[0]);
             const T b14 = densu(T(NRL_PDM(6, 2)), db14, tinf, tlb, T(14.) - xmm, T(-1.), &dummyT, zlb, s, zn1);
             const T dm14 = densu(z, b14, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1);
             d[7] = nrl::Model<T>::dnet(d[7], dm14, zhm28, xmm, T(14.));
@@ -447,10 +540,16 @@ struct Fast {
             d[7] = d[7] * nrl::Model<T>::ccor(z, T(NRL_PDM(6, 3)) * T(NRL_PDL(0)[5]),
                                               T(NRL_PDM(6, 7)) * T(NRL_PDL(0)[4]), T(NRL_PDM(6, 6)) * T(NRL_PDL(0)[3]));
         }
-        // anomalous O
-        const T db16h = T(NRL_PDM(7, 0)) * exp(globe7(10)) * T(NRL_PD(8)[0]);
+        // anomalous O: densu with tinf = tlb = tho, where ln(tlb/tt) = 0
         const T tho = T(NRL_PDM(7, 9)) * T(NRL_PDL(0)[6]);
-        const T dd = densu(z, db16h, tho, tho, T(16.), T(0.0), &dummyT, zlb, s, zn1);
+        T dd;
+        if (direct) {
+            const T g1 = T(1.0) + zlb / re;
+            const T gamma = T(16.0) * (gsurf / (g1 * g1)) / (s * rgas * tho);
+            dd = T(NRL_PDM(7, 0)) * T(NRL_PD(8)[0]) * exp(G[10] - s * gamma * zg2);
+        } else {
+            dd = densu(z, T(NRL_PDM(7, 0)) * exp(G[10]) * T(NRL_PD(8)[0]), tho, tho, T(16.), T(0.0), &dummyT, zlb, s, zn1);
+        }
         const T zsht = T(NRL_PDM(7, 5)), zmho = T(NRL_PDM(7, 4));
         const T gz = T(1.0) + zmho / re;
         const T zsho = T(831.4) * tho / ((gsurf / (gz * gz)) * T(16.0));
@@ -458,8 +557,10 @@ struct Fast {
         for (int i = 0; i < 9; i++) d[i] = d[i] * T(1.0E6);
     }
 
-    // gtd7 + gtd7d total mass density (kg/m^3)
-    __device__ T density(T lat, T lon, T alt, T lst) {
+    // gtd7 + gtd7d total mass density (kg/m^3); lane j of a group of L
+    // lanes starting at groupBase (all lanes of the group get the result)
+    template <int L>
+    __device__ T density(T lat, T lon, T alt, T lst, int j, int groupBase) {
         glat = lat;
         absLat = fabs(lat);
         gLong = lon;
@@ -472,10 +573,16 @@ struct Fast {
         gsurf = T(980.616) * (T(1.0) - T(0.0026373) * c2);
         re = T(2.0) * gsurf / (T(3.085462E-6) + T(2.27E-9) * c2) * T(1.0E-5);
         basis(lat, lst);
+        T G[kGlobeTasks];
+        T aptTlb = T(0), aptLast = T(0);
+        globeTasks<L>(G, aptTlb, aptLast, j, groupBase);
         T d[9];
         const T zn2top = T(72.5);
-        gts7(alt > zn2top ? alt : zn2top, d);
-        if (!(alt >= zn2top)) return lowerAtmosphere(alt, d);
+        gts7(alt > zn2top ? alt : zn2top, G, aptTlb, d);
+        if (!(alt >= zn2top)) {
+            apt0 = aptLast;
+            return lowerAtmosphere(alt, d);
+        }
         return (T(1.66E-24) * (T(4.0) * d[0] + T(16.0) * d[1] + T(28.0) * d[2] + T(32.0) * d[3] + T(40.0) * d[4]
                                + d[6] + T(14.0) * d[7] + T(16.0) * d[8]))
             / T(1000);

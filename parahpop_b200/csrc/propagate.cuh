@@ -104,6 +104,7 @@ struct StepParams {
     int nblocks;
     const LowTable* low;
     const double* diagC;    // c_m, m = 0..M
+    const double2* diagStep;  // per m: (c_{m+1}...c_{m+L}, same x (m+L)/m), nullable
     int useSmemTile;
     // scheduling and errors
     int* workCounter;

@@ -140,6 +140,26 @@ static __device__ __forceinline__ void shAccel(const StepParams& p, const typena
     };
     for (int t = 0; t < j; ++t)
         if (m < M) advance();
+    // block advance m -> m + L in one step where the per-L factor table is
+    // present: P_{m+L} = D_m cos^L P_m and dP_{m+L} = D'_m cos^L dP_m with
+    // D_m = c_{m+1} ... c_{m+L}, D'_m = D_m (m+L)/m (closed forms of the
+    // diagonal recurrences; m = 0 starts from dP_L = -L sin cos^{L-1} D_0), the
+    // phasor rotated by L lambda and alpha^m scaled by alpha^L.
+    const double2* __restrict__ diagStep = p.diagStep;
+    double cosL1 = 1.0, cLam = 1.0, sLam = 0.0, aL = 1.0;
+    if (L > 1 && diagStep) {
+#pragma unroll
+        for (int t = 0; t < L - 1; ++t) cosL1 *= cosPhi;
+#pragma unroll
+        for (int t = 0; t < L; ++t) {
+            const double ns = cosL * sLam + sinL * cLam;
+            const double nc = cosL * cLam - sinL * sLam;
+            sLam = ns;
+            cLam = nc;
+            aL *= alpha;
+        }
+    }
+    const double cosLp = cosL1 * cosPhi;
     const T u = T(alpha * sinPhi), v = T(alpha * cosPhi), a2 = T(alpha * alpha);
     double ar = 0.0, aphi = 0.0, alam = 0.0;
     const int nblocks = p.nblocks;
@@ -215,8 +235,26 @@ static __device__ __forceinline__ void shAccel(const StepParams& p, const typena
             aphi += cML * dc + sML * ds;
             alam -= ((double)mcol * invCos) * (sML * pc - cML * ps);
         }
-        for (int t = 0; t < L; ++t)
-            if (m < M) advance();
+        if (L > 1 && diagStep) {
+            if (m + L <= M) {
+                const double2 f = diagStep[m];
+                const double nP = f.x * cosLp * Pmm;
+                const double ndP = m == 0 ? -(double)L * sinPhi * cosL1 * f.x : f.y * cosLp * dPmm;
+                Pmm = nP;
+                dPmm = ndP;
+                const double ns = cLam * sML + sLam * cML;
+                const double nc = cLam * cML - sLam * sML;
+                sML = ns;
+                cML = nc;
+                am *= aL;
+                m += L;
+            } else {
+                m = M + 1;  // beyond the last order: the lane's later columns are inactive
+            }
+        } else {
+            for (int t = 0; t < L; ++t)
+                if (m < M) advance();
+        }
     }
 #pragma unroll
     for (int off = L / 2; off > 0; off >>= 1) {
@@ -269,6 +307,9 @@ static __device__ __forceinline__ double shadowFactor(const double rS[3], const 
     return 1.0 - (a2 * al + bb * be - c * yv) / (a2 * 3.14159265358979323846);
 }
 
+// NRLMSISE-00 density (kg/km^3) at ITRF position f; the L lanes of a group
+// share the globe7 tables of the model and all return the same value.
+template <int L>
 static __device__ __noinline__ double nrlDensity(const DevEnv& e, const EpochRecord& r, const double f[3]) {
     // geodetic latitude / longitude / altitude (Nrlmsise00.cu:243-266)
     const double rho2 = f[0] * f[0] + f[1] * f[1];
@@ -299,7 +340,8 @@ static __device__ __noinline__ double nrlDensity(const DevEnv& e, const EpochRec
     const double kRad = 57.2957795130823208768;
     nrlf::Fast<double> model(e.nrlBlocks[r.nrlBlock], r.nrlSec);
     const double lst = wrapHours(r.nrlGast + lon * kRad / 15.0);
-    const double rhoSi = model.density(lat * kRad, lon * kRad, alt, lst);
+    const int lane = (int)(threadIdx.x & 31);
+    const double rhoSi = model.template density<L>(lat * kRad, lon * kRad, alt, lst, lane % L, lane - lane % L);
     if (!isfinite(rhoSi) || rhoSi < 0.0) return NAN;
     return (rhoSi * 1.0e9) * e.nrlDensityScale;
 }
@@ -368,7 +410,7 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
             const double fx[3] = {R[0] * pos[0] + R[1] * pos[1] + R[2] * pos[2],
                                   R[3] * pos[0] + R[4] * pos[1] + R[5] * pos[2],
                                   R[6] * pos[0] + R[7] * pos[1] + R[8] * pos[2]};
-            const double rho = nrlDensity(e, r, fx);
+            const double rho = nrlDensity<L>(e, r, fx);
             const double* w = r.w;
             const double vr0 = vel[0] - (w[1] * pos[2] - w[2] * pos[1]);
             const double vr1 = vel[1] - (w[2] * pos[0] - w[0] * pos[2]);
