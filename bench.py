@@ -39,6 +39,18 @@ def sh_flops_per_object_step(degree: int) -> float:
     return 13.0 * SH_FLOP_PER_TERM * (degree + 1) * (degree + 2) / 2.0
 
 
+# DRAM bytes (read + write) of one step-kernel launch over 10^4 objects and 5
+# steps, from an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum);
+# a longer launch reads one more 864-byte epoch record per added stage.
+NCU_BYTES_5_STEPS_1E4 = 1_722_624 + 11_520
+RECORD_BYTES = 864
+
+
+def launch_traffic_bytes(objects: int, steps: int) -> float:
+    per_object = (NCU_BYTES_5_STEPS_1E4 - 13 * 5 * RECORD_BYTES) / 1e4
+    return per_object * objects + 13 * steps * RECORD_BYTES
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -302,7 +314,10 @@ def main():
                        "lanes": prop.stats()["lanes"], "l2": "flushed (256 MiB write) before every timed step",
                        "parallelism": f"object sharding x{ws}, no collective"},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak if peak > 0 else None, "traffic": None,
+                         "frac": achieved / peak if peak > 0 else None,
+                         "traffic": launch_traffic_bytes(n, int(round(span / step_s))),
+                         "traffic_note": "DRAM bytes per launch: ncu capture of a 5-step launch of the same "
+                                         "10^4 objects (1.733 MB read+write) plus 864 B per further stage record",
                          "peak_source": "measured FP64 FMA throughput (phop_fma_peak) on this GPU",
                          "numerator": "29 FLOP x (N+1)(N+2)/2 SH terms x 13 stages per object-step, N = 70"},
             "cpu_baseline": cpu,

@@ -112,7 +112,9 @@ int phop_set_option(phop_context* ctx, const char* key, double value);
  * one batch per process) ----------------------------------------------------
  * A server keeps a device-resident pool of `capacity` object slots (132 bytes
  * of HBM each: the admission budget) on the context's GPU.  Submitted
- * requests queue until their objects fit the pool, then join the running
+ * requests queue until their objects fit the pool and the running batch's
+ * compute budget (objects one step of the measured rate covers in
+ * `slice_ms`, at least 65,536; a larger request runs alone), then join the running
  * batch: each phop_server_step() call admits what fits, launches the step
  * kernel once over every unfinished object of every admitted request for as
  * many fixed steps as fit `slice_ms`, and retires finished requests (their

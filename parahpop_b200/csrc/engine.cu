@@ -450,6 +450,7 @@ Engine::~Engine() {
     for (void* p : owned_) cudaFree(p);
     for (auto& kv : scratch_) cudaFree(kv.second.first);
     for (GraphEntry& g : graphs_) cudaGraphExecDestroy(g.exec);
+    if (captureStream_) cudaStreamDestroy(captureStream_);
     for (auto& kv : tiles_) {
         cudaFree(kv.second.dTile);
         cudaFree(kv.second.dBlocks);
@@ -786,16 +787,19 @@ void Engine::launchStepGraph(const StepParams& p, const LaunchShape& shape, cons
         for (GraphEntry& g : graphs_) cudaGraphExecDestroy(g.exec);
         graphs_.clear();
     }
+    // captured on the engine's own stream (the legacy default stream cannot
+    // be captured); the instantiated graph is launched on the caller's stream
+    if (!captureStream_) PHOP_CUDA(cudaStreamCreateWithFlags(&captureStream_, cudaStreamNonBlocking));
     cudaGraph_t graph = nullptr;
-    PHOP_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed));
+    PHOP_CUDA(cudaStreamBeginCapture(captureStream_, cudaStreamCaptureModeRelaxed));
     try {
-        enqueueStep(p, shape, opt, shared, stream);
+        enqueueStep(p, shape, opt, shared, captureStream_);
     } catch (...) {
-        cudaStreamEndCapture(stream, &graph);
+        cudaStreamEndCapture(captureStream_, &graph);
         if (graph) cudaGraphDestroy(graph);
         throw;
     }
-    PHOP_CUDA(cudaStreamEndCapture(stream, &graph));
+    PHOP_CUDA(cudaStreamEndCapture(captureStream_, &graph));
     const cudaError_t ie = cudaGraphInstantiate(&key.exec, graph, 0);
     cudaGraphDestroy(graph);
     PHOP_CUDA(ie);
@@ -814,7 +818,7 @@ Engine::LaunchShape Engine::prepareStep(StepParams& p, int L, const RunOptions& 
     p.diagStep = tile.dDiagStep;
     // shared memory per CTA: the coefficient tile (when it fits) plus the
     // stage derivatives, 13 x ceil(6/L) doubles per thread
-    const int threadsReq = opt.threads > 0 ? opt.threads : 512;
+    const int threadsReq = std::min(opt.threads > 0 ? opt.threads : 512, maxStepThreads(L));
     const int kPerThread = 13 * ((6 + L - 1) / L) * 8;
     int threads = threadsReq;
     if (tile.bytes + 1024 + 64 * kPerThread <= maxSmem_) {

@@ -192,6 +192,7 @@ private:
         cudaGraphExec_t exec = nullptr;
     };
     std::vector<GraphEntry> graphs_;
+    cudaStream_t captureStream_ = nullptr;
     int tunedLanes(const StepParams& base, const RunOptions& opt, bool shared, cudaStream_t stream, int64_t* launches);
     void runKernel(int64_t n, double* dState, const double* dBc, const double* dAms, const TimeGrid& g,
                    const int64_t* dOrder, int64_t maxSteps, const RunOptions& opt, RunStats* stats,

@@ -229,7 +229,7 @@ void Engine::propagateNoAlloc(int64_t n, double* dState, const double* dBc, cons
     sp.diagC = dDiag_;
     sp.workCounter = ctl;
     sp.errorFlag = ctl + 1;
-    const int threadsReq = opt.threads > 0 ? opt.threads : 512;
+    const int threadsReq = std::min(opt.threads > 0 ? opt.threads : 512, maxStepThreads(L));
     const int kPerThread = 13 * ((6 + L - 1) / L) * 8;
     int threads;
     if ((int)ht.bytes.size() + 1024 + 64 * kPerThread <= maxSmem_) {

@@ -111,6 +111,11 @@ struct StepParams {
     int* errorFlag;
 };
 
+// Threads per CTA the step kernel is compiled for: narrow lane splits run one
+// CTA of few threads per SM (the coefficient tile fills shared memory), so
+// they get up to 255 registers per thread instead of spilling at 128.
+__host__ __device__ constexpr int maxStepThreads(int lanes) { return lanes == 1 ? 256 : lanes == 2 ? 320 : 512; }
+
 void launchEpochRecords(const DevEnv& env, const double* epochs, int count, EpochRecord* out, cudaStream_t stream);
 cudaError_t launchPropagate(const StepParams& p, int lanes, bool split, bool shared, int ctas, int threads,
                             cudaStream_t stream);

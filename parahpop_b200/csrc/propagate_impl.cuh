@@ -532,7 +532,7 @@ static __device__ __noinline__ void epochRecordFromGrid(const StepParams& p, dou
 }
 
 template <int L, typename T, bool SHARED_GRID>
-__global__ void __launch_bounds__(512, 1) propagateKernel(const __grid_constant__ StepParams p) {
+__global__ void __launch_bounds__(maxStepThreads(L), 1) propagateKernel(const __grid_constant__ StepParams p) {
     using Tile = typename TileOf<T>::type;
     constexpr int CPL = (6 + L - 1) / L;
     extern __shared__ __align__(128) unsigned char smem[];

@@ -20,6 +20,7 @@ double mjdToEtS(double mjd) { return std::fma(mjd, 86400.0, -43200.0); }
 double etToMjdS(double et) { return std::fma(et, 1.0 / 86400.0, 0.5); }
 constexpr int64_t kGridMarginPoints = 2880;   // 24 h of 30 s records built ahead
 constexpr int64_t kGridMaxPoints = int64_t(1) << 22;
+constexpr int64_t kMinActive = 65536;          // objects that keep every SM busy
 }  // namespace
 
 Server::Server(Engine& engine, const RunOptions& opt, int64_t capacity, double sliceMs, int64_t maxSteps)
@@ -213,11 +214,25 @@ int Server::step() {
     PHOP_SCUDA(cudaSetDevice(engine_.device()));
     ++stats_.rounds;
     // admission: first come first served, later requests may fill gaps the
-    // head of the queue does not fit
+    // head of the queue does not fit.  Two budgets: pool slots (HBM) and
+    // compute - the unfinished objects of the running batch are kept to what
+    // one step of the measured rate covers in a slice (at least kMinActive,
+    // so the GPU stays full), which bounds how long a newly admitted request
+    // shares each slice with the rest; a request above that limit is
+    // admitted when nothing else runs.
+    int64_t active = 0;
+    for (int64_t id : running_) {
+        const Request& r = requests_.at(id);
+        for (int64_t i = 0; i < (int64_t)r.t.size(); ++i) active += hostUnfinished_[r.off + i];
+    }
+    const int64_t computeLimit =
+        msPerObjectStep_ > 0 ? std::max<int64_t>(kMinActive, (int64_t)(sliceMs_ / msPerObjectStep_)) : capacity_;
     for (auto it = queue_.begin(); it != queue_.end();) {
         Request& r = requests_.at(*it);
+        const int64_t n = (int64_t)r.t.size();
         int64_t off = 0;
-        if (allocate((int64_t)r.t.size(), off)) {
+        if ((active + n <= computeLimit || active == 0) && allocate(n, off)) {
+            active += n;
             r.off = off;
             admit(r);
             running_.push_back(r.id);

@@ -2,7 +2,9 @@
 //
 // Requests (batches of objects with their own epochs, durations and steps)
 // are queued, admitted into a device-resident object pool while it has room
-// (the pool's capacity is the HBM admission budget, fixed at creation), and
+// (the pool's capacity is the HBM admission budget, fixed at creation) and
+// while the running batch is within the compute budget (the objects one step
+// of the measured rate covers in a slice, at least 65,536), and
 // advanced together: every scheduling round launches the per-object-time step
 // kernel once over all unfinished objects of all admitted requests, for as
 // many fixed steps as fit a target time slice.  Requests that finish are

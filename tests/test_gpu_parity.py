@@ -163,3 +163,18 @@ def test_benchmark_size_properties(tmp_path):
     _, _, ost = O.propagate(env, sub.targets_json())
     dpos, dvel = errors(st1[sample], ost)
     assert dpos <= POS_TOL_M and dvel <= VEL_TOL_M_S, (dpos, dvel)
+
+
+def test_graph_replay_equals_plain_launches(golden):
+    """The step launch is cached as a CUDA graph: a replayed graph, a fresh
+    capture and plain launches give bit-identical results."""
+    case = golden("full_600s")
+    plain = api.Propagator(case.config_path, lanes=2)
+    plain.set_option("graph", 0)
+    graphed = api.Propagator(case.config_path, lanes=2)
+    _, ref = plain.propagate_targets(case.targets)
+    for _ in range(3):  # capture, then replays
+        _, st = graphed.propagate_targets(case.targets)
+        np.testing.assert_array_equal(st, ref)
+    plain.close()
+    graphed.close()
