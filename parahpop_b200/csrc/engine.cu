@@ -857,7 +857,7 @@ Engine::LaunchShape Engine::prepareStep(StepParams& p, int L, const RunOptions& 
 
 // Project autotuner for the lane split.  The first batch of each class
 // (log2 of the batch size, time-grid mode, precision) times a short probe
-// (up to four steps, after an untimed warm-up launch) of every lane count on
+// (up to eight steps, best of two after an untimed warm-up launch) of every lane count on
 // scratch copies of the inputs and keeps the fastest; later batches of the
 // class reuse the choice.  PARAHPOP_B200_TUNE_LOG=1 prints the probe times.
 int Engine::tunedLanes(const StepParams& base, const RunOptions& opt, bool shared, cudaStream_t stream,
@@ -873,9 +873,9 @@ int Engine::tunedLanes(const StepParams& base, const RunOptions& opt, bool share
     double* st = (double*)scratch("probeState", (size_t)6 * n * 8);
     p.state = st;
     if (shared) {
-        p.nsteps = std::min(p.nsteps, 4);
+        p.nsteps = std::min(p.nsteps, 8);
     } else {
-        p.maxSteps = 4;
+        p.maxSteps = 8;
         p.cur = (double*)scratch("probeCur", (size_t)n * 8);
         p.dt = (double*)scratch("probeDt", (size_t)n * 8);
         p.unfinished = (int*)scratch("probeUnf", (size_t)n * 4);
@@ -889,9 +889,10 @@ int Engine::tunedLanes(const StepParams& base, const RunOptions& opt, bool share
     const bool tuneLog = logEnv && std::atoi(logEnv) != 0;
     for (int L : {1, 2, 4, 8, 16}) {
         if (L >= 8 && n >= (int64_t)sms_ * 512 * 4) continue;  // enough objects to fill the GPU with narrow groups
-        // an untimed launch first (module loading, attribute set-up), then the timed probe
-        float ms = 0.f;
-        for (int rep = 0; rep < 2; ++rep) {
+        // an untimed launch first (module loading, attribute set-up), then the
+        // fastest of two timed probes
+        float ms = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {
             PHOP_CUDA(cudaMemcpyAsync(st, base.state, (size_t)6 * n * 8, cudaMemcpyDeviceToDevice, stream));
             if (!shared) {
                 PHOP_CUDA(cudaMemcpyAsync(p.cur, base.cur, (size_t)n * 8, cudaMemcpyDeviceToDevice, stream));
@@ -904,7 +905,9 @@ int Engine::tunedLanes(const StepParams& base, const RunOptions& opt, bool share
             PHOP_CUDA(cudaEventRecord(e1, stream));
             PHOP_CUDA(cudaEventSynchronize(e1));
             if (launches) ++*launches;
-            PHOP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            float t = 0.f;
+            PHOP_CUDA(cudaEventElapsedTime(&t, e0, e1));
+            if (rep > 0) ms = std::min(ms, t);
         }
         int err = 0;
         PHOP_CUDA(cudaMemcpy(&err, p.errorFlag, sizeof(int), cudaMemcpyDeviceToHost));

@@ -302,7 +302,9 @@ struct Fast {
         return tt;
     }
 
-    __device__ T densu(T alt, T dlb, T tinf, T tlb, T xm, T alpha, T* tz, T zlb, T s2, const T* zn1) {
+    // out of line: only the rarer paths (below za, the low-altitude species
+    // corrections) call it; the main species densities use the direct form
+    __device__ __noinline__ T densu(T alt, T dlb, T tinf, T tlb, T xm, T alpha, T* tz, T zlb, T s2, const T* zn1) {
         const T rgas = T(831.4);
         T xs[5], ys[5], y2out[5];
         T x = T(0), z1 = T(0), t1 = T(0), zgdif = T(0);

@@ -549,11 +549,20 @@ __global__ void __launch_bounds__(maxStepThreads(L), 1) propagateKernel(const __
     const int g = lane / L;
     constexpr int groups = 32 / L;
     const int groupBase = lane - j;
-    for (;;) {
-        int64_t base = 0;
-        if (lane == 0) base = (int64_t)atomicAdd(p.workCounter, groups);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= p.n) break;
+    // Work items are groups of 32/L consecutive objects (in the processing
+    // order, i.e. by altitude).  The first wave is assigned statically with
+    // consecutive items on different CTAs, so the costly low-altitude groups
+    // spread over all SMs instead of landing on the CTAs that start first;
+    // later items come from the atomic queue.
+    const int64_t nItems = (p.n + groups - 1) / groups;
+    const int64_t firstWave = (int64_t)gridDim.x * (blockDim.x / 32);
+    auto nextItem = [&]() {
+        int64_t next = 0;
+        if (lane == 0) next = firstWave + (int64_t)atomicAdd(p.workCounter, 1);
+        return __shfl_sync(0xffffffffu, next, 0);
+    };
+    for (int64_t item = (int64_t)(threadIdx.x / 32) * gridDim.x + blockIdx.x; item < nItems; item = nextItem()) {
+        const int64_t base = item * groups;
         const int64_t slot = base + g;
         const bool valid = slot < p.n;
         const int64_t sidx = valid ? slot : p.n - 1;
