@@ -105,7 +105,11 @@ int phop_propagate_device_noalloc(phop_context* ctx, int64_t n, double* d_states
  *              radius, 0 = in input order; results are identical either way
  *   "graph"    1 (default) = launch the step as a CUDA graph cached by its
  *              launch parameters (replayed for repeated batches), 0 = plain
- *              launches */
+ *              launches
+ *   "split_floor_km"  split precision only: objects closer than this height
+ *              (km) above the geopotential's reference radius keep the
+ *              n > 8 harmonics in FP64, where FP32 rounding of the largest
+ *              high-degree terms would exceed the 1 cm budget; 0 = none */
 int phop_set_option(phop_context* ctx, const char* key, double value);
 
 /* ---- serving loop (no counterpart in the reference, whose driver propagates

@@ -184,6 +184,12 @@ int phop_set_option(phop_context* ctx, const char* key, double value) {
         ctx->opt.ordered = value != 0.0;
     } else if (k == "graph") {
         ctx->opt.graph = value != 0.0;
+    } else if (k == "split_floor_km") {
+        if (!(value >= 0.0) || !std::isfinite(value)) {
+            ctx->error = "split_floor_km must be finite and non-negative";
+            return 1;
+        }
+        ctx->opt.splitFloorKm = value;
     } else {
         ctx->error = "Unknown option: " + k;
         return 1;

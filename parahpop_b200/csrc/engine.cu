@@ -816,6 +816,12 @@ Engine::LaunchShape Engine::prepareStep(StepParams& p, int L, const RunOptions& 
     p.blocks = tile.dBlocks;
     p.nblocks = tile.nblocks;
     p.diagStep = tile.dDiagStep;
+    p.tile64 = nullptr;
+    p.splitRadius = 0.0;
+    if (opt.split && opt.splitFloorKm > 0.0) {
+        p.tile64 = tileFor(L, false).dTile;
+        p.splitRadius = host_.shR + opt.splitFloorKm;
+    }
     // shared memory per CTA: the coefficient tile (when it fits) plus the
     // stage derivatives, 13 x ceil(6/L) doubles per thread
     const int threadsReq = std::min(opt.threads > 0 ? opt.threads : 512, maxStepThreads(L));

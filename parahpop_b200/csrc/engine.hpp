@@ -99,6 +99,7 @@ struct RunOptions {
     int ctasPerSm = 0; // 0: occupancy
     bool ordered = true;  // process objects in order of geocentric radius
     bool graph = true;    // launch the step as a cached CUDA graph
+    double splitFloorKm = 0.0;  // split precision: FP64 n > 8 below this height over the field radius
 };
 
 class Engine {

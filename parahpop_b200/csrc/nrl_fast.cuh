@@ -126,6 +126,16 @@ __host__ __device__ inline void nrlSlotBlock(int doy, double f107, double f107A,
     }
 }
 
+// Mesosphere temperature nodes and the N2 mixing density of one call, kept
+// apart from Fast so that only this small block needs an address (the
+// out-of-line densu and lower-atmosphere paths write and read it) while the
+// rest of the per-object state stays in registers.
+template <typename T>
+struct NrlMeso {
+    T tn1[5], tgn1[2];
+    T dm28;
+};
+
 // Per-object part.  Returns the gtd7d total mass density in kg/m^3.
 template <typename T>
 struct Fast {
@@ -137,8 +147,6 @@ struct Fast {
     T glat, absLat, gLong;
     T csec, ssec;  // cos / sin (sr * seconds of day)
     T apt0;
-    T meso_tn1[5], meso_tgn1[2];
-    T dm28;
 
     __device__ __forceinline__ Fast(const NrlEpochBlock& b, double sec) : eb(b) {
         double sc, cc;
@@ -269,7 +277,7 @@ struct Fast {
         return tinf;
     }
 
-    __device__ T glob7s(int k) const {
+    __device__ __forceinline__ T glob7s(int k) const {
         const double* p = globSTable(k);
         const NrlGlobSEpoch& g = eb.gs[k];
         const T dfa = T(eb.dfa);
@@ -302,9 +310,14 @@ struct Fast {
         return tt;
     }
 
-    // out of line: only the rarer paths (below za, the low-altitude species
-    // corrections) call it; the main species densities use the direct form
-    __device__ __noinline__ T densu(T alt, T dlb, T tinf, T tlb, T xm, T alpha, T* tz, T zlb, T s2, const T* zn1) {
+    // out of line and without `this`: only the rarer paths (below za, the
+    // low-altitude species corrections) call it; the main species densities
+    // use the direct form
+    static __device__ __noinline__ T densu(T alt, T dlb, T tinf, T tlb, T xm, T alpha, T* tz, T zlb, T s2,
+                                           const T* zn1, T re, T gsurf, NrlMeso<T>& ms) {
+        auto zeta = [re](T zz, T zl) { return ((zz - zl) * (re + zl) / (re + zz)); };
+        T* meso_tn1 = ms.tn1;
+        T* meso_tgn1 = ms.tgn1;
         const T rgas = T(831.4);
         T xs[5], ys[5], y2out[5];
         T x = T(0), z1 = T(0), t1 = T(0), zgdif = T(0);
@@ -411,7 +424,10 @@ struct Fast {
     // is formed as pdm pd exp(g + (1 + alpha + gamma) ln(tlb/tt) - s gamma zg2):
     // the temperature profile tt and its logarithm are shared by the
     // species, and one exponential replaces exp, pow and exp.
-    __device__ void gts7(T alt, const T (&G)[kGlobeTasks], T aptTlb, T* d) {
+    __device__ __forceinline__ void gts7(T alt, const T (&G)[kGlobeTasks], T aptTlb, T* d, NrlMeso<T>& ms) {
+        T* meso_tn1 = ms.tn1;
+        T* meso_tgn1 = ms.tgn1;
+        T& dm28 = ms.dm28;
         T zn1[5] = {T(NRL_PDL(1)[15]), T(110.0), T(100.0), T(90.0), T(72.5)};
         const T za = zn1[0];
         for (int j = 0; j < 9; j++) d[j] = T(0);
@@ -455,7 +471,7 @@ struct Fast {
                 const T gamma = xm * kGamma;
                 return pdm0 * pd0 * exp(g + (T(1.0) + alpha + gamma) * lnX - s * gamma * zg2);
             }
-            return densu(z, pdm0 * exp(g) * pd0, tinf, tlb, xm, alpha, &dummyT, zlb, s, zn1);
+            return densu(z, pdm0 * exp(g) * pd0, tinf, tlb, xm, alpha, &dummyT, zlb, s, zn1, re, gsurf, ms);
         };
         // N2
         const T zhf = T(NRL_PDL(1)[24]) * (T(1.0) + T(NRL_PDL(0)[24]) * plg[0][1] * T(eb.ge[0].cd14));
@@ -464,18 +480,18 @@ struct Fast {
         T b28 = T(0.0);
         if (!(z > T(450.0) && z >= za)) {
             const T db28 = T(NRL_PDM(2, 0)) * exp(G[3]) * T(NRL_PD(2)[0]);
-            b28 = densu(T(NRL_PDM(2, 2)) * zhf, db28, tinf, tlb, T(28.0) - xmm, T(-1.0), &dummyT, zlb, s, zn1);
+            b28 = densu(T(NRL_PDM(2, 2)) * zhf, db28, tinf, tlb, T(28.0) - xmm, T(-1.0), &dummyT, zlb, s, zn1, re, gsurf, ms);
         }
         if (z <= T(160.0)) {
-            dm28 = densu(z, b28, tinf, tlb, xmm, T(0.0), &dummyT, zlb, s, zn1);
+            dm28 = densu(z, b28, tinf, tlb, xmm, T(0.0), &dummyT, zlb, s, zn1, re, gsurf, ms);
             d[2] = nrl::Model<T>::dnet(d[2], dm28, zhm28, xmm, T(28.0));
         }
         // He
         d[0] = mainDensity(G[4], T(NRL_PDM(0, 0)), T(NRL_PD(0)[0]), T(4.), T(-0.38));
         if (z < T(200.0)) {
             const T db04 = T(NRL_PDM(0, 0)) * exp(G[4]) * T(NRL_PD(0)[0]);
-            const T b04 = densu(T(NRL_PDM(0, 2)), db04, tinf, tlb, T(4.) - xmm, T(-1.38), &dummyT, zlb, s, zn1);
-            const T dm04 = densu(z, b04, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1);
+            const T b04 = densu(T(NRL_PDM(0, 2)), db04, tinf, tlb, T(4.) - xmm, T(-1.38), &dummyT, zlb, s, zn1, re, gsurf, ms);
+            const T dm04 = densu(z, b04, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1, re, gsurf, ms);
             d[0] = nrl::Model<T>::dnet(d[0], dm04, zhm28, xmm, T(4.));
             const T rl = log(b28 * T(NRL_PDM(0, 1)) / b04);
             d[0] = d[0] * nrl::Model<T>::ccor(z, rl, T(NRL_PDM(0, 5)) * T(NRL_PDL(1)[1]), T(NRL_PDM(0, 4)) * T(NRL_PDL(1)[0]));
@@ -484,8 +500,8 @@ struct Fast {
         d[1] = mainDensity(G[5], T(NRL_PDM(1, 0)), T(NRL_PD(1)[0]), T(16.), T(0.0));
         if (z <= T(300.0)) {
             const T db16 = T(NRL_PDM(1, 0)) * exp(G[5]) * T(NRL_PD(1)[0]);
-            const T b16 = densu(T(NRL_PDM(1, 2)), db16, tinf, tlb, T(16.0) - xmm, T(-1.0), &dummyT, zlb, s, zn1);
-            const T dm16 = densu(z, b16, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1);
+            const T b16 = densu(T(NRL_PDM(1, 2)), db16, tinf, tlb, T(16.0) - xmm, T(-1.0), &dummyT, zlb, s, zn1, re, gsurf, ms);
+            const T dm16 = densu(z, b16, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1, re, gsurf, ms);
             d[1] = nrl::Model<T>::dnet(d[1], dm16, zhm28, xmm, T(16.));
             const T rl = T(NRL_PDM(1, 1)) * T(NRL_PDL(1)[16]) * (T(1.0) + T(NRL_PDL(0)[23]) * (T(eb.f107A) - T(150.0)));
             d[1] = d[1] * nrl::Model<T>::ccor2(z, rl, T(NRL_PDM(1, 5)) * T(NRL_PDL(1)[3]),
@@ -497,8 +513,8 @@ struct Fast {
         d[3] = mainDensity(G[6], T(NRL_PDM(3, 0)), T(NRL_PD(4)[0]), T(32.), T(0.0));
         if (z <= T(250.0)) {
             const T db32 = T(NRL_PDM(3, 0)) * exp(G[6]) * T(NRL_PD(4)[0]);
-            const T b32 = densu(T(NRL_PDM(3, 2)), db32, tinf, tlb, T(32.) - xmm, T(-1.), &dummyT, zlb, s, zn1);
-            const T dm32 = densu(z, b32, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1);
+            const T b32 = densu(T(NRL_PDM(3, 2)), db32, tinf, tlb, T(32.) - xmm, T(-1.), &dummyT, zlb, s, zn1, re, gsurf, ms);
+            const T dm32 = densu(z, b32, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1, re, gsurf, ms);
             d[3] = nrl::Model<T>::dnet(d[3], dm32, zhm28, xmm, T(32.));
             const T rl = log(b28 * T(NRL_PDM(3, 1)) / b32);
             d[3] = d[3] * nrl::Model<T>::ccor(z, rl, T(NRL_PDM(3, 5)) * T(NRL_PDL(1)[7]), T(NRL_PDM(3, 4)) * T(NRL_PDL(1)[6]));
@@ -512,8 +528,8 @@ struct Fast {
         d[4] = mainDensity(G[7], T(NRL_PDM(4, 0)), T(NRL_PD(5)[0]), T(40.), T(0.17));
         if (z <= T(240.0)) {
             const T db40 = T(NRL_PDM(4, 0)) * exp(G[7]) * T(NRL_PD(5)[0]);
-            const T b40 = densu(T(NRL_PDM(4, 2)), db40, tinf, tlb, T(40.) - xmm, T(-0.83), &dummyT, zlb, s, zn1);
-            const T dm40 = densu(z, b40, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1);
+            const T b40 = densu(T(NRL_PDM(4, 2)), db40, tinf, tlb, T(40.) - xmm, T(-0.83), &dummyT, zlb, s, zn1, re, gsurf, ms);
+            const T dm40 = densu(z, b40, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1, re, gsurf, ms);
             d[4] = nrl::Model<T>::dnet(d[4], dm40, zhm28, xmm, T(40.));
             const T rl = log(b28 * T(NRL_PDM(4, 1)) / b40);
             d[4] = d[4] * nrl::Model<T>::ccor(z, rl, T(NRL_PDM(4, 5)) * T(NRL_PDL(1)[9]), T(NRL_PDM(4, 4)) * T(NRL_PDL(1)[8]));
@@ -522,8 +538,8 @@ struct Fast {
         d[6] = mainDensity(G[8], T(NRL_PDM(5, 0)), T(NRL_PD(6)[0]), T(1.), T(-0.38));
         if (z <= T(320.0)) {
             const T db01 = T(NRL_PDM(5, 0)) * exp(G[8]) * T(NRL_PD(6)[0]);
-            const T b01 = densu(T(NRL_PDM(5, 2)), db01, tinf, tlb, T(1.) - xmm, T(-1.38), &dummyT, zlb, s, zn1);
-            const T dm01 = densu(z, b01, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1);
+            const T b01 = densu(T(NRL_PDM(5, 2)), db01, tinf, tlb, T(1.) - xmm, T(-1.38), &dummyT, zlb, s, zn1, re, gsurf, ms);
+            const T dm01 = densu(z, b01, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1, re, gsurf, ms);
             d[6] = nrl::Model<T>::dnet(d[6], dm01, zhm28, xmm, T(1.));
             const T rl = log(b28 * T(NRL_PDM(5, 1)) * fabs(T(NRL_PDL(1)[17])) / b01);
             d[6] = d[6] * nrl::Model<T>::ccor(z, rl, T(NRL_PDM(5, 5)) * T(NRL_PDL(1)[11]), T(NRL_PDM(5, 4)) * T(NRL_PDL(1)[10]));
@@ -534,8 +550,8 @@ struct Fast {
         d[7] = mainDensity(G[9], T(NRL_PDM(6, 0)), T(NRL_PD(7)[0]), T(14.), T(0.0));
         if (z <= T(450.0)) {
             const T db14 = T(NRL_PDM(6, 0)) * exp(G[9]) * T(NRL_PD(7)[0]);
-            const T b14 = densu(T(NRL_PDM(6, 2)), db14, tinf, tlb, T(14.) - xmm, T(-1.), &dummyT, zlb, s, zn1);
-            const T dm14 = densu(z, b14, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1);
+            const T b14 = densu(T(NRL_PDM(6, 2)), db14, tinf, tlb, T(14.) - xmm, T(-1.), &dummyT, zlb, s, zn1, re, gsurf, ms);
+            const T dm14 = densu(z, b14, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1, re, gsurf, ms);
             d[7] = nrl::Model<T>::dnet(d[7], dm14, zhm28, xmm, T(14.));
             const T rl = log(b28 * T(NRL_PDM(6, 1)) * fabs(T(NRL_PDL(0)[2])) / b14);
             d[7] = d[7] * nrl::Model<T>::ccor(z, rl, T(NRL_PDM(6, 5)) * T(NRL_PDL(0)[1]), T(NRL_PDM(6, 4)) * T(NRL_PDL(0)[0]));
@@ -550,7 +566,7 @@ struct Fast {
             const T gamma = T(16.0) * (gsurf / (g1 * g1)) / (s * rgas * tho);
             dd = T(NRL_PDM(7, 0)) * T(NRL_PD(8)[0]) * exp(G[10] - s * gamma * zg2);
         } else {
-            dd = densu(z, T(NRL_PDM(7, 0)) * exp(G[10]) * T(NRL_PD(8)[0]), tho, tho, T(16.), T(0.0), &dummyT, zlb, s, zn1);
+            dd = densu(z, T(NRL_PDM(7, 0)) * exp(G[10]) * T(NRL_PD(8)[0]), tho, tho, T(16.), T(0.0), &dummyT, zlb, s, zn1, re, gsurf, ms);
         }
         const T zsht = T(NRL_PDM(7, 5)), zmho = T(NRL_PDM(7, 4));
         const T gz = T(1.0) + zmho / re;
@@ -562,14 +578,15 @@ struct Fast {
     // gtd7 + gtd7d total mass density (kg/m^3); lane j of a group of L
     // lanes starting at groupBase (all lanes of the group get the result)
     template <int L>
-    __device__ T density(T lat, T lon, T alt, T lst, int j, int groupBase) {
+    __device__ __forceinline__ T density(T lat, T lon, T alt, T lst, int j, int groupBase) {
         glat = lat;
         absLat = fabs(lat);
         gLong = lon;
         apt0 = T(0);
-        dm28 = T(0);
-        meso_tn1[0] = T(0);
-        meso_tgn1[0] = T(0);
+        NrlMeso<T> ms;
+        ms.dm28 = T(0);
+        ms.tn1[0] = T(0);
+        ms.tgn1[0] = T(0);
         // glatf
         const T c2 = cos(T(2.0) * T(1.74533E-2) * lat);
         gsurf = T(980.616) * (T(1.0) - T(0.0026373) * c2);
@@ -580,10 +597,10 @@ struct Fast {
         globeTasks<L>(G, aptTlb, aptLast, j, groupBase);
         T d[9];
         const T zn2top = T(72.5);
-        gts7(alt > zn2top ? alt : zn2top, G, aptTlb, d);
+        gts7(alt > zn2top ? alt : zn2top, G, aptTlb, d, ms);
         if (!(alt >= zn2top)) {
             apt0 = aptLast;
-            return lowerAtmosphere(alt, d);
+            return lowerAtmosphere(*this, alt, d, ms);
         }
         return (T(1.66E-24) * (T(4.0) * d[0] + T(16.0) * d[1] + T(28.0) * d[2] + T(32.0) * d[3] + T(40.0) * d[4]
                                + d[6] + T(14.0) * d[7] + T(16.0) * d[8]))
@@ -591,7 +608,11 @@ struct Fast {
     }
 
     // below 72.5 km (not reached in orbit, kept for completeness)
-    __device__ __noinline__ T lowerAtmosphere(T alt, const T* d) {
+    static __device__ __noinline__ T lowerAtmosphere(Fast f, T alt, const T* d, const NrlMeso<T>& ms) {
+        const T gsurf = f.gsurf, re = f.re, dm28 = ms.dm28;
+        const T* meso_tn1 = ms.tn1;
+        const T* meso_tgn1 = ms.tgn1;
+        auto glob7s = [&f](int k) { return f.glob7s(k); };
         nrl::Model<T> m;
         m.gsurf = gsurf;
         m.re = re;

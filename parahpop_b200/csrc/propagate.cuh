@@ -105,6 +105,8 @@ struct StepParams {
     const LowTable* low;
     const double* diagC;    // c_m, m = 0..M
     const double2* diagStep;  // per m: (c_{m+1}...c_{m+L}, same x (m+L)/m), nullable
+    const void* tile64;     // split precision: the FP64 tile (global memory, same blocks)
+    double splitRadius;     // split precision: radius (km) below which n > 8 stays FP64; 0 = none
     int useSmemTile;
     // scheduling and errors
     int* workCounter;
@@ -114,7 +116,9 @@ struct StepParams {
 // Threads per CTA the step kernel is compiled for: narrow lane splits run one
 // CTA of few threads per SM (the coefficient tile fills shared memory), so
 // they get up to 255 registers per thread instead of spilling at 128.
-__host__ __device__ constexpr int maxStepThreads(int lanes) { return lanes == 1 ? 256 : lanes == 2 ? 320 : 512; }
+__host__ __device__ constexpr int maxStepThreads(int lanes) {
+    return lanes == 1 ? 256 : lanes == 2 ? 320 : lanes == 4 ? 384 : 512;
+}
 
 void launchEpochRecords(const DevEnv& env, const double* epochs, int count, EpochRecord* out, cudaStream_t stream);
 cudaError_t launchPropagate(const StepParams& p, int lanes, bool split, bool shared, int ctas, int threads,

@@ -4,6 +4,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "nrlmsise00.cuh"
 #include "propagate.cuh"
 
@@ -256,11 +258,14 @@ static __device__ __forceinline__ void shAccel(const StepParams& p, const typena
                 if (m < M) advance();
         }
     }
+    // fold the group's partial sums (the group's lanes only: in split
+    // precision groups of one warp may take different precisions)
+    const unsigned groupMask = L >= 32 ? 0xffffffffu : (((1u << L) - 1u) << ((threadIdx.x & 31) - j));
 #pragma unroll
     for (int off = L / 2; off > 0; off >>= 1) {
-        ar += __shfl_xor_sync(0xffffffffu, ar, off);
-        aphi += __shfl_xor_sync(0xffffffffu, aphi, off);
-        alam += __shfl_xor_sync(0xffffffffu, alam, off);
+        ar += __shfl_xor_sync(groupMask, ar, off);
+        aphi += __shfl_xor_sync(groupMask, aphi, off);
+        alam += __shfl_xor_sync(groupMask, alam, off);
     }
     if (cosPhi == 0.0 && M >= 1) {
         // exact pole: the m = 1 longitudinal term takes its analytical limit
@@ -382,7 +387,16 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
             const double by = R[3] * pos[0] + R[4] * pos[1] + R[5] * pos[2];
             const double bz = R[6] * pos[0] + R[7] * pos[1] + R[8] * pos[2];
             double a[3];
-            shAccel<L, T>(p, tile, r.dC, r.dS, bx, by, bz, a);
+            if constexpr (!std::is_same<T, double>::value) {
+                // split precision: objects below the split radius keep the
+                // n > 8 part in FP64 (from the FP64 tile in global memory)
+                if (p.splitRadius > 0.0 && bx * bx + by * by + bz * bz < p.splitRadius * p.splitRadius)
+                    shAccel<L, double>(p, (const TileD*)p.tile64, r.dC, r.dS, bx, by, bz, a);
+                else
+                    shAccel<L, T>(p, tile, r.dC, r.dS, bx, by, bz, a);
+            } else {
+                shAccel<L, T>(p, tile, r.dC, r.dS, bx, by, bz, a);
+            }
             ax += R[0] * a[0] + R[3] * a[1] + R[6] * a[2];
             ay += R[1] * a[0] + R[4] * a[1] + R[7] * a[2];
             az += R[2] * a[0] + R[5] * a[1] + R[8] * a[2];

@@ -80,6 +80,15 @@ def main(argv=None):
     out["split_vs_fp64_m"] = {"p50": float(np.percentile(err, 50)), "p90": float(np.percentile(err, 90)),
                               "p99": float(np.percentile(err, 99)), "max": float(err.max()),
                               "worst_object": int(err.argmax())}
+    # split-vs-FP64 error by initial geocentric radius (altitude bands, km)
+    r0 = np.linalg.norm(pop.states[:, :3], axis=1) - S.R_EARTH
+    bands = {}
+    for lo, hi in ((0, 400), (400, 600), (600, 1000), (1000, 2000), (2000, 1e9)):
+        m = (r0 >= lo) & (r0 < hi)
+        if m.any():
+            bands[f"{lo:g}-{hi:g}"] = {"objects": int(m.sum()), "p99": float(np.percentile(err[m], 99)),
+                                       "max": float(err[m].max())}
+    out["split_vs_fp64_by_altitude_km"] = bands
     print(json.dumps(out))
     return 0
 
