@@ -106,6 +106,8 @@ int phop_propagate_device_noalloc(phop_context* ctx, int64_t n, double* d_states
  *   "graph"    1 (default) = launch the step as a CUDA graph cached by its
  *              launch parameters (replayed for repeated batches), 0 = plain
  *              launches
+ *   "tile_smem"  1 (default) = stage the coefficient tile in shared memory
+ *              when it fits, 0 = read it through L1 (more threads per SM)
  *   "split_floor_km"  split precision only: objects closer than this height
  *              (km) above the geopotential's reference radius keep the
  *              n > 8 harmonics in FP64, where FP32 rounding of the largest

@@ -184,6 +184,8 @@ int phop_set_option(phop_context* ctx, const char* key, double value) {
         ctx->opt.ordered = value != 0.0;
     } else if (k == "graph") {
         ctx->opt.graph = value != 0.0;
+    } else if (k == "tile_smem") {
+        ctx->opt.tileSmem = value == 0.0 ? 0 : -1;
     } else if (k == "split_floor_km") {
         if (!(value >= 0.0) || !std::isfinite(value)) {
             ctx->error = "split_floor_km must be finite and non-negative";

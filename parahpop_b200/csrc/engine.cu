@@ -827,7 +827,7 @@ Engine::LaunchShape Engine::prepareStep(StepParams& p, int L, const RunOptions& 
     const int threadsReq = std::min(opt.threads > 0 ? opt.threads : 512, maxStepThreads(L));
     const int kPerThread = 13 * ((6 + L - 1) / L) * 8;
     int threads = threadsReq;
-    if (tile.bytes + 1024 + 64 * kPerThread <= maxSmem_) {
+    if (opt.tileSmem != 0 && tile.bytes + 1024 + 64 * kPerThread <= maxSmem_) {
         p.useSmemTile = 1;
         threads = std::min(threadsReq, (maxSmem_ - tile.bytes - 1024) / kPerThread / 32 * 32);
     } else {

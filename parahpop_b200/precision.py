@@ -39,6 +39,8 @@ def main(argv=None):
     ap.add_argument("--mixed", action="store_true")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--lanes", type=int, default=0)
+    ap.add_argument("--split-floor-km", type=float, default=None,
+                    help="split precision: FP64 harmonics below this height (km); default: the library's")
     args = ap.parse_args(argv)
 
     work = Path(tempfile.mkdtemp(prefix="phop_precision_"))
@@ -57,6 +59,8 @@ def main(argv=None):
     res = {}
     for name, split in (("fp64", False), ("split", True)):
         p = api.Propagator(work / "config.json", lanes=args.lanes or None, split=split)
+        if split and args.split_floor_km is not None:
+            p.set_option("split_floor_km", args.split_floor_km)
         warm = pop.subset(np.arange(min(n, 4096)))
         p.propagate(warm.epochs, warm.states, warm.mass, warm.drag_area, warm.srp_area, warm.cd, warm.cr,
                     np.minimum(warm.duration, 1800.0), warm.step)
@@ -70,7 +74,8 @@ def main(argv=None):
         p.close()
     err = _errors_m(res["split"]["states"], res["fp64"]["states"])
     out = {"workload": ("mixed LEO/MEO/GEO" if args.mixed else "LEO") + f", {n} objects, degree {args.degree}, "
-                       f"{args.hours:g} h", "object_steps": int(res["fp64"]["object_steps"])}
+                       f"{args.hours:g} h", "object_steps": int(res["fp64"]["object_steps"]),
+           "split_floor_km": args.split_floor_km}
     for name in ("fp64", "split"):
         r = res[name]
         out[name] = {"object_steps_per_s": r["object_steps"] / ((r["kernel_ms"] + r["records_ms"]) * 1e-3),
