@@ -80,7 +80,15 @@ struct EpochRecord {
     double dC[kTideTri];         // tide coefficient deltas, field units
     double dS[kTideTri];
     double nrlSec, nrlGast;      // UTC seconds of day, apparent sidereal time (h)
-    int nrlBlock, nrlValid, tideValid, pad;
+    double et;                   // the record's epoch, TDB seconds past J2000
+    int nrlBlock, nrlValid;      // nrlValid: 1 / 0, or -1 = time inputs not evaluated yet (from et)
+    int tideValid, pad;
+};
+
+// NRLMSISE-00 time inputs of one epoch
+struct NrlTime {
+    double sec, gast;
+    int block, valid;
 };
 
 #if defined(__CUDACC__)
@@ -342,26 +350,37 @@ static __device__ double gastHours(double mjdUtc) {
     return wrapHours((gmst + eqeq) * 24.0 / kTwoPi);
 }
 
-static __device__ void nrlEpoch(const DevEnv& e, double et, EpochRecord& r) {
+static __device__ __noinline__ NrlTime nrlTime(const DevEnv& e, double et) {
+    NrlTime t;
     const double mjdUtc = etToMjdUtc(et);
     // weather record and 3-hour slot (Nrlmsise00.cu:207-214)
     const int rec = (int)floor(mjdUtc - e.nrlStartMjd);
-    r.nrlValid = (rec >= 3 && rec < e.nrlNdays);
+    t.valid = (rec >= 3 && rec < e.nrlNdays);
     int slot = (int)floor((mjdUtc - floor(mjdUtc)) * 8.0);
     slot = slot < 0 ? 0 : (slot > 7 ? 7 : slot);
-    r.nrlBlock = r.nrlValid ? rec * 8 + slot : 0;
+    t.block = t.valid ? rec * 8 + slot : 0;
     // seconds of day as calendarDate forms them (Nrlmsise00.cu:113-130)
     double sod = (mjdUtc - floor(mjdUtc)) * 86400.0;
     if (sod < 0.0) sod += 86400.0;
     const int hour = (int)(sod / 3600.0);
     const int minute = (int)((sod - hour * 3600.0) / 60.0);
     const double second = sod - hour * 3600.0 - minute * 60.0;
-    r.nrlSec = hour * 3600.0 + minute * 60.0 + second;
-    r.nrlGast = gastHours(mjdUtc);
+    t.sec = hour * 3600.0 + minute * 60.0 + second;
+    t.gast = gastHours(mjdUtc);
+    return t;
+}
+
+static __device__ void nrlEpoch(const DevEnv& e, double et, EpochRecord& r) {
+    const NrlTime t = nrlTime(e, et);
+    r.nrlValid = t.valid;
+    r.nrlBlock = t.block;
+    r.nrlSec = t.sec;
+    r.nrlGast = t.gast;
 }
 
 // ---- full epoch record ------------------------------------------------------------------------
 static __device__ void evalEpochRecord(const DevEnv& e, double et, EpochRecord& r) {
+    r.et = et;
     for (int i = 0; i < 9; ++i) r.R[i] = (i % 4 == 0) ? 1.0 : 0.0;
     r.w[0] = r.w[1] = r.w[2] = 0.0;
     if (e.hasRot) earthRotation(e, et, r.R, r.w);

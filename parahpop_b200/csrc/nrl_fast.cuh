@@ -33,6 +33,9 @@ struct NrlGlobeEpoch {
     double g0[6];                 // Eq. A24d responses to ap[1..6]
     double c131, s131, c97, s97, c136, s136;  // table phase constants
     double c71, s71, c58, s58, c79, s79;      // cos / sin (sr p[k]) for the seconds-of-day phases
+    double apt0;                  // sg0 ap response when it does not depend on latitude (p[138] == 0)
+    int aptEpochOnly;             // 1: apt0 above holds it
+    int pad;
 };
 
 struct NrlGlobSEpoch {
@@ -78,6 +81,17 @@ __host__ __device__ __forceinline__ const double* globSTable(int k) {
     return k < 4 ? NRLT(ptl) + 100 * k : NRLT(pma) + 100 * (k - 4);
 }
 
+// sg0 (Eq. A24a) from the ap decay factor and the six 3-hour responses g0
+template <typename T>
+__host__ __device__ __forceinline__ T sg0FromExp(T exp1, const double g0[6]) {
+    const T e2 = exp1 * exp1, e3 = e2 * exp1, e4 = e2 * e2, e8 = e4 * e4, e12 = e8 * e4;
+    const T e19 = e12 * e4 * e3;
+    const T sumex = T(1.0) + (T(1.0) - e19) / (T(1.0) - exp1) * sqrt(exp1);
+    return (T(g0[0]) + (T(g0[1]) * exp1 + T(g0[2]) * e2 + T(g0[3]) * e3
+                        + (T(g0[4]) * e4 + T(g0[5]) * e12) * (T(1.0) - e8) / (T(1.0) - exp1)))
+        / sumex;
+}
+
 // (day, ap slot) part: day of year, F10.7 of the previous day, 81-day mean,
 // ap history (as Nrlmsise00.cu:207-235 fills them).
 __host__ __device__ inline void nrlSlotBlock(int doy, double f107, double f107A, const double apa[7],
@@ -113,6 +127,15 @@ __host__ __device__ inline void nrlSlotBlock(int doy, double f107, double f107A,
         g.s97 = sin(1.74533E-2 * p[97]);
         g.c136 = cos(1.74533E-2 * p[136]);
         g.s136 = sin(1.74533E-2 * p[136]);
+        // tables whose ap-decay rate has no latitude term: the whole sg0
+        // response is epoch-only
+        g.aptEpochOnly = (p[51] != 0.0 && p[138] == 0.0) ? 1 : 0;
+        g.apt0 = 0.0;
+        if (g.aptEpochOnly) {
+            double exp1 = exp(-10800.0 * fabs(p[51]));
+            if (exp1 > 0.99999) exp1 = 0.99999;
+            g.apt0 = sg0FromExp(exp1, g.g0);
+        }
     }
     for (int k = 0; k < kGlobSTables; ++k) {
         const double* p = globSTable(k);
@@ -227,15 +250,13 @@ struct Fast {
         tinf += f2 * ((T(p[39]) * plg[3][3] + (T(p[93]) * plg[3][4] + T(p[46]) * plg[3][6]) * cd14) * s3tloc
                       + (T(p[40]) * plg[3][3] + (T(p[94]) * plg[3][4] + T(p[48]) * plg[3][6]) * cd14) * c3tloc);
         if (p[51] != 0) {
-            T exp1 = exp(T(-10800.0) * fabs(T(p[51])) / (T(1.0) + T(p[138]) * (T(45.0) - absLat)));
-            if (exp1 > T(0.99999)) exp1 = T(0.99999);
-            // sg0 (Eq. A24a) with the epoch's g0 responses
-            const T e2 = exp1 * exp1, e3 = e2 * exp1, e4 = e2 * e2, e8 = e4 * e4, e12 = e8 * e4;
-            const T e19 = e12 * e4 * e3;
-            const T sumex = T(1.0) + (T(1.0) - e19) / (T(1.0) - exp1) * sqrt(exp1);
-            apt0 = (T(g.g0[0]) + (T(g.g0[1]) * exp1 + T(g.g0[2]) * e2 + T(g.g0[3]) * e3
-                                  + (T(g.g0[4]) * e4 + T(g.g0[5]) * e12) * (T(1.0) - e8) / (T(1.0) - exp1)))
-                / sumex;
+            if (g.aptEpochOnly) {
+                apt0 = T(g.apt0);
+            } else {
+                T exp1 = exp(T(-10800.0) * fabs(T(p[51])) / (T(1.0) + T(p[138]) * (T(45.0) - absLat)));
+                if (exp1 > T(0.99999)) exp1 = T(0.99999);
+                apt0 = sg0FromExp(exp1, g.g0);  // with the epoch's g0 responses
+            }
             const T c131 = T(g.c131), s131 = T(g.s131);
             tinf += apt0 * (T(p[50]) + T(p[96]) * plg[0][2] + T(p[54]) * plg[0][4]
                             + (T(p[125]) * plg[0][1] + T(p[126]) * plg[0][3] + T(p[127]) * plg[0][5]) * cd14
@@ -381,7 +402,7 @@ struct Fast {
     template <int L>
     __device__ __forceinline__ void globeTasks(T (&G)[kGlobeTasks], T& aptTlb, T& aptLast, int j, int groupBase) {
         if (L == 1) {
-#pragma unroll 1
+#pragma unroll
             for (int t = 0; t < kGlobeTasks; ++t) {
                 G[t] = globe7(globeTaskTable(t));
                 if (t == 2) aptTlb = apt0;

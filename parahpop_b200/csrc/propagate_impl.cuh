@@ -341,10 +341,12 @@ static __device__ __noinline__ double nrlDensity(const DevEnv& e, const EpochRec
     const double alt = nh - nn;
     if (!(isfinite(lat) && isfinite(lon) && isfinite(alt))) return NAN;
     if (alt > e.nrlHcutoff) return 0.0;
-    if (!r.nrlValid) return NAN;
+    NrlTime t{r.nrlSec, r.nrlGast, r.nrlBlock, r.nrlValid};
+    if (t.valid < 0) t = nrlTime(e, r.et);
+    if (!t.valid) return NAN;
     const double kRad = 57.2957795130823208768;
-    nrlf::Fast<double> model(e.nrlBlocks[r.nrlBlock], r.nrlSec);
-    const double lst = wrapHours(r.nrlGast + lon * kRad / 15.0);
+    nrlf::Fast<double> model(e.nrlBlocks[t.block], t.sec);
+    const double lst = wrapHours(t.gast + lon * kRad / 15.0);
     const int lane = (int)(threadIdx.x & 31);
     const double rhoSi = model.template density<L>(lat * kRad, lon * kRad, alt, lst, lane % L, lane - lane % L);
     if (!isfinite(rhoSi) || rhoSi < 0.0) return NAN;
@@ -497,7 +499,8 @@ static __device__ __noinline__ void epochRecordOutOfLine(const DevEnv& env, doub
 // Stage record of a mixed batch: 4-point Lagrange interpolation in the
 // batch's record grid (rotation, angular velocity, body positions, tide
 // deltas; a 30 s spacing keeps the interpolation error of the rotation below
-// 1e-12 relative), with the NRLMSISE-00 time inputs evaluated exactly.
+// 1e-12 relative); the NRLMSISE-00 time inputs are evaluated exactly at the
+// stage epoch by the drag model when it needs them.
 static __device__ __noinline__ void epochRecordFromGrid(const StepParams& p, double et, EpochRecord& r) {
     // stencil k0 - 1 .. k0 + 2 around the absolute grid index k0 = floor(et / H);
     // q depends on et alone, so the weights are the same in every batch
@@ -541,8 +544,10 @@ static __device__ __noinline__ void epochRecordFromGrid(const StepParams& p, dou
     } else {
         for (int k = 0; k < kTideTri; ++k) r.dC[k] = r.dS[k] = 0.0;
     }
-    if (p.env.hasNrl) nrlEpoch(p.env, et, r);
-    else r.nrlValid = 0;
+    // NRLMSISE-00 time inputs: evaluated at the first drag evaluation below
+    // the density cut-off (objects above it never need them)
+    r.et = et;
+    r.nrlValid = p.env.hasNrl ? -1 : 0;
 }
 
 template <int L, typename T, bool SHARED_GRID>
