@@ -187,6 +187,8 @@ def main():
     ap.add_argument("--objects", type=int, default=10000)
     ap.add_argument("--hours", type=float, default=24.0, help="propagated span covered by the K timed steps")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--serving-seconds", type=float, default=15.0,
+                    help="length of the request trace replayed for the p50/p99 latency leg (0: skip)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -303,6 +305,21 @@ def main():
             cpu = {"value": r["value"], "unit": "object-steps/s", "cores": threads, "kind": "reference",
                    "sample": f"{nc} objects x 1 h (60 steps), same force model and field, "
                              f"{r['seconds']:.2f} s on {threads} threads"}
+    # ---- serving latency (request trace, continuous batching) ----------------
+    serving = None
+    if rank == 0 and args.serving_seconds > 0:
+        from parahpop_b200 import serving as SV
+        summ = SV.run_trace("fit", seconds=args.serving_seconds, drain=60.0, split=args.split, device=local)
+        serving = {"trace": f"{summ['requests']} requests, Poisson {summ['trace']['rate']:g}/s over "
+                            f"{summ['trace']['seconds']:g} s, sizes log-U(1, {summ['trace']['size_max']:g}), "
+                            f"durations log-U({summ['trace']['dur_min']:g}, {summ['trace']['dur_max']:g}) s, "
+                            "half central+J2-J6, half full force degree 70",
+                   "unfinished": summ["unfinished"]}
+        for kind in ("zonal", "full"):
+            k = summ[kind]
+            serving[kind] = {"p50_ms": k["p50_ms"], "p99_ms": k["p99_ms"], "queue_p99_ms": k["queue_p99_ms"],
+                             "completed": k["completed"],
+                             "served_object_steps_per_s": k["served_object_steps_per_s"]}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "object-steps/s", "n_gpus": ws, "steps": K, "warmup": W,
@@ -323,6 +340,7 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "object-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
+            "serving": serving,
             "gpu_launches": launches,
             "clocks": clk,
             "fp32_peak_tflops": fp32_peak,

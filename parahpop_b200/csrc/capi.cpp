@@ -184,6 +184,13 @@ int phop_set_option(phop_context* ctx, const char* key, double value) {
         ctx->opt.ordered = value != 0.0;
     } else if (k == "graph") {
         ctx->opt.graph = value != 0.0;
+    } else if (k == "mixed_order") {
+        const int m = (int)value;
+        if (m < 0 || m > 2) {
+            ctx->error = "mixed_order must be 0, 1 or 2";
+            return 1;
+        }
+        ctx->opt.mixedOrder = m;
     } else if (k == "tile_smem") {
         ctx->opt.tileSmem = value == 0.0 ? 0 : -1;
     } else if (k == "split_floor_km") {

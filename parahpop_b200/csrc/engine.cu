@@ -1100,18 +1100,26 @@ void Engine::propagate(const TargetSet& t, int64_t maxSteps, const RunOptions& o
             st->objectSteps += cost[i];
         }
         // longest objects first (in buckets of 2^(1/16) in step count), then
-        // by geocentric radius inside a bucket
-        std::vector<int> bucket(n);
+        // inside a bucket by geocentric radius (mixedOrder 0: warps take the
+        // same drag-model branches), by start epoch (1: a warp's objects read
+        // the same few epoch records), or drag / no drag and then epoch (2)
+        std::vector<int> bucket(n), drag(n);
         std::vector<float> radius(n);
+        const double dragR = host_.hasNrl ? (host_.shR > 0 ? host_.shR : 6378.137) + host_.nrlHcutoff + 200.0 : 0.0;
         for (int64_t i = 0; i < n; ++i) {
             bucket[i] = (int)std::floor(16.0 * std::log2((double)std::max<int64_t>(cost[i], 1)));
             const double* x = &t.state[(size_t)6 * i];
             radius[i] = (float)(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+            drag[i] = radius[i] < dragR * dragR ? 1 : 0;
         }
         std::iota(order.begin(), order.end(), 0);
+        const int mode = opt.ordered ? opt.mixedOrder : -1;
         std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
             if (bucket[a] != bucket[b]) return bucket[a] > bucket[b];
-            return opt.ordered && radius[a] < radius[b];
+            if (mode == 0) return radius[a] < radius[b];
+            if (mode == 2 && drag[a] != drag[b]) return drag[a] > drag[b];
+            if (mode >= 1) return cur[a] < cur[b];
+            return false;
         });
         double lo = cur[0], hi = end[0];
         for (int64_t i = 1; i < n; ++i) {

@@ -330,6 +330,13 @@ int Server::step() {
         }
     }
     running_.swap(still);
+    // unfinished objects of the requests still running
+    int64_t remaining = 0;
+    for (int64_t id : running_) {
+        const Request& r = requests_.at(id);
+        for (int64_t i = 0; i < (int64_t)r.t.size(); ++i) remaining += hostUnfinished_[r.off + i];
+    }
+    stats_.activeObjects = remaining;
     return finished;
 }
 
@@ -361,9 +368,6 @@ Server::Stats Server::stats() const {
     Stats s = stats_;
     s.queued = (int64_t)queue_.size();
     s.running = (int64_t)running_.size();
-    int64_t a = 0;
-    for (int v : hostUnfinished_) a += v;
-    s.activeObjects = a;
     return s;
 }
 
