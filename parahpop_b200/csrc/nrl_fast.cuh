@@ -66,6 +66,9 @@ struct NrlEpochBlock {
 __host__ __device__ __forceinline__ const double* globeTable(int k) {
     return k == 0 ? NRLT(pt) : k == 1 ? NRLT(ps) : NRLT(pd) + 150 * (k - 2);
 }
+__device__ __forceinline__ const double* globSTableGlobal(int k) {
+    return k < 4 ? gdev_nrl_ptl + 100 * k : gdev_nrl_pma + 100 * (k - 4);
+}
 __device__ __forceinline__ const double* globeTableGlobal(int k) {
     return k == 0 ? gdev_nrl_pt : k == 1 ? gdev_nrl_ps : gdev_nrl_pd + 150 * (k - 2);
 }
@@ -298,8 +301,9 @@ struct Fast {
         return tinf;
     }
 
-    __device__ __forceinline__ T glob7s(int k) const {
-        const double* p = globSTable(k);
+    __device__ __forceinline__ T glob7s(int k) const { return glob7sAt(k, globSTable(k)); }
+
+    __device__ __forceinline__ T glob7sAt(int k, const double* __restrict__ p) const {
         const NrlGlobSEpoch& g = eb.gs[k];
         const T dfa = T(eb.dfa);
         T tt = T(p[21]) * dfa;
@@ -445,7 +449,9 @@ struct Fast {
     // is formed as pdm pd exp(g + (1 + alpha + gamma) ln(tlb/tt) - s gamma zg2):
     // the temperature profile tt and its logarithm are shared by the
     // species, and one exponential replaces exp, pow and exp.
-    __device__ __forceinline__ void gts7(T alt, const T (&G)[kGlobeTasks], T aptTlb, T* d, NrlMeso<T>& ms) {
+    template <int L>
+    __device__ __forceinline__ void gts7(T alt, const T (&G)[kGlobeTasks], T aptTlb, T* d, NrlMeso<T>& ms, int j,
+                                         int groupBase) {
         T* meso_tn1 = ms.tn1;
         T* meso_tgn1 = ms.tgn1;
         T& dm28 = ms.dm28;
@@ -461,11 +467,29 @@ struct Fast {
         const T ptl30 = T(NRL_PTM(4)) * T(NRL_PTL(3)[0]);
         if (z < T(300.0)) {
             apt0 = aptTlb;
-            meso_tn1[1] = T(NRL_PTM(6)) * T(NRL_PTL(0)[0]) / (T(1.0) - glob7s(0));
-            meso_tn1[2] = T(NRL_PTM(2)) * T(NRL_PTL(1)[0]) / (T(1.0) - glob7s(1));
-            meso_tn1[3] = T(NRL_PTM(7)) * T(NRL_PTL(2)[0]) / (T(1.0) - glob7s(2));
-            meso_tn1[4] = ptl30 / (T(1.0) - glob7s(3));
-            meso_tgn1[1] = T(NRL_PTM(8)) * T(NRL_PMA(8)[0]) * (T(1.0) + glob7s(4 + 8)) * meso_tn1[4] * meso_tn1[4]
+            // the five glob7s tables of the mesosphere nodes (ptl[0..3], pma[8]);
+            // L > 1 lanes share them as for globe7
+            T gs[5];
+            if (L == 1) {
+#pragma unroll
+                for (int k = 0; k < 5; ++k) gs[k] = glob7s(k < 4 ? k : 12);
+            } else {
+                const unsigned mask = ((1u << L) - 1u) << groupBase;
+#pragma unroll
+                for (int r = 0; r < (5 + L - 1) / L; ++r) {
+                    const int k = r * L + j;
+                    T v = T(0.0);
+                    if (k < 5) v = glob7sAt(k < 4 ? k : 12, globSTableGlobal(k < 4 ? k : 12));
+#pragma unroll
+                    for (int jj = 0; jj < L; ++jj)
+                        if (r * L + jj < 5) gs[r * L + jj] = __shfl_sync(mask, v, groupBase + jj);
+                }
+            }
+            meso_tn1[1] = T(NRL_PTM(6)) * T(NRL_PTL(0)[0]) / (T(1.0) - gs[0]);
+            meso_tn1[2] = T(NRL_PTM(2)) * T(NRL_PTL(1)[0]) / (T(1.0) - gs[1]);
+            meso_tn1[3] = T(NRL_PTM(7)) * T(NRL_PTL(2)[0]) / (T(1.0) - gs[2]);
+            meso_tn1[4] = ptl30 / (T(1.0) - gs[3]);
+            meso_tgn1[1] = T(NRL_PTM(8)) * T(NRL_PMA(8)[0]) * (T(1.0) + gs[4]) * meso_tn1[4] * meso_tn1[4]
                 / (ptl30 * ptl30);
         } else {
             meso_tn1[1] = T(NRL_PTM(6)) * T(NRL_PTL(0)[0]);
@@ -494,25 +518,83 @@ struct Fast {
             }
             return densu(z, pdm0 * exp(g) * pd0, tinf, tlb, xm, alpha, &dummyT, zlb, s, zn1, re, gsurf, ms);
         };
-        // N2
+        // Low-altitude corrections: for species s below its altitude limit,
+        // b_s = densu(zb_s, db_s, tinf, tlb, xm_s - xmm, alpha_s - 1) and the
+        // mixing density dm_s = densu(z, b_s, tinf, tlb, xmm, 0).  Task t =
+        // N2, He, O, O2, Ar, H, N.  With L > 1 lanes the tasks are spread over
+        // the group's lanes (the costly spline path of densu then runs once
+        // per lane instead of once per task on every lane) and exchanged by
+        // shuffles; the combination below is the same for every L.
         const T zhf = T(NRL_PDL(1)[24]) * (T(1.0) + T(NRL_PDL(0)[24]) * plg[0][1] * T(eb.ge[0].cd14));
+        auto needTask = [&](int t) -> bool {
+            switch (t) {
+                case 0: return !(z > T(450.0) && z >= za);
+                case 1: return z < T(200.0);
+                case 2: return z <= T(300.0);
+                case 3: return z <= T(250.0);
+                case 4: return z <= T(240.0);
+                case 5: return z <= T(320.0);
+                default: return z <= T(450.0);
+            }
+        };
+        auto corrTask = [&](int t, T& bOut, T& dmOut) {
+            T zb, xm, al, pdm0, pd0, g;
+            switch (t) {
+                case 0: zb = T(NRL_PDM(2, 2)) * zhf; xm = T(28.0); al = T(-1.0); pdm0 = T(NRL_PDM(2, 0)); pd0 = T(NRL_PD(2)[0]); g = G[3]; break;
+                case 1: zb = T(NRL_PDM(0, 2)); xm = T(4.); al = T(-1.38); pdm0 = T(NRL_PDM(0, 0)); pd0 = T(NRL_PD(0)[0]); g = G[4]; break;
+                case 2: zb = T(NRL_PDM(1, 2)); xm = T(16.0); al = T(-1.0); pdm0 = T(NRL_PDM(1, 0)); pd0 = T(NRL_PD(1)[0]); g = G[5]; break;
+                case 3: zb = T(NRL_PDM(3, 2)); xm = T(32.); al = T(-1.); pdm0 = T(NRL_PDM(3, 0)); pd0 = T(NRL_PD(4)[0]); g = G[6]; break;
+                case 4: zb = T(NRL_PDM(4, 2)); xm = T(40.); al = T(-0.83); pdm0 = T(NRL_PDM(4, 0)); pd0 = T(NRL_PD(5)[0]); g = G[7]; break;
+                case 5: zb = T(NRL_PDM(5, 2)); xm = T(1.); al = T(-1.38); pdm0 = T(NRL_PDM(5, 0)); pd0 = T(NRL_PD(6)[0]); g = G[8]; break;
+                default: zb = T(NRL_PDM(6, 2)); xm = T(14.); al = T(-1.); pdm0 = T(NRL_PDM(6, 0)); pd0 = T(NRL_PD(7)[0]); g = G[9]; break;
+            }
+            const T db = pdm0 * exp(g) * pd0;
+            bOut = densu(zb, db, tinf, tlb, xm - xmm, al, &dummyT, zlb, s, zn1, re, gsurf, ms);
+            dmOut = (t != 0 || z <= T(160.0)) ? densu(z, bOut, tinf, tlb, xmm, T(0.0), &dummyT, zlb, s, zn1, re, gsurf, ms)
+                                               : T(0.0);
+        };
+        T bv[7], dmv[7];
+#pragma unroll
+        for (int t = 0; t < 7; ++t) bv[t] = dmv[t] = T(0.0);
+        if (L == 1) {
+#pragma unroll
+            for (int t = 0; t < 7; ++t)
+                if (needTask(t)) corrTask(t, bv[t], dmv[t]);
+        } else if (needTask(0)) {  // every other task's limit is below N2's
+            // slots in order of decreasing altitude limit (N2, N, H, O, O2, Ar,
+            // He), so the tasks active at an altitude fill the first rounds
+            constexpr int kSlot[7] = {0, 6, 5, 2, 3, 4, 1};
+            const unsigned mask = ((1u << L) - 1u) << groupBase;
+#pragma unroll
+            for (int r = 0; r < (7 + L - 1) / L; ++r) {
+                const int k = r * L + j;
+                T bb = T(0.0), dd = T(0.0);
+                if (k < 7) {
+                    const int t = k == 0 ? 0 : k == 1 ? 6 : k == 2 ? 5 : k == 3 ? 2 : k == 4 ? 3 : k == 5 ? 4 : 1;
+                    if (needTask(t)) corrTask(t, bb, dd);
+                }
+#pragma unroll
+                for (int jj = 0; jj < L; ++jj) {
+                    const int kk = r * L + jj;
+                    if (kk < 7) {
+                        bv[kSlot[kk]] = __shfl_sync(mask, bb, groupBase + jj);
+                        dmv[kSlot[kk]] = __shfl_sync(mask, dd, groupBase + jj);
+                    }
+                }
+            }
+        }
+        // N2
         d[2] = mainDensity(G[3], T(NRL_PDM(2, 0)), T(NRL_PD(2)[0]), T(28.0), T(0.0));
         const T zhm28 = T(NRL_PDM(2, 3)) * T(NRL_PDL(1)[5]);
-        T b28 = T(0.0);
-        if (!(z > T(450.0) && z >= za)) {
-            const T db28 = T(NRL_PDM(2, 0)) * exp(G[3]) * T(NRL_PD(2)[0]);
-            b28 = densu(T(NRL_PDM(2, 2)) * zhf, db28, tinf, tlb, T(28.0) - xmm, T(-1.0), &dummyT, zlb, s, zn1, re, gsurf, ms);
-        }
+        const T b28 = bv[0];
         if (z <= T(160.0)) {
-            dm28 = densu(z, b28, tinf, tlb, xmm, T(0.0), &dummyT, zlb, s, zn1, re, gsurf, ms);
+            dm28 = dmv[0];
             d[2] = nrl::Model<T>::dnet(d[2], dm28, zhm28, xmm, T(28.0));
         }
         // He
         d[0] = mainDensity(G[4], T(NRL_PDM(0, 0)), T(NRL_PD(0)[0]), T(4.), T(-0.38));
         if (z < T(200.0)) {
-            const T db04 = T(NRL_PDM(0, 0)) * exp(G[4]) * T(NRL_PD(0)[0]);
-            const T b04 = densu(T(NRL_PDM(0, 2)), db04, tinf, tlb, T(4.) - xmm, T(-1.38), &dummyT, zlb, s, zn1, re, gsurf, ms);
-            const T dm04 = densu(z, b04, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1, re, gsurf, ms);
+            const T b04 = bv[1], dm04 = dmv[1];
             d[0] = nrl::Model<T>::dnet(d[0], dm04, zhm28, xmm, T(4.));
             const T rl = log(b28 * T(NRL_PDM(0, 1)) / b04);
             d[0] = d[0] * nrl::Model<T>::ccor(z, rl, T(NRL_PDM(0, 5)) * T(NRL_PDL(1)[1]), T(NRL_PDM(0, 4)) * T(NRL_PDL(1)[0]));
@@ -520,9 +602,7 @@ struct Fast {
         // O
         d[1] = mainDensity(G[5], T(NRL_PDM(1, 0)), T(NRL_PD(1)[0]), T(16.), T(0.0));
         if (z <= T(300.0)) {
-            const T db16 = T(NRL_PDM(1, 0)) * exp(G[5]) * T(NRL_PD(1)[0]);
-            const T b16 = densu(T(NRL_PDM(1, 2)), db16, tinf, tlb, T(16.0) - xmm, T(-1.0), &dummyT, zlb, s, zn1, re, gsurf, ms);
-            const T dm16 = densu(z, b16, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1, re, gsurf, ms);
+            const T dm16 = dmv[2];
             d[1] = nrl::Model<T>::dnet(d[1], dm16, zhm28, xmm, T(16.));
             const T rl = T(NRL_PDM(1, 1)) * T(NRL_PDL(1)[16]) * (T(1.0) + T(NRL_PDL(0)[23]) * (T(eb.f107A) - T(150.0)));
             d[1] = d[1] * nrl::Model<T>::ccor2(z, rl, T(NRL_PDM(1, 5)) * T(NRL_PDL(1)[3]),
@@ -533,9 +613,7 @@ struct Fast {
         // O2
         d[3] = mainDensity(G[6], T(NRL_PDM(3, 0)), T(NRL_PD(4)[0]), T(32.), T(0.0));
         if (z <= T(250.0)) {
-            const T db32 = T(NRL_PDM(3, 0)) * exp(G[6]) * T(NRL_PD(4)[0]);
-            const T b32 = densu(T(NRL_PDM(3, 2)), db32, tinf, tlb, T(32.) - xmm, T(-1.), &dummyT, zlb, s, zn1, re, gsurf, ms);
-            const T dm32 = densu(z, b32, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1, re, gsurf, ms);
+            const T b32 = bv[3], dm32 = dmv[3];
             d[3] = nrl::Model<T>::dnet(d[3], dm32, zhm28, xmm, T(32.));
             const T rl = log(b28 * T(NRL_PDM(3, 1)) / b32);
             d[3] = d[3] * nrl::Model<T>::ccor(z, rl, T(NRL_PDM(3, 5)) * T(NRL_PDL(1)[7]), T(NRL_PDM(3, 4)) * T(NRL_PDL(1)[6]));
@@ -548,9 +626,7 @@ struct Fast {
         // Ar
         d[4] = mainDensity(G[7], T(NRL_PDM(4, 0)), T(NRL_PD(5)[0]), T(40.), T(0.17));
         if (z <= T(240.0)) {
-            const T db40 = T(NRL_PDM(4, 0)) * exp(G[7]) * T(NRL_PD(5)[0]);
-            const T b40 = densu(T(NRL_PDM(4, 2)), db40, tinf, tlb, T(40.) - xmm, T(-0.83), &dummyT, zlb, s, zn1, re, gsurf, ms);
-            const T dm40 = densu(z, b40, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1, re, gsurf, ms);
+            const T b40 = bv[4], dm40 = dmv[4];
             d[4] = nrl::Model<T>::dnet(d[4], dm40, zhm28, xmm, T(40.));
             const T rl = log(b28 * T(NRL_PDM(4, 1)) / b40);
             d[4] = d[4] * nrl::Model<T>::ccor(z, rl, T(NRL_PDM(4, 5)) * T(NRL_PDL(1)[9]), T(NRL_PDM(4, 4)) * T(NRL_PDL(1)[8]));
@@ -558,9 +634,7 @@ struct Fast {
         // H
         d[6] = mainDensity(G[8], T(NRL_PDM(5, 0)), T(NRL_PD(6)[0]), T(1.), T(-0.38));
         if (z <= T(320.0)) {
-            const T db01 = T(NRL_PDM(5, 0)) * exp(G[8]) * T(NRL_PD(6)[0]);
-            const T b01 = densu(T(NRL_PDM(5, 2)), db01, tinf, tlb, T(1.) - xmm, T(-1.38), &dummyT, zlb, s, zn1, re, gsurf, ms);
-            const T dm01 = densu(z, b01, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1, re, gsurf, ms);
+            const T b01 = bv[5], dm01 = dmv[5];
             d[6] = nrl::Model<T>::dnet(d[6], dm01, zhm28, xmm, T(1.));
             const T rl = log(b28 * T(NRL_PDM(5, 1)) * fabs(T(NRL_PDL(1)[17])) / b01);
             d[6] = d[6] * nrl::Model<T>::ccor(z, rl, T(NRL_PDM(5, 5)) * T(NRL_PDL(1)[11]), T(NRL_PDM(5, 4)) * T(NRL_PDL(1)[10]));
@@ -570,9 +644,7 @@ struct Fast {
         // N
         d[7] = mainDensity(G[9], T(NRL_PDM(6, 0)), T(NRL_PD(7)[0]), T(14.), T(0.0));
         if (z <= T(450.0)) {
-            const T db14 = T(NRL_PDM(6, 0)) * exp(G[9]) * T(NRL_PD(7)[0]);
-            const T b14 = densu(T(NRL_PDM(6, 2)), db14, tinf, tlb, T(14.) - xmm, T(-1.), &dummyT, zlb, s, zn1, re, gsurf, ms);
-            const T dm14 = densu(z, b14, tinf, tlb, xmm, T(0.), &dummyT, zlb, s, zn1, re, gsurf, ms);
+            const T b14 = bv[6], dm14 = dmv[6];
             d[7] = nrl::Model<T>::dnet(d[7], dm14, zhm28, xmm, T(14.));
             const T rl = log(b28 * T(NRL_PDM(6, 1)) * fabs(T(NRL_PDL(0)[2])) / b14);
             d[7] = d[7] * nrl::Model<T>::ccor(z, rl, T(NRL_PDM(6, 5)) * T(NRL_PDL(0)[1]), T(NRL_PDM(6, 4)) * T(NRL_PDL(0)[0]));
@@ -618,7 +690,7 @@ struct Fast {
         globeTasks<L>(G, aptTlb, aptLast, j, groupBase);
         T d[9];
         const T zn2top = T(72.5);
-        gts7(alt > zn2top ? alt : zn2top, G, aptTlb, d, ms);
+        gts7<L>(alt > zn2top ? alt : zn2top, G, aptTlb, d, ms, j, groupBase);
         if (!(alt >= zn2top)) {
             apt0 = aptLast;
             return lowerAtmosphere(*this, alt, d, ms);
