@@ -397,6 +397,69 @@ struct Fast {
         return densu_temp * pow((t1 / *tz), (T(1.0) + alpha)) * exp(-expl);
     }
 
+    // densu below za shares everything but the altitude between calls with
+    // the same tinf / tlb: the temperature at za, the mesosphere node
+    // profile and its spline.  lowProfile forms that part once (with densu's
+    // side effect on the first node); densuBelow evaluates one call from it,
+    // in the same operations as densu.
+    struct LowProfile {
+        T xs[5], ys[5], y2[5];
+        T zgdif, t1, zg2, tt;
+    };
+    static __device__ __noinline__ void lowProfile(LowProfile& lp, T tinf, T tlb, T zlb, T s2, const T* zn1, T re,
+                                                   NrlMeso<T>& ms) {
+        auto zeta = [re](T zz, T zl) { return ((zz - zl) * (re + zl) / (re + zz)); };
+        const int mn1 = 5;
+        const T za = zn1[0];
+        lp.zg2 = zeta(za, zlb);
+        lp.tt = tinf - (tinf - tlb) * exp(-s2 * lp.zg2);
+        const T ta = lp.tt;
+        const T q = (re + zlb) / (re + za);
+        ms.tgn1[0] = (tinf - ta) * s2 * (q * q);
+        ms.tn1[0] = ta;
+        const T z1 = zn1[0];
+        const T z2 = zn1[mn1 - 1];
+        lp.t1 = ms.tn1[0];
+        const T t2 = ms.tn1[mn1 - 1];
+        lp.zgdif = zeta(z2, z1);
+        for (int k = 0; k < mn1; k++) {
+            lp.xs[k] = zeta(zn1[k], z1) / lp.zgdif;
+            lp.ys[k] = T(1.0) / ms.tn1[k];
+        }
+        const T r2 = (re + z2) / (re + z1);
+        const T yd1 = -ms.tgn1[0] / (lp.t1 * lp.t1) * lp.zgdif;
+        const T yd2 = -ms.tgn1[1] / (t2 * t2) * lp.zgdif * (r2 * r2);
+        nrl::Model<T>::spline(lp.xs, lp.ys, mn1, yd1, yd2, lp.y2);
+    }
+    static __device__ __noinline__ T densuBelow(T alt, T dlb, T tinf, T tlb, T xm, T alpha, T zlb, T s2,
+                                                const T* zn1, T re, T gsurf, const LowProfile& lp) {
+        auto zeta = [re](T zz, T zl) { return ((zz - zl) * (re + zl) / (re + zz)); };
+        const T rgas = T(831.4);
+        const int mn1 = 5;
+        const T z = (alt > zn1[mn1 - 1]) ? alt : zn1[mn1 - 1];
+        const T z1 = zn1[0];
+        const T zg = zeta(z, z1);
+        const T x = zg / lp.zgdif;
+        const T y = nrl::Model<T>::splint(lp.xs, lp.ys, lp.y2, mn1, x);
+        const T tz = T(1.0) / y;
+        if (xm == T(0)) return tz;
+        const T g1 = T(1.0) + zlb / re;
+        T glb = gsurf / (g1 * g1);
+        const T gamma = xm * glb / (s2 * rgas * tinf);
+        T expl = exp(-s2 * gamma * lp.zg2);
+        if (expl > T(50.0)) expl = T(50.0);
+        if (lp.tt <= T(0)) expl = T(50.0);
+        const T densu_temp = dlb * pow((tlb / lp.tt), ((T(1.0) + alpha + gamma))) * expl;
+        const T g2 = T(1.0) + z1 / re;
+        glb = gsurf / (g2 * g2);
+        const T gamm = xm * glb * lp.zgdif / rgas;
+        const T yi = nrl::Model<T>::splini(lp.xs, lp.ys, lp.y2, mn1, x);
+        expl = gamm * yi;
+        if (expl > T(50.0)) expl = T(50.0);
+        if (tz <= T(0)) expl = T(50.0);
+        return densu_temp * pow((lp.t1 / tz), (T(1.0) + alpha)) * exp(-expl);
+    }
+
     // The 11 globe7 values of one gts7 call (task order above), with the ap
     // response apt0 left by the pd[3] table (used by the mesosphere glob7s
     // terms) and by the last table (used below 72.5 km).  L lanes of a group
@@ -537,6 +600,8 @@ struct Fast {
                 default: return z <= T(450.0);
             }
         };
+        LowProfile low;
+        if (needTask(0)) lowProfile(low, tinf, tlb, zlb, s, zn1, re, ms);
         auto corrTask = [&](int t, T& bOut, T& dmOut) {
             T zb, xm, al, pdm0, pd0, g;
             switch (t) {
@@ -549,9 +614,18 @@ struct Fast {
                 default: zb = T(NRL_PDM(6, 2)); xm = T(14.); al = T(-1.); pdm0 = T(NRL_PDM(6, 0)); pd0 = T(NRL_PD(7)[0]); g = G[9]; break;
             }
             const T db = pdm0 * exp(g) * pd0;
-            bOut = densu(zb, db, tinf, tlb, xm - xmm, al, &dummyT, zlb, s, zn1, re, gsurf, ms);
-            dmOut = (t != 0 || z <= T(160.0)) ? densu(z, bOut, tinf, tlb, xmm, T(0.0), &dummyT, zlb, s, zn1, re, gsurf, ms)
-                                               : T(0.0);
+            bOut = zb < za ? densuBelow(zb, db, tinf, tlb, xm - xmm, al, zlb, s, zn1, re, gsurf, low)
+                           : densu(zb, db, tinf, tlb, xm - xmm, al, &dummyT, zlb, s, zn1, re, gsurf, ms);
+            dmOut = T(0.0);
+            if (t != 0 || z <= T(160.0)) {
+                if (direct) {
+                    // densu(z, b, tinf, tlb, xmm, 0) above za, from the shared profile
+                    const T gamma = xmm * kGamma;
+                    dmOut = bOut * exp((T(1.0) + gamma) * lnX - s * gamma * zg2);
+                } else {
+                    dmOut = densu(z, bOut, tinf, tlb, xmm, T(0.0), &dummyT, zlb, s, zn1, re, gsurf, ms);
+                }
+            }
         };
         T bv[7], dmv[7];
 #pragma unroll
