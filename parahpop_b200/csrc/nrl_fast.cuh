@@ -528,11 +528,13 @@ struct Fast {
         const T tlb = T(NRL_PTM(1)) * (T(1.0) + G[2]) * T(NRL_PD(3)[0]);
         const T s = g0v / (tinf - tlb);
         const T ptl30 = T(NRL_PTM(4)) * T(NRL_PTL(3)[0]);
-        if (z < T(300.0)) {
+        // the five glob7s tables of the mesosphere nodes (ptl[0..3], pma[8]),
+        // evaluated on all converged lanes when any object is below 300 km;
+        // L > 1 lanes share them as for globe7
+        T gs[5];
+        const bool meso = z < T(300.0);
+        if (__any_sync(__activemask(), meso)) {
             apt0 = aptTlb;
-            // the five glob7s tables of the mesosphere nodes (ptl[0..3], pma[8]);
-            // L > 1 lanes share them as for globe7
-            T gs[5];
             if (L == 1) {
 #pragma unroll
                 for (int k = 0; k < 5; ++k) gs[k] = glob7s(k < 4 ? k : 12);
@@ -548,6 +550,8 @@ struct Fast {
                         if (r * L + jj < 5) gs[r * L + jj] = __shfl_sync(mask, v, groupBase + jj);
                 }
             }
+        }
+        if (meso) {
             meso_tn1[1] = T(NRL_PTM(6)) * T(NRL_PTL(0)[0]) / (T(1.0) - gs[0]);
             meso_tn1[2] = T(NRL_PTM(2)) * T(NRL_PTL(1)[0]) / (T(1.0) - gs[1]);
             meso_tn1[3] = T(NRL_PTM(7)) * T(NRL_PTL(2)[0]) / (T(1.0) - gs[2]);
@@ -600,8 +604,18 @@ struct Fast {
                 default: return z <= T(450.0);
             }
         };
+        // Tasks any object of the converged lanes needs run on all of them
+        // (results unused where not needed): objects of one warp differ by a
+        // few km in altitude, and running each one's own subset would split
+        // the warp into serialised paths.
+        unsigned needBits = 0;
+#pragma unroll
+        for (int t = 0; t < 7; ++t)
+            if (needTask(t)) needBits |= 1u << t;
+        needBits = __reduce_or_sync(__activemask(), needBits);
+        auto taskOn = [&](int t) { return (needBits >> t) & 1u; };
         LowProfile low;
-        if (needTask(0)) lowProfile(low, tinf, tlb, zlb, s, zn1, re, ms);
+        if (taskOn(0)) lowProfile(low, tinf, tlb, zlb, s, zn1, re, ms);
         auto corrTask = [&](int t, T& bOut, T& dmOut) {
             T zb, xm, al, pdm0, pd0, g;
             switch (t) {
@@ -633,8 +647,8 @@ struct Fast {
         if (L == 1) {
 #pragma unroll
             for (int t = 0; t < 7; ++t)
-                if (needTask(t)) corrTask(t, bv[t], dmv[t]);
-        } else if (needTask(0)) {  // every other task's limit is below N2's
+                if (taskOn(t)) corrTask(t, bv[t], dmv[t]);
+        } else if (taskOn(0)) {  // every other task's limit is below N2's
             // slots in order of decreasing altitude limit (N2, N, H, O, O2, Ar,
             // He), so the tasks active at an altitude fill the first rounds
             constexpr int kSlot[7] = {0, 6, 5, 2, 3, 4, 1};
@@ -645,7 +659,7 @@ struct Fast {
                 T bb = T(0.0), dd = T(0.0);
                 if (k < 7) {
                     const int t = k == 0 ? 0 : k == 1 ? 6 : k == 2 ? 5 : k == 3 ? 2 : k == 4 ? 3 : k == 5 ? 4 : 1;
-                    if (needTask(t)) corrTask(t, bb, dd);
+                    if (taskOn(t)) corrTask(t, bb, dd);
                 }
 #pragma unroll
                 for (int jj = 0; jj < L; ++jj) {

@@ -39,6 +39,17 @@ def test_null_context_calls_fail_cleanly():
     assert lib.phop_propagate_device(None, 1, None, 0.0, D(z), D(z), D(z), D(z), D(z), 1.0, 1.0, D(z)) == 1
     assert lib.phop_set_option(None, b"lanes", 4.0) == 1
     assert lib.phop_last_stats(None, None) == 1
+    out = C.c_void_p()
+    assert lib.phop_server_create(None, 16, 20.0, C.byref(out)) == 1
+    rid = C.c_int64()
+    assert lib.phop_server_submit(None, 1, D(z), D(z), D(z), D(z), D(z), D(z), D(z), None, None, C.byref(rid)) == 1
+    assert lib.phop_server_step(None, None) == 1
+    assert lib.phop_server_take(None, 1, D(z), D(z), D(z), D(z)) == 1
+    assert lib.phop_server_get_stats(None, None) == 1
+    f = lib.phop_propagate_device_noalloc
+    f.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double,
+                  C.POINTER(C.c_double)]
+    assert f(None, 1, None, None, None, 0.0, 1.0, 1.0, None) == 1
 
 
 def _has_gpu():
