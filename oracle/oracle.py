@@ -31,7 +31,7 @@ LIB = HERE / "lib" / "liboracle.so"
 NAIF = {"Sun": 10, "Moon": 301, "Earth": 399, "MercuryBarycenter": 1, "VenusBarycenter": 2, "MarsBarycenter": 4,
         "JupiterBarycenter": 5, "SaturnBarycenter": 6, "UranusBarycenter": 7, "NeptuneBarycenter": 8,
         "PlutoBarycenter": 9}
-F_GRAVITY, F_SHAPE, F_RADIATION, F_ATMOSPHERE, F_OCCULTING = 1, 2, 4, 8, 16
+F_GRAVITY, F_SHAPE, F_RADIATION, F_ATMOSPHERE, F_OCCULTING, F_OBLATENESS = 1, 2, 4, 8, 16, 32
 
 
 def build(force=False):
@@ -117,6 +117,8 @@ class _Env(C.Structure):
         ("nrl_density_scale", C.c_double), ("nrl_weather", C.POINTER(C.c_double)),
         ("solid", C.c_int), ("ocean", C.c_int), ("relativity", C.c_int), ("zero_tide", C.c_int),
         ("eop_n", C.c_int), ("eop_first_mjd", C.c_double), ("eop", C.POINTER(C.c_double)),
+        ("body_j2", C.POINTER(C.c_double)), ("body_gm_const", C.POINTER(C.c_double)),
+        ("body_soi", C.POINTER(C.c_double)), ("n_exp", C.c_int), ("exp_seg", C.POINTER(C.c_double)),
     ]
 
 
@@ -169,6 +171,7 @@ def load_environment(config_path) -> Environment:
     flattening = 0.0
     shape = None
     atm = None
+    exp_segments = []
     for name, bc in envc["bodies"].items():
         nid = NAIF[name]
         flags = 0
@@ -178,24 +181,48 @@ def load_environment(config_path) -> Environment:
             if isinstance(g, dict) and "shape" in g:
                 flags |= F_SHAPE
                 shape = g["shape"]
+            if (isinstance(g, dict) and g.get("oblateness")) or (isinstance(g, list) and "oblateness" in g):
+                flags |= F_OBLATENESS
         if bc.get("radiation"):
             flags |= F_RADIATION
         if "atmosphere" in bc:
             flags |= F_ATMOSPHERE
-            atm = bc["atmosphere"]["nrlmsise00"]
+            model = {k.lower(): v for k, v in bc["atmosphere"].items()}
+            if "nrlmsise00" in model or "nrlmsise-00" in model:
+                atm = model.get("nrlmsise00", model.get("nrlmsise-00"))
+            else:
+                blocks = model["exponential"]
+                blocks = blocks if isinstance(blocks, list) else [blocks]
+                segs = []
+                for b in blocks:
+                    b = {k.lower(): v for k, v in b.items()}
+                    segs.append((b["h0"], b["rho0"], b["scaleheight"], b["hcutoff"]))
+                segs.sort()
+                exp_segments = segs
         if bc.get("occulting"):
             flags |= F_OCCULTING
         if name == "Earth":
             flattening = bc.get("flattening", 0.0)
-        gm = bc.get("gm", byid.get(nid, {}).get("GM", 0.0))
-        radius = byid.get(nid, {}).get("R", 0.0)
-        rows.append((nid, gm, radius, flags))
+        cst = byid.get(nid, {})
+        gm = bc.get("gm", cst.get("GM", 0.0))
+        radius = cst.get("R", 0.0)
+        soi = cst.get("SOIOld", cst.get("SOI", 1e20))
+        rows.append((nid, gm, radius, flags, cst.get("J2", 0.0), cst.get("GM", 0.0), soi))
     rows.sort()
     e.nbodies = len(rows)
     e.body_id = _ip(hold(np.array([r[0] for r in rows], dtype=np.int32)))
     e.body_gm = _dp(hold(np.array([r[1] for r in rows], dtype=np.float64)))
     e.body_radius = _dp(hold(np.array([r[2] for r in rows], dtype=np.float64)))
     e.body_flags = _ip(hold(np.array([r[3] for r in rows], dtype=np.int32)))
+    e.body_j2 = _dp(hold(np.array([r[4] for r in rows], dtype=np.float64)))
+    e.body_gm_const = _dp(hold(np.array([r[5] for r in rows], dtype=np.float64)))
+    e.body_soi = _dp(hold(np.array([r[6] for r in rows], dtype=np.float64)))
+    e.n_exp = len(exp_segments)
+    if exp_segments:
+        # component-major: rho0, h0, scaleHeight, hCutoff
+        seg = np.array([[s[1] for s in exp_segments], [s[0] for s in exp_segments],
+                        [s[2] for s in exp_segments], [s[3] for s in exp_segments]], dtype=np.float64)
+        e.exp_seg = _dp(hold(np.ascontiguousarray(seg.reshape(-1))))
     e.flattening = flattening
     # geopotential
     if shape is not None:

@@ -41,7 +41,7 @@
 
 extern "C" {
 
-enum { F_GRAVITY = 1, F_SHAPE = 2, F_RADIATION = 4, F_ATMOSPHERE = 8, F_OCCULTING = 16 };
+enum { F_GRAVITY = 1, F_SHAPE = 2, F_RADIATION = 4, F_ATMOSPHERE = 8, F_OCCULTING = 16, F_OBLATENESS = 32 };
 
 typedef struct {
     // geopotential (normalised), triangle index n(n+1)/2+m
@@ -77,6 +77,12 @@ typedef struct {
     int eop_n;
     double eop_first_mjd;
     const double* eop;  // 4 x n: xp, yp, ut1-utc, tai-utc (component-major)
+    // oblateness (J2) model and exponential atmosphere
+    const double* body_j2;        // per body, from the constants file (0 when absent)
+    const double* body_gm_const;  // per body GM from the constants file (the J2 model's)
+    const double* body_soi;       // per body sphere of influence, km (1e20 when absent)
+    int n_exp;                    // exponential atmosphere bands (0: none)
+    const double* exp_seg;        // 4 x n_exp component-major: rho0, h0, scaleHeight, hCutoff; ascending h0
 } OracleEnv;
 
 }  // extern "C"
@@ -699,6 +705,43 @@ V3 earthCorrections(const OracleEnv& e, V3 pos, V3 vel, double et) {
             1.0e-3 * (solid[2] + ocean[2] + rel[2])};
 }
 
+// ---- oblateness and exponential drag --------------------------------------------
+// J2 acceleration in the body frame (J2.h:17-33)
+V3 j2BodyFixed(V3 p, double gm, double j2, double radius) {
+    const double invr = 1.0 / norm(p);
+    const double invr2 = invr * invr;
+    const double invr5 = invr2 * invr2 * invr;
+    const double base = 1.0 - 5.0 * (p.z * p.z) * invr2;
+    const double c = -1.5 * gm * j2 * invr5 * radius * radius;
+    return V3{c * p.x * base, c * p.y * base, c * p.z * (base + 2.0)};
+}
+
+// Geodetic altitude about the body's polar axis (atmosphere/Geodetic.h:40-75)
+double geodeticAltitude(V3 r, V3 pole, double Req, double flattening) {
+    if (flattening == 0.0) return norm(r) - Req;
+    const double r2 = dot(r, r);
+    const double z = dot(r, pole);
+    const double xy = r2 - z * z;
+    const double flatsq = (2.0 - flattening) * flattening;
+    double d0 = 0.0, d = 1e10, sfq = 0.0, zd = z;
+    while (std::fabs(d - d0) > 1e-9) {
+        d0 = d;
+        const double z2 = zd * zd;
+        sfq = z2 / (xy + z2);
+        d = Req * flatsq * std::sqrt(sfq / (1.0 - flatsq * sfq));
+        zd = z + std::copysign(d, z);
+    }
+    return std::sqrt(xy + zd * zd) - Req / std::sqrt(1.0 - flatsq * sfq);
+}
+
+// Piecewise exponential profile: band = number of bands above the first
+// whose base h0 <= h (PiecewiseExponentialAtmosphere.h:40-90)
+int expBand(const OracleEnv& e, double h) {
+    int band = 0;
+    for (int s = 1; s < e.n_exp; ++s) band += e.exp_seg[e.n_exp + s] <= h ? 1 : 0;
+    return band;
+}
+
 // ---- right-hand side ----------------------------------------------------------
 struct Object {
     double mass, area, cd, cr;  // area km^2, cr folded with srp/drag area ratio
@@ -708,7 +751,6 @@ V3 acceleration(const OracleEnv& e, const ShFactors& F, V3 pos, V3 vel, double e
     V3 acc = {0, 0, 0};
     const double AMS = o.cr * o.area / o.mass;
     const double BC = o.cd * o.area / o.mass;
-    (void)BC;
     bool haveRot = false;
     double R[9];
     V3 w = {0, 0, 0};
@@ -733,6 +775,17 @@ V3 acceleration(const OracleEnv& e, const ShFactors& F, V3 pos, V3 vel, double e
             }
             acc = acc + matT(R, shBodyFixed(e, F, mat(R, dp)));
         }
+        if ((fl & F_OBLATENESS) && !(fl & F_SHAPE)) {
+            // J2 model (PrivateAccelerations.h:88-97, J2.h:63-78)
+            const V3 dp = (body != kEarth) ? pos - bodyPos : pos;
+            if (norm(dp) <= e.body_soi[bi]) {
+                if (!haveRot) {
+                    earthRotation(e, et, R, &w);
+                    haveRot = true;
+                }
+                acc = acc + matT(R, j2BodyFixed(mat(R, dp), e.body_gm_const[bi], e.body_j2[bi], e.body_radius[bi]));
+            }
+        }
         if (fl & F_RADIATION) {
             const V3 dp = pos - bodyPos;
             double occ = 1.0;
@@ -751,6 +804,22 @@ V3 acceleration(const OracleEnv& e, const ShFactors& F, V3 pos, V3 vel, double e
                 acc = acc + occ * srp;
             } else {
                 acc = acc + srp;
+            }
+        }
+        if ((fl & F_ATMOSPHERE) && !e.has_nrl && e.n_exp > 0) {
+            // exponential drag (PrivateAccelerations.h:137-206)
+            if (!haveRot) {
+                earthRotation(e, et, R, &w);
+                haveRot = true;
+            }
+            const V3 pole = {R[6], R[7], R[8]};  // body z axis in inertial axes
+            const double h = geodeticAltitude(pos, pole, e.body_radius[bi], e.flattening);
+            const int band = expBand(e, h);
+            const int n = e.n_exp;
+            if (h <= e.exp_seg[3 * n + band]) {
+                const V3 vr = vel - cross(w, pos);
+                const double rho = e.exp_seg[band] * std::exp(-(h - e.exp_seg[n + band]) / e.exp_seg[2 * n + band]);
+                acc = acc + ((-0.5 * rho * BC * norm(vr)) * vr);
             }
         }
         if ((fl & F_ATMOSPHERE) && e.has_nrl) {

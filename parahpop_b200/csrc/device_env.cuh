@@ -29,7 +29,9 @@ constexpr int kMaxBodies = 12;
 constexpr int kMaxChain = 4;
 constexpr int kTideTri = 28;  // n <= 6 triangle, index n(n+1)/2 + m
 
-enum BodyFlag : int { kGravity = 1, kShape = 2, kRadiation = 4, kAtmosphere = 8, kOcculting = 16 };
+constexpr int kMaxExpBands = 16;
+
+enum BodyFlag : int { kGravity = 1, kShape = 2, kRadiation = 4, kAtmosphere = 8, kOcculting = 16, kOblateness = 32 };
 
 struct DevEnv {
     // geopotential (normalised), triangle n(n+1)/2+m, device pointers
@@ -52,6 +54,12 @@ struct DevEnv {
     int moonUnitsPlus[kMaxChain], moonUnitsMinus[kMaxChain];
     double flattening, au, earthRadius;
     int anyOcculter;
+    // oblateness (J2) model: constants-file J2, GM and sphere of influence
+    double bodyJ2[kMaxBodies], bodyGmConst[kMaxBodies], bodySoi[kMaxBodies];
+    // exponential atmosphere (when no NRLMSISE-00): bands ascending in h0,
+    // each {rho0 (kg/km^3), h0, scaleHeight, hCutoff (km)}
+    int nExp;
+    double expSeg[kMaxExpBands][4];
     // Type-2 Chebyshev units
     int neph;
     const int* ephNint;

@@ -46,6 +46,10 @@ static void loadConstants(const std::string& path, HostEnvironment& env) {
             const int nid = (int)id->asInt();
             if (const Value* gm = item.find("GM")) env.constGm[nid] = gm->asDouble();
             if (const Value* r = item.find("R")) env.constRadius[nid] = r->asDouble();
+            // ConstantsJson.h:57-76: J2 defaults to 0, SOIOld takes precedence over SOI
+            env.constJ2[nid] = item.find("J2") ? item.at("J2").asDouble() : 0.0;
+            env.constSoi[nid] = item.find("SOIOld") ? item.at("SOIOld").asDouble()
+                                                    : (item.find("SOI") ? item.at("SOI").asDouble() : 1e20);
         }
     }
     if (env.au <= 0) throw std::runtime_error("Constants file lacks AU: " + path);
@@ -283,6 +287,49 @@ static void loadEop(const std::string& path, HostEnvironment& env) {
         for (int k = 0; k < 4; ++k) env.eop[(size_t)k * n + i] = rec[i][k + 1];
 }
 
+// Piecewise exponential atmosphere: one block or a list of blocks
+// {rho0, h0, scaleHeight, hCutoff} (interface Atmosphere.h:436-508, 337-350).
+static void loadExponentialAtmosphere(const Value& v, HostEnvironment& env) {
+    std::vector<const Value*> blocks;
+    if (v.isArray()) {
+        if (v.size() == 0) throw std::runtime_error("Piecewise atmosphere list must contain at least one block.");
+        for (const Value& b : v.items()) blocks.push_back(&b);
+    } else if (v.isObject()) {
+        blocks.push_back(&v);
+    } else {
+        throw std::runtime_error("Exponential atmosphere must be an object (single block) or a list of objects "
+                                 "(piecewise).");
+    }
+    env.expSeg.clear();
+    for (const Value* b : blocks) {
+        if (!b->isObject()) throw std::runtime_error("Each exponential atmosphere block must be an object.");
+        std::array<double, 4> seg{0.0, 0.0, 1.0, 0.0};
+        bool found[4] = {false, false, false, false};
+        for (const auto& kv : b->members()) {
+            std::string k = kv.first;
+            std::transform(k.begin(), k.end(), k.begin(), ::tolower);
+            const int idx = k == "rho0" ? 0 : k == "h0" ? 1 : k == "scaleheight" ? 2 : k == "hcutoff" ? 3 : -1;
+            if (idx < 0) throw std::runtime_error("Unsupported atmosphere option: " + kv.first);
+            seg[idx] = kv.second.asDouble();
+            found[idx] = true;
+        }
+        if (!found[0]) throw std::runtime_error("Atmosphere rho0 not specified.");
+        if (!found[1]) throw std::runtime_error("Atmosphere h0 not specified.");
+        if (!found[2]) throw std::runtime_error("Atmosphere scaleHeight not specified.");
+        if (!found[3]) throw std::runtime_error("Atmosphere hCutoff not specified.");
+        if (!(seg[0] >= 0.0)) throw std::runtime_error("Atmosphere rho0 must be non-negative.");
+        if (!(seg[2] > 0.0)) throw std::runtime_error("Atmosphere scaleHeight must be positive.");
+        env.expSeg.push_back(seg);
+    }
+    std::sort(env.expSeg.begin(), env.expSeg.end(), [](const auto& a, const auto& b) { return a[1] < b[1]; });
+    for (size_t i = 1; i < env.expSeg.size(); ++i)
+        if (!(env.expSeg[i][1] >= env.expSeg[i - 1][3]))
+            throw std::runtime_error("Overlapping atmosphere segments: a band with h0=" + std::to_string(env.expSeg[i][1])
+                                     + " km starts below the previous band's hCutoff="
+                                     + std::to_string(env.expSeg[i - 1][3]) + " km.");
+    if (env.expSeg.size() > (size_t)kMaxExpBands) throw std::runtime_error("Too many atmosphere bands for this backend.");
+}
+
 void loadEnvironment(const Value& model, HostEnvironment& env) {
     const Value& e = model.at("environment");
     for (const auto& kv : e.members()) {
@@ -307,10 +354,33 @@ void loadEnvironment(const Value& model, HostEnvironment& env) {
                     if (f.second.asBool()) b.flags |= kGravity;
                 } else if (f.second.isObject()) {
                     b.flags |= kGravity;
-                    if (const Value* sh = f.second.find("shape")) {
-                        if (b.id != 399) throw std::runtime_error("Spherical-harmonic gravity is supported for the Earth only.");
-                        b.flags |= kShape;
-                        loadShTable(*sh, env);
+                    for (const auto& g : f.second.members()) {
+                        std::string gk = g.first;
+                        std::transform(gk.begin(), gk.end(), gk.begin(), ::tolower);
+                        if (gk == "shape") {
+                            if (b.id != 399)
+                                throw std::runtime_error("Spherical-harmonic gravity is supported for the Earth only.");
+                            b.flags |= kShape;
+                            loadShTable(g.second, env);
+                        } else if (gk == "oblateness") {
+                            if (g.second.isBool() ? g.second.asBool() : !g.second.isNull()) {
+                                if (b.id != 399)
+                                    throw std::runtime_error("The oblateness (J2) model is supported for the Earth only.");
+                                b.flags |= kOblateness;
+                            }
+                        } else {
+                            throw std::runtime_error("Unsupported gravity feature for " + b.name + ": " + g.first);
+                        }
+                    }
+                } else if (f.second.isArray()) {
+                    b.flags |= kGravity;
+                    for (const Value& g : f.second.items()) {
+                        std::string gk = g.asString();
+                        std::transform(gk.begin(), gk.end(), gk.begin(), ::tolower);
+                        if (gk != "oblateness")
+                            throw std::runtime_error("Unsupported gravity feature for " + b.name + ": " + g.asString());
+                        if (b.id != 399) throw std::runtime_error("The oblateness (J2) model is supported for the Earth only.");
+                        b.flags |= kOblateness;
                     }
                 } else {
                     throw std::runtime_error("Body gravity must be a boolean or an object: " + b.name);
@@ -324,17 +394,28 @@ void loadEnvironment(const Value& model, HostEnvironment& env) {
                 if (f.second.asBool()) b.flags |= kOcculting;
             } else if (k == "atmosphere") {
                 if (b.id != 399) throw std::runtime_error("Atmospheric drag is supported for the Earth only.");
-                const Value* nrl = f.second.find("nrlmsise00");
-                if (!nrl) throw std::runtime_error("Only the nrlmsise00 atmosphere is supported by this backend.");
+                // single-key model dispatch (interface Atmosphere.h:136-166)
+                if (!f.second.isObject() || f.second.size() != 1)
+                    throw std::runtime_error("Atmosphere block must be a single-key dispatch dict naming the model.");
+                std::string mk = f.second.members()[0].first;
+                std::transform(mk.begin(), mk.end(), mk.begin(), ::tolower);
+                const Value& mv = f.second.members()[0].second;
                 b.flags |= kAtmosphere;
-                atmosphere = nrl;
+                if (mk == "nrlmsise00" || mk == "nrlmsise-00") {
+                    atmosphere = &mv;
+                } else if (mk == "exponential") {
+                    loadExponentialAtmosphere(mv, env);
+                } else {
+                    throw std::runtime_error("Unknown atmosphere model: '" + f.second.members()[0].first
+                                             + "'.  Supported: exponential, nrlmsise00.");
+                }
             } else if (k == "flattening") {
                 if (b.id == 399) env.flattening = f.second.asDouble();
             } else if (k == "gm") {
                 b.gm = f.second.asDouble();
-            } else if (k == "oblateness") {
-                if (f.second.isBool() ? f.second.asBool() : true)
-                    throw std::runtime_error("The oblateness (J2) model is not supported by this backend.");
+            } else if (k == "oblateness" || k == "shape") {
+                throw std::runtime_error("Gravity sub-features (oblateness, shape) must be nested under the gravity "
+                                         "block of " + b.name + ".");
             } else {
                 throw std::runtime_error("Unsupported body option for " + b.name + ": " + k);
             }
@@ -346,6 +427,9 @@ void loadEnvironment(const Value& model, HostEnvironment& env) {
         }
         auto r = env.constRadius.find(b.id);
         b.radius = r != env.constRadius.end() ? r->second : 0.0;
+        if (env.constJ2.count(b.id)) b.j2 = env.constJ2[b.id];
+        if (env.constGm.count(b.id)) b.gmConst = env.constGm[b.id];
+        if (env.constSoi.count(b.id)) b.soi = env.constSoi[b.id];
         env.bodies.push_back(b);
     }
     std::sort(env.bodies.begin(), env.bodies.end(), [](auto& a, auto& b) { return a.id < b.id; });
@@ -501,6 +585,9 @@ void Engine::uploadEnvironment() {
         e.bodyFlags[b] = B.flags;
         e.bodyGm[b] = B.gm;
         e.bodyRadius[b] = B.radius;
+        e.bodyJ2[b] = B.j2;
+        e.bodyGmConst[b] = B.gmConst;
+        e.bodySoi[b] = B.soi;
         if (B.id == 10) e.sunIndex = b;
         if (B.id == 301) e.moonIndex = b;
         if (B.id == 399) e.earthIndex = b;
@@ -508,6 +595,9 @@ void Engine::uploadEnvironment() {
         chainUnits(h, B.id, 399, e.chainPlus[b], e.chainMinus[b]);
     }
     e.anyOcculter = anyOcc;
+    e.nExp = (int)h.expSeg.size();
+    for (int k = 0; k < e.nExp; ++k)
+        for (int c = 0; c < 4; ++c) e.expSeg[k][c] = h.expSeg[k][c];
     e.earthRadius = h.bodies[e.earthIndex].radius;
     e.flattening = h.flattening;
     e.au = h.au;

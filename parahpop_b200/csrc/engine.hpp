@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cstdint>
 #include <map>
 #include <memory>
@@ -29,13 +30,14 @@ struct EphUnitHost {
 struct HostEnvironment {
     // constants
     double au = 0.0;
-    std::map<int, double> constGm, constRadius;
+    std::map<int, double> constGm, constRadius, constJ2, constSoi;
     // bodies sorted by NAIF id
     struct Body {
         std::string name;
         int id = 0;
         int flags = 0;
         double gm = 0.0, radius = 0.0;
+        double j2 = 0.0, gmConst = 0.0, soi = 1e20;  // oblateness model (constants file)
     };
     std::vector<Body> bodies;
     double flattening = 0.0;
@@ -51,6 +53,8 @@ struct HostEnvironment {
     int rotNnut = 0, rotNerp = 0;
     double rotStart = 0.0, rotFinal = 0.0;
     std::vector<double> rotData;
+    // exponential atmosphere bands {rho0, h0, scaleHeight, hCutoff}, ascending h0
+    std::vector<std::array<double, 4>> expSeg;
     // NRLMSISE-00
     bool hasNrl = false;
     double nrlStartMjd = 0.0, nrlHcutoff = 1000.0, nrlDensityScale = 1.0;

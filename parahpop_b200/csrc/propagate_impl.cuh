@@ -353,6 +353,26 @@ static __device__ __noinline__ double nrlDensity(const DevEnv& e, const EpochRec
     return (rhoSi * 1.0e9) * e.nrlDensityScale;
 }
 
+// Geodetic altitude about the polar axis `pole` (atmosphere/Geodetic.h:40-75);
+// the fixed-point iteration converges quadratically, bounded here.
+static __device__ __forceinline__ double geodeticHeight(const double r[3], const double pole[3], double Req,
+                                                        double flattening) {
+    const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    if (flattening == 0.0) return sqrt(r2) - Req;
+    const double z = r[0] * pole[0] + r[1] * pole[1] + r[2] * pole[2];
+    const double xy = r2 - z * z;
+    const double flatsq = (2.0 - flattening) * flattening;
+    double d0 = 0.0, d = 1e10, sfq = 0.0, zd = z;
+    for (int it = 0; it < 64 && fabs(d - d0) > 1e-9; ++it) {
+        d0 = d;
+        const double z2 = zd * zd;
+        sfq = z2 / (xy + z2);
+        d = Req * flatsq * sqrt(sfq / (1.0 - flatsq * sfq));
+        zd = z + copysign(d, z);
+    }
+    return sqrt(xy + zd * zd) - Req / sqrt(1.0 - flatsq * sfq);
+}
+
 // full right-hand side acceleration (km/s^2); every lane of the group calls it
 template <int L, typename T>
 static __device__ __forceinline__ void accelerations(const StepParams& p, const typename TileOf<T>::type* tile,
@@ -403,6 +423,25 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
             ay += R[1] * a[0] + R[4] * a[1] + R[7] * a[2];
             az += R[2] * a[0] + R[5] * a[1] + R[8] * a[2];
         }
+        if ((fl & kOblateness) && !(fl & kShape)) {
+            // J2 model in the body frame (J2.h:17-33,63-78), inside the sphere of influence
+            const double* R = r.R;
+            const double rr = sqrt(pos[0] * pos[0] + pos[1] * pos[1] + pos[2] * pos[2]);
+            if (rr <= e.bodySoi[bi]) {
+                const double bx = R[0] * pos[0] + R[1] * pos[1] + R[2] * pos[2];
+                const double by = R[3] * pos[0] + R[4] * pos[1] + R[5] * pos[2];
+                const double bz = R[6] * pos[0] + R[7] * pos[1] + R[8] * pos[2];
+                const double invr = 1.0 / sqrt(bx * bx + by * by + bz * bz);
+                const double invr2 = invr * invr;
+                const double invr5 = invr2 * invr2 * invr;
+                const double base = 1.0 - 5.0 * (bz * bz) * invr2;
+                const double c = -1.5 * e.bodyGmConst[bi] * e.bodyJ2[bi] * invr5 * e.bodyRadius[bi] * e.bodyRadius[bi];
+                const double a0 = c * bx * base, a1 = c * by * base, a2 = c * bz * (base + 2.0);
+                ax += R[0] * a0 + R[3] * a1 + R[6] * a2;
+                ay += R[1] * a0 + R[4] * a1 + R[7] * a2;
+                az += R[2] * a0 + R[5] * a1 + R[8] * a2;
+            }
+        }
         if (fl & kRadiation) {
             const double* rb = r.body[bi];
             const double dp[3] = {pos[0] - rb[0], pos[1] - rb[1], pos[2] - rb[2]};
@@ -420,6 +459,26 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
             ax += f * dp[0];
             ay += f * dp[1];
             az += f * dp[2];
+        }
+        if ((fl & kAtmosphere) && !e.hasNrl && e.nExp > 0) {
+            // piecewise exponential drag (PrivateAccelerations.h:137-206,
+            // PiecewiseExponentialAtmosphere.h:40-90): band = bands above the
+            // first whose base h0 <= h; no drag above the band's cut-off
+            const double pole[3] = {r.R[6], r.R[7], r.R[8]};  // body z axis in inertial axes
+            const double h = geodeticHeight(pos, pole, e.bodyRadius[bi], e.flattening);
+            int band = 0;
+            for (int sgi = 1; sgi < e.nExp; ++sgi) band += e.expSeg[sgi][1] <= h ? 1 : 0;
+            if (h <= e.expSeg[band][3]) {
+                const double rho = e.expSeg[band][0] * exp(-(h - e.expSeg[band][1]) / e.expSeg[band][2]);
+                const double* w = r.w;
+                const double vr0 = vel[0] - (w[1] * pos[2] - w[2] * pos[1]);
+                const double vr1 = vel[1] - (w[2] * pos[0] - w[0] * pos[2]);
+                const double vr2 = vel[2] - (w[0] * pos[1] - w[1] * pos[0]);
+                const double f = -0.5 * rho * bc * sqrt(vr0 * vr0 + vr1 * vr1 + vr2 * vr2);
+                ax += f * vr0;
+                ay += f * vr1;
+                az += f * vr2;
+            }
         }
         if ((fl & kAtmosphere) && e.hasNrl) {
             const double* R = r.R;

@@ -486,22 +486,44 @@ def write_environment(directory, spec: EnvSpec = EnvSpec()) -> Path:
     return d
 
 
+# Exponential atmosphere bands (rho0 in kg/km^3 = SI x 1e9, heights in km):
+# textbook base densities and scale heights of a static exponential model.
+EXPONENTIAL_BANDS = [
+    {"rho0": 2.418e-2, "h0": 300.0, "scaleHeight": 53.628, "hCutoff": 500.0},
+    {"rho0": 6.967e-4, "h0": 500.0, "scaleHeight": 63.822, "hCutoff": 700.0},
+    {"rho0": 3.614e-5, "h0": 700.0, "scaleHeight": 88.667, "hCutoff": 1000.0},
+]
+
+
 def make_config(env_dir, duration, step, max_steps=1000000, threads=1, force="full",
                 degree=70, bodies=("Sun", "Moon", "JupiterBarycenter"), tides=True,
-                relativity=True, drag=True, srp=True, start_mjd=4016.0, end_mjd=4064.0) -> dict:
+                relativity=True, drag=True, srp=True, start_mjd=4016.0, end_mjd=4064.0,
+                gravity="shape", atmosphere="nrlmsise00") -> dict:
     """Run configuration in the reference schema (``example/config/envisat_full.json``).
-    Paths are relative to ``env_dir`` (where the config file is written)."""
+    Paths are relative to ``env_dir`` (where the config file is written).
+    ``gravity``: "shape" (the spherical-harmonic file) or "oblateness" (the
+    J2 model from the constants file); ``atmosphere``: "nrlmsise00",
+    "exponential" (one band) or "piecewise" (three bands)."""
     earth: dict = {}
     if force == "central":
         earth = {"gravity": True}
     else:
-        earth = {"occulting": True, "flattening": 0.0033528106647474805,
-                 "gravity": {"shape": {"body": "Earth", "file": "gravity.tab", "delimiter": ",",
-                                       "headerLines": 0, "degree": degree, "order": degree}}}
+        if gravity == "oblateness":
+            grav = {"oblateness": True}
+        else:
+            grav = {"shape": {"body": "Earth", "file": "gravity.tab", "delimiter": ",",
+                              "headerLines": 0, "degree": degree, "order": degree}}
+        earth = {"occulting": True, "flattening": 0.0033528106647474805, "gravity": grav}
         if drag and force == "full":
-            earth["atmosphere"] = {"nrlmsise00": {
-                "spaceWeatherFile": "SW-All.txt", "coverageStartMjdUtc": start_mjd + 51544.0 - 1.0,
-                "coverageEndMjdUtc": end_mjd + 51544.0 + 1.0, "hCutoff": 1000.0, "densityScale": 1.0}}
+            if atmosphere == "exponential":
+                earth["atmosphere"] = {"exponential": {"rho0": 3.725e-3, "h0": 400.0, "scaleHeight": 58.515,
+                                                       "hCutoff": 1000.0}}
+            elif atmosphere == "piecewise":
+                earth["atmosphere"] = {"exponential": [dict(b) for b in EXPONENTIAL_BANDS[::-1]]}
+            else:
+                earth["atmosphere"] = {"nrlmsise00": {
+                    "spaceWeatherFile": "SW-All.txt", "coverageStartMjdUtc": start_mjd + 51544.0 - 1.0,
+                    "coverageEndMjdUtc": end_mjd + 51544.0 + 1.0, "hCutoff": 1000.0, "densityScale": 1.0}}
     bodies_cfg = {"Earth": earth}
     if force == "full":
         for b in bodies:

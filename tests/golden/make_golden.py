@@ -9,7 +9,8 @@ Runs where the reference sources are available and built into oracle/_ref
   own validation script (scripts/validate.py): full force 600 s, central
   600 s, final-step shortening at 65 s and 5 s, per-object epochs / masses,
   33 objects across a block boundary, central-gravity invariants; plus the
-  benchmark configurations' shapes at small sizes.
+  benchmark configurations' shapes at small sizes and the reference's other
+  force options (J2 model, single-band and piecewise exponential drag).
 * ``nrlmsise00_kat.json`` - NRLMSISE-00 densities from the reference model
   sources (oracle/_ref/ref_kat) on an input grid.
 * ``tides_kat.json`` - solid / ocean tide coefficient sets and the tide and
@@ -95,6 +96,12 @@ def per_object_epochs():
 
 
 CASES["batch_4_epochs"] = (per_object_epochs, 1800.0, 60.0, {"threads": 2}, {})
+# the J2 model and the exponential atmospheres (one band; three bands over
+# 300-1000 km with cut-offs) instead of the geopotential file / NRLMSISE-00
+CASES["j2_exponential_2h"] = (lambda: S.population_leo(16, 13, alt=(300.0, 1200.0)), 7200.0, 60.0,
+                              {"gravity": "oblateness", "atmosphere": "exponential"}, {})
+CASES["piecewise_drag_3h"] = (lambda: S.population_leo(24, 14, alt=(300.0, 1100.0)), 10800.0, 60.0,
+                              {"atmosphere": "piecewise"}, {})
 
 
 def make_propagation_goldens(only=None):
