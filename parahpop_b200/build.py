@@ -8,6 +8,7 @@
 from __future__ import annotations
 
 import argparse
+import hashlib
 import os
 import shutil
 import subprocess
@@ -32,11 +33,21 @@ HEADERS = ["propagate.cuh", "propagate_impl.cuh", "device_env.cuh", "nrlmsise00.
            "tables/nrlmsise00_coeffs.inc", "tables/tide_tables.inc"]
 
 
-def _stale(out: Path, deps) -> bool:
-    if not out.exists():
-        return True
-    t = out.stat().st_mtime
-    return any(Path(d).stat().st_mtime > t for d in deps)
+def _digest(cmd, deps) -> str:
+    """Hash of a build step's command line and the contents of its inputs."""
+    h = hashlib.sha256("\0".join(map(str, cmd)).encode())
+    for d in deps:
+        h.update(Path(d).read_bytes())
+    return h.hexdigest()
+
+
+def _stale(out: Path, cmd, deps) -> bool:
+    """An output is rebuilt unless its stamp records the digest of exactly the
+    inputs it was built from (content hashes, not modification times: an
+    object compiled while a header was being edited is never taken as
+    current)."""
+    stamp = out.with_name(out.name + ".sha")
+    return not out.exists() or not stamp.exists() or stamp.read_text() != _digest(cmd, deps)
 
 
 def _run(cmd):
@@ -44,6 +55,18 @@ def _run(cmd):
     if r.returncode != 0:
         raise RuntimeError("build step failed:\n" + " ".join(map(str, cmd)) + "\n" + r.stdout)
     return r.stdout
+
+
+def _run_stamped(step):
+    """Runs one compile step; the digest is taken before the compiler starts,
+    so an input edited during the compile leaves the output stale."""
+    cmd, out, deps = step
+    digest = _digest(cmd, deps)
+    stamp = out.with_name(out.name + ".sha")
+    stamp.unlink(missing_ok=True)
+    text = _run(cmd)
+    stamp.write_text(digest)
+    return text
 
 
 def build(force: bool = False, jobs: int = 4, verbose_ptxas: bool = False) -> Path:
@@ -56,37 +79,41 @@ def build(force: bool = False, jobs: int = 4, verbose_ptxas: bool = False) -> Pa
     for s in CU_SOURCES:
         o = OBJ / (s + ".o")
         objs.append(o)
-        if force or _stale(o, [SRC / s] + hdrs):
-            cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
-                   "-I", str(SRC), "-c", str(SRC / s), "-o", str(o)]
-            steps.append(cmd)
+        cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+               "-I", str(SRC), "-c", str(SRC / s), "-o", str(o)]
+        if force or _stale(o, cmd, [SRC / s] + hdrs):
+            steps.append((cmd, o, [SRC / s] + hdrs))
     for sfx, defs in INST:
         o = OBJ / f"propagate_{sfx}.o"
         objs.append(o)
-        if force or _stale(o, [SRC / "propagate_inst.cu"] + hdrs):
-            cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
-                   *defs, f"-DPHOP_SUFFIX={sfx}", "-I", str(SRC), "-c", str(SRC / "propagate_inst.cu"), "-o", str(o)]
-            if verbose_ptxas:
-                cmd.insert(1, "-Xptxas=-v")
-            steps.append(cmd)
+        cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+               *defs, f"-DPHOP_SUFFIX={sfx}", "-I", str(SRC), "-c", str(SRC / "propagate_inst.cu"), "-o", str(o)]
+        deps = [SRC / "propagate_inst.cu"] + hdrs
+        if verbose_ptxas:
+            cmd.insert(1, "-Xptxas=-v")
+        if force or _stale(o, cmd, deps):
+            steps.append((cmd, o, deps))
     for s in CPP_SOURCES:
         o = OBJ / (s + ".o")
         objs.append(o)
-        if force or _stale(o, [SRC / s] + hdrs):
-            steps.append(["g++", "-O2", "-std=c++17", "-fPIC", "-I", str(SRC), "-I", str(CUDA_HOME / "include"),
-                          "-c", str(SRC / s), "-o", str(o)])
+        cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-I", str(SRC), "-I", str(CUDA_HOME / "include"),
+               "-c", str(SRC / s), "-o", str(o)]
+        if force or _stale(o, cmd, [SRC / s] + hdrs):
+            steps.append((cmd, o, [SRC / s] + hdrs))
     with ThreadPoolExecutor(max_workers=max(1, jobs)) as ex:
-        outs = list(ex.map(_run, steps))
+        outs = list(ex.map(_run_stamped, steps))
     if verbose_ptxas:
         for o in outs:
             if "registers" in o:
                 print(o)
-    if force or steps or not LIB.exists():
-        _run([NVCC, *ARCH, "-shared", *map(str, objs), "-o", str(LIB), "-Xlinker", "-soname=libparahpop_engine.so"])
+    link = [NVCC, *ARCH, "-shared", *map(str, objs), "-o", str(LIB), "-Xlinker", "-soname=libparahpop_engine.so"]
+    if force or steps or _stale(LIB, link, objs):
+        _run_stamped((link, LIB, objs))
     main = SRC / "main_gpu.cpp"
-    if force or _stale(CLI, [main, LIB]):
-        _run(["g++", "-O2", str(main), "-o", str(CLI), "-L", str(LIB.parent), "-lparahpop_engine",
-              "-Wl,-rpath,$ORIGIN/../lib"])
+    cli = ["g++", "-O2", str(main), "-o", str(CLI), "-L", str(LIB.parent), "-lparahpop_engine",
+           "-Wl,-rpath,$ORIGIN/../lib"]
+    if force or _stale(CLI, cli, [main, LIB]):
+        _run_stamped((cli, CLI, [main, LIB]))
     return LIB
 
 

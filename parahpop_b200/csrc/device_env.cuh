@@ -76,6 +76,7 @@ struct DevEnv {
     const nrlf::NrlEpochBlock* nrlBlocks;  // per (UTC day record, 3-hour ap slot): index record * 8 + slot
     // Earth corrections
     int solid, ocean, relativity, zeroTide;
+    int tidesAlone;  // tides on without a gravity field: the deltas are summed on their own (degree <= 6)
     int eopN;
     double eopFirstMjd;
     const double* eop;  // 4 x n component-major

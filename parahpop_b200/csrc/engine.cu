@@ -551,9 +551,11 @@ void Engine::uploadEnvironment() {
     e.shNormalized = h.shNormalized;
     e.shR = h.shR;
     e.shGM = h.shGM;
-    // tide coefficients are defined with the tide model's GM and radius
+    // tide coefficients are defined with the tide model's GM and radius: they
+    // join the field's low-degree block rescaled to its GM and radius, or are
+    // summed on their own (scale 1) when the Earth has no gravity field file
     for (int n = 0; n <= 6; ++n)
-        e.tideScale[n] = h.hasShape ? (tides::Consts::muEarth * 1e-9 / h.shGM) * std::pow(tides::Consts::radius * 1e-3 / h.shR, (double)n) : 0.0;
+        e.tideScale[n] = h.hasShape ? (tides::Consts::muEarth * 1e-9 / h.shGM) * std::pow(tides::Consts::radius * 1e-3 / h.shR, (double)n) : 1.0;
     if (h.hasShape) {
         e.shC = upload(owned_, h.shC);
         e.shS = upload(owned_, h.shS);
@@ -683,6 +685,7 @@ void Engine::uploadEnvironment() {
     e.solid = h.solid;
     e.ocean = h.ocean;
     e.relativity = h.relativity;
+    e.tidesAlone = (h.solid || h.ocean) && !h.hasShape;
     e.zeroTide = h.zeroTide;
     e.eopN = h.eopN;
     e.eopFirstMjd = h.eopFirstMjd;

@@ -7,8 +7,8 @@
 namespace phop {
 
 #define PHOP_DECL(sfx)                                                                                     \
-    cudaError_t launchPropagate_##sfx(const StepParams& p, int lanes, int ctas, int threads, int smem,       \
-                                      cudaStream_t stream);                                                 \
+    cudaError_t launchPropagate_##sfx(const StepParams& p, size_t paramsBytes, int lanes, int ctas, int threads, \
+                                      int smem, cudaStream_t stream);                                       \
     int occupancy_##sfx(int lanes, int threads, int smem);
 PHOP_DECL(f64_grid)
 PHOP_DECL(f64_mixed)
@@ -43,12 +43,15 @@ int propagateMaxCtasPerSm(int lanes, bool split, bool shared, int threads, int s
 
 cudaError_t launchPropagate(const StepParams& p, int lanes, bool split, bool shared, int ctas, int threads,
                             cudaStream_t stream) {
+    // every family checks the parameter block's size against its own view
+    // of the layout (the families are separate translation units)
     const int smem = propagateSmemBytes(p, lanes, threads);
+    const size_t b = sizeof(StepParams);
     if (split)
-        return shared ? launchPropagate_f32_grid(p, lanes, ctas, threads, smem, stream)
-                      : launchPropagate_f32_mixed(p, lanes, ctas, threads, smem, stream);
-    return shared ? launchPropagate_f64_grid(p, lanes, ctas, threads, smem, stream)
-                  : launchPropagate_f64_mixed(p, lanes, ctas, threads, smem, stream);
+        return shared ? launchPropagate_f32_grid(p, b, lanes, ctas, threads, smem, stream)
+                      : launchPropagate_f32_mixed(p, b, lanes, ctas, threads, smem, stream);
+    return shared ? launchPropagate_f64_grid(p, b, lanes, ctas, threads, smem, stream)
+                  : launchPropagate_f64_mixed(p, b, lanes, ctas, threads, smem, stream);
 }
 
 }  // namespace phop

@@ -373,6 +373,77 @@ static __device__ __forceinline__ double geodeticHeight(const double r[3], const
     return sqrt(xy + zd * zd) - Req / sqrt(1.0 - flatsq * sfq);
 }
 
+// Tide potential alone (solid + ocean coefficient deltas of the epoch, degree
+// <= 6, the tide model's GM and radius), for an Earth without a gravity field
+// file: the deltas otherwise join the field's low-degree block.  The body-
+// frame gradient of sum_nm (mu/r)(R/r)^n P_nm (dC cos m lon + dS sin m lon)
+// in geocentric latitude/longitude, as the reference's Earth corrections
+// evaluate it (hpop_compat/HpopCorrections.h:336-367); fully normalised
+// Legendre functions by the column recurrences and their latitude
+// derivatives in closed form (the reference recurses them alongside,
+// HpopCorrections.h:121-145).
+static __device__ __noinline__ void tideAloneAccel(const EpochRecord& r, const double pos[3], double acc[3]) {
+    const double* R = r.R;
+    const double x = R[0] * pos[0] + R[1] * pos[1] + R[2] * pos[2];
+    const double y = R[3] * pos[0] + R[4] * pos[1] + R[5] * pos[2];
+    const double z = R[6] * pos[0] + R[7] * pos[1] + R[8] * pos[2];
+    const double mu = tides::Consts::muEarth * 1e-9, Re = tides::Consts::radius * 1e-3;  // km^3/s^2, km
+    const double xy2 = x * x + y * y, xy = sqrt(xy2);
+    const double d = sqrt(xy2 + z * z);
+    const double sphi = z / d, cphi = xy / d, tphi = z / xy;
+    const double cl = x / xy, sl = y / xy;
+    double p[7][7], dp[7][7];
+    // column recurrences: P_mm from P_{m-1,m-1}, then upward in n
+    p[0][0] = 1.0;
+    for (int m = 0; m <= 6; ++m) {
+        if (m > 0) p[m][m] = sqrt((2.0 * m + 1.0) / (m == 1 ? 1.0 : 2.0 * m)) * cphi * p[m - 1][m - 1];
+        if (m < 6) p[m + 1][m] = sqrt(2.0 * m + 3.0) * sphi * p[m][m];
+        for (int n = m + 2; n <= 6; ++n) {
+            const double nn = (double)n, mm = (double)m;
+            const double a = sqrt((4.0 * nn * nn - 1.0) / (nn * nn - mm * mm));
+            const double b = sqrt((2.0 * nn + 1.0) * (nn - 1.0 - mm) * (nn - 1.0 + mm) / ((2.0 * nn - 3.0) * (nn * nn - mm * mm)));
+            p[n][m] = a * sphi * p[n - 1][m] - b * p[n - 2][m];
+        }
+    }
+    // d/dphi P_nm = k_nm P_{n,m+1} - m tan(phi) P_nm, k_n0 = sqrt(n(n+1)/2), k_nm = sqrt((n-m)(n+m+1))
+    for (int n = 0; n <= 6; ++n)
+        for (int m = 0; m <= n; ++m) {
+            const double up = m < n ? p[n][m + 1] : 0.0;
+            const double k = m == 0 ? sqrt(0.5 * n * (n + 1.0)) : sqrt((double)(n - m) * (n + m + 1.0));
+            dp[n][m] = k * up - (double)m * tphi * p[n][m];
+        }
+    double cm[7], sm[7];
+    cm[0] = 1.0;
+    sm[0] = 0.0;
+    for (int m = 1; m <= 6; ++m) {
+        cm[m] = cl * cm[m - 1] - sl * sm[m - 1];
+        sm[m] = sl * cm[m - 1] + cl * sm[m - 1];
+    }
+    double dUdr = 0.0, dUdlat = 0.0, dUdlon = 0.0, power = 1.0;
+    const double ratio = Re / d;
+    for (int n = 0; n <= 6; ++n) {
+        double q1 = 0.0, q2 = 0.0, q3 = 0.0;
+        for (int m = 0; m <= n; ++m) {
+            const int ti = n * (n + 1) / 2 + m;
+            const double c = r.dC[ti], s = r.dS[ti];
+            const double v = c * cm[m] + s * sm[m];
+            q1 += p[n][m] * v;
+            q2 += dp[n][m] * v;
+            q3 += (double)m * p[n][m] * (s * cm[m] - c * sm[m]);
+        }
+        dUdr += q1 * (-mu / (d * d)) * power * (n + 1.0);
+        dUdlat += q2 * (mu / d) * power;
+        dUdlon += q3 * (mu / d) * power;
+        power *= ratio;
+    }
+    const double q = dUdr / d - z / (d * d * xy) * dUdlat;
+    const double bf0 = q * x - (dUdlon / xy2) * y, bf1 = q * y + (dUdlon / xy2) * x;
+    const double bf2 = dUdr / d * z + xy / (d * d) * dUdlat;
+    acc[0] += R[0] * bf0 + R[3] * bf1 + R[6] * bf2;
+    acc[1] += R[1] * bf0 + R[4] * bf1 + R[7] * bf2;
+    acc[2] += R[2] * bf0 + R[5] * bf1 + R[8] * bf2;
+}
+
 // full right-hand side acceleration (km/s^2); every lane of the group calls it
 template <int L, typename T>
 static __device__ __forceinline__ void accelerations(const StepParams& p, const typename TileOf<T>::type* tile,
@@ -495,6 +566,13 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
             ay += f * vr1;
             az += f * vr2;
         }
+    }
+    if (e.tidesAlone) {
+        double t[3] = {0.0, 0.0, 0.0};
+        tideAloneAccel(r, pos, t);
+        ax += t[0];
+        ay += t[1];
+        az += t[2];
     }
     if (e.relativity) {
         const double mu = tides::Consts::muEarth, c = tides::Consts::c;

@@ -41,8 +41,9 @@ static int occupancyOne(int threads, int smem) {
     return n;
 }
 
-cudaError_t PHOP_CAT(launchPropagate_, PHOP_SUFFIX)(const StepParams& p, int lanes, int ctas, int threads, int smem,
-                                                    cudaStream_t stream) {
+cudaError_t PHOP_CAT(launchPropagate_, PHOP_SUFFIX)(const StepParams& p, size_t paramsBytes, int lanes, int ctas,
+                                                    int threads, int smem, cudaStream_t stream) {
+    if (paramsBytes != sizeof(StepParams)) return cudaErrorInvalidValue;  // objects built from different headers
     switch (lanes) {
         case 1: return launchOne<1>(p, ctas, threads, smem, stream);
         case 2: return launchOne<2>(p, ctas, threads, smem, stream);
