@@ -179,6 +179,15 @@ int phop_last_stats(const phop_context* ctx, phop_stats* out);
  * counterpart (the reference reports no roofline). */
 int phop_fma_peak(int device, double* fp64_tflops, double* fp32_tflops);
 
+/* NRLMSISE-00 total mass density (kg/m^3, gtd7d with switch 9 = -1) of n
+ * input rows {doy, sec, alt_km, g_lat_deg, g_long_deg, lst_h, f107A, f107,
+ * ap, ap_a[0..6]} (16 doubles each, row-major), evaluated on `device` by the
+ * step kernel's own per-object model with `lanes` (1, 2, 4 or 8) lanes per
+ * row.  A known-answer entry: it replaces the reference's gtd7d
+ * (model/atmosphere/detail/Nrlmsise00Model.inl:959-1100) called directly.
+ * Returns 0, or nonzero with the message in phop_last_error(NULL). */
+int phop_nrlmsise00_density(int device, int64_t n, const double* inputs, int lanes, double* out_rho);
+
 #ifdef __cplusplus
 }
 #endif

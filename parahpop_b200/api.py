@@ -53,6 +53,7 @@ def library() -> C.CDLL:
         lib.paraHPOP_run.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.c_char_p]
         lib.paraHPOP_setLogLevel.argtypes = [C.c_int]
         lib.phop_fma_peak.argtypes = [C.c_int, D, D]
+        lib.phop_nrlmsise00_density.argtypes = [C.c_int, C.c_int64, D, C.c_int, D]
         lib.phop_server_create.argtypes = [C.c_void_p, C.c_int64, C.c_double, C.POINTER(C.c_void_p)]
         lib.phop_server_destroy.argtypes = [C.c_void_p]
         lib.phop_server_last_error.argtypes = [C.c_void_p]
@@ -257,6 +258,18 @@ def fma_peak(device: int = 0) -> tuple[float, float]:
     if library().phop_fma_peak(device, C.byref(a), C.byref(b)) != 0:
         raise PhopError("FMA peak measurement failed")
     return a.value, b.value
+
+
+def nrlmsise00_density(inputs, lanes: int = 4, device: int = 0) -> np.ndarray:
+    """NRLMSISE-00 total mass density (kg/m^3) of input rows {doy, sec, alt,
+    g_lat, g_long, lst, f107A, f107, ap, ap_a[0..6]} on the device, through
+    the step kernel's per-object model split over `lanes` lanes."""
+    a = np.ascontiguousarray(inputs, dtype=np.float64).reshape(-1, 16)
+    out = np.empty(len(a))
+    lib = library()
+    if lib.phop_nrlmsise00_density(device, len(a), _dp(a), lanes, _dp(out)) != 0:
+        raise PhopError(lib.phop_last_error(None).decode())
+    return out
 
 
 def run(config, targets, output, backend="device") -> int:

@@ -24,7 +24,7 @@ NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 CUDA_HOME = Path(NVCC).resolve().parent.parent
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["propagate.cu", "engine.cu", "peak.cu", "noalloc.cu", "server.cu"]
+CU_SOURCES = ["propagate.cu", "engine.cu", "peak.cu", "noalloc.cu", "server.cu", "nrl_diag.cu"]
 # the step-kernel families: (object name, macro definitions)
 INST = [("f64_grid", ["-DPHOP_T=double", "-DPHOP_SG=1"]), ("f64_mixed", ["-DPHOP_T=double", "-DPHOP_SG=0"]),
         ("f32_grid", ["-DPHOP_T=float", "-DPHOP_SG=1"]), ("f32_mixed", ["-DPHOP_T=float", "-DPHOP_SG=0"])]

@@ -24,6 +24,10 @@
 namespace fs = std::filesystem;
 using phop::Value;
 
+namespace phop {
+void nrlDensityBatch(int device, int64_t n, const double* inputs, int lanes, double* outRho);  // nrl_diag.cu
+}
+
 static int g_logLevel = 1;
 static thread_local std::string g_createError;
 
@@ -556,6 +560,17 @@ int paraHPOP_run(int argc, char** argv, const char* backend) {
         return 0;
     } catch (const std::exception& e) {
         std::cerr << "ParaHPOP: " << e.what() << '\n';
+        return 1;
+    }
+}
+
+int phop_nrlmsise00_density(int device, int64_t n, const double* inputs, int lanes, double* out_rho) {
+    try {
+        phop::nrlDensityBatch(device, n, inputs, lanes, out_rho);
+        g_createError.clear();
+        return 0;
+    } catch (const std::exception& e) {
+        g_createError = e.what();
         return 1;
     }
 }

@@ -679,6 +679,9 @@ void Engine::uploadEnvironment() {
                 int doy = day;
                 for (int m = 1; m < month; ++m) doy += mdays[m - 1];
                 nrlf::nrlSlotBlock(doy, at(2, rec - 1), at(3, rec), apa, b);
+                if (!b.valid)
+                    throw std::runtime_error("NRLMSISE-00: a coefficient table outside pt / pd[0] has a "
+                                             "latitude-dependent ap response; this backend does not support it.");
             }
         e.nrlBlocks = upload(owned_, blocks);
     }

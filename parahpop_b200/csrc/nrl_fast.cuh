@@ -44,7 +44,24 @@ struct NrlGlobSEpoch {
     double lonB;  // p83 cos(dr(doy-p84)) + p87 cos(2dr(doy-p88))
 };
 
+// globe7 as dot products.  Every term of G(L) (globe7) is a coefficient that
+// depends only on the table and the (day, ap slot) times a monomial of the
+// object's Legendre functions and its local-time, longitude and seconds-of-day
+// phases; the 71 monomials of globeMonomial cover every table.  Per block the
+// rows hold those coefficients in task order (rows 0..10), with each table's
+// ap response folded in where it is epoch-only; the two tables whose ap
+// response depends on latitude (pt and pd[0]: p[138] != 0) keep their ap
+// terms apart in rows 11 and 12, scaled per object.  Rows 13..15 are zero so
+// that every lane split takes the same number of rows.  Stored pair-major:
+// globeRows[q][t] = row t's coefficients of monomials 2q and 2q + 1, so the
+// L lanes of a group, reading rows rL .. rL + L - 1 of one pair, read one
+// contiguous 16L-byte span (one cache line for L <= 8).
+constexpr int kGlobeBasis = 72;  // 71 monomials and a zero pad (16-byte rows)
+constexpr int kGlobeRows = 16;
+constexpr int kApRowPt = 11, kApRowPd0 = 12;
+
 struct NrlEpochBlock {
+    alignas(16) double globeRows[kGlobeBasis / 2][kGlobeRows][2];
     NrlGlobeEpoch ge[kGlobeTables];
     NrlGlobSEpoch gs[kGlobSTables];
     double dfa;
@@ -95,6 +112,139 @@ __host__ __device__ __forceinline__ T sg0FromExp(T exp1, const double g0[6]) {
         / sumex;
 }
 
+// Coefficient rows of one (day, ap slot) block (layout above; monomial
+// order in globeMonomial).  The expansion is exact algebra of globe7
+// (Nrlmsise00Model.inl:686 globe7): products of the table's factors that do
+// not depend on the object (f1, f2, 1 + p80 dfa, the UT factor
+// (1 + p95 x)(1 + p81 dfa)(1 + p119 cd14 x) multiplied out in powers of
+// x = P(1,0), and the phase constants of cos(a - p)) are formed here once.
+// Returns false when a table other than pt / pd[0] has a latitude-dependent
+// ap response (the coefficient set is fixed, so this never happens).
+__host__ __device__ inline bool nrlGlobeRows(NrlEpochBlock& b) {
+    bool ok = true;
+    double M[kGlobeRows][kGlobeBasis];
+    for (int r = 0; r < kGlobeRows; ++r)
+        for (int i = 0; i < kGlobeBasis; ++i) M[r][i] = 0.0;
+    const double dfa = b.dfa;
+    for (int t = 0; t < kGlobeTasks; ++t) {
+        const int k = globeTaskTable(t);
+        const double* p = globeTable(k);
+        const NrlGlobeEpoch& g = b.ge[k];
+        double* E = M[t];
+        double A[kGlobeBasis];
+        for (int i = 0; i < kGlobeBasis; ++i) A[i] = 0.0;
+        const double f1 = g.f1, f2 = g.f2, cd14 = g.cd14;
+        // time-independent, annual / semiannual
+        E[0] = p[30] + g.t0 + p[18] * g.cd32 + p[15] * g.cd18;
+        E[1] = p[26] + f1 * p[9] * cd14 + p[37] * g.cd39;
+        E[2] = p[1] + p[14] * dfa + p[16] * g.cd18;
+        E[3] = f1 * p[10] * cd14;
+        E[4] = p[2];
+        E[6] = p[22];
+        // diurnal (P11, P12, P13, P15) x (cos, sin) of the local time
+        E[7] = f2 * p[3];
+        E[8] = f2 * p[11] * cd14;
+        E[9] = f2 * p[4];
+        E[10] = f2 * p[27];
+        E[11] = f2 * p[6];
+        E[12] = f2 * p[12] * cd14;
+        E[13] = f2 * p[7];
+        E[14] = f2 * p[28];
+        // semidiurnal (P22, P23, P24, P25)
+        E[15] = f2 * p[5];
+        E[16] = f2 * p[23] * cd14;
+        E[17] = f2 * p[41];
+        E[18] = f2 * p[35] * cd14;
+        E[19] = f2 * p[8];
+        E[20] = f2 * p[33] * cd14;
+        E[21] = f2 * p[42];
+        E[22] = f2 * p[36] * cd14;
+        // terdiurnal (P33, P34, P36) x (sin, cos)
+        E[23] = f2 * p[39];
+        E[24] = f2 * p[93] * cd14;
+        E[25] = f2 * p[46] * cd14;
+        E[26] = f2 * p[40];
+        E[27] = f2 * p[94] * cd14;
+        E[28] = f2 * p[48] * cd14;
+        // longitudinal (P11 .. P16) x (cos, sin) of the longitude
+        const double lf = 1.0 + p[80] * dfa;
+        E[29] = lf * (p[103] + p[109] * cd14);
+        E[30] = lf * p[64];
+        E[31] = lf * (p[104] + p[110] * cd14);
+        E[32] = lf * p[65];
+        E[33] = lf * (p[105] + p[111] * cd14);
+        E[34] = lf * p[66];
+        E[35] = lf * (p[106] + p[112] * cd14);
+        E[36] = lf * p[90];
+        E[37] = lf * (p[107] + p[113] * cd14);
+        E[38] = lf * p[91];
+        E[39] = lf * (p[108] + p[114] * cd14);
+        E[40] = lf * p[92];
+        // UT: x^q {x, P30, P50} x (cos, sin) of the seconds-of-day phase
+        const double uf = 1.0 + p[81] * dfa;
+        const double w[3] = {1.0, p[95] + p[119] * cd14, p[95] * p[119] * cd14};
+        const double v[3] = {p[68], p[69], p[70]};
+        for (int q = 0; q < 3; ++q)
+            for (int m = 0; m < 3; ++m) {
+                E[47 + 3 * q + m] = uf * w[q] * v[m] * g.c71;
+                E[56 + 3 * q + m] = uf * w[q] * v[m] * g.s71;
+            }
+        // mixed UT / longitude: (P23, P25, P27) x (cos, sin)(sr sec + 2 lon)
+        const double q79 = 1.0 + p[137] * dfa;
+        for (int i = 0; i < 3; ++i) {
+            const double c = p[76 + i];
+            E[65 + i] = q79 * c * g.c79;
+            E[68 + i] = q79 * c * g.s79;
+        }
+        if (p[51] != 0.0) {
+            // magnetic activity terms, multiplied by the ap response apt0
+            A[0] = p[50];
+            A[2] = p[96];
+            A[4] = p[54];
+            A[1] = p[125] * cd14;
+            A[3] = p[126] * cd14;
+            A[5] = p[127] * cd14;
+            A[7] = p[128] * g.c131;
+            A[9] = p[129] * g.c131;
+            A[10] = p[130] * g.c131;
+            A[11] = p[128] * g.s131;
+            A[13] = p[129] * g.s131;
+            A[14] = p[130] * g.s131;
+            const int k97[3] = {52, 98, 67};
+            for (int i = 0; i < 3; ++i) {
+                const double c = p[k97[i]];
+                A[30 + 2 * i] += c * g.c97;
+                A[36 + 2 * i] += c * g.s97;
+                A[41 + i] = p[132] * c * g.c97;
+                A[44 + i] = p[132] * c * g.s97;
+            }
+            for (int i = 0; i < 3; ++i) {
+                const double c = p[133 + i] * cd14;
+                A[29 + 2 * i] += c * g.c136;
+                A[35 + 2 * i] += c * g.s136;
+            }
+            for (int i = 0; i < 3; ++i) {
+                A[47 + i] += p[55 + i] * g.c58;
+                A[56 + i] += p[55 + i] * g.s58;
+            }
+            if (g.aptEpochOnly) {
+                for (int i = 0; i < kGlobeBasis; ++i) E[i] += g.apt0 * A[i];
+            } else if (k == 0 || k == 2) {
+                double* R = M[k == 0 ? kApRowPt : kApRowPd0];
+                for (int i = 0; i < kGlobeBasis; ++i) R[i] = A[i];
+            } else {
+                ok = false;
+            }
+        }
+    }
+    for (int q = 0; q < kGlobeBasis / 2; ++q)
+        for (int r = 0; r < kGlobeRows; ++r) {
+            b.globeRows[q][r][0] = M[r][2 * q];
+            b.globeRows[q][r][1] = M[r][2 * q + 1];
+        }
+    return ok;
+}
+
 // (day, ap slot) part: day of year, F10.7 of the previous day, 81-day mean,
 // ap history (as Nrlmsise00.cu:207-235 fills them).
 __host__ __device__ inline void nrlSlotBlock(int doy, double f107, double f107A, const double apa[7],
@@ -140,6 +290,7 @@ __host__ __device__ inline void nrlSlotBlock(int doy, double f107, double f107A,
             g.apt0 = sg0FromExp(exp1, g.g0);
         }
     }
+    if (!nrlGlobeRows(b)) b.valid = 0;
     for (int k = 0; k < kGlobSTables; ++k) {
         const double* p = globSTable(k);
         NrlGlobSEpoch& g = b.gs[k];
@@ -220,85 +371,6 @@ struct Fast {
         sincos(dgtr * gLong, &sgl, &cgl);
         s2gl = T(2.0) * sgl * cgl;
         c2gl = (cgl - sgl) * (cgl + sgl);
-    }
-
-    // G(L), upper thermosphere; table k of the globe7 sequence
-    __device__ __forceinline__ T globe7(int k) { return globe7At(k, globeTable(k)); }
-
-    __device__ __forceinline__ T globe7At(int k, const double* __restrict__ p) {
-        const NrlGlobeEpoch& g = eb.ge[k];
-        const T hr = T(0.2618), dgtr = T(1.74533E-2);
-        const T dfa = T(eb.dfa);
-        const T cd32 = T(g.cd32), cd18 = T(g.cd18), cd14 = T(g.cd14), cd39 = T(g.cd39);
-        const T f1 = T(g.f1), f2 = T(g.f2);
-        T tinf = T(p[30]) + T(g.t0);
-        tinf += (T(p[1]) * plg[0][2] + T(p[2]) * plg[0][4] + T(p[22]) * plg[0][6]) + (T(p[14]) * plg[0][2]) * dfa
-            + T(p[26]) * plg[0][1];
-        tinf += T(p[18]) * cd32;
-        tinf += (T(p[15]) + T(p[16]) * plg[0][2]) * cd18;
-        tinf += f1 * (T(p[9]) * plg[0][1] + T(p[10]) * plg[0][3]) * cd14;
-        tinf += T(p[37]) * plg[0][1] * cd39;
-        {
-            const T t71 = (T(p[11]) * plg[1][2]) * cd14;
-            const T t72 = (T(p[12]) * plg[1][2]) * cd14;
-            tinf += f2 * ((T(p[3]) * plg[1][1] + T(p[4]) * plg[1][3] + T(p[27]) * plg[1][5] + t71) * ctloc
-                          + (T(p[6]) * plg[1][1] + T(p[7]) * plg[1][3] + T(p[28]) * plg[1][5] + t72) * stloc);
-        }
-        {
-            const T t81 = (T(p[23]) * plg[2][3] + T(p[35]) * plg[2][5]) * cd14;
-            const T t82 = (T(p[33]) * plg[2][3] + T(p[36]) * plg[2][5]) * cd14;
-            tinf += f2 * ((T(p[5]) * plg[2][2] + T(p[41]) * plg[2][4] + t81) * c2tloc
-                          + (T(p[8]) * plg[2][2] + T(p[42]) * plg[2][4] + t82) * s2tloc);
-        }
-        tinf += f2 * ((T(p[39]) * plg[3][3] + (T(p[93]) * plg[3][4] + T(p[46]) * plg[3][6]) * cd14) * s3tloc
-                      + (T(p[40]) * plg[3][3] + (T(p[94]) * plg[3][4] + T(p[48]) * plg[3][6]) * cd14) * c3tloc);
-        if (p[51] != 0) {
-            if (g.aptEpochOnly) {
-                apt0 = T(g.apt0);
-            } else {
-                T exp1 = exp(T(-10800.0) * fabs(T(p[51])) / (T(1.0) + T(p[138]) * (T(45.0) - absLat)));
-                if (exp1 > T(0.99999)) exp1 = T(0.99999);
-                apt0 = sg0FromExp(exp1, g.g0);  // with the epoch's g0 responses
-            }
-            const T c131 = T(g.c131), s131 = T(g.s131);
-            tinf += apt0 * (T(p[50]) + T(p[96]) * plg[0][2] + T(p[54]) * plg[0][4]
-                            + (T(p[125]) * plg[0][1] + T(p[126]) * plg[0][3] + T(p[127]) * plg[0][5]) * cd14
-                            + (T(p[128]) * plg[1][1] + T(p[129]) * plg[1][3] + T(p[130]) * plg[1][5])
-                                * (ctloc * c131 + stloc * s131));
-        }
-        // longitudinal
-        tinf += (T(1.0) + T(p[80]) * dfa)
-            * ((T(p[64]) * plg[1][2] + T(p[65]) * plg[1][4] + T(p[66]) * plg[1][6] + T(p[103]) * plg[1][1]
-                + T(p[104]) * plg[1][3] + T(p[105]) * plg[1][5]
-                + (T(p[109]) * plg[1][1] + T(p[110]) * plg[1][3] + T(p[111]) * plg[1][5]) * cd14)
-                   * cgl
-               + (T(p[90]) * plg[1][2] + T(p[91]) * plg[1][4] + T(p[92]) * plg[1][6] + T(p[106]) * plg[1][1]
-                  + T(p[107]) * plg[1][3] + T(p[108]) * plg[1][5]
-                  + (T(p[112]) * plg[1][1] + T(p[113]) * plg[1][3] + T(p[114]) * plg[1][5]) * cd14)
-                   * sgl);
-        // ut and mixed ut / longitude
-        tinf += (T(1.0) + T(p[95]) * plg[0][1]) * (T(1.0) + T(p[81]) * dfa) * (T(1.0) + T(p[119]) * plg[0][1] * cd14)
-            * ((T(p[68]) * plg[0][1] + T(p[69]) * plg[0][3] + T(p[70]) * plg[0][5])
-               * (csec * T(g.c71) + ssec * T(g.s71)));
-        {
-            // cos(sr (sec - p79) + 2 dgtr g_long)
-            const T c79 = csec * T(g.c79) + ssec * T(g.s79), s79 = ssec * T(g.c79) - csec * T(g.s79);
-            tinf += (T(p[76]) * plg[2][3] + T(p[77]) * plg[2][5] + T(p[78]) * plg[2][7]) * (c79 * c2gl - s79 * s2gl)
-                * (T(1.0) + T(p[137]) * dfa);
-        }
-        if (p[51] != 0) {
-            const T c97 = T(g.c97), s97 = T(g.s97);
-            const T c136 = T(g.c136), s136 = T(g.s136);
-            tinf += apt0 * (T(1.) + T(p[132]) * plg[0][1])
-                    * ((T(p[52]) * plg[1][2] + T(p[98]) * plg[1][4] + T(p[67]) * plg[1][6]) * (cgl * c97 + sgl * s97))
-                + apt0 * (T(p[133]) * plg[1][1] + T(p[134]) * plg[1][3] + T(p[135]) * plg[1][5]) * cd14
-                    * (cgl * c136 + sgl * s136)
-                + apt0 * (T(p[55]) * plg[0][1] + T(p[56]) * plg[0][3] + T(p[57]) * plg[0][5])
-                    * (csec * T(g.c58) + ssec * T(g.s58));
-        }
-        (void)hr;
-        (void)dgtr;
-        return tinf;
     }
 
     __device__ __forceinline__ T glob7s(int k) const { return glob7sAt(k, globSTable(k)); }
@@ -460,50 +532,153 @@ struct Fast {
         return densu_temp * pow((lp.t1 / tz), (T(1.0) + alpha)) * exp(-expl);
     }
 
+    // Monomial i of the globe7 basis (order of the coefficient rows; i is a
+    // compile-time constant after unrolling).  x = P(1,0); U1, U2 = cos, sin of
+    // (sr sec + 2 dgtr lon).
+    __device__ __forceinline__ T globeMonomial(int i, T x, T x2, T U1, T U2) const {
+        switch (i) {
+            case 0: return T(1.0);
+            case 1: return x;
+            case 2: return plg[0][2];
+            case 3: return plg[0][3];
+            case 4: return plg[0][4];
+            case 5: return plg[0][5];
+            case 6: return plg[0][6];
+            case 7: return plg[1][1] * ctloc;
+            case 8: return plg[1][2] * ctloc;
+            case 9: return plg[1][3] * ctloc;
+            case 10: return plg[1][5] * ctloc;
+            case 11: return plg[1][1] * stloc;
+            case 12: return plg[1][2] * stloc;
+            case 13: return plg[1][3] * stloc;
+            case 14: return plg[1][5] * stloc;
+            case 15: return plg[2][2] * c2tloc;
+            case 16: return plg[2][3] * c2tloc;
+            case 17: return plg[2][4] * c2tloc;
+            case 18: return plg[2][5] * c2tloc;
+            case 19: return plg[2][2] * s2tloc;
+            case 20: return plg[2][3] * s2tloc;
+            case 21: return plg[2][4] * s2tloc;
+            case 22: return plg[2][5] * s2tloc;
+            case 23: return plg[3][3] * s3tloc;
+            case 24: return plg[3][4] * s3tloc;
+            case 25: return plg[3][6] * s3tloc;
+            case 26: return plg[3][3] * c3tloc;
+            case 27: return plg[3][4] * c3tloc;
+            case 28: return plg[3][6] * c3tloc;
+            case 29: return plg[1][1] * cgl;
+            case 30: return plg[1][2] * cgl;
+            case 31: return plg[1][3] * cgl;
+            case 32: return plg[1][4] * cgl;
+            case 33: return plg[1][5] * cgl;
+            case 34: return plg[1][6] * cgl;
+            case 35: return plg[1][1] * sgl;
+            case 36: return plg[1][2] * sgl;
+            case 37: return plg[1][3] * sgl;
+            case 38: return plg[1][4] * sgl;
+            case 39: return plg[1][5] * sgl;
+            case 40: return plg[1][6] * sgl;
+            case 41: return x * plg[1][2] * cgl;
+            case 42: return x * plg[1][4] * cgl;
+            case 43: return x * plg[1][6] * cgl;
+            case 44: return x * plg[1][2] * sgl;
+            case 45: return x * plg[1][4] * sgl;
+            case 46: return x * plg[1][6] * sgl;
+            case 47: return csec * x;
+            case 48: return csec * plg[0][3];
+            case 49: return csec * plg[0][5];
+            case 50: return csec * x2;
+            case 51: return csec * (x * plg[0][3]);
+            case 52: return csec * (x * plg[0][5]);
+            case 53: return csec * (x2 * x);
+            case 54: return csec * (x2 * plg[0][3]);
+            case 55: return csec * (x2 * plg[0][5]);
+            case 56: return ssec * x;
+            case 57: return ssec * plg[0][3];
+            case 58: return ssec * plg[0][5];
+            case 59: return ssec * x2;
+            case 60: return ssec * (x * plg[0][3]);
+            case 61: return ssec * (x * plg[0][5]);
+            case 62: return ssec * (x2 * x);
+            case 63: return ssec * (x2 * plg[0][3]);
+            case 64: return ssec * (x2 * plg[0][5]);
+            case 65: return plg[2][3] * U1;
+            case 66: return plg[2][5] * U1;
+            case 67: return plg[2][7] * U1;
+            case 68: return plg[2][3] * U2;
+            case 69: return plg[2][5] * U2;
+            case 70: return plg[2][7] * U2;
+            default: return T(0.0);
+        }
+    }
+
+    // Latitude-dependent ap response sg0 of table k (pt or pd[0]).
+    __device__ __forceinline__ T aptLatitude(const double* __restrict__ p, const double* g0) const {
+        T exp1 = exp(T(-10800.0) * fabs(T(p[51])) / (T(1.0) + T(p[138]) * (T(45.0) - absLat)));
+        if (exp1 > T(0.99999)) exp1 = T(0.99999);
+        return sg0FromExp(exp1, g0);
+    }
+
     // The 11 globe7 values of one gts7 call (task order above), with the ap
     // response apt0 left by the pd[3] table (used by the mesosphere glob7s
-    // terms) and by the last table (used below 72.5 km).  L lanes of a group
-    // share the tables round-robin and exchange the values by shuffles; the
-    // tables are then read from global memory, since the lanes read
-    // different ones.
+    // terms) and by the last table (used below 72.5 km).  Each lane of a
+    // group of L takes kGlobeRows / L coefficient rows (rows j, j + L, ...)
+    // and forms their dot products with the monomials (two partial sums per
+    // row, read two coefficients at a time); the row values are exchanged by
+    // shuffles.  The latitude-dependent ap responses of pt and pd[0] are
+    // formed on lanes 0 and 1.
     template <int L>
     __device__ __forceinline__ void globeTasks(T (&G)[kGlobeTasks], T& aptTlb, T& aptLast, int j, int groupBase) {
-        if (L == 1) {
+        static_assert(kGlobeRows % L == 0, "lane split of the coefficient rows");
+        constexpr int R = kGlobeRows / L;
+        const T x = plg[0][1], x2 = x * x;
+        const T U1 = csec * c2gl - ssec * s2gl, U2 = ssec * c2gl + csec * s2gl;
+        const double2* __restrict__ rows = reinterpret_cast<const double2*>(&eb.globeRows[0][0][0]);
+        T acc[R], acc2[R];
 #pragma unroll
-            for (int t = 0; t < kGlobeTasks; ++t) {
-                G[t] = globe7(globeTaskTable(t));
-                if (t == 2) aptTlb = apt0;
+        for (int r = 0; r < R; ++r) acc[r] = acc2[r] = T(0.0);
+#pragma unroll
+        for (int i = 0; i < kGlobeBasis; i += 2) {
+            const T b0 = globeMonomial(i, x, x2, U1, U2), b1 = globeMonomial(i + 1, x, x2, U1, U2);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const double2 c = __ldg(rows + (i / 2) * kGlobeRows + r * L + j);
+                acc[r] = fma(T(c.x), b0, acc[r]);
+                acc2[r] = fma(T(c.y), b1, acc2[r]);
             }
-            aptLast = apt0;
-            return;
         }
-        // the group's lanes only: groups of a warp may leave the density
-        // evaluation at different points (altitude cut-off), a group never splits
-        const unsigned mask = ((1u << L) - 1u) << groupBase;
+        const unsigned mask = L >= 32 ? 0xffffffffu : ((1u << L) - 1u) << groupBase;
+        // value of row t: accumulator t / L of lane t % L
+        auto rowValue = [&](int t) -> T {
+            const T v = acc[t / L] + acc2[t / L];
+            if (L == 1) return v;
+            return __shfl_sync(mask, v, groupBase + t % L);
+        };
+        T aptPt, aptPd0;
+        if (L == 1) {
+            aptPt = aptLatitude(globeTable(0), eb.ge[0].g0);
+            aptPd0 = aptLatitude(globeTable(2), eb.ge[2].g0);
+        } else {
+            const int k = (j & 1) ? 2 : 0;
+            const T a = aptLatitude(globeTableGlobal(k), eb.ge[k].g0);
+            aptPt = __shfl_sync(mask, a, groupBase);
+            aptPd0 = __shfl_sync(mask, a, groupBase + 1);
+        }
+#pragma unroll
+        for (int t = 0; t < kGlobeTasks; ++t) G[t] = rowValue(t);
+        G[0] = fma(aptPt, rowValue(kApRowPt), G[0]);
+        G[4] = fma(aptPd0, rowValue(kApRowPd0), G[4]);
         // apt0 after task t in the sequential order: the value set by the last
         // table up to t whose ap term is present (p[51] != 0)
         T aptSeq = apt0;
 #pragma unroll
-        for (int r = 0; r < (kGlobeTasks + L - 1) / L; ++r) {
-            const int t = r * L + j;
-            T v = T(0), a = T(0);
-            if (t < kGlobeTasks) {
-                const int k = globeTaskTable(t);
-                v = globe7At(k, globeTableGlobal(k));
-                a = apt0;
-            }
-#pragma unroll
-            for (int jj = 0; jj < L; ++jj) {
-                const int tt = r * L + jj;
-                if (tt < kGlobeTasks) {
-                    G[tt] = __shfl_sync(mask, v, groupBase + jj);
-                    const T at = __shfl_sync(mask, a, groupBase + jj);
-                    if (globeTable(globeTaskTable(tt))[51] != 0.0) aptSeq = at;
-                    if (tt == 2) aptTlb = aptSeq;
-                }
-            }
+        for (int t = 0; t < kGlobeTasks; ++t) {
+            const int k = globeTaskTable(t);
+            if (globeTable(k)[51] != 0.0) aptSeq = k == 0 ? aptPt : k == 2 ? aptPd0 : T(eb.ge[k].apt0);
+            if (t == 2) aptTlb = aptSeq;
         }
         aptLast = aptSeq;
+        apt0 = aptLast;
     }
 
     // thermosphere (alt >= 72.5 km): number densities d[0..8] (m^-3), from

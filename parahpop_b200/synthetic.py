@@ -498,7 +498,8 @@ EXPONENTIAL_BANDS = [
 def make_config(env_dir, duration, step, max_steps=1000000, threads=1, force="full",
                 degree=70, bodies=("Sun", "Moon", "JupiterBarycenter"), tides=True,
                 relativity=True, drag=True, srp=True, start_mjd=4016.0, end_mjd=4064.0,
-                gravity="shape", atmosphere="nrlmsise00") -> dict:
+                gravity="shape", atmosphere="nrlmsise00", tide_system="zero_tide",
+                occulting=("Earth",)) -> dict:
     """Run configuration in the reference schema (``example/config/envisat_full.json``).
     Paths are relative to ``env_dir`` (where the config file is written).
     ``gravity``: "shape" (the spherical-harmonic file) or "oblateness" (the
@@ -513,7 +514,7 @@ def make_config(env_dir, duration, step, max_steps=1000000, threads=1, force="fu
         else:
             grav = {"shape": {"body": "Earth", "file": "gravity.tab", "delimiter": ",",
                               "headerLines": 0, "degree": degree, "order": degree}}
-        earth = {"occulting": True, "flattening": 0.0033528106647474805, "gravity": grav}
+        earth = {"occulting": "Earth" in occulting, "flattening": 0.0033528106647474805, "gravity": grav}
         if drag and force == "full":
             if atmosphere == "exponential":
                 earth["atmosphere"] = {"exponential": {"rho0": 3.725e-3, "h0": 400.0, "scaleHeight": 58.515,
@@ -530,14 +531,14 @@ def make_config(env_dir, duration, step, max_steps=1000000, threads=1, force="fu
             if b == "Sun":
                 bodies_cfg["Sun"] = {"gravity": True, "radiation": bool(srp)}
             elif b == "Moon":
-                bodies_cfg["Moon"] = {"gravity": True}
+                bodies_cfg["Moon"] = {"gravity": True, "occulting": True} if "Moon" in occulting else {"gravity": True}
             elif b == "JupiterBarycenter":
                 bodies_cfg["JupiterBarycenter"] = {"gm": 126712764.1, "gravity": True}
     env = {"bodies": bodies_cfg, "ephemeris": ["bodies.brie"], "constants": "constants.json", "preferSSB": True}
     if force != "central":
         env["orientations"] = ["earth.brot2"]
     if force == "full" and (tides or relativity):
-        env["earthCorrections"] = {"model": "iers2010_fes2004", "tideSystem": "zero_tide",
+        env["earthCorrections"] = {"model": "iers2010_fes2004", "tideSystem": tide_system,
                                    "solidEarthTides": bool(tides), "oceanTides": bool(tides),
                                    "relativity": bool(relativity), "eopFile": "EOP-All.txt"}
     return {"run": {"duration_seconds": float(duration)},

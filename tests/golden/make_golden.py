@@ -104,6 +104,48 @@ CASES["piecewise_drag_3h"] = (lambda: S.population_leo(24, 14, alt=(300.0, 1100.
                               {"atmosphere": "piecewise"}, {})
 
 
+def lunar_penumbra():
+    """Objects placed, at their epoch, inside and around the Moon's shadow
+    cone where it grazes the Earth in the synthetic ephemeris (its Sun-Moon
+    alignment at MJD2000 4027.166): the Moon occults the Sun for part of the
+    run (annular on the axis, partial across the penumbra, none outside), the
+    Earth for part of each orbit."""
+    f = S.body_functions()
+    t0 = 4027.16577
+    sun = f["sun"](np.array([t0]))[0] - f["earth"](np.array([t0]))[0]
+    moon = f["moon"](np.array([t0]))[0]
+    u = (moon - sun) / np.linalg.norm(moon - sun)
+    w = np.cross(u, moon)
+    w /= np.linalg.norm(w)
+    s_near = -(moon @ u)
+    rng = np.random.default_rng(15)
+    states, n = [], 0
+    for off in (0.0, 800.0, 1600.0, 2400.0, 3200.0, 4200.0):
+        for sgn in (1.0, -1.0):
+            # walk back from the Earth along the axis until 420+ km up
+            s = s_near
+            while True:
+                p = moon + s * u + sgn * off * w
+                if np.linalg.norm(p) >= S.R_EARTH + 420.0:
+                    break
+                s -= 20.0
+            r = np.linalg.norm(p)
+            h = np.cross(p, rng.normal(size=3))
+            v = h / np.linalg.norm(h) * np.sqrt(398600.4418 / r)
+            states.append(np.concatenate([p, v]))
+            n += 1
+    states = np.array(states)
+    return S.Population(np.arange(1, n + 1), np.full(n, t0), states, np.full(n, 800.0), np.full(n, 20.0),
+                        np.full(n, 30.0), np.full(n, 2.2), np.full(n, 1.3), seed=15,
+                        note="lunar penumbra at the synthetic alignment")
+
+
+# the Moon as a second occulter (product of the two shadow factors) and the
+# tide-free tide system
+CASES["lunar_shadow_30m"] = (lunar_penumbra, 1800.0, 60.0, {"occulting": ("Earth", "Moon")}, {})
+CASES["tide_free_2h"] = (lambda: S.population_leo(16, 16), 7200.0, 60.0, {"tide_system": "tide_free"}, {})
+
+
 def make_propagation_goldens(only=None):
     for name, (pop_fn, dur, step, ckw, ekw) in CASES.items():
         if only and name not in only:
