@@ -60,8 +60,24 @@ constexpr int kGlobeBasis = 72;  // 71 monomials and a zero pad (16-byte rows)
 constexpr int kGlobeRows = 16;
 constexpr int kApRowPt = 11, kApRowPd0 = 12;
 
+// Per-species parameters of the thermospheric number densities (gts7 of
+// Nrlmsise00Model.inl:522-720), one row per species in the lane order of
+// Fast::gts7 (N, H, O, O2, Ar, He, N2): every species is
+//   d = main(g, pdm0, pd0, xm, alpha)
+//   if z <= lim:  d = dnet(d, dm, zhm28, xmm, xm) * ccor2(z, r1, c1h1, c1zh, c1h2) * ccor2(z, r2, c2h, c2zh, c2h)
+//   d *= ccor2(z, rc, cah1, cazh, cah2)
+// with r1 = log(b28 k1 k2 / b) (rlLog) or k1, ccor(z, r, h, zh) written as
+// ccor2 with h2 = h (the same value bit for bit), and a zero r for a factor
+// that species does not have (ccor2 with r = 0 is exactly 1).
+enum NrlSpeciesParam {
+    kSpPdm0, kSpPd0, kSpXm, kSpAlpha, kSpLim, kSpRlLog, kSpK1, kSpK2, kSpC1H1, kSpC1Zh, kSpC1H2,
+    kSpR2, kSpC2H, kSpC2Zh, kSpRc, kSpCaH1, kSpCaZh, kSpCaH2, kSpParams
+};
+constexpr int kNrlSpecies = 7;
+
 struct NrlEpochBlock {
     alignas(16) double globeRows[kGlobeBasis / 2][kGlobeRows][2];
+    double species[kNrlSpecies][kSpParams];
     NrlGlobeEpoch ge[kGlobeTables];
     NrlGlobSEpoch gs[kGlobSTables];
     double dfa;
@@ -245,6 +261,71 @@ __host__ __device__ inline bool nrlGlobeRows(NrlEpochBlock& b) {
     return ok;
 }
 
+// Species rows (layout above) from the model tables; the F10.7 factor of the
+// O and O2 terms is the block's.
+__host__ __device__ inline void nrlSpeciesRows(NrlEpochBlock& b) {
+    const double f107Term = 1.0 + NRL_PDL(0)[23] * (b.f107A - 150.0);
+    auto row = [&](int r, double pdm0, double pd0, double xm, double alpha, double lim) {
+        double* q = b.species[r];
+        for (int k = 0; k < kSpParams; ++k) q[k] = 0.0;
+        q[kSpPdm0] = pdm0;
+        q[kSpPd0] = pd0;
+        q[kSpXm] = xm;
+        q[kSpAlpha] = alpha;
+        q[kSpLim] = lim;
+        q[kSpK2] = 1.0;
+        q[kSpC1H1] = q[kSpC1H2] = q[kSpC2H] = q[kSpCaH1] = q[kSpCaH2] = 1.0;
+        return q;
+    };
+    auto c1 = [](double* q, int rlLog, double k1, double k2, double h1, double zh, double h2) {
+        q[kSpRlLog] = rlLog;
+        q[kSpK1] = k1;
+        q[kSpK2] = k2;
+        q[kSpC1H1] = h1;
+        q[kSpC1Zh] = zh;
+        q[kSpC1H2] = h2;
+    };
+    auto c2 = [](double* q, double r, double h, double zh) {
+        q[kSpR2] = r;
+        q[kSpC2H] = h;
+        q[kSpC2Zh] = zh;
+    };
+    double* q;
+    // N
+    q = row(0, NRL_PDM(6, 0), NRL_PD(7)[0], 14.0, 0.0, 450.0);
+    c1(q, 1, NRL_PDM(6, 1), fabs(NRL_PDL(0)[2]), NRL_PDM(6, 5) * NRL_PDL(0)[1], NRL_PDM(6, 4) * NRL_PDL(0)[0],
+       NRL_PDM(6, 5) * NRL_PDL(0)[1]);
+    c2(q, NRL_PDM(6, 3) * NRL_PDL(0)[5], NRL_PDM(6, 7) * NRL_PDL(0)[4], NRL_PDM(6, 6) * NRL_PDL(0)[3]);
+    // H
+    q = row(1, NRL_PDM(5, 0), NRL_PD(6)[0], 1.0, -0.38, 320.0);
+    c1(q, 1, NRL_PDM(5, 1), fabs(NRL_PDL(1)[17]), NRL_PDM(5, 5) * NRL_PDL(1)[11], NRL_PDM(5, 4) * NRL_PDL(1)[10],
+       NRL_PDM(5, 5) * NRL_PDL(1)[11]);
+    c2(q, NRL_PDM(5, 3) * NRL_PDL(1)[20], NRL_PDM(5, 7) * NRL_PDL(1)[19], NRL_PDM(5, 6) * NRL_PDL(1)[18]);
+    // O: constant r1 with a two-scale-height correction
+    q = row(2, NRL_PDM(1, 0), NRL_PD(1)[0], 16.0, 0.0, 300.0);
+    c1(q, 0, NRL_PDM(1, 1) * NRL_PDL(1)[16] * f107Term, 1.0, NRL_PDM(1, 5) * NRL_PDL(1)[3],
+       NRL_PDM(1, 4) * NRL_PDL(1)[2], NRL_PDM(1, 5) * NRL_PDL(1)[4]);
+    c2(q, NRL_PDM(1, 3) * NRL_PDL(1)[14], NRL_PDM(1, 7) * NRL_PDL(1)[13], NRL_PDM(1, 6) * NRL_PDL(1)[12]);
+    // O2, with its correction at every altitude
+    q = row(3, NRL_PDM(3, 0), NRL_PD(4)[0], 32.0, 0.0, 250.0);
+    c1(q, 1, NRL_PDM(3, 1), 1.0, NRL_PDM(3, 5) * NRL_PDL(1)[7], NRL_PDM(3, 4) * NRL_PDL(1)[6],
+       NRL_PDM(3, 5) * NRL_PDL(1)[7]);
+    q[kSpRc] = NRL_PDM(3, 3) * NRL_PDL(1)[23] * f107Term;
+    q[kSpCaH1] = NRL_PDM(3, 7) * NRL_PDL(1)[22];
+    q[kSpCaZh] = NRL_PDM(3, 6) * NRL_PDL(1)[21];
+    q[kSpCaH2] = NRL_PDM(3, 7) * NRL_PDL(0)[22];
+    // Ar
+    q = row(4, NRL_PDM(4, 0), NRL_PD(5)[0], 40.0, 0.17, 240.0);
+    c1(q, 1, NRL_PDM(4, 1), 1.0, NRL_PDM(4, 5) * NRL_PDL(1)[9], NRL_PDM(4, 4) * NRL_PDL(1)[8],
+       NRL_PDM(4, 5) * NRL_PDL(1)[9]);
+    // He (z < 200 km: the largest double below 200)
+    q = row(5, NRL_PDM(0, 0), NRL_PD(0)[0], 4.0, -0.38, 199.99999999999997);
+    c1(q, 1, NRL_PDM(0, 1), 1.0, NRL_PDM(0, 5) * NRL_PDL(1)[1], NRL_PDM(0, 4) * NRL_PDL(1)[0],
+       NRL_PDM(0, 5) * NRL_PDL(1)[1]);
+    // N2: mixing only (below 160 km)
+    row(6, NRL_PDM(2, 0), NRL_PD(2)[0], 28.0, 0.0, 160.0);
+}
+
 // (day, ap slot) part: day of year, F10.7 of the previous day, 81-day mean,
 // ap history (as Nrlmsise00.cu:207-235 fills them).
 __host__ __device__ inline void nrlSlotBlock(int doy, double f107, double f107A, const double apa[7],
@@ -291,6 +372,7 @@ __host__ __device__ inline void nrlSlotBlock(int doy, double f107, double f107A,
         }
     }
     if (!nrlGlobeRows(b)) b.valid = 0;
+    nrlSpeciesRows(b);
     for (int k = 0; k < kGlobSTables; ++k) {
         const double* p = globSTable(k);
         NrlGlobSEpoch& g = b.gs[k];
@@ -846,73 +928,53 @@ struct Fast {
                 }
             }
         }
-        // N2
-        d[2] = mainDensity(G[3], T(NRL_PDM(2, 0)), T(NRL_PD(2)[0]), T(28.0), T(0.0));
         const T zhm28 = T(NRL_PDM(2, 3)) * T(NRL_PDL(1)[5]);
         const T b28 = bv[0];
-        if (z <= T(160.0)) {
-            dm28 = dmv[0];
-            d[2] = nrl::Model<T>::dnet(d[2], dm28, zhm28, xmm, T(28.0));
-        }
-        // He
-        d[0] = mainDensity(G[4], T(NRL_PDM(0, 0)), T(NRL_PD(0)[0]), T(4.), T(-0.38));
-        if (z < T(200.0)) {
-            const T b04 = bv[1], dm04 = dmv[1];
-            d[0] = nrl::Model<T>::dnet(d[0], dm04, zhm28, xmm, T(4.));
-            const T rl = log(b28 * T(NRL_PDM(0, 1)) / b04);
-            d[0] = d[0] * nrl::Model<T>::ccor(z, rl, T(NRL_PDM(0, 5)) * T(NRL_PDL(1)[1]), T(NRL_PDM(0, 4)) * T(NRL_PDL(1)[0]));
-        }
-        // O
-        d[1] = mainDensity(G[5], T(NRL_PDM(1, 0)), T(NRL_PD(1)[0]), T(16.), T(0.0));
-        if (z <= T(300.0)) {
-            const T dm16 = dmv[2];
-            d[1] = nrl::Model<T>::dnet(d[1], dm16, zhm28, xmm, T(16.));
-            const T rl = T(NRL_PDM(1, 1)) * T(NRL_PDL(1)[16]) * (T(1.0) + T(NRL_PDL(0)[23]) * (T(eb.f107A) - T(150.0)));
-            d[1] = d[1] * nrl::Model<T>::ccor2(z, rl, T(NRL_PDM(1, 5)) * T(NRL_PDL(1)[3]),
-                                               T(NRL_PDM(1, 4)) * T(NRL_PDL(1)[2]), T(NRL_PDM(1, 5)) * T(NRL_PDL(1)[4]));
-            d[1] = d[1] * nrl::Model<T>::ccor(z, T(NRL_PDM(1, 3)) * T(NRL_PDL(1)[14]),
-                                              T(NRL_PDM(1, 7)) * T(NRL_PDL(1)[13]), T(NRL_PDM(1, 6)) * T(NRL_PDL(1)[12]));
-        }
-        // O2
-        d[3] = mainDensity(G[6], T(NRL_PDM(3, 0)), T(NRL_PD(4)[0]), T(32.), T(0.0));
-        if (z <= T(250.0)) {
-            const T b32 = bv[3], dm32 = dmv[3];
-            d[3] = nrl::Model<T>::dnet(d[3], dm32, zhm28, xmm, T(32.));
-            const T rl = log(b28 * T(NRL_PDM(3, 1)) / b32);
-            d[3] = d[3] * nrl::Model<T>::ccor(z, rl, T(NRL_PDM(3, 5)) * T(NRL_PDL(1)[7]), T(NRL_PDM(3, 4)) * T(NRL_PDL(1)[6]));
-        }
+        if (z <= T(160.0)) dm28 = dmv[0];
+        // The seven species densities, lane-parallel: lane j of the group
+        // takes species rows j, j + L, ... of eb.species (N, H, O, O2 first:
+        // the ones corrected at orbital altitudes) in one data-driven form,
+        // so the lanes of a group run the same instructions; the results are
+        // exchanged by shuffles.  Row -> d index, G task and correction task:
+        constexpr int kDPos[kNrlSpecies] = {7, 6, 1, 3, 4, 0, 2};
+        constexpr int kGIdx[kNrlSpecies] = {9, 8, 5, 6, 7, 4, 3};
+        constexpr int kTask[kNrlSpecies] = {6, 5, 2, 3, 4, 1, 0};
+        auto speciesDensity = [&](int r) -> T {
+            const double* __restrict__ q = eb.species[r];
+            T g = T(0), b = T(0), dm = T(0);
+#pragma unroll
+            for (int k = 0; k < kNrlSpecies; ++k)
+                if (k == r) {
+                    g = G[kGIdx[k]];
+                    b = bv[kTask[k]];
+                    dm = dmv[kTask[k]];
+                }
+            const T xm = T(q[kSpXm]);
+            T dn = mainDensity(g, T(q[kSpPdm0]), T(q[kSpPd0]), xm, T(q[kSpAlpha]));
+            if (z <= T(q[kSpLim])) {
+                dn = nrl::Model<T>::dnet(dn, dm, zhm28, xmm, xm);
+                const T r1 = q[kSpRlLog] != 0.0 ? log(b28 * T(q[kSpK1]) * T(q[kSpK2]) / b) : T(q[kSpK1]);
+                dn = dn * nrl::Model<T>::ccor2(z, r1, T(q[kSpC1H1]), T(q[kSpC1Zh]), T(q[kSpC1H2]));
+                if (q[kSpR2] != 0.0)
+                    dn = dn * nrl::Model<T>::ccor2(z, T(q[kSpR2]), T(q[kSpC2H]), T(q[kSpC2Zh]), T(q[kSpC2H]));
+            }
+            if (q[kSpRc] != 0.0)
+                dn = dn * nrl::Model<T>::ccor2(z, T(q[kSpRc]), T(q[kSpCaH1]), T(q[kSpCaZh]), T(q[kSpCaH2]));
+            return dn;
+        };
         {
-            const T rc32 = T(NRL_PDM(3, 3)) * T(NRL_PDL(1)[23]) * (T(1.) + T(NRL_PDL(0)[23]) * (T(eb.f107A) - T(150.)));
-            d[3] = d[3] * nrl::Model<T>::ccor2(z, rc32, T(NRL_PDM(3, 7)) * T(NRL_PDL(1)[22]),
-                                               T(NRL_PDM(3, 6)) * T(NRL_PDL(1)[21]), T(NRL_PDM(3, 7)) * T(NRL_PDL(0)[22]));
-        }
-        // Ar
-        d[4] = mainDensity(G[7], T(NRL_PDM(4, 0)), T(NRL_PD(5)[0]), T(40.), T(0.17));
-        if (z <= T(240.0)) {
-            const T b40 = bv[4], dm40 = dmv[4];
-            d[4] = nrl::Model<T>::dnet(d[4], dm40, zhm28, xmm, T(40.));
-            const T rl = log(b28 * T(NRL_PDM(4, 1)) / b40);
-            d[4] = d[4] * nrl::Model<T>::ccor(z, rl, T(NRL_PDM(4, 5)) * T(NRL_PDL(1)[9]), T(NRL_PDM(4, 4)) * T(NRL_PDL(1)[8]));
-        }
-        // H
-        d[6] = mainDensity(G[8], T(NRL_PDM(5, 0)), T(NRL_PD(6)[0]), T(1.), T(-0.38));
-        if (z <= T(320.0)) {
-            const T b01 = bv[5], dm01 = dmv[5];
-            d[6] = nrl::Model<T>::dnet(d[6], dm01, zhm28, xmm, T(1.));
-            const T rl = log(b28 * T(NRL_PDM(5, 1)) * fabs(T(NRL_PDL(1)[17])) / b01);
-            d[6] = d[6] * nrl::Model<T>::ccor(z, rl, T(NRL_PDM(5, 5)) * T(NRL_PDL(1)[11]), T(NRL_PDM(5, 4)) * T(NRL_PDL(1)[10]));
-            d[6] = d[6] * nrl::Model<T>::ccor(z, T(NRL_PDM(5, 3)) * T(NRL_PDL(1)[20]),
-                                              T(NRL_PDM(5, 7)) * T(NRL_PDL(1)[19]), T(NRL_PDM(5, 6)) * T(NRL_PDL(1)[18]));
-        }
-        // N
-        d[7] = mainDensity(G[9], T(NRL_PDM(6, 0)), T(NRL_PD(7)[0]), T(14.), T(0.0));
-        if (z <= T(450.0)) {
-            const T b14 = bv[6], dm14 = dmv[6];
-            d[7] = nrl::Model<T>::dnet(d[7], dm14, zhm28, xmm, T(14.));
-            const T rl = log(b28 * T(NRL_PDM(6, 1)) * fabs(T(NRL_PDL(0)[2])) / b14);
-            d[7] = d[7] * nrl::Model<T>::ccor(z, rl, T(NRL_PDM(6, 5)) * T(NRL_PDL(0)[1]), T(NRL_PDM(6, 4)) * T(NRL_PDL(0)[0]));
-            d[7] = d[7] * nrl::Model<T>::ccor(z, T(NRL_PDM(6, 3)) * T(NRL_PDL(0)[5]),
-                                              T(NRL_PDM(6, 7)) * T(NRL_PDL(0)[4]), T(NRL_PDM(6, 6)) * T(NRL_PDL(0)[3]));
+            const unsigned smask = L >= 32 ? 0xffffffffu : ((1u << L) - 1u) << groupBase;
+#pragma unroll
+            for (int rr = 0; rr < (kNrlSpecies + L - 1) / L; ++rr) {
+                const int r = rr * L + j;
+                T v = T(0);
+                if (r < kNrlSpecies) v = speciesDensity(r);
+#pragma unroll
+                for (int jj = 0; jj < L; ++jj) {
+                    const int rk = rr * L + jj;
+                    if (rk < kNrlSpecies) d[kDPos[rk]] = L == 1 ? v : __shfl_sync(smask, v, groupBase + jj);
+                }
+            }
         }
         // anomalous O: densu with tinf = tlb = tho, where ln(tlb/tt) = 0
         const T tho = T(NRL_PDM(7, 9)) * T(NRL_PDL(0)[6]);

@@ -117,7 +117,7 @@ struct StepParams {
 // CTA of few threads per SM (the coefficient tile fills shared memory), so
 // they get up to 255 registers per thread instead of spilling at 128.
 __host__ __device__ constexpr int maxStepThreads(int lanes) {
-    return lanes == 1 ? 256 : lanes == 2 ? 320 : lanes == 4 ? 384 : 512;
+    return lanes == 1 ? 256 : lanes == 2 ? 320 : 384;
 }
 
 void launchEpochRecords(const DevEnv& env, const double* epochs, int count, EpochRecord* out, cudaStream_t stream);
