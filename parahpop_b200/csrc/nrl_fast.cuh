@@ -558,60 +558,125 @@ struct Fast {
     // in the same operations as densu.
     struct LowProfile {
         T xs[5], ys[5], y2[5];
-        T zgdif, t1, zg2, tt;
+        T zgdif, rzgdif, t1, zg2, tt;
     };
+
+    // 1 / x for the positive, well-scaled denominators of the mesosphere
+    // profile (heights, temperatures, gravity ratios): a single-precision
+    // estimate refined by two Newton-Raphson steps r <- r + r (1 - x r)
+    // (relative error 2^-21 -> 2^-42 -> below one ulp), without the branches
+    // of the IEEE division sequence, so that independent quotients overlap.
+    static __device__ __forceinline__ double rcp(double x) {
+        double r = (double)__fdividef(1.0f, (float)x);
+        r = fma(r, fma(-x, r, 1.0), r);
+        return fma(r, fma(-x, r, 1.0), r);
+    }
+    static __device__ __forceinline__ float rcp(float x) { return 1.0f / x; }
+
+    // Clamped cubic spline through the five mesosphere nodes: the reference's
+    // tridiagonal sweep (spline, Nrlmsise00Model.inl:289) with the interval
+    // reciprocals and slopes formed once.
+    static __device__ __forceinline__ void spline5(const T* x, const T* y, T yp1, T ypn, T* y2) {
+        T r[4], d[4], u[4];
+        for (int i = 0; i < 4; ++i) {
+            r[i] = rcp(x[i + 1] - x[i]);
+            d[i] = (y[i + 1] - y[i]) * r[i];
+        }
+        y2[0] = T(-0.5);
+        u[0] = (T(3.0) * r[0]) * (d[0] - yp1);
+        for (int i = 1; i < 4; ++i) {
+            const T w = rcp(x[i + 1] - x[i - 1]);
+            const T sig = (x[i] - x[i - 1]) * w;
+            const T rp = rcp(sig * y2[i - 1] + T(2.0));
+            y2[i] = (sig - T(1.0)) * rp;
+            u[i] = (T(6.0) * (d[i] - d[i - 1]) * w - sig * u[i - 1]) * rp;
+        }
+        const T un = (T(3.0) * r[3]) * (ypn - d[3]);
+        y2[4] = (un - T(0.5) * u[3]) * rcp(T(0.5) * y2[3] + T(1.0));
+        for (int k = 3; k >= 0; --k) y2[k] = y2[k] * y2[k + 1] + u[k];
+    }
+
+    // spline value and integral from xa[0] (splint :256, splini :218) on the
+    // five nodes, with one reciprocal per interval
+    static __device__ __forceinline__ T splint5(const T* xa, const T* ya, const T* y2a, T x) {
+        int klo = 0, khi = 4;
+        while (khi - klo > 1) {
+            const int k = (khi + klo) >> 1;
+            if (xa[k] > x) khi = k;
+            else klo = k;
+        }
+        const T h = xa[khi] - xa[klo];
+        const T rh = rcp(h);
+        const T a = (xa[khi] - x) * rh;
+        const T b = (x - xa[klo]) * rh;
+        return a * ya[klo] + b * ya[khi] + ((a * a * a - a) * y2a[klo] + (b * b * b - b) * y2a[khi]) * h * h / T(6.0);
+    }
+    static __device__ __forceinline__ T splini5(const T* xa, const T* ya, const T* y2a, T x) {
+        T yi = T(0);
+        for (int klo = 0, khi = 1; x > xa[klo] && khi < 5; ++klo, ++khi) {
+            const T xx = khi < 4 ? (x < xa[khi] ? x : xa[khi]) : x;
+            const T h = xa[khi] - xa[klo];
+            const T rh = rcp(h);
+            const T a = (xa[khi] - xx) * rh;
+            const T b = (xx - xa[klo]) * rh;
+            const T a2 = a * a;
+            const T b2 = b * b;
+            yi += ((T(1.0) - a2) * ya[klo] * T(0.5) + b2 * ya[khi] * T(0.5)
+                   + ((-(T(1.0) + a2 * a2) * T(0.25) + a2 * T(0.5)) * y2a[klo]
+                      + (b2 * b2 * T(0.25) - b2 * T(0.5)) * y2a[khi]) * h * h / T(6.0)) * h;
+        }
+        return yi;
+    }
+
     static __device__ __noinline__ void lowProfile(LowProfile& lp, T tinf, T tlb, T zlb, T s2, const T* zn1, T re,
                                                    NrlMeso<T>& ms) {
-        auto zeta = [re](T zz, T zl) { return ((zz - zl) * (re + zl) / (re + zz)); };
-        const int mn1 = 5;
+        auto zeta = [re](T zz, T zl) { return (zz - zl) * (re + zl) * rcp(re + zz); };
         const T za = zn1[0];
         lp.zg2 = zeta(za, zlb);
         lp.tt = tinf - (tinf - tlb) * exp(-s2 * lp.zg2);
         const T ta = lp.tt;
-        const T q = (re + zlb) / (re + za);
+        const T q = (re + zlb) * rcp(re + za);
         ms.tgn1[0] = (tinf - ta) * s2 * (q * q);
         ms.tn1[0] = ta;
         const T z1 = zn1[0];
-        const T z2 = zn1[mn1 - 1];
+        const T z2 = zn1[4];
         lp.t1 = ms.tn1[0];
-        const T t2 = ms.tn1[mn1 - 1];
+        const T t2 = ms.tn1[4];
         lp.zgdif = zeta(z2, z1);
-        for (int k = 0; k < mn1; k++) {
-            lp.xs[k] = zeta(zn1[k], z1) / lp.zgdif;
-            lp.ys[k] = T(1.0) / ms.tn1[k];
-        }
-        const T r2 = (re + z2) / (re + z1);
-        const T yd1 = -ms.tgn1[0] / (lp.t1 * lp.t1) * lp.zgdif;
-        const T yd2 = -ms.tgn1[1] / (t2 * t2) * lp.zgdif * (r2 * r2);
-        nrl::Model<T>::spline(lp.xs, lp.ys, mn1, yd1, yd2, lp.y2);
+        lp.rzgdif = rcp(lp.zgdif);
+        lp.xs[0] = T(0.0);
+        lp.xs[4] = T(1.0);
+        for (int k = 1; k < 4; k++) lp.xs[k] = zeta(zn1[k], z1) * lp.rzgdif;
+        for (int k = 0; k < 5; k++) lp.ys[k] = rcp(ms.tn1[k]);
+        const T r2 = (re + z2) * rcp(re + z1);
+        const T yd1 = -ms.tgn1[0] * rcp(lp.t1 * lp.t1) * lp.zgdif;
+        const T yd2 = -ms.tgn1[1] * rcp(t2 * t2) * lp.zgdif * (r2 * r2);
+        spline5(lp.xs, lp.ys, yd1, yd2, lp.y2);
     }
     static __device__ __noinline__ T densuBelow(T alt, T dlb, T tinf, T tlb, T xm, T alpha, T zlb, T s2,
                                                 const T* zn1, T re, T gsurf, const LowProfile& lp) {
-        auto zeta = [re](T zz, T zl) { return ((zz - zl) * (re + zl) / (re + zz)); };
         const T rgas = T(831.4);
-        const int mn1 = 5;
-        const T z = (alt > zn1[mn1 - 1]) ? alt : zn1[mn1 - 1];
+        const T z = (alt > zn1[4]) ? alt : zn1[4];
         const T z1 = zn1[0];
-        const T zg = zeta(z, z1);
-        const T x = zg / lp.zgdif;
-        const T y = nrl::Model<T>::splint(lp.xs, lp.ys, lp.y2, mn1, x);
-        const T tz = T(1.0) / y;
+        const T zg = (z - z1) * (re + z1) * rcp(re + z);
+        const T x = zg * lp.rzgdif;
+        const T y = splint5(lp.xs, lp.ys, lp.y2, x);
+        const T tz = rcp(y);
         if (xm == T(0)) return tz;
         const T g1 = T(1.0) + zlb / re;
-        T glb = gsurf / (g1 * g1);
-        const T gamma = xm * glb / (s2 * rgas * tinf);
+        const T glb = gsurf * rcp(g1 * g1);
+        const T gamma = xm * glb * rcp(s2 * rgas * tinf);
         T expl = exp(-s2 * gamma * lp.zg2);
         if (expl > T(50.0)) expl = T(50.0);
         if (lp.tt <= T(0)) expl = T(50.0);
-        const T densu_temp = dlb * pow((tlb / lp.tt), ((T(1.0) + alpha + gamma))) * expl;
+        const T densuTemp = dlb * exp((T(1.0) + alpha + gamma) * log(tlb * rcp(lp.tt))) * expl;
         const T g2 = T(1.0) + z1 / re;
-        glb = gsurf / (g2 * g2);
-        const T gamm = xm * glb * lp.zgdif / rgas;
-        const T yi = nrl::Model<T>::splini(lp.xs, lp.ys, lp.y2, mn1, x);
+        const T gamm = xm * (gsurf * rcp(g2 * g2)) * lp.zgdif / rgas;
+        const T yi = splini5(lp.xs, lp.ys, lp.y2, x);
         expl = gamm * yi;
         if (expl > T(50.0)) expl = T(50.0);
         if (tz <= T(0)) expl = T(50.0);
-        return densu_temp * pow((lp.t1 / tz), (T(1.0) + alpha)) * exp(-expl);
+        return densuTemp * exp((T(1.0) + alpha) * log(lp.t1 * rcp(tz))) * exp(-expl);
     }
 
     // Monomial i of the globe7 basis (order of the coefficient rows; i is a
@@ -712,7 +777,9 @@ struct Fast {
     template <int L>
     __device__ __forceinline__ void globeTasks(T (&G)[kGlobeTasks], T& aptTlb, T& aptLast, int j, int groupBase) {
         static_assert(kGlobeRows % L == 0, "lane split of the coefficient rows");
-        constexpr int R = kGlobeRows / L;
+        // rows 13..15 are zero: lane j takes rows j, j + L, ... below 13 only
+        // (rows r L + j < 16 stay inside the block for every lane)
+        constexpr int R = (kApRowPd0 + 1 + L - 1) / L;
         const T x = plg[0][1], x2 = x * x;
         const T U1 = csec * c2gl - ssec * s2gl, U2 = ssec * c2gl + csec * s2gl;
         const double2* __restrict__ rows = reinterpret_cast<const double2*>(&eb.globeRows[0][0][0]);
