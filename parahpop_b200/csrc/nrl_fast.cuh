@@ -561,8 +561,9 @@ struct Fast {
         T zgdif, rzgdif, t1, zg2, tt;
     };
 
-    // 1 / x for the positive, well-scaled denominators of the mesosphere
-    // profile (heights, temperatures, gravity ratios): a single-precision
+    // 1 / x for the nonzero, well-scaled denominators of the mesosphere
+    // profile and the species corrections (heights, scale heights,
+    // temperatures, gravity ratios, mass differences): a single-precision
     // estimate refined by two Newton-Raphson steps r <- r + r (1 - x r)
     // (relative error 2^-21 -> 2^-42 -> below one ulp), without the branches
     // of the IEEE division sequence, so that independent quotients overlap.
@@ -626,6 +627,33 @@ struct Fast {
                       + (b2 * b2 * T(0.25) - b2 * T(0.5)) * y2a[khi]) * h * h / T(6.0)) * h;
         }
         return yi;
+    }
+
+    // dnet (Nrlmsise00Model.inl:180) and ccor2 (:138) for the species
+    // corrections: the same branches and operations, quotients by reciprocal
+    // and the power as exp(log(.) / a); ccor(z, r, h, zh) is ccor2 with
+    // h2 = h, whose second exponential is then the first.
+    static __device__ __forceinline__ T dnetFast(T dd, T dm, T zhm, T xmm, T xm) {
+        const T a = zhm * rcp(xmm - xm);
+        const T ra = (xmm - xm) * rcp(zhm);  // 1 / a
+        if (!((dm > T(0)) && (dd > T(0)))) {
+            if ((dd == T(0)) && (dm == T(0))) dd = T(1);
+            if (dm == T(0)) return dd;
+            if (dd == T(0)) return dm;
+        }
+        const T ylog = a * log(dm * rcp(dd));
+        if (ylog < T(-10)) return dd;
+        if (ylog > T(10)) return dm;
+        return dd * exp(log(T(1.0) + exp(ylog)) * ra);
+    }
+    static __device__ __forceinline__ T ccor2Fast(T alt, T r, T h1, T zh, T h2) {
+        const T e1 = (alt - zh) * rcp(h1);
+        const T e2 = h2 == h1 ? e1 : (alt - zh) * rcp(h2);
+        if ((e1 > T(70)) || (e2 > T(70))) return T(1.0);
+        if ((e1 < T(-70)) && (e2 < T(-70))) return exp(r);
+        const T ex1 = exp(e1);
+        const T ex2 = h2 == h1 ? ex1 : exp(e2);
+        return exp(r * rcp(T(1.0) + T(0.5) * (ex1 + ex2)));
     }
 
     static __device__ __noinline__ void lowProfile(LowProfile& lp, T tinf, T tlb, T zlb, T s2, const T* zn1, T re,
@@ -1019,14 +1047,13 @@ struct Fast {
             const T xm = T(q[kSpXm]);
             T dn = mainDensity(g, T(q[kSpPdm0]), T(q[kSpPd0]), xm, T(q[kSpAlpha]));
             if (z <= T(q[kSpLim])) {
-                dn = nrl::Model<T>::dnet(dn, dm, zhm28, xmm, xm);
-                const T r1 = q[kSpRlLog] != 0.0 ? log(b28 * T(q[kSpK1]) * T(q[kSpK2]) / b) : T(q[kSpK1]);
-                dn = dn * nrl::Model<T>::ccor2(z, r1, T(q[kSpC1H1]), T(q[kSpC1Zh]), T(q[kSpC1H2]));
-                if (q[kSpR2] != 0.0)
-                    dn = dn * nrl::Model<T>::ccor2(z, T(q[kSpR2]), T(q[kSpC2H]), T(q[kSpC2Zh]), T(q[kSpC2H]));
+                dn = dnetFast(dn, dm, zhm28, xmm, xm);
+                const T r1 = q[kSpRlLog] != 0.0 ? log(b28 * T(q[kSpK1]) * T(q[kSpK2]) * rcp(b)) : T(q[kSpK1]);
+                dn = dn * ccor2Fast(z, r1, T(q[kSpC1H1]), T(q[kSpC1Zh]), T(q[kSpC1H2]));
+                if (q[kSpR2] != 0.0) dn = dn * ccor2Fast(z, T(q[kSpR2]), T(q[kSpC2H]), T(q[kSpC2Zh]), T(q[kSpC2H]));
             }
             if (q[kSpRc] != 0.0)
-                dn = dn * nrl::Model<T>::ccor2(z, T(q[kSpRc]), T(q[kSpCaH1]), T(q[kSpCaZh]), T(q[kSpCaH2]));
+                dn = dn * ccor2Fast(z, T(q[kSpRc]), T(q[kSpCaH1]), T(q[kSpCaZh]), T(q[kSpCaH2]));
             return dn;
         };
         {
