@@ -139,8 +139,12 @@ static void loadEphemeris(const std::string& path, HostEnvironment& env) {
     for (const Value& u : core.items()) {
         const Value& md = u.at("metadata");
         if (md.at("frame").asInt() != 1) throw std::runtime_error("Ephemeris units must use the ICRF frame (1): " + path);
-        if (md.at("dtype").asInt() != 2)
-            throw std::runtime_error("Only Type-2 Chebyshev position units are supported: " + path);
+        // Type 2: position coefficients; Type 3: position and velocity
+        // coefficients (brie/core/Type3BodyUnit.h: six component blocks, the
+        // position blocks first).  The force model reads positions only.
+        const int64_t dtype = md.at("dtype").asInt();
+        if (dtype != 2 && dtype != 3)
+            throw std::runtime_error("Only Type-2 and Type-3 Chebyshev units are supported: " + path);
         EphUnitHost e;
         e.target = (int)md.at("target").asInt();
         e.center = (int)md.at("center").asInt();
@@ -151,8 +155,11 @@ static void loadEphemeris(const std::string& path, HostEnvironment& env) {
         const Value& d = u.at("data");
         e.data.resize(d.size());
         for (size_t k = 0; k < d.size(); ++k) e.data[k] = d[k].asDouble();
-        if (e.data.size() != (size_t)(1 + e.nint + 3 * (e.pdeg + 1) * e.nint))
+        const size_t positions = (size_t)(1 + e.nint + 3 * (e.pdeg + 1) * e.nint);
+        const size_t expected = dtype == 3 ? positions + (size_t)(3 * (e.pdeg + 1) * e.nint) : positions;
+        if (e.data.size() != expected)
             throw std::runtime_error("Ephemeris unit size mismatch for target " + std::to_string(e.target));
+        e.data.resize(positions);  // the velocity blocks of a Type-3 unit are not used
         env.eph.push_back(std::move(e));
     }
 }

@@ -312,6 +312,7 @@ class EnvSpec:
     relativity: bool = True
     drag: bool = True
     srp: bool = True
+    ephemeris_type: int = 2       # 2: Chebyshev positions; 3: positions and velocities (6 blocks)
 
 
 def kaula_field(degree, seed, zonal_only=False):
@@ -379,8 +380,11 @@ def body_functions():
     return {"earth": earth_ssb, "sun": sun_ssb, "moon": moon_earth, "jupiter": jupiter_ssb}
 
 
-def cheb_unit(fn, target, center, start_mjd, end_mjd, seg_days, pdeg=13):
-    """Fit a Type-2 Chebyshev unit (positions) to ``fn`` over [start, end)."""
+def cheb_unit(fn, target, center, start_mjd, end_mjd, seg_days, pdeg=13, dtype=2):
+    """Fit a Chebyshev unit to ``fn`` over [start, end): Type 2 holds the
+    position coefficients (X, Y, Z blocks); Type 3 adds velocity blocks (VX,
+    VY, VZ: the time derivative of the position fit, km/s, padded to the same
+    degree), as ``brie/core/Type3BodyUnit.h`` reads them."""
     nint = int(math.ceil((end_mjd - start_mjd) / seg_days))
     radius = seg_days * SECONDS_PER_DAY / 2.0
     starts = [mjd2000_to_et(start_mjd + k * seg_days) for k in range(nint)]
@@ -396,18 +400,24 @@ def cheb_unit(fn, target, center, start_mjd, end_mjd, seg_days, pdeg=13):
     data = [radius] + starts
     for d in range(3):
         data += coef[d].reshape(-1).tolist()  # index k + j*n
-    meta = {"frame": 1, "dtype": 2, "target": target, "center": center, "nintervals": nint,
+    if dtype == 3:
+        for d in range(3):
+            vel = np.zeros((pdeg + 1, nint))
+            for k in range(nint):
+                vel[:pdeg, k] = np.polynomial.chebyshev.chebder(coef[d, :, k]) / radius
+            data += vel.reshape(-1).tolist()
+    meta = {"frame": 1, "dtype": dtype, "target": target, "center": center, "nintervals": nint,
             "pdeg": pdeg, "startEpoch": starts[0], "finalEpoch": starts[0] + nint * 2 * radius}
     return {"metadata": meta, "data": data}
 
 
-def write_brie(path, start_mjd, end_mjd):
+def write_brie(path, start_mjd, end_mjd, dtype=2):
     f = body_functions()
     units = [
-        cheb_unit(f["sun"], 10, 0, start_mjd, end_mjd, 8.0),
-        cheb_unit(f["earth"], 399, 0, start_mjd, end_mjd, 8.0),
-        cheb_unit(f["moon"], 301, 399, start_mjd, end_mjd, 4.0),
-        cheb_unit(f["jupiter"], 5, 0, start_mjd, end_mjd, 32.0),
+        cheb_unit(f["sun"], 10, 0, start_mjd, end_mjd, 8.0, dtype=dtype),
+        cheb_unit(f["earth"], 399, 0, start_mjd, end_mjd, 8.0, dtype=dtype),
+        cheb_unit(f["moon"], 301, 399, start_mjd, end_mjd, 4.0, dtype=dtype),
+        cheb_unit(f["jupiter"], 5, 0, start_mjd, end_mjd, 32.0, dtype=dtype),
     ]
     with open(path, "wb") as fh:
         fh.write(cbor_dumps({"layout": 1, "core": units}))
@@ -478,7 +488,7 @@ def write_environment(directory, spec: EnvSpec = EnvSpec()) -> Path:
     d.mkdir(parents=True, exist_ok=True)
     C, S = kaula_field(spec.degree, spec.seed, spec.zonal_only)
     write_tab(d / "gravity.tab", C, S, spec.gm_tab, spec.r_tab, spec.degree)
-    write_brie(d / "bodies.brie", spec.start_mjd, spec.end_mjd)
+    write_brie(d / "bodies.brie", spec.start_mjd, spec.end_mjd, spec.ephemeris_type)
     write_brot2(d / "earth.brot2", spec.start_mjd, spec.end_mjd)
     write_space_weather(d / "SW-All.txt", spec.start_mjd, spec.end_mjd)
     write_eop(d / "EOP-All.txt", spec.start_mjd, spec.end_mjd)

@@ -10,7 +10,9 @@ Runs where the reference sources are available and built into oracle/_ref
   600 s, final-step shortening at 65 s and 5 s, per-object epochs / masses,
   33 objects across a block boundary, central-gravity invariants; plus the
   benchmark configurations' shapes at small sizes and the reference's other
-  force options (J2 model, single-band and piecewise exponential drag).
+  force options (J2 model, single-band and piecewise exponential drag, the
+  Moon as a second occulter, the tide-free tide system) and Type-3
+  Chebyshev ephemeris units.
 * ``nrlmsise00_kat.json`` - NRLMSISE-00 densities from the reference model
   sources (oracle/_ref/ref_kat) on an input grid.
 * ``tides_kat.json`` - solid / ocean tide coefficient sets and the tide and
@@ -144,6 +146,8 @@ def lunar_penumbra():
 # tide-free tide system
 CASES["lunar_shadow_30m"] = (lunar_penumbra, 1800.0, 60.0, {"occulting": ("Earth", "Moon")}, {})
 CASES["tide_free_2h"] = (lambda: S.population_leo(16, 16), 7200.0, 60.0, {"tide_system": "tide_free"}, {})
+# Type-3 Chebyshev ephemeris units (position and velocity blocks)
+CASES["type3_ephemeris_1h"] = (lambda: S.population_leo(16, 17), 3600.0, 60.0, {}, {"ephemeris_type": 3})
 
 
 def make_propagation_goldens(only=None):
