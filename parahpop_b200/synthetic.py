@@ -313,6 +313,8 @@ class EnvSpec:
     drag: bool = True
     srp: bool = True
     ephemeris_type: int = 2       # 2: Chebyshev positions; 3: positions and velocities (6 blocks)
+    ephemeris_chain: str = "direct"  # "direct": Earth, Sun, Jupiter -> SSB, Moon -> Earth; "emb": DE440's
+                                     # Earth and Moon -> Earth-Moon barycenter (3) -> SSB
 
 
 def kaula_field(degree, seed, zonal_only=False):
@@ -411,14 +413,26 @@ def cheb_unit(fn, target, center, start_mjd, end_mjd, seg_days, pdeg=13, dtype=2
     return {"metadata": meta, "data": data}
 
 
-def write_brie(path, start_mjd, end_mjd, dtype=2):
+def write_brie(path, start_mjd, end_mjd, dtype=2, chain="direct"):
     f = body_functions()
-    units = [
-        cheb_unit(f["sun"], 10, 0, start_mjd, end_mjd, 8.0, dtype=dtype),
-        cheb_unit(f["earth"], 399, 0, start_mjd, end_mjd, 8.0, dtype=dtype),
-        cheb_unit(f["moon"], 301, 399, start_mjd, end_mjd, 4.0, dtype=dtype),
-        cheb_unit(f["jupiter"], 5, 0, start_mjd, end_mjd, 32.0, dtype=dtype),
-    ]
+    if chain == "emb":
+        # DE440's layout: the Earth-Moon barycenter about the SSB, the Earth
+        # and the Moon about the barycenter (mass ratio from the constants)
+        k = 4902.800192171393 / (398600.4415 + 4902.800192171393)
+        units = [
+            cheb_unit(f["sun"], 10, 0, start_mjd, end_mjd, 8.0, dtype=dtype),
+            cheb_unit(lambda t: f["earth"](t) + k * f["moon"](t), 3, 0, start_mjd, end_mjd, 8.0, dtype=dtype),
+            cheb_unit(lambda t: -k * f["moon"](t), 399, 3, start_mjd, end_mjd, 4.0, dtype=dtype),
+            cheb_unit(lambda t: (1.0 - k) * f["moon"](t), 301, 3, start_mjd, end_mjd, 4.0, dtype=dtype),
+            cheb_unit(f["jupiter"], 5, 0, start_mjd, end_mjd, 32.0, dtype=dtype),
+        ]
+    else:
+        units = [
+            cheb_unit(f["sun"], 10, 0, start_mjd, end_mjd, 8.0, dtype=dtype),
+            cheb_unit(f["earth"], 399, 0, start_mjd, end_mjd, 8.0, dtype=dtype),
+            cheb_unit(f["moon"], 301, 399, start_mjd, end_mjd, 4.0, dtype=dtype),
+            cheb_unit(f["jupiter"], 5, 0, start_mjd, end_mjd, 32.0, dtype=dtype),
+        ]
     with open(path, "wb") as fh:
         fh.write(cbor_dumps({"layout": 1, "core": units}))
 
@@ -488,7 +502,7 @@ def write_environment(directory, spec: EnvSpec = EnvSpec()) -> Path:
     d.mkdir(parents=True, exist_ok=True)
     C, S = kaula_field(spec.degree, spec.seed, spec.zonal_only)
     write_tab(d / "gravity.tab", C, S, spec.gm_tab, spec.r_tab, spec.degree)
-    write_brie(d / "bodies.brie", spec.start_mjd, spec.end_mjd, spec.ephemeris_type)
+    write_brie(d / "bodies.brie", spec.start_mjd, spec.end_mjd, spec.ephemeris_type, spec.ephemeris_chain)
     write_brot2(d / "earth.brot2", spec.start_mjd, spec.end_mjd)
     write_space_weather(d / "SW-All.txt", spec.start_mjd, spec.end_mjd)
     write_eop(d / "EOP-All.txt", spec.start_mjd, spec.end_mjd)

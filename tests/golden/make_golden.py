@@ -148,6 +148,10 @@ CASES["lunar_shadow_30m"] = (lunar_penumbra, 1800.0, 60.0, {"occulting": ("Earth
 CASES["tide_free_2h"] = (lambda: S.population_leo(16, 16), 7200.0, 60.0, {"tide_system": "tide_free"}, {})
 # Type-3 Chebyshev ephemeris units (position and velocity blocks)
 CASES["type3_ephemeris_1h"] = (lambda: S.population_leo(16, 17), 3600.0, 60.0, {}, {"ephemeris_type": 3})
+# DE440's chain layout: Earth and Moon about the Earth-Moon barycenter
+CASES["emb_chain_1h"] = (lambda: S.population_leo(16, 19), 3600.0, 60.0, {}, {"ephemeris_chain": "emb"})
+# a degree-120 field file truncated to degree / order 70 by the configuration
+CASES["truncated_120_to_70_1h"] = (lambda: S.population_leo(16, 18), 3600.0, 60.0, {"degree": 70}, {"degree": 120})
 
 
 def make_propagation_goldens(only=None):
