@@ -747,6 +747,8 @@ __global__ void __launch_bounds__(maxStepThreads(L), 1) propagateKernel(const __
             }
             const double t0 = SHARED_GRID ? p.stepT0[kstep] : cur;
             const double dt = SHARED_GRID ? p.stepDt[kstep] : dtv;
+            // one copy of the force model: the stage loop is not unrolled
+#pragma unroll 1
             for (int s = 0; s < 13; ++s) {
                 double ys[CPL];
                 combine<CPL>(s, y, kst, dt, ys);
