@@ -122,6 +122,32 @@ class _Env(C.Structure):
     ]
 
 
+STATE_INT_KEYS = ["frame", "dtype", "target", "center", "nintervals", "pdeg", "@offset", "@size"]
+ORIENTATION_INT_KEYS = ["unit_type", "target", "model_id", "interp_id", "n_nodes_nut", "n_nodes_erp",
+                        "lag_order_nut", "lag_order_erp", "", "", "@offset", "@size"]
+
+
+def brie_units(j, int_keys):
+    """Units of a BRIE file in layout 1 (a list of {metadata, data}) or layout
+    2 (member-major metadata arrays over one data array; brie/util/cbor.cpp
+    211-379 and the readers' member enums)."""
+    while isinstance(j, list) and len(j) == 1:
+        j = j[0]
+    if j["layout"] == 1:
+        return j["core"]
+    assert j["layout"] == 2, "unknown BRIE layout"
+    md, data = j["core"]["metadata"], j["core"]["data"]
+    n, im, dm = md["nBodyUnits"], md["intMetadata"], md.get("doubleMetadata")
+    assert len(im) == len(int_keys) * n
+    units = []
+    for i in range(n):
+        meta = {k: im[q * n + i] for q, k in enumerate(int_keys) if k}
+        if dm is not None:
+            meta["startEpoch"], meta["finalEpoch"] = dm[i], dm[n + i]
+        units.append({"metadata": meta, "data": data[meta["@offset"]:meta["@offset"] + meta["@size"]]})
+    return units
+
+
 def _dp(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
@@ -246,9 +272,7 @@ def load_environment(config_path) -> Environment:
     # ephemeris
     units = []
     for f in envc.get("ephemeris", []):
-        j = cbor_loads(P(f).read_bytes())
-        assert j["layout"] == 1, "only layout 1 is read by the oracle"
-        units += j["core"]
+        units += brie_units(cbor_loads(P(f).read_bytes()), STATE_INT_KEYS)
     off = np.zeros(len(units), dtype=np.int64)
     data = []
     o = 0
@@ -265,8 +289,7 @@ def load_environment(config_path) -> Environment:
     e.eph_data = _dp(hold(np.array(data, dtype=np.float64)))
     # orientation
     for f in envc.get("orientations", []):
-        j = cbor_loads(P(f).read_bytes())
-        for u in j["core"]:
+        for u in brie_units(cbor_loads(P(f).read_bytes()), ORIENTATION_INT_KEYS):
             if u["metadata"]["unit_type"] == 4:
                 e.has_rot = 1
                 e.rot_nnut = u["metadata"]["n_nodes_nut"]

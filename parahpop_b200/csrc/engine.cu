@@ -125,36 +125,94 @@ static void loadShTable(const Value& shape, HostEnvironment& env) {
     env.hasShape = true;
 }
 
-static const Value& cborCore(const Value& root, const std::string& path) {
-    const Value* layout = root.find("layout");
+// One unit of a BRIE file: its metadata fields by name and its data.
+struct BrieUnit {
+    std::map<std::string, double> md;
+    std::vector<double> data;
+    double at(const std::string& k) const {
+        auto it = md.find(k);
+        if (it == md.end()) throw std::runtime_error("BRIE unit lacks metadata field '" + k + "'");
+        return it->second;
+    }
+};
+
+// Units of a BRIE file in either layout (brie/util/cbor.cpp:211-379).
+// Layout 1: core = [{metadata: {...}, data: [...]}, ...].  Layout 2: core =
+// {metadata: {nBodyUnits, intMetadata, doubleMetadata}, data: [...]}, the
+// reader's member arrays written out member-major (member k of unit i at
+// k * nBodyUnits + i); `intKeys` names the integer members in order ("" for
+// members the reader here does not use), and the two real members are the
+// start and final epochs.  Single-element array wrappers around the top-level
+// map are removed, as the reference's reader does.
+static std::vector<BrieUnit> brieUnits(const Value& file, const std::string& path,
+                                       const std::vector<std::string>& intKeys) {
+    const Value* root = &file;
+    while (root->isArray() && root->size() == 1) root = &root->items()[0];
+    const Value* layout = root->find("layout");
     if (!layout) throw std::runtime_error("Unknown BRIE layout type: " + path);
-    if (layout->asInt() != 1)
+    std::vector<BrieUnit> out;
+    if (layout->asInt() == 1) {
+        for (const Value& u : root->at("core").items()) {
+            BrieUnit b;
+            for (const auto& kv : u.at("metadata").members())
+                if (kv.second.isNumber()) b.md[kv.first] = kv.second.asDouble();
+            const Value& d = u.at("data");
+            b.data.resize(d.size());
+            for (size_t k = 0; k < d.size(); ++k) b.data[k] = d[k].asDouble();
+            out.push_back(std::move(b));
+        }
+        return out;
+    }
+    if (layout->asInt() != 2)
         throw std::runtime_error("BRIE layout " + std::to_string(layout->asInt()) + " is not supported: " + path);
-    return root.at("core");
+    const Value& core = root->at("core");
+    const Value& meta = core.at("metadata");
+    const int64_t n = meta.at("nBodyUnits").asInt();
+    const Value& im = meta.at("intMetadata");
+    const Value* dm = meta.find("doubleMetadata");
+    const Value& data = core.at("data");
+    const int64_t nk = (int64_t)intKeys.size();
+    if (n < 0 || (int64_t)im.size() != nk * n || (dm && (int64_t)dm->size() != 2 * n))
+        throw std::runtime_error("BRIE layout-2 metadata sizes do not match nBodyUnits: " + path);
+    for (int64_t i = 0; i < n; ++i) {
+        BrieUnit b;
+        for (int64_t k = 0; k < nk; ++k)
+            if (!intKeys[k].empty()) b.md[intKeys[k]] = (double)im[(size_t)(k * n + i)].asInt();
+        if (dm) {
+            b.md["startEpoch"] = (*dm)[(size_t)i].asDouble();
+            b.md["finalEpoch"] = (*dm)[(size_t)(n + i)].asDouble();
+        }
+        const int64_t off = (int64_t)b.at("@offset"), size = (int64_t)b.at("@size");
+        if (off < 0 || size < 0 || off + size > (int64_t)data.size())
+            throw std::runtime_error("BRIE layout-2 unit data out of range: " + path);
+        b.data.resize((size_t)size);
+        for (int64_t k = 0; k < size; ++k) b.data[(size_t)k] = data[(size_t)(off + k)].asDouble();
+        out.push_back(std::move(b));
+    }
+    return out;
 }
 
 static void loadEphemeris(const std::string& path, HostEnvironment& env) {
     const Value root = parseCbor(readBinaryFile(path));
-    const Value& core = cborCore(root, path);
-    for (const Value& u : core.items()) {
-        const Value& md = u.at("metadata");
-        if (md.at("frame").asInt() != 1) throw std::runtime_error("Ephemeris units must use the ICRF frame (1): " + path);
+    // state units' integer members (brie/states/metadata/RefEphUnit.h:13-25)
+    for (const BrieUnit& u : brieUnits(root, path, {"frame", "dtype", "target", "center", "nintervals", "pdeg",
+                                                   "@offset", "@size"})) {
+        const BrieUnit& md = u;
+        if ((int)md.at("frame") != 1) throw std::runtime_error("Ephemeris units must use the ICRF frame (1): " + path);
         // Type 2: position coefficients; Type 3: position and velocity
         // coefficients (brie/core/Type3BodyUnit.h: six component blocks, the
         // position blocks first).  The force model reads positions only.
-        const int64_t dtype = md.at("dtype").asInt();
+        const int64_t dtype = (int64_t)md.at("dtype");
         if (dtype != 2 && dtype != 3)
             throw std::runtime_error("Only Type-2 and Type-3 Chebyshev units are supported: " + path);
         EphUnitHost e;
-        e.target = (int)md.at("target").asInt();
-        e.center = (int)md.at("center").asInt();
-        e.nint = (int)md.at("nintervals").asInt();
-        e.pdeg = (int)md.at("pdeg").asInt();
-        e.startEpoch = md.at("startEpoch").asDouble();
-        e.finalEpoch = md.at("finalEpoch").asDouble();
-        const Value& d = u.at("data");
-        e.data.resize(d.size());
-        for (size_t k = 0; k < d.size(); ++k) e.data[k] = d[k].asDouble();
+        e.target = (int)md.at("target");
+        e.center = (int)md.at("center");
+        e.nint = (int)md.at("nintervals");
+        e.pdeg = (int)md.at("pdeg");
+        e.startEpoch = md.at("startEpoch");
+        e.finalEpoch = md.at("finalEpoch");
+        e.data = u.data;
         const size_t positions = (size_t)(1 + e.nint + 3 * (e.pdeg + 1) * e.nint);
         const size_t expected = dtype == 3 ? positions + (size_t)(3 * (e.pdeg + 1) * e.nint) : positions;
         if (e.data.size() != expected)
@@ -166,22 +224,23 @@ static void loadEphemeris(const std::string& path, HostEnvironment& env) {
 
 static void loadOrientation(const std::string& path, HostEnvironment& env) {
     const Value root = parseCbor(readBinaryFile(path));
-    const Value& core = cborCore(root, path);
-    for (const Value& u : core.items()) {
-        const Value& md = u.at("metadata");
-        const int type = (int)md.at("unit_type").asInt();
+    // orientation units' integer members, model-based family
+    // (brie/orientations/metadata/Layout.h:10-84)
+    for (const BrieUnit& u : brieUnits(root, path, {"unit_type", "target", "model_id", "interp_id", "n_nodes_nut",
+                                                   "n_nodes_erp", "lag_order_nut", "lag_order_erp", "", "",
+                                                   "@offset", "@size"})) {
+        const BrieUnit& md = u;
+        const int type = (int)md.at("unit_type");
         if (type != 4)
             throw std::runtime_error("Orientation unit type " + std::to_string(type) + " is not supported: " + path);
-        if (md.at("lag_order_nut").asInt() != 5 || md.at("lag_order_erp").asInt() != 3)
+        if ((int)md.at("lag_order_nut") != 5 || (int)md.at("lag_order_erp") != 3)
             throw std::runtime_error("IERS2000 units must use Lagrange orders 5 (nutation) and 3 (ERP): " + path);
         env.hasRot = true;
-        env.rotNnut = (int)md.at("n_nodes_nut").asInt();
-        env.rotNerp = (int)md.at("n_nodes_erp").asInt();
-        env.rotStart = md.at("startEpoch").asDouble();
-        env.rotFinal = md.at("finalEpoch").asDouble();
-        const Value& d = u.at("data");
-        env.rotData.resize(d.size());
-        for (size_t k = 0; k < d.size(); ++k) env.rotData[k] = d[k].asDouble();
+        env.rotNnut = (int)md.at("n_nodes_nut");
+        env.rotNerp = (int)md.at("n_nodes_erp");
+        env.rotStart = md.at("startEpoch");
+        env.rotFinal = md.at("finalEpoch");
+        env.rotData = u.data;
         if (env.rotData.size() != (size_t)(3 * env.rotNnut + 6 * env.rotNerp + 4))
             throw std::runtime_error("IERS2000 unit size mismatch: " + path);
     }

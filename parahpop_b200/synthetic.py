@@ -315,6 +315,7 @@ class EnvSpec:
     ephemeris_type: int = 2       # 2: Chebyshev positions; 3: positions and velocities (6 blocks)
     ephemeris_chain: str = "direct"  # "direct": Earth, Sun, Jupiter -> SSB, Moon -> Earth; "emb": DE440's
                                      # Earth and Moon -> Earth-Moon barycenter (3) -> SSB
+    brie_layout: int = 1          # CBOR layout of bodies.brie and earth.brot2 (1: unit list; 2: member arrays)
 
 
 def kaula_field(degree, seed, zonal_only=False):
@@ -413,7 +414,32 @@ def cheb_unit(fn, target, center, start_mjd, end_mjd, seg_days, pdeg=13, dtype=2
     return {"metadata": meta, "data": data}
 
 
-def write_brie(path, start_mjd, end_mjd, dtype=2, chain="direct"):
+STATE_INT_KEYS = ("frame", "dtype", "target", "center", "nintervals", "pdeg")
+ORIENTATION_INT_KEYS = ("unit_type", "target", "model_id", "interp_id", "n_nodes_nut", "n_nodes_erp",
+                        "lag_order_nut", "lag_order_erp", None, None)
+
+
+def brie_layout2(units, int_keys) -> dict:
+    """Layout-2 form of a unit list: the reader's member arrays written out
+    member-major (member k of unit i at k * n + i), each unit's data offset
+    and size as the last two integer members, then the start and final
+    epochs as the real members, over one concatenated data array."""
+    n = len(units)
+    cols = [[] for _ in range(len(int_keys) + 2)]
+    data = []
+    for u in units:
+        for q, k in enumerate(int_keys):
+            cols[q].append(int(u["metadata"][k]) if k else 0)
+        cols[-2].append(len(data))
+        cols[-1].append(len(u["data"]))
+        data += [float(x) for x in u["data"]]
+    return {"layout": 2, "core": {"metadata": {
+        "nBodyUnits": n, "intMetadata": [v for c in cols for v in c],
+        "doubleMetadata": [float(u["metadata"]["startEpoch"]) for u in units]
+        + [float(u["metadata"]["finalEpoch"]) for u in units]}, "data": data}}
+
+
+def write_brie(path, start_mjd, end_mjd, dtype=2, chain="direct", layout=1):
     f = body_functions()
     if chain == "emb":
         # DE440's layout: the Earth-Moon barycenter about the SSB, the Earth
@@ -434,10 +460,10 @@ def write_brie(path, start_mjd, end_mjd, dtype=2, chain="direct"):
             cheb_unit(f["jupiter"], 5, 0, start_mjd, end_mjd, 32.0, dtype=dtype),
         ]
     with open(path, "wb") as fh:
-        fh.write(cbor_dumps({"layout": 1, "core": units}))
+        fh.write(cbor_dumps(brie_layout2(units, STATE_INT_KEYS) if layout == 2 else {"layout": 1, "core": units}))
 
 
-def write_brot2(path, start_mjd, end_mjd):
+def write_brot2(path, start_mjd, end_mjd, layout=1):
     """IERS2000 unit: X, Y, s (rad) on a 1-day TT grid, ERP on daily keys.
     Constant EOP: xp = yp = 0, UT1-UTC = 0.3 s, TAI-UTC = 34 s."""
     t0 = start_mjd - 3.0
@@ -458,7 +484,9 @@ def write_brot2(path, start_mjd, end_mjd):
             "n_nodes_nut": n_nut, "n_nodes_erp": n_erp, "lag_order_nut": 5, "lag_order_erp": 3,
             "startEpoch": mjd2000_to_et(start_mjd - 1.0), "finalEpoch": mjd2000_to_et(end_mjd + 1.0)}
     with open(path, "wb") as fh:
-        fh.write(cbor_dumps({"layout": 1, "core": [{"metadata": meta, "data": data}]}))
+        unit = {"metadata": meta, "data": data}
+        fh.write(cbor_dumps(brie_layout2([unit], ORIENTATION_INT_KEYS) if layout == 2
+                            else {"layout": 1, "core": [unit]}))
 
 
 def write_space_weather(path, start_mjd, end_mjd, f107=150.0, ap=15):
@@ -502,8 +530,9 @@ def write_environment(directory, spec: EnvSpec = EnvSpec()) -> Path:
     d.mkdir(parents=True, exist_ok=True)
     C, S = kaula_field(spec.degree, spec.seed, spec.zonal_only)
     write_tab(d / "gravity.tab", C, S, spec.gm_tab, spec.r_tab, spec.degree)
-    write_brie(d / "bodies.brie", spec.start_mjd, spec.end_mjd, spec.ephemeris_type, spec.ephemeris_chain)
-    write_brot2(d / "earth.brot2", spec.start_mjd, spec.end_mjd)
+    write_brie(d / "bodies.brie", spec.start_mjd, spec.end_mjd, spec.ephemeris_type, spec.ephemeris_chain,
+               spec.brie_layout)
+    write_brot2(d / "earth.brot2", spec.start_mjd, spec.end_mjd, spec.brie_layout)
     write_space_weather(d / "SW-All.txt", spec.start_mjd, spec.end_mjd)
     write_eop(d / "EOP-All.txt", spec.start_mjd, spec.end_mjd)
     (d / "constants.json").write_text(json.dumps(CONSTANTS, indent=2) + "\n")

@@ -150,6 +150,8 @@ CASES["tide_free_2h"] = (lambda: S.population_leo(16, 16), 7200.0, 60.0, {"tide_
 CASES["type3_ephemeris_1h"] = (lambda: S.population_leo(16, 17), 3600.0, 60.0, {}, {"ephemeris_type": 3})
 # DE440's chain layout: Earth and Moon about the Earth-Moon barycenter
 CASES["emb_chain_1h"] = (lambda: S.population_leo(16, 19), 3600.0, 60.0, {}, {"ephemeris_chain": "emb"})
+# the ephemeris and orientation files in CBOR layout 2 (member arrays)
+CASES["layout2_files_1h"] = (lambda: S.population_leo(16, 20), 3600.0, 60.0, {}, {"brie_layout": 2})
 # a degree-120 field file truncated to degree / order 70 by the configuration
 CASES["truncated_120_to_70_1h"] = (lambda: S.population_leo(16, 18), 3600.0, 60.0, {"degree": 70}, {"degree": 120})
 
