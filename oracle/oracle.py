@@ -119,12 +119,17 @@ class _Env(C.Structure):
         ("eop_n", C.c_int), ("eop_first_mjd", C.c_double), ("eop", C.POINTER(C.c_double)),
         ("body_j2", C.POINTER(C.c_double)), ("body_gm_const", C.POINTER(C.c_double)),
         ("body_soi", C.POINTER(C.c_double)), ("n_exp", C.c_int), ("exp_seg", C.POINTER(C.c_double)),
+        ("rot_kind", C.c_int), ("rot_nint", C.c_int), ("rot_pdeg", C.c_int), ("rot_ecliptic", C.c_int),
     ]
 
 
 STATE_INT_KEYS = ["frame", "dtype", "target", "center", "nintervals", "pdeg", "@offset", "@size"]
-ORIENTATION_INT_KEYS = ["unit_type", "target", "model_id", "interp_id", "n_nodes_nut", "n_nodes_erp",
-                        "lag_order_nut", "lag_order_erp", "", "", "@offset", "@size"]
+ORIENTATION_INT_KEYS = ["unit_type", "@m1", "@m2", "@m3", "@m4", "@m5", "@m6", "@m7", "", "", "@offset", "@size"]
+# names of the positional members per orientation unit type (Layout.h)
+ORIENTATION_FIELDS = {4: {"target": "@m1", "model_id": "@m2", "interp_id": "@m3", "n_nodes_nut": "@m4",
+                          "n_nodes_erp": "@m5", "lag_order_nut": "@m6", "lag_order_erp": "@m7"},
+                      3: {"frameClassID": "@m1", "inertialFrame": "@m2", "dtype": "@m3", "nintervals": "@m4",
+                          "pdeg": "@m5"}}
 
 
 def brie_units(j, int_keys):
@@ -195,6 +200,7 @@ def load_environment(config_path) -> Environment:
     # bodies (sorted by NAIF id, Bodies.h:105-120)
     rows = []
     flattening = 0.0
+    earth_orientation = None
     shape = None
     atm = None
     exp_segments = []
@@ -229,6 +235,7 @@ def load_environment(config_path) -> Environment:
             flags |= F_OCCULTING
         if name == "Earth":
             flattening = bc.get("flattening", 0.0)
+            earth_orientation = bc.get("orientation")
         cst = byid.get(nid, {})
         gm = bc.get("gm", cst.get("GM", 0.0))
         radius = cst.get("R", 0.0)
@@ -288,13 +295,36 @@ def load_environment(config_path) -> Environment:
     e.eph_offset = hold(off).ctypes.data_as(C.POINTER(C.c_int64))
     e.eph_data = _dp(hold(np.array(data, dtype=np.float64)))
     # orientation
+    # Earth frames: ITRF93 (binary Chebyshev angles, target 3000) and the
+    # IERS2000 model unit (3001); bodies.Earth.orientation picks one, else
+    # the unique loaded one (interface naming/orientations Resolver.h)
+    frames = {}
     for f in envc.get("orientations", []):
         for u in brie_units(cbor_loads(P(f).read_bytes()), ORIENTATION_INT_KEYS):
-            if u["metadata"]["unit_type"] == 4:
-                e.has_rot = 1
-                e.rot_nnut = u["metadata"]["n_nodes_nut"]
-                e.rot_nerp = u["metadata"]["n_nodes_erp"]
-                e.rot_data = _dp(hold(np.array(u["data"], dtype=np.float64)))
+            md = u["metadata"]
+            kind = md["unit_type"]
+            if kind not in ORIENTATION_FIELDS:
+                continue
+            for name, member in ORIENTATION_FIELDS[kind].items():
+                md.setdefault(name, md.get(member))
+            target = md["target"] if kind == 4 else md["frameClassID"]
+            if target in (3000, 3001):
+                frames[target] = (kind, md, u["data"])
+    want = {"ITRF93": 3000, "ITRF": 3000, "EARTH_FIXED": 3000, "ITRF_IERS2000": 3001, "ITRF_IPF": 3001,
+            "ITRF_NATIVE": 3001}.get(str(earth_orientation).upper()) if earth_orientation else None
+    if want is None and len(frames) > 1:
+        raise ValueError("Body 399 has more than one loaded high-precision orientation frame")
+    sel = frames.get(want) if want else (next(iter(frames.values())) if frames else None)
+    if sel is not None:
+        kind, md, data = sel
+        e.has_rot = 1
+        e.rot_kind = kind
+        e.rot_data = _dp(hold(np.array(data, dtype=np.float64)))
+        if kind == 4:
+            e.rot_nnut, e.rot_nerp = md["n_nodes_nut"], md["n_nodes_erp"]
+        else:
+            e.rot_nint, e.rot_pdeg = md["nintervals"], md["pdeg"]
+            e.rot_ecliptic = 1 if md["inertialFrame"] == 17 else 0
     # atmosphere
     if atm is not None:
         recs = []

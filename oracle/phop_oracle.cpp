@@ -83,6 +83,9 @@ typedef struct {
     const double* body_soi;       // per body sphere of influence, km (1e20 when absent)
     int n_exp;                    // exponential atmosphere bands (0: none)
     const double* exp_seg;        // 4 x n_exp component-major: rho0, h0, scaleHeight, hCutoff; ascending h0
+    // Earth frame: 4 = the IERS2000 unit above; 3 = binary Chebyshev Euler
+    // angles in rot_data ([r, starts, 3 angle blocks], ITRF93)
+    int rot_kind, rot_nint, rot_pdeg, rot_ecliptic;
 } OracleEnv;
 
 }  // extern "C"
@@ -239,7 +242,85 @@ void mat3mul(double C[9], const double A[9], const double B[9]) {
 }
 
 // ICRF -> ITRF rotation R and inertial angular velocity w at ET `t`
+// ICRF -> ITRF93 from a binary orientation unit (orientations/RefEphUnit.h
+// :769-790 and :890-900, frames/Rotation.h:124-133, frames/Frames.h:57-166):
+// angles RA = v0 - pi/2, Dec = pi/2 - v1, PM = v2 mod 2 pi from three
+// Chebyshev series, R = Rz(PM) Rx(pi/2 - Dec) Rz(pi/2 + RA) [Rx(obliquity)
+// for ECLIPJ2000-based units], omega from the 3-1-3 Euler kinematics.
+void binaryEarthRotation(const OracleEnv& e, double t, double R[9], V3* w) {
+    const double* d = e.rot_data;
+    const int n = e.rot_nint, deg = e.rot_pdeg;
+    const double r = d[0];
+    const double* starts = d + 1;
+    const double* cf = d + 1 + n;
+    long idx = (long)((t - starts[0]) / (2 * r));
+    if (idx < 0) idx = 0;
+    if (idx >= n) idx = n - 1;
+    const double s = (t - starts[idx]) / r - 1.0;
+    double v[3], vd[3];
+    for (int dim = 0; dim < 3; ++dim) {
+        // Chebyshev series and its derivative by the three-term recurrences
+        // T_{k+1} = 2 s T_k - T_{k-1}, T'_{k+1} = 2 T_k + 2 s T'_k - T'_{k-1}
+        const double* c = cf + (int64_t)dim * (deg + 1) * n;
+        double T0 = 1.0, T1 = s, D0 = 0.0, D1 = 1.0;
+        double sum = c[idx], dsum = 0.0;
+        if (deg >= 1) {
+            sum += c[idx + n] * T1;
+            dsum += c[idx + n] * D1;
+        }
+        for (int k = 2; k <= deg; ++k) {
+            const double T2 = 2.0 * s * T1 - T0, D2 = 2.0 * T1 + 2.0 * s * D1 - D0;
+            sum += c[idx + (int64_t)k * n] * T2;
+            dsum += c[idx + (int64_t)k * n] * D2;
+            T0 = T1;
+            T1 = T2;
+            D0 = D1;
+            D1 = D2;
+        }
+        v[dim] = sum;
+        vd[dim] = dsum / r;
+    }
+    const double ra = v[0] - M_PI / 2, dec = M_PI / 2 - v[1], pm = fmod(v[2], 2 * M_PI);
+    const double a1 = M_PI / 2 + ra, a2 = M_PI / 2 - dec;
+    auto rz = [](double a, double M[9]) {
+        const double c = cos(a), sn = sin(a);
+        const double m[9] = {c, sn, 0, -sn, c, 0, 0, 0, 1};
+        for (int k = 0; k < 9; ++k) M[k] = m[k];
+    };
+    auto rx = [](double a, double M[9]) {
+        const double c = cos(a), sn = sin(a);
+        const double m[9] = {1, 0, 0, 0, c, sn, 0, -sn, c};
+        for (int k = 0; k < 9; ++k) M[k] = m[k];
+    };
+    auto mul = [](const double A[9], const double B[9], double C[9]) {
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) C[3 * i + j] = A[3 * i] * B[j] + A[3 * i + 1] * B[3 + j] + A[3 * i + 2] * B[6 + j];
+    };
+    double Z1[9], X[9], Z3[9], T[9], A[9];
+    rz(a1, Z1);
+    rx(a2, X);
+    rz(pm, Z3);
+    mul(X, Z1, T);
+    mul(Z3, T, A);
+    const double raDot = vd[0], decDot = -vd[1], pmDot = vd[2];
+    V3 om = {decDot * sin(ra) + pmDot * cos(ra) * cos(dec), -decDot * cos(ra) + pmDot * sin(ra) * cos(dec),
+             raDot + pmDot * sin(dec)};
+    if (e.rot_ecliptic) {
+        double E[9];
+        rx(84381.448 / 3600.0 * (M_PI / 180.0), E);
+        mul(A, E, R);
+        om = {om.x, E[4] * om.y + E[7] * om.z, E[5] * om.y + E[8] * om.z};  // E^T omega
+    } else {
+        for (int k = 0; k < 9; ++k) R[k] = A[k];
+    }
+    if (w) *w = om;
+}
+
 void earthRotation(const OracleEnv& e, double t, double R[9], V3* w) {
+    if (e.rot_kind == 3) {
+        binaryEarthRotation(e, t, R, w);
+        return;
+    }
     const double inv = 1.0 / 86400.0;
     const double tdbMjd = t * inv + 0.5;
     const double g = (M_PI / 180.0) * (357.53 + 0.9856003 * (tdbMjd - 0.5));

@@ -68,6 +68,7 @@ struct DevEnv {
     const double* ephData;
     // IERS2000 orientation unit
     int hasRot, rotNnut, rotNerp;
+    int rotKind, rotNint, rotPdeg, rotEcliptic;  // 4: IERS2000 model unit; 3: binary Chebyshev Euler angles
     const double* rotData;
     // NRLMSISE-00 weather
     int hasNrl, nrlNdays;
@@ -209,8 +210,79 @@ static __device__ __forceinline__ void mat3mul(double C[9], const double A[9], c
         for (int j = 0; j < 3; ++j) C[3 * i + j] = A[3 * i] * B[j] + A[3 * i + 1] * B[3 + j] + A[3 * i + 2] * B[6 + j];
 }
 
+// ICRF -> ITRF93 rotation and inertial angular velocity from a binary
+// orientation unit: three Chebyshev angle series (v0, v1, v2) and their rates
+// (the Type-2 evaluation of the ephemeris, parm chebyshev Interpolator.h),
+// RA = v0 - pi/2, Dec = pi/2 - v1, PM = v2 mod 2 pi
+// (orientations/RefEphUnit.h:769-790, rates :890-900 with the Dec sign
+// flipped), the rotation Rz(PM) Rx(pi/2 - Dec) Rz(pi/2 + RA)
+// (frames/Rotation.h:124-133), composed with the ICRF -> ECLIPJ2000 bias
+// Rx(obliquity) for ecliptic-based units, and the body rate from the 3-1-3
+// Euler kinematics mapped back to ICRF (frames/Frames.h:57-166).
+static __device__ void binaryEarthRotation(const DevEnv& e, double t, double R[9], double w[3]) {
+    const double* d = e.rotData;
+    const int n = e.rotNint, deg = e.rotPdeg;
+    const double r = d[0];
+    const double* starts = d + 1;
+    const double* cf = d + 1 + n;
+    long idx = (long)((t - starts[0]) / (2 * r));
+    idx = idx < 0 ? 0 : (idx >= n ? n - 1 : idx);
+    const double s = (t - starts[idx]) / r - 1.0;
+    const double s2 = 2 * s;
+    double val[3], rate[3];
+    for (int dim = 0; dim < 3; ++dim) {
+        const double* c = cf + (int64_t)dim * (deg + 1) * n;
+        double b1 = 0, b0 = 0, db1 = 0, db0 = 0;
+        for (int i = 0; i < deg; ++i) {
+            b1 = c[idx + (int64_t)(deg - i) * n] - b1;
+            const double nb = fma(s2, b0, b1);
+            b1 = b0;
+            b0 = nb;
+            const double nd = fma(s2, db0, fma(2.0, b1, -db1));
+            db1 = db0;
+            db0 = nd;
+        }
+        val[dim] = fma(s, b0, c[idx] - b1);
+        rate[dim] = (1.0 / r) * fma(s, db0, b0 - db1);
+    }
+    const double ra = val[0] - M_PI / 2, dec = M_PI / 2 - val[1], pm = fmod(val[2], 2 * M_PI);
+    const double raDot = rate[0], decDot = -rate[1], pmDot = rate[2];
+    // passive Z-X-Z rotation with angles a1 = pi/2 + RA, a2 = pi/2 - Dec, a3 = PM
+    double s1, c1, sx, cx, s3, c3;
+    sincos(M_PI / 2 + ra, &s1, &c1);
+    sincos(M_PI / 2 - dec, &sx, &cx);
+    sincos(pm, &s3, &c3);
+    const double A[9] = {c3 * c1 - s3 * cx * s1, c3 * s1 + s3 * cx * c1, s3 * sx,
+                         -s3 * c1 - c3 * cx * s1, -s3 * s1 + c3 * cx * c1, c3 * sx,
+                         sx * s1, -sx * c1, cx};
+    double sa, ca, sd, cd;
+    sincos(ra, &sa, &ca);
+    sincos(dec, &sd, &cd);
+    double om[3] = {decDot * sa + pmDot * ca * cd, -decDot * ca + pmDot * sa * cd, raDot + pmDot * sd};
+    if (e.rotEcliptic) {
+        const double eps = 84381.448 / 3600.0 * (M_PI / 180.0);
+        double se, ce;
+        sincos(eps, &se, &ce);
+        const double E[9] = {1, 0, 0, 0, ce, se, 0, -se, ce};  // ICRF -> ECLIPJ2000
+        mat3mul(R, A, E);
+        // omega_icrf = E^T omega_ecl
+        const double o1 = ce * om[1] - se * om[2], o2 = se * om[1] + ce * om[2];
+        om[1] = o1;
+        om[2] = o2;
+    } else {
+        for (int k = 0; k < 9; ++k) R[k] = A[k];
+    }
+    w[0] = om[0];
+    w[1] = om[1];
+    w[2] = om[2];
+}
+
 // ICRF -> ITRF rotation and inertial angular velocity of the IERS2000 unit
 static __device__ void earthRotation(const DevEnv& e, double t, double R[9], double w[3]) {
+    if (e.rotKind == 3) {
+        binaryEarthRotation(e, t, R, w);
+        return;
+    }
     const double inv = 1.0 / 86400.0;
     const double tdbMjd = t * inv + 0.5;
     const double g = (M_PI / 180.0) * (357.53 + 0.9856003 * (tdbMjd - 0.5));

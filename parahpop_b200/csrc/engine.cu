@@ -222,28 +222,107 @@ static void loadEphemeris(const std::string& path, HostEnvironment& env) {
     }
 }
 
-static void loadOrientation(const std::string& path, HostEnvironment& env) {
+// An Earth orientation unit of an orientation file.
+struct EarthFrameUnit {
+    int kind = 0, target = 0;
+    int nnut = 0, nerp = 0, nint = 0, pdeg = 0, ecliptic = 0;
+    double start = 0.0, final = 0.0;
+    std::vector<double> data;
+};
+
+// Orientation units (brie/orientations/metadata/Layout.h:10-84,
+// orientations/metadata/EphUnit.cpp:60-160): integer member 0 is the unit
+// type, member 1 the rotation-data target, members 2.. depend on the type
+// (binary frames: inertialFrame, dtype, nintervals, pdeg; model units:
+// model_id, interp_id, n_nodes_nut, n_nodes_erp, lag_order_nut,
+// lag_order_erp).  Earth units are kept: the binary ITRF93 frame (target
+// 3000) and the IERS2000 model frame (target 3001); units of other bodies
+// are not used by the force model.
+static void loadOrientation(const std::string& path, std::vector<EarthFrameUnit>& earth) {
     const Value root = parseCbor(readBinaryFile(path));
-    // orientation units' integer members, model-based family
-    // (brie/orientations/metadata/Layout.h:10-84)
-    for (const BrieUnit& u : brieUnits(root, path, {"unit_type", "target", "model_id", "interp_id", "n_nodes_nut",
-                                                   "n_nodes_erp", "lag_order_nut", "lag_order_erp", "", "",
-                                                   "@offset", "@size"})) {
-        const BrieUnit& md = u;
-        const int type = (int)md.at("unit_type");
-        if (type != 4)
+    const std::vector<std::string> members = {"unit_type", "@m1", "@m2", "@m3", "@m4", "@m5", "@m6", "@m7",
+                                              "", "", "@offset", "@size"};
+    for (const BrieUnit& u : brieUnits(root, path, members)) {
+        // a layout-1 unit names its fields; a layout-2 unit has them by position
+        auto field = [&](const char* name, const char* member) {
+            auto it = u.md.find(name);
+            return it != u.md.end() ? it->second : u.at(member);
+        };
+        const int type = (int)u.at("unit_type");
+        EarthFrameUnit f;
+        f.kind = type;
+        f.data = u.data;
+        if (type == 4) {
+            f.target = (int)field("target", "@m1");
+            if ((int)field("lag_order_nut", "@m6") != 5 || (int)field("lag_order_erp", "@m7") != 3)
+                throw std::runtime_error("IERS2000 units must use Lagrange orders 5 (nutation) and 3 (ERP): " + path);
+            f.nnut = (int)field("n_nodes_nut", "@m4");
+            f.nerp = (int)field("n_nodes_erp", "@m5");
+            if (f.data.size() != (size_t)(3 * f.nnut + 6 * f.nerp + 4))
+                throw std::runtime_error("IERS2000 unit size mismatch: " + path);
+        } else if (type == 3) {
+            f.target = (int)field("frameClassID", "@m1");
+            const int inertial = (int)field("inertialFrame", "@m2");
+            if (inertial != 1 && inertial != 17)
+                throw std::runtime_error("Binary orientation units must be relative to J2000 (1) or ECLIPJ2000 (17): "
+                                         + path);
+            f.ecliptic = inertial == 17;
+            if ((int)field("dtype", "@m3") != 2)
+                throw std::runtime_error("Binary orientation units must hold Chebyshev angles (dtype 2): " + path);
+            f.nint = (int)field("nintervals", "@m4");
+            f.pdeg = (int)field("pdeg", "@m5");
+            if (f.nint <= 0 || f.pdeg < 0 || f.data.size() != (size_t)(1 + f.nint + 3 * (f.pdeg + 1) * f.nint))
+                throw std::runtime_error("Binary orientation unit size mismatch: " + path);
+        } else if (type == 1 || type == 2) {
+            continue;  // IAU body models and their barycentric terms: not used for the Earth here
+        } else {
             throw std::runtime_error("Orientation unit type " + std::to_string(type) + " is not supported: " + path);
-        if ((int)md.at("lag_order_nut") != 5 || (int)md.at("lag_order_erp") != 3)
-            throw std::runtime_error("IERS2000 units must use Lagrange orders 5 (nutation) and 3 (ERP): " + path);
-        env.hasRot = true;
-        env.rotNnut = (int)md.at("n_nodes_nut");
-        env.rotNerp = (int)md.at("n_nodes_erp");
-        env.rotStart = md.at("startEpoch");
-        env.rotFinal = md.at("finalEpoch");
-        env.rotData = u.data;
-        if (env.rotData.size() != (size_t)(3 * env.rotNnut + 6 * env.rotNerp + 4))
-            throw std::runtime_error("IERS2000 unit size mismatch: " + path);
+        }
+        if (f.target != 3000 && f.target != 3001) continue;
+        f.start = u.at("startEpoch");
+        f.final = u.at("finalEpoch");
+        earth.push_back(std::move(f));
     }
+}
+
+// The Earth frame the force model uses (interface/naming/orientations
+// Resolver.h:40-88, Registry.h:580-640): an explicit
+// bodies.Earth.orientation picks ITRF93 (aliases ITRF, EARTH_FIXED; target
+// 3000) or ITRF_IERS2000 (ITRF_IPF, ITRF_NATIVE; 3001); otherwise the unique
+// loaded one.
+static void selectEarthFrame(const std::vector<EarthFrameUnit>& earth, HostEnvironment& env) {
+    int want = 0;
+    if (!env.earthOrientation.empty()) {
+        std::string n = env.earthOrientation;
+        std::transform(n.begin(), n.end(), n.begin(), ::toupper);
+        if (n == "ITRF93" || n == "ITRF" || n == "EARTH_FIXED") want = 3000;
+        else if (n == "ITRF_IERS2000" || n == "ITRF_IPF" || n == "ITRF_NATIVE") want = 3001;
+        else throw std::runtime_error("Unknown Earth orientation '" + env.earthOrientation
+                                      + "'; this backend supports ITRF93 and ITRF_IERS2000.");
+    }
+    const EarthFrameUnit* pick = nullptr;
+    for (const EarthFrameUnit& f : earth) {
+        if (want && f.target != want) continue;
+        if (pick && pick->target != f.target)
+            throw std::runtime_error("Body 399 has more than one loaded high-precision orientation frame; set "
+                                     "bodies.<name>.orientation explicitly to choose between them");
+        if (!pick) pick = &f;
+    }
+    if (want && !pick)
+        throw std::runtime_error("Body orientation '" + env.earthOrientation
+                                 + "' needs its rotation data loaded; add the defining .brot to the "
+                                   "environment's orientations");
+    if (!pick) return;
+    env.hasRot = true;
+    env.rotKind = pick->kind;
+    env.rotNnut = pick->nnut;
+    env.rotNerp = pick->nerp;
+    env.rotNint = pick->nint;
+    env.rotPdeg = pick->pdeg;
+    env.rotEcliptic = pick->ecliptic;
+    env.rotStart = pick->start;
+    env.rotFinal = pick->final;
+    env.rotData = pick->data;
 }
 
 static double calendarMjd(int year, int month, int day) {
@@ -475,6 +554,9 @@ void loadEnvironment(const Value& model, HostEnvironment& env) {
                     throw std::runtime_error("Unknown atmosphere model: '" + f.second.members()[0].first
                                              + "'.  Supported: exponential, nrlmsise00.");
                 }
+            } else if (k == "orientation") {
+                if (b.id != 399) throw std::runtime_error("Body orientations are supported for the Earth only.");
+                env.earthOrientation = f.second.asString();
             } else if (k == "flattening") {
                 if (b.id == 399) env.flattening = f.second.asDouble();
             } else if (k == "gm") {
@@ -505,8 +587,12 @@ void loadEnvironment(const Value& model, HostEnvironment& env) {
     if (!haveEarth) throw std::runtime_error("The Earth (center of integration) must be configured.");
     if (const Value* eph = e.find("ephemeris"))
         for (const Value& p : eph->items()) loadEphemeris(p.asString(), env);
-    if (const Value* ori = e.find("orientations"))
-        for (const Value& p : ori->items()) loadOrientation(p.asString(), env);
+    {
+        std::vector<EarthFrameUnit> earthFrames;
+        if (const Value* ori = e.find("orientations"))
+            for (const Value& p : ori->items()) loadOrientation(p.asString(), earthFrames);
+        selectEarthFrame(earthFrames, env);
+    }
     if (atmosphere) loadSpaceWeather(*atmosphere, env);
     if (const Value* ec = e.find("earthCorrections")) {
         env.solid = ec->find("solidEarthTides") && ec->at("solidEarthTides").asBool();
@@ -518,7 +604,8 @@ void loadEnvironment(const Value& model, HostEnvironment& env) {
         if (env.solid || env.ocean) loadEop(ec->at("eopFile").asString(), env);
     }
     if ((env.hasShape || env.hasNrl || env.solid || env.ocean) && !env.hasRot)
-        throw std::runtime_error("An Earth orientation (IERS2000) unit is required for the configured forces.");
+        throw std::runtime_error("An Earth orientation unit (ITRF93 or IERS2000) is required for the configured "
+                                 "forces.");
 }
 
 // ---- engine --------------------------------------------------------------------------------------------
@@ -688,8 +775,12 @@ void Engine::uploadEnvironment() {
     e.ephOffset = upload(owned_, off);
     e.ephData = upload(owned_, data);
     e.hasRot = h.hasRot;
+    e.rotKind = h.rotKind;
     e.rotNnut = h.rotNnut;
     e.rotNerp = h.rotNerp;
+    e.rotNint = h.rotNint;
+    e.rotPdeg = h.rotPdeg;
+    e.rotEcliptic = h.rotEcliptic;
     e.rotData = upload(owned_, h.rotData);
     e.hasNrl = h.hasNrl;
     e.nrlNdays = h.nrlNdays;

@@ -50,9 +50,15 @@ struct HostEnvironment {
     std::vector<EphUnitHost> eph;
     // orientation (IERS2000 unit)
     bool hasRot = false;
-    int rotNnut = 0, rotNerp = 0;
+    // the Earth frame in use: 4 = IERS2000 model unit (target 3001), 3 =
+    // binary Chebyshev Euler angles (ITRF93, target 3000)
+    int rotKind = 0;
+    int rotNnut = 0, rotNerp = 0;      // kind 4: Lagrange node counts
+    int rotNint = 0, rotPdeg = 0;      // kind 3: Chebyshev intervals and degree
+    int rotEcliptic = 0;               // kind 3: angles relative to ECLIPJ2000 (inertialFrame 17)
     double rotStart = 0.0, rotFinal = 0.0;
     std::vector<double> rotData;
+    std::string earthOrientation;      // bodies.Earth.orientation (empty: the unique loaded frame)
     // exponential atmosphere bands {rho0, h0, scaleHeight, hCutoff}, ascending h0
     std::vector<std::array<double, 4>> expSeg;
     // NRLMSISE-00

@@ -316,6 +316,8 @@ class EnvSpec:
     ephemeris_chain: str = "direct"  # "direct": Earth, Sun, Jupiter -> SSB, Moon -> Earth; "emb": DE440's
                                      # Earth and Moon -> Earth-Moon barycenter (3) -> SSB
     brie_layout: int = 1          # CBOR layout of bodies.brie and earth.brot2 (1: unit list; 2: member arrays)
+    earth_frame: str = "iers"     # earth.brot2 holds: "iers" the IERS2000 model unit (3001), "itrf93" a binary
+                                  # Chebyshev Euler-angle unit (3000, ECLIPJ2000-based), "both" the two
 
 
 def kaula_field(degree, seed, zonal_only=False):
@@ -415,8 +417,10 @@ def cheb_unit(fn, target, center, start_mjd, end_mjd, seg_days, pdeg=13, dtype=2
 
 
 STATE_INT_KEYS = ("frame", "dtype", "target", "center", "nintervals", "pdeg")
-ORIENTATION_INT_KEYS = ("unit_type", "target", "model_id", "interp_id", "n_nodes_nut", "n_nodes_erp",
-                        "lag_order_nut", "lag_order_erp", None, None)
+ORIENTATION_INT_KEYS = {4: ("unit_type", "target", "model_id", "interp_id", "n_nodes_nut", "n_nodes_erp",
+                            "lag_order_nut", "lag_order_erp", None, None),
+                        3: ("unit_type", "frameClassID", "inertialFrame", "dtype", "nintervals", "pdeg",
+                            None, None, None, None)}
 
 
 def brie_layout2(units, int_keys) -> dict:
@@ -425,10 +429,12 @@ def brie_layout2(units, int_keys) -> dict:
     and size as the last two integer members, then the start and final
     epochs as the real members, over one concatenated data array."""
     n = len(units)
-    cols = [[] for _ in range(len(int_keys) + 2)]
+    width = len(next(iter(int_keys.values()))) if isinstance(int_keys, dict) else len(int_keys)
+    cols = [[] for _ in range(width + 2)]
     data = []
     for u in units:
-        for q, k in enumerate(int_keys):
+        keys = int_keys[u["metadata"]["unit_type"]] if isinstance(int_keys, dict) else int_keys
+        for q, k in enumerate(keys):
             cols[q].append(int(u["metadata"][k]) if k else 0)
         cols[-2].append(len(data))
         cols[-1].append(len(u["data"]))
@@ -463,7 +469,29 @@ def write_brie(path, start_mjd, end_mjd, dtype=2, chain="direct", layout=1):
         fh.write(cbor_dumps(brie_layout2(units, STATE_INT_KEYS) if layout == 2 else {"layout": 1, "core": units}))
 
 
-def write_brot2(path, start_mjd, end_mjd, layout=1):
+def itrf93_unit(start_mjd, end_mjd, seg_days=8.0, pdeg=13):
+    """Binary orientation unit for ITRF93 (target 3000) relative to
+    ECLIPJ2000: Chebyshev series of the three Euler angles v0 = pi/2 + RA,
+    v1 = pi/2 - Dec, v2 = W of the pole and prime meridian in ecliptic
+    coordinates — the ICRF pole (RA pi/2, Dec pi/2 - obliquity) with small
+    slow pole and rate perturbations, W the Earth rotation angle."""
+    eps = math.radians(84381.448 / 3600.0)
+
+    def angles(t):  # t in days from MJD2000 0 (TDB)
+        v0 = math.pi + 1.0e-4 * np.sin(2.0 * math.pi * t / 6798.4) + 2.0e-7 * t
+        v1 = eps + 4.0e-5 * np.cos(2.0 * math.pi * t / 6798.4)
+        w = 2.0 * math.pi * (0.7790572732640 + 1.00273781191135448 * (t - 0.5)) + 3.0e-6 * np.sin(2.0 * math.pi * t)
+        return np.stack([v0, v1, w], -1)
+
+    u = cheb_unit(angles, 3000, 0, start_mjd, end_mjd, seg_days, pdeg)
+    md = u["metadata"]
+    u["metadata"] = {"unit_type": 3, "frameClassID": 3000, "inertialFrame": 17, "dtype": 2,
+                     "nintervals": md["nintervals"], "pdeg": md["pdeg"], "startEpoch": md["startEpoch"],
+                     "finalEpoch": md["finalEpoch"]}
+    return u
+
+
+def write_brot2(path, start_mjd, end_mjd, layout=1, frame="iers"):
     """IERS2000 unit: X, Y, s (rad) on a 1-day TT grid, ERP on daily keys.
     Constant EOP: xp = yp = 0, UT1-UTC = 0.3 s, TAI-UTC = 34 s."""
     t0 = start_mjd - 3.0
@@ -484,9 +512,13 @@ def write_brot2(path, start_mjd, end_mjd, layout=1):
             "n_nodes_nut": n_nut, "n_nodes_erp": n_erp, "lag_order_nut": 5, "lag_order_erp": 3,
             "startEpoch": mjd2000_to_et(start_mjd - 1.0), "finalEpoch": mjd2000_to_et(end_mjd + 1.0)}
     with open(path, "wb") as fh:
-        unit = {"metadata": meta, "data": data}
-        fh.write(cbor_dumps(brie_layout2([unit], ORIENTATION_INT_KEYS) if layout == 2
-                            else {"layout": 1, "core": [unit]}))
+        units = []
+        if frame in ("iers", "both"):
+            units.append({"metadata": meta, "data": data})
+        if frame in ("itrf93", "both"):
+            units.append(itrf93_unit(start_mjd - 2.0, end_mjd + 2.0))
+        fh.write(cbor_dumps(brie_layout2(units, ORIENTATION_INT_KEYS) if layout == 2
+                            else {"layout": 1, "core": units}))
 
 
 def write_space_weather(path, start_mjd, end_mjd, f107=150.0, ap=15):
@@ -532,7 +564,7 @@ def write_environment(directory, spec: EnvSpec = EnvSpec()) -> Path:
     write_tab(d / "gravity.tab", C, S, spec.gm_tab, spec.r_tab, spec.degree)
     write_brie(d / "bodies.brie", spec.start_mjd, spec.end_mjd, spec.ephemeris_type, spec.ephemeris_chain,
                spec.brie_layout)
-    write_brot2(d / "earth.brot2", spec.start_mjd, spec.end_mjd, spec.brie_layout)
+    write_brot2(d / "earth.brot2", spec.start_mjd, spec.end_mjd, spec.brie_layout, spec.earth_frame)
     write_space_weather(d / "SW-All.txt", spec.start_mjd, spec.end_mjd)
     write_eop(d / "EOP-All.txt", spec.start_mjd, spec.end_mjd)
     (d / "constants.json").write_text(json.dumps(CONSTANTS, indent=2) + "\n")
@@ -552,7 +584,7 @@ def make_config(env_dir, duration, step, max_steps=1000000, threads=1, force="fu
                 degree=70, bodies=("Sun", "Moon", "JupiterBarycenter"), tides=True,
                 relativity=True, drag=True, srp=True, start_mjd=4016.0, end_mjd=4064.0,
                 gravity="shape", atmosphere="nrlmsise00", tide_system="zero_tide",
-                occulting=("Earth",)) -> dict:
+                occulting=("Earth",), earth_orientation=None) -> dict:
     """Run configuration in the reference schema (``example/config/envisat_full.json``).
     Paths are relative to ``env_dir`` (where the config file is written).
     ``gravity``: "shape" (the spherical-harmonic file) or "oblateness" (the
@@ -568,6 +600,8 @@ def make_config(env_dir, duration, step, max_steps=1000000, threads=1, force="fu
             grav = {"shape": {"body": "Earth", "file": "gravity.tab", "delimiter": ",",
                               "headerLines": 0, "degree": degree, "order": degree}}
         earth = {"occulting": "Earth" in occulting, "flattening": 0.0033528106647474805, "gravity": grav}
+        if earth_orientation:
+            earth["orientation"] = earth_orientation
         if drag and force == "full":
             if atmosphere == "exponential":
                 earth["atmosphere"] = {"exponential": {"rho0": 3.725e-3, "h0": 400.0, "scaleHeight": 58.515,

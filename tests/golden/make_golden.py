@@ -152,6 +152,11 @@ CASES["type3_ephemeris_1h"] = (lambda: S.population_leo(16, 17), 3600.0, 60.0, {
 CASES["emb_chain_1h"] = (lambda: S.population_leo(16, 19), 3600.0, 60.0, {}, {"ephemeris_chain": "emb"})
 # the ephemeris and orientation files in CBOR layout 2 (member arrays)
 CASES["layout2_files_1h"] = (lambda: S.population_leo(16, 20), 3600.0, 60.0, {}, {"brie_layout": 2})
+# the Earth frame from a binary Chebyshev Euler-angle unit (ITRF93,
+# ECLIPJ2000-based), alone and chosen explicitly beside the IERS2000 unit
+CASES["itrf93_frame_1h"] = (lambda: S.population_leo(16, 21), 3600.0, 60.0, {}, {"earth_frame": "itrf93"})
+CASES["itrf93_selected_1h"] = (lambda: S.population_leo(16, 22), 3600.0, 60.0, {"earth_orientation": "ITRF93"},
+                               {"earth_frame": "both", "brie_layout": 2})
 # a degree-120 field file truncated to degree / order 70 by the configuration
 CASES["truncated_120_to_70_1h"] = (lambda: S.population_leo(16, 18), 3600.0, 60.0, {"degree": 70}, {"degree": 120})
 
