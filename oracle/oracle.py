@@ -120,16 +120,23 @@ class _Env(C.Structure):
         ("body_j2", C.POINTER(C.c_double)), ("body_gm_const", C.POINTER(C.c_double)),
         ("body_soi", C.POINTER(C.c_double)), ("n_exp", C.c_int), ("exp_seg", C.POINTER(C.c_double)),
         ("rot_kind", C.c_int), ("rot_nint", C.c_int), ("rot_pdeg", C.c_int), ("rot_ecliptic", C.c_int),
+        ("iau_deg", C.c_int * 3), ("iau_np", C.c_int * 3), ("iau_bary_offset", C.c_int), ("iau_np_deg", C.c_int),
+        ("iau_np_angles", C.c_int),
     ]
 
 
 STATE_INT_KEYS = ["frame", "dtype", "target", "center", "nintervals", "pdeg", "@offset", "@size"]
-ORIENTATION_INT_KEYS = ["unit_type", "@m1", "@m2", "@m3", "@m4", "@m5", "@m6", "@m7", "", "", "@offset", "@size"]
+ORIENTATION_INT_KEYS = ["unit_type", "@m1", "@m2", "@m3", "@m4", "@m5", "@m6", "@m7", "@m8", "@m9", "@offset",
+                        "@size"]
 # names of the positional members per orientation unit type (Layout.h)
 ORIENTATION_FIELDS = {4: {"target": "@m1", "model_id": "@m2", "interp_id": "@m3", "n_nodes_nut": "@m4",
                           "n_nodes_erp": "@m5", "lag_order_nut": "@m6", "lag_order_erp": "@m7"},
                       3: {"frameClassID": "@m1", "inertialFrame": "@m2", "dtype": "@m3", "nintervals": "@m4",
-                          "pdeg": "@m5"}}
+                          "pdeg": "@m5"},
+                      1: {"target": "@m1", "pdeg_ra": "@m2", "pdeg_dec": "@m3", "pdeg_pm": "@m4",
+                          "num_dims_radii": "@m5", "barycenter": "@m6", "num_np_terms_ra": "@m7",
+                          "num_np_terms_dec": "@m8", "num_np_terms_pm": "@m9"},
+                      2: {"target": "@m1", "pdeg_np": "@m2", "num_np_angles": "@m3"}}
 
 
 def brie_units(j, int_keys):
@@ -298,7 +305,7 @@ def load_environment(config_path) -> Environment:
     # Earth frames: ITRF93 (binary Chebyshev angles, target 3000) and the
     # IERS2000 model unit (3001); bodies.Earth.orientation picks one, else
     # the unique loaded one (interface naming/orientations Resolver.h)
-    frames = {}
+    frames, barys = {}, {}
     for f in envc.get("orientations", []):
         for u in brie_units(cbor_loads(P(f).read_bytes()), ORIENTATION_INT_KEYS):
             md = u["metadata"]
@@ -307,14 +314,21 @@ def load_environment(config_path) -> Environment:
                 continue
             for name, member in ORIENTATION_FIELDS[kind].items():
                 md.setdefault(name, md.get(member))
-            target = md["target"] if kind == 4 else md["frameClassID"]
-            if target in (3000, 3001):
+            if kind == 2:
+                barys[md["target"]] = (md, u["data"])
+                continue
+            target = md["frameClassID"] if kind == 3 else md["target"]
+            if target in (3000, 3001, 399):
                 frames[target] = (kind, md, u["data"])
     want = {"ITRF93": 3000, "ITRF": 3000, "EARTH_FIXED": 3000, "ITRF_IERS2000": 3001, "ITRF_IPF": 3001,
-            "ITRF_NATIVE": 3001}.get(str(earth_orientation).upper()) if earth_orientation else None
-    if want is None and len(frames) > 1:
+            "ITRF_NATIVE": 3001, "EARTH_BODY_FIXED": 399, "IAU_EARTH": 399}.get(
+                str(earth_orientation).upper()) if earth_orientation else None
+    binary = {k: v for k, v in frames.items() if k != 399}
+    if want is None and len(binary) > 1:
         raise ValueError("Body 399 has more than one loaded high-precision orientation frame")
-    sel = frames.get(want) if want else (next(iter(frames.values())) if frames else None)
+    if want is None:
+        want = next(iter(binary)) if binary else 399
+    sel = frames.get(want)
     if sel is not None:
         kind, md, data = sel
         e.has_rot = 1
@@ -322,9 +336,19 @@ def load_environment(config_path) -> Environment:
         e.rot_data = _dp(hold(np.array(data, dtype=np.float64)))
         if kind == 4:
             e.rot_nnut, e.rot_nerp = md["n_nodes_nut"], md["n_nodes_erp"]
-        else:
+        elif kind == 3:
             e.rot_nint, e.rot_pdeg = md["nintervals"], md["pdeg"]
             e.rot_ecliptic = 1 if md["inertialFrame"] == 17 else 0
+        else:
+            for k, name in enumerate(("ra", "dec", "pm")):
+                e.iau_deg[k] = md["pdeg_" + name] + 1
+                e.iau_np[k] = md["num_np_terms_" + name]
+            e.iau_bary_offset = -1
+            if md["barycenter"] in barys:
+                bmd, bdata = barys[md["barycenter"]]
+                e.iau_bary_offset = len(data)
+                e.iau_np_deg, e.iau_np_angles = bmd["pdeg_np"] + 1, bmd["num_np_angles"]
+                e.rot_data = _dp(hold(np.array(list(data) + list(bdata), dtype=np.float64)))
     # atmosphere
     if atm is not None:
         recs = []

@@ -86,6 +86,11 @@ typedef struct {
     // Earth frame: 4 = the IERS2000 unit above; 3 = binary Chebyshev Euler
     // angles in rot_data ([r, starts, 3 angle blocks], ITRF93)
     int rot_kind, rot_nint, rot_pdeg, rot_ecliptic;
+    // kind 1, IAU body model: RA, Dec, PM coefficient counts, their
+    // nutation-precession amplitude counts, and the barycentric angle
+    // polynomials appended to rot_data (offset -1: none)
+    int iau_deg[3], iau_np[3];
+    int iau_bary_offset, iau_np_deg, iau_np_angles;
 } OracleEnv;
 
 }  // extern "C"
@@ -247,6 +252,9 @@ void mat3mul(double C[9], const double A[9], const double B[9]) {
 // angles RA = v0 - pi/2, Dec = pi/2 - v1, PM = v2 mod 2 pi from three
 // Chebyshev series, R = Rz(PM) Rx(pi/2 - Dec) Rz(pi/2 + RA) [Rx(obliquity)
 // for ECLIPJ2000-based units], omega from the 3-1-3 Euler kinematics.
+void eulerRotation(double ra, double dec, double pm, double raDot, double decDot, double pmDot, bool ecliptic,
+                   double R[9], V3* w);
+
 void binaryEarthRotation(const OracleEnv& e, double t, double R[9], V3* w) {
     const double* d = e.rot_data;
     const int n = e.rot_nint, deg = e.rot_pdeg;
@@ -281,6 +289,57 @@ void binaryEarthRotation(const OracleEnv& e, double t, double R[9], V3* w) {
         vd[dim] = dsum / r;
     }
     const double ra = v[0] - M_PI / 2, dec = M_PI / 2 - v[1], pm = fmod(v[2], 2 * M_PI);
+    eulerRotation(ra, dec, pm, vd[0], -vd[1], vd[2], e.rot_ecliptic != 0, R, w);
+}
+
+// IAU body model (orientations/RefEphUnit.h:100-330, 640-770): RA and Dec
+// polynomials in Julian centuries, PM in days (degrees), with the
+// nutation-precession series over the barycentric angle polynomials; angles
+// mod 360, then as for a binary unit.
+void iauEarthRotation(const OracleEnv& e, double t, double R[9], V3* w) {
+    const double* d = e.rot_data;
+    const double cy = 3155760000.0, dy = 86400.0, deg = M_PI / 180.0;
+    const double T = t / cy, D = t / dy;
+    auto poly = [](const double* c, int n, double x, double* der) {
+        // ascending coefficients: value and derivative by powers
+        double v = 0.0, dv = 0.0, p = 1.0;
+        for (int k = 0; k < n; ++k) {
+            v += c[k] * p;
+            if (k + 1 < n) dv += c[k + 1] * (k + 1) * p;
+            p *= x;
+        }
+        *der = dv;
+        return v;
+    };
+    const int n0 = e.iau_deg[0], n1 = e.iau_deg[1], n2 = e.iau_deg[2];
+    double r0, r1, r2;
+    double ang[3] = {poly(d, n0, T, &r0), poly(d + n0, n1, T, &r1), poly(d + n0 + n1, n2, D, &r2)};
+    double rate[3] = {r0 / cy, r1 / cy, r2 / dy};
+    if (e.iau_bary_offset >= 0) {
+        const double* amp = d + n0 + n1 + n2;
+        for (int comp = 0; comp < 3; ++comp) {
+            for (int i = 0; i < e.iau_np[comp]; ++i) {
+                double dp;
+                const double a = poly(d + e.iau_bary_offset + (int64_t)i * e.iau_np_deg, e.iau_np_deg, T, &dp);
+                if (comp == 1) {
+                    ang[comp] += amp[i] * cos(a * deg);
+                    rate[comp] += -amp[i] * sin(a * deg) * dp * deg / cy;
+                } else {
+                    ang[comp] += amp[i] * sin(a * deg);
+                    rate[comp] += amp[i] * cos(a * deg) * dp * deg / cy;
+                }
+            }
+            amp += e.iau_np[comp];
+        }
+    }
+    eulerRotation(fmod(ang[0], 360.0) * deg, fmod(ang[1], 360.0) * deg, fmod(ang[2], 360.0) * deg, rate[0] * deg,
+                  rate[1] * deg, rate[2] * deg, false, R, w);
+}
+
+// passive Z-X-Z rotation (pi/2 + RA, pi/2 - Dec, PM) [then the ICRF ->
+// ECLIPJ2000 bias], omega from the 3-1-3 Euler kinematics mapped to ICRF
+void eulerRotation(double ra, double dec, double pm, double raDot, double decDot, double pmDot, bool ecliptic,
+                   double R[9], V3* w) {
     const double a1 = M_PI / 2 + ra, a2 = M_PI / 2 - dec;
     auto rz = [](double a, double M[9]) {
         const double c = cos(a), sn = sin(a);
@@ -302,10 +361,9 @@ void binaryEarthRotation(const OracleEnv& e, double t, double R[9], V3* w) {
     rz(pm, Z3);
     mul(X, Z1, T);
     mul(Z3, T, A);
-    const double raDot = vd[0], decDot = -vd[1], pmDot = vd[2];
     V3 om = {decDot * sin(ra) + pmDot * cos(ra) * cos(dec), -decDot * cos(ra) + pmDot * sin(ra) * cos(dec),
              raDot + pmDot * sin(dec)};
-    if (e.rot_ecliptic) {
+    if (ecliptic) {
         double E[9];
         rx(84381.448 / 3600.0 * (M_PI / 180.0), E);
         mul(A, E, R);
@@ -319,6 +377,10 @@ void binaryEarthRotation(const OracleEnv& e, double t, double R[9], V3* w) {
 void earthRotation(const OracleEnv& e, double t, double R[9], V3* w) {
     if (e.rot_kind == 3) {
         binaryEarthRotation(e, t, R, w);
+        return;
+    }
+    if (e.rot_kind == 1) {
+        iauEarthRotation(e, t, R, w);
         return;
     }
     const double inv = 1.0 / 86400.0;

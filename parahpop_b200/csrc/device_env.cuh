@@ -68,7 +68,10 @@ struct DevEnv {
     const double* ephData;
     // IERS2000 orientation unit
     int hasRot, rotNnut, rotNerp;
-    int rotKind, rotNint, rotPdeg, rotEcliptic;  // 4: IERS2000 model unit; 3: binary Chebyshev Euler angles
+    int rotKind, rotNint, rotPdeg, rotEcliptic;  // 4: IERS2000 model unit; 3: binary Chebyshev Euler angles;
+                                                 // 1: IAU body model
+    int iauDeg[3], iauNp[3];                     // kind 1: RA, Dec, PM coefficient and amplitude counts
+    int iauBaryOffset, iauNpDeg, iauNpAngles;    // kind 1: barycentric angle polynomials in rotData (-1: none)
     const double* rotData;
     // NRLMSISE-00 weather
     int hasNrl, nrlNdays;
@@ -210,6 +213,42 @@ static __device__ __forceinline__ void mat3mul(double C[9], const double A[9], c
         for (int j = 0; j < 3; ++j) C[3 * i + j] = A[3 * i] * B[j] + A[3 * i + 1] * B[3 + j] + A[3 * i + 2] * B[6 + j];
 }
 
+// Rotation ICRF -> body from RA, Dec, PM (rad) and the inertial angular
+// velocity from their rates: the passive Z-X-Z rotation with angles
+// pi/2 + RA, pi/2 - Dec, PM (frames/Rotation.h:124-133), composed with the
+// ICRF -> ECLIPJ2000 bias Rx(obliquity) for ecliptic-based angles, and the
+// 3-1-3 Euler kinematics mapped back to ICRF (frames/Frames.h:57-166).
+static __device__ void eulerBodyRotation(double ra, double dec, double pm, double raDot, double decDot, double pmDot,
+                                         bool ecliptic, double R[9], double w[3]) {
+    double s1, c1, sx, cx, s3, c3;
+    sincos(M_PI / 2 + ra, &s1, &c1);
+    sincos(M_PI / 2 - dec, &sx, &cx);
+    sincos(pm, &s3, &c3);
+    const double A[9] = {c3 * c1 - s3 * cx * s1, c3 * s1 + s3 * cx * c1, s3 * sx,
+                         -s3 * c1 - c3 * cx * s1, -s3 * s1 + c3 * cx * c1, c3 * sx,
+                         sx * s1, -sx * c1, cx};
+    double sa, ca, sd, cd;
+    sincos(ra, &sa, &ca);
+    sincos(dec, &sd, &cd);
+    double om[3] = {decDot * sa + pmDot * ca * cd, -decDot * ca + pmDot * sa * cd, raDot + pmDot * sd};
+    if (ecliptic) {
+        const double eps = 84381.448 / 3600.0 * (M_PI / 180.0);
+        double se, ce;
+        sincos(eps, &se, &ce);
+        const double E[9] = {1, 0, 0, 0, ce, se, 0, -se, ce};  // ICRF -> ECLIPJ2000
+        mat3mul(R, A, E);
+        // omega_icrf = E^T omega_ecl
+        const double o1 = ce * om[1] - se * om[2], o2 = se * om[1] + ce * om[2];
+        om[1] = o1;
+        om[2] = o2;
+    } else {
+        for (int k = 0; k < 9; ++k) R[k] = A[k];
+    }
+    w[0] = om[0];
+    w[1] = om[1];
+    w[2] = om[2];
+}
+
 // ICRF -> ITRF93 rotation and inertial angular velocity from a binary
 // orientation unit: three Chebyshev angle series (v0, v1, v2) and their rates
 // (the Type-2 evaluation of the ephemeris, parm chebyshev Interpolator.h),
@@ -246,41 +285,70 @@ static __device__ void binaryEarthRotation(const DevEnv& e, double t, double R[9
         rate[dim] = (1.0 / r) * fma(s, db0, b0 - db1);
     }
     const double ra = val[0] - M_PI / 2, dec = M_PI / 2 - val[1], pm = fmod(val[2], 2 * M_PI);
-    const double raDot = rate[0], decDot = -rate[1], pmDot = rate[2];
-    // passive Z-X-Z rotation with angles a1 = pi/2 + RA, a2 = pi/2 - Dec, a3 = PM
-    double s1, c1, sx, cx, s3, c3;
-    sincos(M_PI / 2 + ra, &s1, &c1);
-    sincos(M_PI / 2 - dec, &sx, &cx);
-    sincos(pm, &s3, &c3);
-    const double A[9] = {c3 * c1 - s3 * cx * s1, c3 * s1 + s3 * cx * c1, s3 * sx,
-                         -s3 * c1 - c3 * cx * s1, -s3 * s1 + c3 * cx * c1, c3 * sx,
-                         sx * s1, -sx * c1, cx};
-    double sa, ca, sd, cd;
-    sincos(ra, &sa, &ca);
-    sincos(dec, &sd, &cd);
-    double om[3] = {decDot * sa + pmDot * ca * cd, -decDot * ca + pmDot * sa * cd, raDot + pmDot * sd};
-    if (e.rotEcliptic) {
-        const double eps = 84381.448 / 3600.0 * (M_PI / 180.0);
-        double se, ce;
-        sincos(eps, &se, &ce);
-        const double E[9] = {1, 0, 0, 0, ce, se, 0, -se, ce};  // ICRF -> ECLIPJ2000
-        mat3mul(R, A, E);
-        // omega_icrf = E^T omega_ecl
-        const double o1 = ce * om[1] - se * om[2], o2 = se * om[1] + ce * om[2];
-        om[1] = o1;
-        om[2] = o2;
-    } else {
-        for (int k = 0; k < 9; ++k) R[k] = A[k];
-    }
-    w[0] = om[0];
-    w[1] = om[1];
-    w[2] = om[2];
+    eulerBodyRotation(ra, dec, pm, rate[0], -rate[1], rate[2], e.rotEcliptic != 0, R, w);
 }
+
+// IAU body model (orientations/RefEphUnit.h:100-330, 640-770,
+// core/Polynomial.h:33-160, frames/Frames.h:224-290): RA, Dec polynomials in
+// Julian centuries and PM in days of TDB (degrees, ascending coefficients),
+// plus sum_i a_i sin(p_i(T)) (RA, PM) / a_i cos(p_i(T)) (Dec) over the
+// body's barycentric angle polynomials p_i (degrees, centuries); the angles
+// reduced mod 360, then the rotation and rate as for a binary unit.
+static __device__ void iauEarthRotation(const DevEnv& e, double t, double R[9], double w[3]) {
+    const double* d = e.rotData;
+    const double secToCenturies = 3155760000.0, secToDays = 86400.0, deg = M_PI / 180.0;
+    const double T = t / secToCenturies, D = t / secToDays;
+    auto horner = [](const double* c, int n, double x) {
+        double r = 0.0;
+        for (int i = 0; i < n; ++i) r = fma(r, x, c[n - 1 - i]);
+        return r;
+    };
+    auto hornerRate = [](const double* c, int n, double x) {
+        double r = 0.0;
+        for (int i = 0; i + 1 < n; ++i) r = fma(r, x, c[n - 1 - i] * (double)(n - 1 - i));
+        return r;
+    };
+    const int nRa = e.iauDeg[0], nDec = e.iauDeg[1], nPm = e.iauDeg[2];
+    double ang[3] = {horner(d, nRa, T), horner(d + nRa, nDec, T), horner(d + nRa + nDec, nPm, D)};
+    double rate[3] = {hornerRate(d, nRa, T) / secToCenturies, hornerRate(d + nRa, nDec, T) / secToCenturies,
+                      hornerRate(d + nRa + nDec, nPm, D) / secToDays};
+    if (e.iauBaryOffset >= 0) {
+        const double* amp = d + nRa + nDec + nPm;
+        const double* bary = d + e.iauBaryOffset;
+        for (int comp = 0; comp < 3; ++comp) {
+            const bool isSin = comp != 1;
+            double sum = 0.0, dsum = 0.0;
+            for (int i = 0; i < e.iauNp[comp]; ++i) {
+                const double* p = bary + (int64_t)i * e.iauNpDeg;
+                double v = 0.0, dv = 0.0, tp = 1.0;
+                for (int j = 0; j < e.iauNpDeg; ++j) {
+                    v = fma(p[j], tp, v);
+                    if (j + 1 < e.iauNpDeg) dv = fma(p[j + 1] * (double)(j + 1), tp, dv);
+                    tp *= T;
+                }
+                double sv, cv;
+                sincos(v * deg, &sv, &cv);
+                sum = fma(amp[i], isSin ? sv : cv, sum);
+                dsum = fma(amp[i], (isSin ? cv : -sv) * dv * deg, dsum);
+            }
+            ang[comp] += sum;
+            rate[comp] += dsum / secToCenturies;
+            amp += e.iauNp[comp];
+        }
+    }
+    eulerBodyRotation(fmod(ang[0], 360.0) * deg, fmod(ang[1], 360.0) * deg, fmod(ang[2], 360.0) * deg,
+                      rate[0] * deg, rate[1] * deg, rate[2] * deg, false, R, w);
+}
+
 
 // ICRF -> ITRF rotation and inertial angular velocity of the IERS2000 unit
 static __device__ void earthRotation(const DevEnv& e, double t, double R[9], double w[3]) {
     if (e.rotKind == 3) {
         binaryEarthRotation(e, t, R, w);
+        return;
+    }
+    if (e.rotKind == 1) {
+        iauEarthRotation(e, t, R, w);
         return;
     }
     const double inv = 1.0 / 86400.0;

@@ -226,6 +226,8 @@ static void loadEphemeris(const std::string& path, HostEnvironment& env) {
 struct EarthFrameUnit {
     int kind = 0, target = 0;
     int nnut = 0, nerp = 0, nint = 0, pdeg = 0, ecliptic = 0;
+    int deg[3] = {0, 0, 0}, np[3] = {0, 0, 0}, barycenter = -1;  // kind 1
+    int npDeg = 0, npAngles = 0;                                   // kind 2 (barycentric angles)
     double start = 0.0, final = 0.0;
     std::vector<double> data;
 };
@@ -233,15 +235,18 @@ struct EarthFrameUnit {
 // Orientation units (brie/orientations/metadata/Layout.h:10-84,
 // orientations/metadata/EphUnit.cpp:60-160): integer member 0 is the unit
 // type, member 1 the rotation-data target, members 2.. depend on the type
-// (binary frames: inertialFrame, dtype, nintervals, pdeg; model units:
-// model_id, interp_id, n_nodes_nut, n_nodes_erp, lag_order_nut,
-// lag_order_erp).  Earth units are kept: the binary ITRF93 frame (target
-// 3000) and the IERS2000 model frame (target 3001); units of other bodies
-// are not used by the force model.
+// (IAU body models: pdeg_ra, pdeg_dec, pdeg_pm, num_dims_radii,
+// barycenter, num_np_terms_ra/dec/pm; barycentric units: pdeg_np,
+// num_np_angles; binary frames: inertialFrame, dtype, nintervals, pdeg;
+// model units: model_id, interp_id, n_nodes_nut, n_nodes_erp,
+// lag_order_nut, lag_order_erp).  Earth units are kept — the IAU model
+// (target 399), the binary ITRF93 frame (3000), the IERS2000 model frame
+// (3001) — with every barycentric unit; other bodies' frames are not used
+// by the force model.
 static void loadOrientation(const std::string& path, std::vector<EarthFrameUnit>& earth) {
     const Value root = parseCbor(readBinaryFile(path));
     const std::vector<std::string> members = {"unit_type", "@m1", "@m2", "@m3", "@m4", "@m5", "@m6", "@m7",
-                                              "", "", "@offset", "@size"};
+                                              "@m8", "@m9", "@offset", "@size"};
     for (const BrieUnit& u : brieUnits(root, path, members)) {
         // a layout-1 unit names its fields; a layout-2 unit has them by position
         auto field = [&](const char* name, const char* member) {
@@ -273,14 +278,49 @@ static void loadOrientation(const std::string& path, std::vector<EarthFrameUnit>
             f.pdeg = (int)field("pdeg", "@m5");
             if (f.nint <= 0 || f.pdeg < 0 || f.data.size() != (size_t)(1 + f.nint + 3 * (f.pdeg + 1) * f.nint))
                 throw std::runtime_error("Binary orientation unit size mismatch: " + path);
-        } else if (type == 1 || type == 2) {
-            continue;  // IAU body models and their barycentric terms: not used for the Earth here
+        } else if (type == 1) {
+            // IAU body model: RA, Dec (centuries), PM (days) polynomials in
+            // degrees, nutation-precession amplitudes (RefEphUnit.h:100-330)
+            f.target = (int)field("target", "@m1");
+            f.deg[0] = (int)field("pdeg_ra", "@m2") + 1;
+            f.deg[1] = (int)field("pdeg_dec", "@m3") + 1;
+            f.deg[2] = (int)field("pdeg_pm", "@m4") + 1;
+            f.barycenter = (int)field("barycenter", "@m6");
+            f.np[0] = (int)field("num_np_terms_ra", "@m7");
+            const auto np = [&](const char* name, int pos) {
+                auto it = u.md.find(name);
+                if (it != u.md.end()) return (int)it->second;
+                return (int)u.at("@m" + std::to_string(pos));
+            };
+            f.np[1] = np("num_np_terms_dec", 8);
+            f.np[2] = np("num_np_terms_pm", 9);
+            size_t need = 0;
+            for (int k = 0; k < 3; ++k) {
+                if (f.deg[k] < 1 || f.np[k] < 0)
+                    throw std::runtime_error("IAU orientation unit with invalid degrees: " + path);
+                need += (size_t)(f.deg[k] + f.np[k]);
+            }
+            if (f.data.size() < need) throw std::runtime_error("IAU orientation unit size mismatch: " + path);
+        } else if (type == 2) {
+            // barycentric nutation-precession angles (degrees, centuries)
+            f.target = (int)field("target", "@m1");
+            f.npDeg = (int)field("pdeg_np", "@m2") + 1;
+            f.npAngles = (int)field("num_np_angles", "@m3");
+            if (f.npDeg < 1 || f.npAngles < 0 || f.data.size() < (size_t)(f.npDeg * f.npAngles))
+                throw std::runtime_error("Barycentric orientation unit size mismatch: " + path);
+            earth.push_back(std::move(f));  // kept for the body units that reference it
+            continue;
         } else {
             throw std::runtime_error("Orientation unit type " + std::to_string(type) + " is not supported: " + path);
         }
-        if (f.target != 3000 && f.target != 3001) continue;
-        f.start = u.at("startEpoch");
-        f.final = u.at("finalEpoch");
+        if (f.target != 3000 && f.target != 3001 && f.target != 399) continue;
+        if (type != 1) {
+            f.start = u.at("startEpoch");
+            f.final = u.at("finalEpoch");
+        } else {
+            f.start = -1e300;  // polynomial models hold at every epoch
+            f.final = 1e300;
+        }
         earth.push_back(std::move(f));
     }
 }
@@ -288,8 +328,9 @@ static void loadOrientation(const std::string& path, std::vector<EarthFrameUnit>
 // The Earth frame the force model uses (interface/naming/orientations
 // Resolver.h:40-88, Registry.h:580-640): an explicit
 // bodies.Earth.orientation picks ITRF93 (aliases ITRF, EARTH_FIXED; target
-// 3000) or ITRF_IERS2000 (ITRF_IPF, ITRF_NATIVE; 3001); otherwise the unique
-// loaded one.
+// 3000), ITRF_IERS2000 (ITRF_IPF, ITRF_NATIVE; 3001) or the IAU model
+// (EARTH_BODY_FIXED, IAU_EARTH; 399); otherwise the unique loaded binary
+// frame, else the IAU model.
 static void selectEarthFrame(const std::vector<EarthFrameUnit>& earth, HostEnvironment& env) {
     int want = 0;
     if (!env.earthOrientation.empty()) {
@@ -297,21 +338,30 @@ static void selectEarthFrame(const std::vector<EarthFrameUnit>& earth, HostEnvir
         std::transform(n.begin(), n.end(), n.begin(), ::toupper);
         if (n == "ITRF93" || n == "ITRF" || n == "EARTH_FIXED") want = 3000;
         else if (n == "ITRF_IERS2000" || n == "ITRF_IPF" || n == "ITRF_NATIVE") want = 3001;
+        else if (n == "EARTH_BODY_FIXED" || n == "IAU_EARTH") want = 399;
         else throw std::runtime_error("Unknown Earth orientation '" + env.earthOrientation
-                                      + "'; this backend supports ITRF93 and ITRF_IERS2000.");
+                                      + "'; this backend supports ITRF93, ITRF_IERS2000 and IAU_EARTH.");
     }
     const EarthFrameUnit* pick = nullptr;
+    bool anyBinary = false;
+    for (const EarthFrameUnit& f : earth) anyBinary |= f.target == 3000 || f.target == 3001;
+    // no binary Earth frame and no explicit choice: the IAU polynomial
+    if (!want && !anyBinary) want = 399;
     for (const EarthFrameUnit& f : earth) {
+        if (f.kind == 2) continue;
         if (want && f.target != want) continue;
+        if (!want && f.target == 399) continue;
         if (pick && pick->target != f.target)
             throw std::runtime_error("Body 399 has more than one loaded high-precision orientation frame; set "
                                      "bodies.<name>.orientation explicitly to choose between them");
         if (!pick) pick = &f;
     }
-    if (want && !pick)
+    if (want && !pick) {
+        if (env.earthOrientation.empty()) return;  // no Earth orientation at all
         throw std::runtime_error("Body orientation '" + env.earthOrientation
                                  + "' needs its rotation data loaded; add the defining .brot to the "
                                    "environment's orientations");
+    }
     if (!pick) return;
     env.hasRot = true;
     env.rotKind = pick->kind;
@@ -323,6 +373,27 @@ static void selectEarthFrame(const std::vector<EarthFrameUnit>& earth, HostEnvir
     env.rotStart = pick->start;
     env.rotFinal = pick->final;
     env.rotData = pick->data;
+    if (pick->kind == 1) {
+        for (int k = 0; k < 3; ++k) {
+            env.iauDeg[k] = pick->deg[k];
+            env.iauNp[k] = pick->np[k];
+        }
+        // the body's barycentric angles, when loaded (RefEphUnit.h:670-698)
+        env.iauBaryOffset = -1;
+        for (const EarthFrameUnit& b : earth)
+            if (b.kind == 2 && b.target == pick->barycenter) {
+                int need = 0;
+                for (int k = 0; k < 3; ++k) need = std::max(need, pick->np[k]);
+                if (need > b.npAngles)
+                    throw std::runtime_error("The barycentric orientation unit has fewer angles than the IAU model's "
+                                             "nutation-precession terms.");
+                env.iauBaryOffset = (int)env.rotData.size();
+                env.iauNpDeg = b.npDeg;
+                env.iauNpAngles = b.npAngles;
+                env.rotData.insert(env.rotData.end(), b.data.begin(), b.data.end());
+                break;
+            }
+    }
 }
 
 static double calendarMjd(int year, int month, int day) {
@@ -781,6 +852,13 @@ void Engine::uploadEnvironment() {
     e.rotNint = h.rotNint;
     e.rotPdeg = h.rotPdeg;
     e.rotEcliptic = h.rotEcliptic;
+    for (int k = 0; k < 3; ++k) {
+        e.iauDeg[k] = h.iauDeg[k];
+        e.iauNp[k] = h.iauNp[k];
+    }
+    e.iauBaryOffset = h.iauBaryOffset;
+    e.iauNpDeg = h.iauNpDeg;
+    e.iauNpAngles = h.iauNpAngles;
     e.rotData = upload(owned_, h.rotData);
     e.hasNrl = h.hasNrl;
     e.nrlNdays = h.nrlNdays;

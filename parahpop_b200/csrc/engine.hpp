@@ -56,6 +56,12 @@ struct HostEnvironment {
     int rotNnut = 0, rotNerp = 0;      // kind 4: Lagrange node counts
     int rotNint = 0, rotPdeg = 0;      // kind 3: Chebyshev intervals and degree
     int rotEcliptic = 0;               // kind 3: angles relative to ECLIPJ2000 (inertialFrame 17)
+    // kind 1 (IAU body model, degrees): coefficient counts of the RA, Dec
+    // and PM polynomials and of their nutation-precession amplitudes; the
+    // barycentric angle polynomials follow the body data in rotData at
+    // iauBaryOffset (-1: none), iauNpAngles of iauNpDeg coefficients each
+    int iauDeg[3] = {0, 0, 0}, iauNp[3] = {0, 0, 0};
+    int iauBaryOffset = -1, iauNpDeg = 0, iauNpAngles = 0;
     double rotStart = 0.0, rotFinal = 0.0;
     std::vector<double> rotData;
     std::string earthOrientation;      // bodies.Earth.orientation (empty: the unique loaded frame)

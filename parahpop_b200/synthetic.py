@@ -317,7 +317,8 @@ class EnvSpec:
                                      # Earth and Moon -> Earth-Moon barycenter (3) -> SSB
     brie_layout: int = 1          # CBOR layout of bodies.brie and earth.brot2 (1: unit list; 2: member arrays)
     earth_frame: str = "iers"     # earth.brot2 holds: "iers" the IERS2000 model unit (3001), "itrf93" a binary
-                                  # Chebyshev Euler-angle unit (3000, ECLIPJ2000-based), "both" the two
+                                  # Chebyshev Euler-angle unit (3000, ECLIPJ2000-based), "both" the two, "iau"
+                                  # an IAU body model (399) with barycentric nutation-precession terms
 
 
 def kaula_field(degree, seed, zonal_only=False):
@@ -420,7 +421,10 @@ STATE_INT_KEYS = ("frame", "dtype", "target", "center", "nintervals", "pdeg")
 ORIENTATION_INT_KEYS = {4: ("unit_type", "target", "model_id", "interp_id", "n_nodes_nut", "n_nodes_erp",
                             "lag_order_nut", "lag_order_erp", None, None),
                         3: ("unit_type", "frameClassID", "inertialFrame", "dtype", "nintervals", "pdeg",
-                            None, None, None, None)}
+                            None, None, None, None),
+                        1: ("unit_type", "target", "pdeg_ra", "pdeg_dec", "pdeg_pm", "num_dims_radii",
+                            "barycenter", "num_np_terms_ra", "num_np_terms_dec", "num_np_terms_pm"),
+                        2: ("unit_type", "target", "pdeg_np", "num_np_angles", None, None, None, None, None, None)}
 
 
 def brie_layout2(units, int_keys) -> dict:
@@ -491,6 +495,23 @@ def itrf93_unit(start_mjd, end_mjd, seg_days=8.0, pdeg=13):
     return u
 
 
+def iau_earth_units(start_mjd, end_mjd):
+    """IAU body model of the Earth (RA = -0.641 T, Dec = 90 - 0.557 T,
+    W = 190.147 + 360.9856235 d, degrees; T in centuries, d in days) with two
+    small nutation-precession terms on the angles of an Earth-Moon barycenter
+    unit (3), so that both series are exercised."""
+    t0, t1 = mjd2000_to_et(start_mjd), mjd2000_to_et(end_mjd)
+    body = {"metadata": {"unit_type": 1, "target": 399, "pdeg_ra": 1, "pdeg_dec": 1, "pdeg_pm": 1,
+                         "num_dims_radii": 0, "barycenter": 3, "num_np_terms_ra": 2, "num_np_terms_dec": 2,
+                         "num_np_terms_pm": 2, "startEpoch": t0, "finalEpoch": t1},
+            "data": [0.0, -0.641, 90.0, -0.557, 190.147, 360.9856235,
+                     -3.6e-3, 5.0e-4, 1.3e-3, -2.0e-4, 2.1e-3, -3.0e-4]}
+    bary = {"metadata": {"unit_type": 2, "target": 3, "pdeg_np": 1, "num_np_angles": 2,
+                         "startEpoch": t0, "finalEpoch": t1},
+            "data": [125.045, -1935.5364525, 250.089, -3871.0729]}
+    return [body, bary]
+
+
 def write_brot2(path, start_mjd, end_mjd, layout=1, frame="iers"):
     """IERS2000 unit: X, Y, s (rad) on a 1-day TT grid, ERP on daily keys.
     Constant EOP: xp = yp = 0, UT1-UTC = 0.3 s, TAI-UTC = 34 s."""
@@ -517,6 +538,8 @@ def write_brot2(path, start_mjd, end_mjd, layout=1, frame="iers"):
             units.append({"metadata": meta, "data": data})
         if frame in ("itrf93", "both"):
             units.append(itrf93_unit(start_mjd - 2.0, end_mjd + 2.0))
+        if frame == "iau":
+            units += iau_earth_units(start_mjd - 2.0, end_mjd + 2.0)
         fh.write(cbor_dumps(brie_layout2(units, ORIENTATION_INT_KEYS) if layout == 2
                             else {"layout": 1, "core": units}))
 

@@ -157,6 +157,11 @@ CASES["layout2_files_1h"] = (lambda: S.population_leo(16, 20), 3600.0, 60.0, {},
 CASES["itrf93_frame_1h"] = (lambda: S.population_leo(16, 21), 3600.0, 60.0, {}, {"earth_frame": "itrf93"})
 CASES["itrf93_selected_1h"] = (lambda: S.population_leo(16, 22), 3600.0, 60.0, {"earth_orientation": "ITRF93"},
                                {"earth_frame": "both", "brie_layout": 2})
+# the Earth's IAU body model (no high-precision frame loaded: the
+# reference's fallback), in layout 1 and in layout 2
+CASES["iau_earth_1h"] = (lambda: S.population_leo(16, 23), 3600.0, 60.0, {}, {"earth_frame": "iau"})
+CASES["iau_earth_layout2_1h"] = (lambda: S.population_leo(16, 24), 3600.0, 60.0, {},
+                                 {"earth_frame": "iau", "brie_layout": 2})
 # a degree-120 field file truncated to degree / order 70 by the configuration
 CASES["truncated_120_to_70_1h"] = (lambda: S.population_leo(16, 18), 3600.0, 60.0, {"degree": 70}, {"degree": 120})
 
