@@ -76,6 +76,19 @@ int phop_propagate_device(phop_context* ctx, int64_t n, double* d_states_soa, do
                           const double* cd, const double* cr, double duration_s, double step_s,
                           double* out_epoch_mjd2000_tdb);
 
+/* Trajectory of a batch that shares one epoch, duration and step: the
+ * states (n x 6, km and km/s, host arrays in and out) after every
+ * `every`-th fixed step, written by the step kernel as it goes.  out_states
+ * holds records x n x 6 doubles and out_epochs records doubles (MJD2000 TDB),
+ * records = floor(steps / every) with steps = ceil(duration / step); the
+ * last record is the final state when `every` divides the step count.  The
+ * reference writes final states only; this is the per-step output a serving
+ * or screening caller wants instead of re-propagating to each epoch. */
+int phop_propagate_trajectory(phop_context* ctx, int64_t n, double epoch_mjd2000_tdb, const double* states,
+                              const double* mass_kg, const double* drag_area_m2, const double* srp_area_m2,
+                              const double* cd, const double* cr, double duration_s, double step_s, int64_t every,
+                              int64_t max_records, double* out_epochs, double* out_states, int64_t* out_records);
+
 /* Allocation-free form of phop_propagate_device, for callers that cannot
  * call cudaMalloc while they propagate (inside a stream capture that must not
  * allocate, under a fixed memory budget, or as a plug-in in a process whose

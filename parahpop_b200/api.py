@@ -48,6 +48,8 @@ def library() -> C.CDLL:
         lib.phop_propagate_device.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_double] + [D] * 5 + \
             [C.c_double, C.c_double, D]
         lib.phop_propagate_device.restype = C.c_int
+        lib.phop_propagate_trajectory.argtypes = [C.c_void_p, C.c_int64, C.c_double] + [D] * 6 + \
+            [C.c_double, C.c_double, C.c_int64, C.c_int64, D, D, C.POINTER(C.c_int64)]
         lib.phop_set_option.argtypes = [C.c_void_p, C.c_char_p, C.c_double]
         lib.phop_last_stats.argtypes = [C.c_void_p, C.POINTER(PhopStats)]
         lib.paraHPOP_run.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.c_char_p]
@@ -156,6 +158,26 @@ class Propagator:
         if rc != 0:
             raise PhopError(library().phop_last_error(self._h).decode())
         return out.value
+
+    def trajectory(self, epoch: float, states, mass, drag_area, srp_area, cd, cr, duration: float, step: float,
+                   every: int = 1):
+        """States of a batch with one epoch, duration and step after every
+        ``every``-th fixed step: (epochs (records,), states (records, n, 6))."""
+        st = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 6)
+        n = len(st)
+        f = lambda a: np.ascontiguousarray(np.broadcast_to(np.asarray(a, dtype=np.float64), (n,)))
+        ma, ad, asr, cdd, crr = map(f, (mass, drag_area, srp_area, cd, cr))
+        steps = int(np.ceil(duration / step))
+        cap = max(1, steps // every) if every > 0 else 1  # the library refuses every <= 0
+        ep = np.empty(cap)
+        out = np.empty((cap, n, 6))
+        got = C.c_int64()
+        rc = library().phop_propagate_trajectory(self._h, n, epoch, _dp(st), _dp(ma), _dp(ad), _dp(asr), _dp(cdd),
+                                                 _dp(crr), duration, step, every, cap, _dp(ep), _dp(out),
+                                                 C.byref(got))
+        if rc != 0:
+            raise PhopError(library().phop_last_error(self._h).decode())
+        return ep[:got.value], out[:got.value]
 
     def stats(self) -> dict:
         s = PhopStats()

@@ -304,6 +304,74 @@ int phop_propagate_device(phop_context* ctx, int64_t n, double* dState, double e
     }
 }
 
+int phop_propagate_trajectory(phop_context* ctx, int64_t n, double epoch, const double* states, const double* mass,
+                              const double* dragArea, const double* srpArea, const double* cd, const double* cr,
+                              double duration, double step, int64_t every, int64_t maxRecords, double* outEpochs,
+                              double* outStates, int64_t* outRecords) {
+    if (!ctx) return 1;
+    double* dState = nullptr;
+    double* dTraj = nullptr;
+    try {
+        if (n <= 0) throw std::runtime_error("targets must be a nonempty array.");
+        if (!states || !outEpochs || !outStates || !outRecords) throw std::runtime_error("null array argument");
+        if (!(duration > 0) || !(step > 0) || !std::isfinite(duration) || !std::isfinite(step))
+            throw std::runtime_error("Duration and step must be finite and positive.");
+        if (every <= 0) throw std::runtime_error("every must be positive.");
+        const int64_t steps = (int64_t)std::ceil(duration / step);
+        if (steps > ctx->maxSteps) throw std::runtime_error("A target stopped without reaching the requested end of simulation.");
+        const int64_t records = steps / every;
+        if (records > maxRecords) throw std::runtime_error("max_records is smaller than the trajectory's record count");
+        std::vector<double> bc(n), ams(n), ep(n, epoch), soa((size_t)6 * n);
+        for (int64_t i = 0; i < n; ++i) {
+            if (!(mass[i] > 0) || !(dragArea[i] > 0) || srpArea[i] < 0 || cd[i] < 0 || cr[i] < 0)
+                throw std::runtime_error("Invalid target epoch or physical parameter.");
+            const double area = dragArea[i] * 1e-6;
+            const double crf = cr[i] * srpArea[i] / dragArea[i];
+            ams[i] = crf * area / mass[i];
+            bc[i] = cd[i] * area / mass[i];
+            for (int d = 0; d < 6; ++d) {
+                if (!std::isfinite(states[6 * i + d])) throw std::runtime_error("Non-finite target state.");
+                soa[(size_t)d * n + i] = states[6 * i + d];
+            }
+        }
+        ctx->engine->assertCoverage(epoch, epoch + duration / 86400.0);
+        cudaSetDevice(ctx->engine->device());
+        if (cudaMalloc(&dState, soa.size() * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&dTraj, (size_t)std::max<int64_t>(records, 1) * 6 * n * sizeof(double)) != cudaSuccess)
+            throw std::runtime_error("device allocation failed for the trajectory");
+        if (cudaMemcpy(dState, soa.data(), soa.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+            throw std::runtime_error("copy to the device failed");
+        phop::RunOptions opt = ctx->opt;
+        opt.dTraj = dTraj;
+        opt.trajEvery = (int)every;
+        std::vector<double> oe;
+        ctx->stats = phop::RunStats{};
+        ctx->engine->propagateResident(n, dState, ep.data(), bc.data(), ams.data(), duration, step, ctx->maxSteps, opt,
+                                       oe, &ctx->stats);
+        std::vector<double> rec((size_t)records * 6 * n);
+        if (records > 0 &&
+            cudaMemcpy(rec.data(), dTraj, rec.size() * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+            throw std::runtime_error("copy from the device failed");
+        for (int64_t r = 0; r < records; ++r) {
+            // record r after step (r + 1) every: t0 + k step, or the end for a
+            // shortened final step
+            outEpochs[r] = epoch + std::min((double)((r + 1) * every) * step, duration) / 86400.0;
+            for (int64_t i = 0; i < n; ++i)
+                for (int d = 0; d < 6; ++d)
+                    outStates[((size_t)r * n + i) * 6 + d] = rec[((size_t)r * 6 + d) * n + i];
+        }
+        *outRecords = records;
+        cudaFree(dState);
+        cudaFree(dTraj);
+        return 0;
+    } catch (const std::exception& e) {
+        if (dState) cudaFree(dState);
+        if (dTraj) cudaFree(dTraj);
+        ctx->error = e.what();
+        return 1;
+    }
+}
+
 int phop_propagate_device_noalloc(phop_context* ctx, int64_t n, double* dState, const double* dBc,
                                   const double* dAms, double epoch, double duration, double step, double* outEpoch) {
     if (!ctx) return 1;

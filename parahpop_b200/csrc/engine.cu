@@ -1314,11 +1314,17 @@ void Engine::runKernel(int64_t n, double* dState, const double* dBc, const doubl
         p.stepDt = dDtv;
         p.records = dRec;
     }
+    if (opt.dTraj && (!shared || opt.trajEvery <= 0))
+        throw std::runtime_error("Trajectory records need a batch with one epoch, duration and step.");
     int* dCtl = (int*)scratch("ctl", 2 * sizeof(int));
     p.workCounter = dCtl;
     p.errorFlag = dCtl + 1;
     PHOP_CUDA(cudaMemsetAsync(dCtl, 0, 2 * sizeof(int), stream));
     const int L = opt.lanes > 0 ? opt.lanes : tunedLanes(p, opt, shared, stream, &launches);
+    if (opt.dTraj) {  // after the autotuner's probes, which must not write records
+        p.traj = opt.dTraj;
+        p.trajEvery = opt.trajEvery;
+    }
     const LaunchShape shape = prepareStep(p, L, opt, shared);
     PHOP_CUDA(cudaEventRecord(e1, stream));
     if (opt.graph) launchStepGraph(p, shape, opt, shared, stream);

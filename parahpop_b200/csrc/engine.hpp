@@ -118,6 +118,10 @@ struct RunOptions {
     double splitFloorKm = 0.0;  // split precision: FP64 n > 8 below this height over the field radius
     int tileSmem = -1;    // coefficient tile in shared memory: -1 when it fits, 0 never (read through L1)
     int mixedOrder = 0;   // mixed batches inside a step-count bucket: 0 radius, 1 epoch, 2 drag band + epoch
+    // trajectory records of a uniform batch: device buffer of
+    // (steps / trajEvery) x 6 x n doubles, null for none
+    double* dTraj = nullptr;
+    int trajEvery = 0;
 };
 
 class Engine {

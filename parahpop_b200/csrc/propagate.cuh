@@ -80,6 +80,10 @@ struct StepParams {
     const double* stepT0;
     const double* stepDt;
     const EpochRecord* records;  // [nsteps][13]
+    // trajectory records (uniform batches): after every trajEvery-th step the
+    // states go to traj[r][component][object], object in input order
+    double* traj;
+    int trajEvery;
     // per-object time (mixed batches)
     double* cur;
     const double* end;

@@ -776,6 +776,14 @@ __global__ void __launch_bounds__(maxStepThreads(L), 1) propagateKernel(const __
                 }
             }
             finalUpdate<CPL>(y, kst, dt, SHARED_GRID || !done);
+            if (SHARED_GRID && p.traj && (kstep + 1) % p.trajEvery == 0 && valid) {
+                double* rec = p.traj + (int64_t)((kstep + 1) / p.trajEvery - 1) * 6 * p.n;
+#pragma unroll
+                for (int c = 0; c < CPL; ++c) {
+                    const int d = j + c * L;
+                    if (d < 6) rec[(int64_t)d * p.n + oi] = y[c];
+                }
+            }
             if (!SHARED_GRID && !done) {
                 // FixedStep.h:30-37
                 cur += dtv;
