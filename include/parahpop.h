@@ -182,6 +182,7 @@ typedef struct {
     int64_t object_steps;    /* sum over objects of RKF78 steps taken */
     int64_t launches;        /* kernels launched by the last call */
     int lanes, ctas, threads, split, shared_grid, tile_in_smem;
+    double tune_ms;          /* lane-count autotuner probes of the last call (first batch of a size class) */
 } phop_stats;
 
 int phop_last_stats(const phop_context* ctx, phop_stats* out);

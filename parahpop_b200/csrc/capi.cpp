@@ -489,6 +489,7 @@ int phop_last_stats(const phop_context* ctx, phop_stats* out) {
     if (!ctx || !out) return 1;
     out->kernel_ms = ctx->stats.kernelMs;
     out->records_ms = ctx->stats.recordsMs;
+    out->tune_ms = ctx->stats.tuneMs;
     out->total_ms = ctx->stats.totalMs;
     out->object_steps = ctx->stats.objectSteps;
     out->launches = ctx->stats.launches;

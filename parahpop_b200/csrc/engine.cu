@@ -1286,10 +1286,11 @@ void Engine::runKernel(int64_t n, double* dState, const double* dBc, const doubl
     p.gridN = g.gridN;
     p.stride = g.stride;
     const bool shared = g.shared;
-    cudaEvent_t e0, e1, e2;
+    cudaEvent_t e0, e1, e2, eTuned;
     PHOP_CUDA(cudaEventCreate(&e0));
     PHOP_CUDA(cudaEventCreate(&e1));
     PHOP_CUDA(cudaEventCreate(&e2));
+    PHOP_CUDA(cudaEventCreate(&eTuned));
     int64_t launches = launchesBefore;
     PHOP_CUDA(cudaEventRecord(e0, stream));
     if (shared) {
@@ -1320,6 +1321,7 @@ void Engine::runKernel(int64_t n, double* dState, const double* dBc, const doubl
     p.workCounter = dCtl;
     p.errorFlag = dCtl + 1;
     PHOP_CUDA(cudaMemsetAsync(dCtl, 0, 2 * sizeof(int), stream));
+    PHOP_CUDA(cudaEventRecord(eTuned, stream));  // end of the epoch records
     const int L = opt.lanes > 0 ? opt.lanes : tunedLanes(p, opt, shared, stream, &launches);
     if (opt.dTraj) {  // after the autotuner's probes, which must not write records
         p.traj = opt.dTraj;
@@ -1336,10 +1338,12 @@ void Engine::runKernel(int64_t n, double* dState, const double* dBc, const doubl
     PHOP_CUDA(cudaMemcpy(&err, dCtl + 1, sizeof(int), cudaMemcpyDeviceToHost));
     if (err) throw std::runtime_error("Propagation kernel reported error " + std::to_string(err) + ".");
     if (stats) {
-        float a = 0, b = 0;
-        cudaEventElapsedTime(&a, e0, e1);
+        float a = 0, b = 0, c = 0;
+        cudaEventElapsedTime(&a, e0, eTuned);
+        cudaEventElapsedTime(&c, eTuned, e1);
         cudaEventElapsedTime(&b, e1, e2);
         stats->recordsMs += a;
+        stats->tuneMs += c;
         stats->kernelMs += b;
         stats->launches += launches;
         stats->lanes = shape.lanes;
@@ -1352,6 +1356,7 @@ void Engine::runKernel(int64_t n, double* dState, const double* dBc, const doubl
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaEventDestroy(e2);
+    cudaEventDestroy(eTuned);
 }
 
 // time grid of one object (FixedStep.h:7-37): step start epochs and sizes

@@ -97,6 +97,7 @@ struct TargetSet {
 struct RunStats {
     double kernelMs = 0.0;         // step kernel, CUDA events
     double recordsMs = 0.0;        // epoch-record kernel
+    double tuneMs = 0.0;           // lane-count autotuner probes (first batch of a size class)
     double totalMs = 0.0;          // whole propagate call incl. copies
     int64_t objectSteps = 0;       // sum over objects of steps taken
     int64_t launches = 0;          // kernels launched by this call

@@ -69,6 +69,7 @@ def main(argv=None):
         wall = time.perf_counter() - t0
         s = p.stats()
         res[name] = {"epochs": ep, "states": st, "kernel_ms": s["kernel_ms"], "records_ms": s["records_ms"],
+                     "tune_ms": s["tune_ms"],
                      "total_ms": s["total_ms"], "object_steps": s["object_steps"], "lanes": s["lanes"],
                      "wall_s": wall}
         p.close()
@@ -80,7 +81,8 @@ def main(argv=None):
         r = res[name]
         out[name] = {"object_steps_per_s": r["object_steps"] / ((r["kernel_ms"] + r["records_ms"]) * 1e-3),
                      "e2e_object_steps_per_s": r["object_steps"] / (r["total_ms"] * 1e-3),
-                     "kernel_ms": r["kernel_ms"], "lanes": r["lanes"]}
+                     "kernel_ms": r["kernel_ms"], "records_ms": r["records_ms"], "tune_ms": r["tune_ms"],
+                     "lanes": r["lanes"]}
     out["split_speedup"] = out["split"]["object_steps_per_s"] / out["fp64"]["object_steps_per_s"]
     out["split_vs_fp64_m"] = {"p50": float(np.percentile(err, 50)), "p90": float(np.percentile(err, 90)),
                               "p99": float(np.percentile(err, 99)), "max": float(err.max()),
