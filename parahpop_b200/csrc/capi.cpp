@@ -316,7 +316,7 @@ int phop_propagate_trajectory(phop_context* ctx, int64_t n, double epoch, const 
         if (!states || !outEpochs || !outStates || !outRecords) throw std::runtime_error("null array argument");
         if (!(duration > 0) || !(step > 0) || !std::isfinite(duration) || !std::isfinite(step))
             throw std::runtime_error("Duration and step must be finite and positive.");
-        if (every <= 0) throw std::runtime_error("every must be positive.");
+        if (every <= 0 || every > std::numeric_limits<int>::max()) throw std::runtime_error("every must be positive.");
         const int64_t steps = (int64_t)std::ceil(duration / step);
         if (steps > ctx->maxSteps) throw std::runtime_error("A target stopped without reaching the requested end of simulation.");
         const int64_t records = steps / every;
@@ -344,6 +344,7 @@ int phop_propagate_trajectory(phop_context* ctx, int64_t n, double epoch, const 
         phop::RunOptions opt = ctx->opt;
         opt.dTraj = dTraj;
         opt.trajEvery = (int)every;
+        opt.trajRecords = (int)records;
         std::vector<double> oe;
         ctx->stats = phop::RunStats{};
         ctx->engine->propagateResident(n, dState, ep.data(), bc.data(), ams.data(), duration, step, ctx->maxSteps, opt,

@@ -1326,6 +1326,7 @@ void Engine::runKernel(int64_t n, double* dState, const double* dBc, const doubl
     if (opt.dTraj) {  // after the autotuner's probes, which must not write records
         p.traj = opt.dTraj;
         p.trajEvery = opt.trajEvery;
+        p.trajRecords = opt.trajRecords;
     }
     const LaunchShape shape = prepareStep(p, L, opt, shared);
     PHOP_CUDA(cudaEventRecord(e1, stream));

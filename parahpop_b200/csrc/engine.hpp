@@ -123,6 +123,7 @@ struct RunOptions {
     // (steps / trajEvery) x 6 x n doubles, null for none
     double* dTraj = nullptr;
     int trajEvery = 0;
+    int trajRecords = 0;  // capacity of dTraj in records
 };
 
 class Engine {

@@ -84,6 +84,7 @@ struct StepParams {
     // states go to traj[r][component][object], object in input order
     double* traj;
     int trajEvery;
+    int trajRecords;  // capacity of traj in records: writes beyond it are skipped
     // per-object time (mixed batches)
     double* cur;
     const double* end;

@@ -776,7 +776,8 @@ __global__ void __launch_bounds__(maxStepThreads(L), 1) propagateKernel(const __
                 }
             }
             finalUpdate<CPL>(y, kst, dt, SHARED_GRID || !done);
-            if (SHARED_GRID && p.traj && (kstep + 1) % p.trajEvery == 0 && valid) {
+            if (SHARED_GRID && p.traj && (kstep + 1) % p.trajEvery == 0 && valid
+                && (kstep + 1) / p.trajEvery <= p.trajRecords) {
                 double* rec = p.traj + (int64_t)((kstep + 1) / p.trajEvery - 1) * 6 * p.n;
 #pragma unroll
                 for (int c = 0; c < CPL; ++c) {
