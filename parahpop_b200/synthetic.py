@@ -316,6 +316,8 @@ class EnvSpec:
     ephemeris_chain: str = "direct"  # "direct": Earth, Sun, Jupiter -> SSB, Moon -> Earth; "emb": DE440's
                                      # Earth and Moon -> Earth-Moon barycenter (3) -> SSB
     brie_layout: int = 1          # CBOR layout of bodies.brie and earth.brot2 (1: unit list; 2: member arrays)
+    ephemeris_files: int = 1      # 2: Sun, Earth and Moon in bodies.brie; Jupiter and a displaced duplicate
+                                  # Moon unit (which the first file's unit must shadow) in bodies2.brie
     earth_frame: str = "iers"     # earth.brot2 holds: "iers" the IERS2000 model unit (3001), "itrf93" a binary
                                   # Chebyshev Euler-angle unit (3000, ECLIPJ2000-based), "both" the two, "iau"
                                   # an IAU body model (399) with barycentric nutation-precession terms
@@ -447,6 +449,20 @@ def brie_layout2(units, int_keys) -> dict:
         "nBodyUnits": n, "intMetadata": [v for c in cols for v in c],
         "doubleMetadata": [float(u["metadata"]["startEpoch"]) for u in units]
         + [float(u["metadata"]["finalEpoch"]) for u in units]}, "data": data}}
+
+
+def write_brie_split(path1, path2, start_mjd, end_mjd):
+    """The direct-chain units over two files: Sun, Earth and Moon in the
+    first; Jupiter and a Moon unit displaced by 20,000 km in the second, which
+    a reader that keeps the first file's unit for a body ignores."""
+    f = body_functions()
+    first = [cheb_unit(f["sun"], 10, 0, start_mjd, end_mjd, 8.0), cheb_unit(f["earth"], 399, 0, start_mjd, end_mjd, 8.0),
+             cheb_unit(f["moon"], 301, 399, start_mjd, end_mjd, 4.0)]
+    second = [cheb_unit(f["jupiter"], 5, 0, start_mjd, end_mjd, 32.0),
+              cheb_unit(lambda t: f["moon"](t) + 20000.0, 301, 399, start_mjd, end_mjd, 4.0)]
+    for path, units in ((path1, first), (path2, second)):
+        with open(path, "wb") as fh:
+            fh.write(cbor_dumps({"layout": 1, "core": units}))
 
 
 def write_brie(path, start_mjd, end_mjd, dtype=2, chain="direct", layout=1):
@@ -585,8 +601,11 @@ def write_environment(directory, spec: EnvSpec = EnvSpec()) -> Path:
     d.mkdir(parents=True, exist_ok=True)
     C, S = kaula_field(spec.degree, spec.seed, spec.zonal_only)
     write_tab(d / "gravity.tab", C, S, spec.gm_tab, spec.r_tab, spec.degree)
-    write_brie(d / "bodies.brie", spec.start_mjd, spec.end_mjd, spec.ephemeris_type, spec.ephemeris_chain,
-               spec.brie_layout)
+    if spec.ephemeris_files == 2:
+        write_brie_split(d / "bodies.brie", d / "bodies2.brie", spec.start_mjd, spec.end_mjd)
+    else:
+        write_brie(d / "bodies.brie", spec.start_mjd, spec.end_mjd, spec.ephemeris_type, spec.ephemeris_chain,
+                   spec.brie_layout)
     write_brot2(d / "earth.brot2", spec.start_mjd, spec.end_mjd, spec.brie_layout, spec.earth_frame)
     write_space_weather(d / "SW-All.txt", spec.start_mjd, spec.end_mjd)
     write_eop(d / "EOP-All.txt", spec.start_mjd, spec.end_mjd)
@@ -607,7 +626,7 @@ def make_config(env_dir, duration, step, max_steps=1000000, threads=1, force="fu
                 degree=70, bodies=("Sun", "Moon", "JupiterBarycenter"), tides=True,
                 relativity=True, drag=True, srp=True, start_mjd=4016.0, end_mjd=4064.0,
                 gravity="shape", atmosphere="nrlmsise00", tide_system="zero_tide",
-                occulting=("Earth",), earth_orientation=None) -> dict:
+                occulting=("Earth",), earth_orientation=None, ephemeris=("bodies.brie",)) -> dict:
     """Run configuration in the reference schema (``example/config/envisat_full.json``).
     Paths are relative to ``env_dir`` (where the config file is written).
     ``gravity``: "shape" (the spherical-harmonic file) or "oblateness" (the
@@ -644,7 +663,7 @@ def make_config(env_dir, duration, step, max_steps=1000000, threads=1, force="fu
                 bodies_cfg["Moon"] = {"gravity": True, "occulting": True} if "Moon" in occulting else {"gravity": True}
             elif b == "JupiterBarycenter":
                 bodies_cfg["JupiterBarycenter"] = {"gm": 126712764.1, "gravity": True}
-    env = {"bodies": bodies_cfg, "ephemeris": ["bodies.brie"], "constants": "constants.json", "preferSSB": True}
+    env = {"bodies": bodies_cfg, "ephemeris": list(ephemeris), "constants": "constants.json", "preferSSB": True}
     if force != "central":
         env["orientations"] = ["earth.brot2"]
     if force == "full" and (tides or relativity):

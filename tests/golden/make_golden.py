@@ -162,6 +162,9 @@ CASES["itrf93_selected_1h"] = (lambda: S.population_leo(16, 22), 3600.0, 60.0, {
 CASES["iau_earth_1h"] = (lambda: S.population_leo(16, 23), 3600.0, 60.0, {}, {"earth_frame": "iau"})
 CASES["iau_earth_layout2_1h"] = (lambda: S.population_leo(16, 24), 3600.0, 60.0, {},
                                  {"earth_frame": "iau", "brie_layout": 2})
+# two ephemeris files: a body's unit comes from the first file that holds it
+CASES["two_ephemeris_files_1h"] = (lambda: S.population_leo(16, 25), 3600.0, 60.0,
+                                   {"ephemeris": ("bodies.brie", "bodies2.brie")}, {"ephemeris_files": 2})
 # a degree-120 field file truncated to degree / order 70 by the configuration
 CASES["truncated_120_to_70_1h"] = (lambda: S.population_leo(16, 18), 3600.0, 60.0, {"degree": 70}, {"degree": 120})
 
