@@ -414,7 +414,7 @@ struct Fast {
         ssec = T(sc);
     }
 
-    __device__ __forceinline__ T zeta(T zz, T zl) const { return ((zz - zl) * (re + zl) / (re + zz)); }
+    __device__ __forceinline__ T zeta(T zz, T zl) const { return (zz - zl) * (re + zl) * rcp(re + zz); }
 
     __device__ __forceinline__ void basis(T lat, T lst) {
         const T dgtr = T(1.74533E-2), hr = T(0.2618);
@@ -878,7 +878,7 @@ struct Fast {
         const T tinf = (z > za) ? T(NRL_PTM(0)) * T(NRL_PT[0]) * (T(1.0) + G[0]) : T(NRL_PTM(0)) * T(NRL_PT[0]);
         const T g0v = (z > zn1[4]) ? T(NRL_PTM(3)) * T(NRL_PS[0]) * (T(1.0) + G[1]) : T(NRL_PTM(3)) * T(NRL_PS[0]);
         const T tlb = T(NRL_PTM(1)) * (T(1.0) + G[2]) * T(NRL_PD(3)[0]);
-        const T s = g0v / (tinf - tlb);
+        const T s = g0v * rcp(tinf - tlb);
         const T ptl30 = T(NRL_PTM(4)) * T(NRL_PTL(3)[0]);
         // the five glob7s tables of the mesosphere nodes (ptl[0..3], pma[8]),
         // evaluated on all converged lanes when any object is below 300 km;
@@ -926,9 +926,9 @@ struct Fast {
         const bool direct = z >= za && tt > T(0);
         T lnX = T(0), kGamma = T(0);
         if (direct) {
-            lnX = log(tlb / tt);
+            lnX = log(tlb * rcp(tt));
             const T g1 = T(1.0) + zlb / re;
-            kGamma = (gsurf / (g1 * g1)) / (s * rgas * tinf);  // gamma = xm * kGamma
+            kGamma = gsurf * rcp(g1 * g1 * s * rgas * tinf);  // gamma = xm * kGamma
         }
         auto mainDensity = [&](T g, T pdm0, T pd0, T xm, T alpha) -> T {
             if (direct) {
@@ -1075,15 +1075,16 @@ struct Fast {
         T dd;
         if (direct) {
             const T g1 = T(1.0) + zlb / re;
-            const T gamma = T(16.0) * (gsurf / (g1 * g1)) / (s * rgas * tho);
+            const T gamma = T(16.0) * gsurf * rcp(g1 * g1 * s * rgas * tho);
             dd = T(NRL_PDM(7, 0)) * T(NRL_PD(8)[0]) * exp(G[10] - s * gamma * zg2);
         } else {
             dd = densu(z, T(NRL_PDM(7, 0)) * exp(G[10]) * T(NRL_PD(8)[0]), tho, tho, T(16.), T(0.0), &dummyT, zlb, s, zn1, re, gsurf, ms);
         }
         const T zsht = T(NRL_PDM(7, 5)), zmho = T(NRL_PDM(7, 4));
         const T gz = T(1.0) + zmho / re;
-        const T zsho = T(831.4) * tho / ((gsurf / (gz * gz)) * T(16.0));
-        d[8] = dd * exp(-zsht / zsho * (exp(-(z - zmho) / zsht) - T(1.)));
+        const T rzsht = rcp(zsht);
+        const T rzsho = gsurf * T(16.0) * rcp(T(831.4) * tho * gz * gz);  // 1 / zsho
+        d[8] = dd * exp(-zsht * rzsho * (exp(-(z - zmho) * rzsht) - T(1.)));
         for (int i = 0; i < 9; i++) d[i] = d[i] * T(1.0E6);
     }
 
@@ -1102,7 +1103,7 @@ struct Fast {
         // glatf
         const T c2 = cos(T(2.0) * T(1.74533E-2) * lat);
         gsurf = T(980.616) * (T(1.0) - T(0.0026373) * c2);
-        re = T(2.0) * gsurf / (T(3.085462E-6) + T(2.27E-9) * c2) * T(1.0E-5);
+        re = T(2.0) * gsurf * rcp(T(3.085462E-6) + T(2.27E-9) * c2) * T(1.0E-5);
         basis(lat, lst);
         T G[kGlobeTasks];
         T aptTlb = T(0), aptLast = T(0);

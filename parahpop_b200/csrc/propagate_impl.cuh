@@ -324,9 +324,8 @@ static __device__ __noinline__ double nrlDensity(const DevEnv& e, const EpochRec
     double dz = e2 * f[2], zdz = f[2] + dz, nn = radius, nh = 0.0;
     for (int it = 0; it < 20; ++it) {
         zdz = f[2] + dz;
-        nh = sqrt(rho2 + zdz * zdz);
-        const double sp = zdz / nh;
-        nn = radius / sqrt(1.0 - e2 * sp * sp);
+        const double sp = zdz * rsqrt(rho2 + zdz * zdz);
+        nn = radius * rsqrt(1.0 - e2 * sp * sp);
         const double next = nn * e2 * sp;
         if (fabs(dz - next) < 1.0e-12 * radius) {
             dz = next;
