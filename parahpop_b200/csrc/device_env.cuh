@@ -90,6 +90,7 @@ struct EpochRecord {
     double R[9];                 // ICRF -> ITRF
     double w[3];                 // Earth angular velocity, inertial, rad/s
     double body[kMaxBodies][3];  // body positions relative to the Earth, km
+    double indirect[3];          // sum over third bodies of -gm rb / |rb|^3 (km/s^2): epoch-only
     double dC[kTideTri];         // tide coefficient deltas, field units
     double dS[kTideTri];
     double nrlSec, nrlGast;      // UTC seconds of day, apparent sidereal time (h)
@@ -534,6 +535,18 @@ static __device__ void evalEpochRecord(const DevEnv& e, double et, EpochRecord& 
     r.w[0] = r.w[1] = r.w[2] = 0.0;
     if (e.hasRot) earthRotation(e, et, r.R, r.w);
     for (int b = 0; b < e.nbodies; ++b) chainPosition(e, e.chainPlus[b], e.chainMinus[b], et, r.body[b]);
+    // the indirect part of the third-body attraction (PointGravity.h:76-105):
+    // the Earth's acceleration towards each body, the same for every object
+    r.indirect[0] = r.indirect[1] = r.indirect[2] = 0.0;
+    for (int b = 0; b < e.nbodies; ++b) {
+        if (!(e.bodyFlags[b] & kGravity) || b == e.earthIndex) continue;
+        const double* rb = r.body[b];
+        const double rbn = sqrt(rb[0] * rb[0] + rb[1] * rb[1] + rb[2] * rb[2]);
+        const double f2 = -e.bodyGm[b] * (1.0 / (rbn * rbn * rbn));
+        r.indirect[0] += f2 * rb[0];
+        r.indirect[1] += f2 * rb[1];
+        r.indirect[2] += f2 * rb[2];
+    }
     for (int k = 0; k < kTideTri; ++k) r.dC[k] = r.dS[k] = 0.0;
     r.tideValid = 1;
     if (e.solid || e.ocean) {

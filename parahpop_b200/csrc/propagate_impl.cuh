@@ -299,6 +299,17 @@ static __device__ __forceinline__ double shadowFactor(const double rS[3], const 
     const double sb = rS[0] * rB[0] + rS[1] * rB[1] + rS[2] * rB[2];
     const double iS = 1.0 / sqrt(s2), iB = 1.0 / sqrt(b2);
     if (b2 <= RBody * RBody) return 0.0;
+    {
+        // clear full sunlight (c > a + b) or full shadow of a body larger
+        // than the Sun's disc (c < b - a), decided on cosines without the
+        // inverse trigonometric functions; within 1e-9 of either boundary
+        // the angles below decide, as the reference's evaluation does
+        const double sa = fmin(fmax(RSun * iS, 0.0), 1.0), sbd = fmin(fmax(RBody * iB, 0.0), 1.0);
+        const double ca = sqrt(1.0 - sa * sa), cb = sqrt(1.0 - sbd * sbd);
+        const double cc = fmin(fmax(sb * iS * iB, -1.0), 1.0);
+        if (cc < ca * cb - sa * sbd - 1e-9) return 1.0;
+        if (sbd > sa && cc > ca * cb + sa * sbd + 1e-9) return 0.0;
+    }
     const double a = asin(fmin(fmax(RSun * iS, 0.0), 1.0));
     const double b = asin(fmin(fmax(RBody * iB, 0.0), 1.0));
     const double c = acos(fmin(fmax(sb * iS * iB, -1.0), 1.0));
@@ -462,15 +473,15 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
                 ay += f * pos[1];
                 az += f * pos[2];
             } else {
+                // direct part per object; the indirect part (epoch-only) is
+                // the record's sum, added after the loop
                 const double* rb = r.body[bi];
                 const double d0 = pos[0] - rb[0], d1 = pos[1] - rb[1], d2 = pos[2] - rb[2];
-                const double rd = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
-                const double rbn = sqrt(rb[0] * rb[0] + rb[1] * rb[1] + rb[2] * rb[2]);
-                const double f1 = -gm * (1.0 / (rd * rd * rd));
-                const double f2 = -gm * (1.0 / (rbn * rbn * rbn));
-                ax += f1 * d0 + f2 * rb[0];
-                ay += f1 * d1 + f2 * rb[1];
-                az += f1 * d2 + f2 * rb[2];
+                const double ird = rsqrt(d0 * d0 + d1 * d1 + d2 * d2);
+                const double f1 = -gm * (ird * ird * ird);
+                ax += f1 * d0;
+                ay += f1 * d1;
+                az += f1 * d2;
             }
         }
         if (fl & kShape) {
@@ -566,6 +577,9 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
             az += f * vr2;
         }
     }
+    ax += r.indirect[0];
+    ay += r.indirect[1];
+    az += r.indirect[2];
     if (e.tidesAlone) {
         double t[3] = {0.0, 0.0, 0.0};
         tideAloneAccel(r, pos, t);
@@ -671,6 +685,8 @@ static __device__ __noinline__ void epochRecordFromGrid(const StepParams& p, dou
     for (int b = 0; b < p.env.nbodies; ++b)
 #pragma unroll
         for (int i = 0; i < 3; ++i) r.body[b][i] = interp(f0, offsetof(EpochRecord, body) / 8 + 3 * b + i);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) r.indirect[i] = interp(f0, offsetof(EpochRecord, indirect) / 8 + i);
     r.tideValid = g[0].tideValid & g[1].tideValid & g[2].tideValid & g[3].tideValid;
     if (p.env.solid || p.env.ocean) {
         for (int k = 0; k < kTideTri; ++k) {
