@@ -297,7 +297,7 @@ static __device__ __forceinline__ double shadowFactor(const double rS[3], const 
     const double s2 = rS[0] * rS[0] + rS[1] * rS[1] + rS[2] * rS[2];
     const double b2 = rB[0] * rB[0] + rB[1] * rB[1] + rB[2] * rB[2];
     const double sb = rS[0] * rB[0] + rS[1] * rB[1] + rS[2] * rB[2];
-    const double iS = 1.0 / sqrt(s2), iB = 1.0 / sqrt(b2);
+    const double iS = rsqrt(s2), iB = rsqrt(b2);
     if (b2 <= RBody * RBody) return 0.0;
     {
         // clear full sunlight (c > a + b) or full shadow of a body larger
@@ -526,7 +526,7 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
         if (fl & kRadiation) {
             const double* rb = r.body[bi];
             const double dp[3] = {pos[0] - rb[0], pos[1] - rb[1], pos[2] - rb[2]};
-            const double rd = sqrt(dp[0] * dp[0] + dp[1] * dp[1] + dp[2] * dp[2]);
+            const double ird = rsqrt(dp[0] * dp[0] + dp[1] * dp[1] + dp[2] * dp[2]);
             double occ = 1.0;
             if (e.anyOcculter) {
                 for (int oj = 0; oj < e.nbodies; ++oj) {
@@ -536,7 +536,7 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
                     occ *= shadowFactor(dp, rB, e.bodyRadius[bi], e.bodyRadius[oj]);
                 }
             }
-            const double f = occ * ((e.au * e.au * 4.56e-3 * ams) * (1.0 / (rd * rd * rd)));
+            const double f = occ * ((e.au * e.au * 4.56e-3 * ams) * (ird * ird * ird));
             ax += f * dp[0];
             ay += f * dp[1];
             az += f * dp[2];
@@ -591,11 +591,11 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
         const double mu = tides::Consts::muEarth, c = tides::Consts::c;
         const double r0 = 1000.0 * pos[0], r1 = 1000.0 * pos[1], r2 = 1000.0 * pos[2];
         const double v0 = 1000.0 * vel[0], v1 = 1000.0 * vel[1], v2 = 1000.0 * vel[2];
-        const double rr = sqrt(r0 * r0 + r1 * r1 + r2 * r2);
-        const double vv = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+        const double irr = rsqrt(r0 * r0 + r1 * r1 + r2 * r2);
+        const double v2n = v0 * v0 + v1 * v1 + v2 * v2;
         const double rv = r0 * v0 + r1 * v1 + r2 * v2;
-        const double f = mu / (c * c * (rr * rr * rr));
-        const double g = 4.0 * mu / rr - vv * vv;
+        const double f = mu * (irr * irr * irr) / (c * c);
+        const double g = 4.0 * mu * irr - v2n;
         ax += 1.0e-3 * (f * (g * r0 + 4.0 * rv * v0));
         ay += 1.0e-3 * (f * (g * r1 + 4.0 * rv * v1));
         az += 1.0e-3 * (f * (g * r2 + 4.0 * rv * v2));
