@@ -41,10 +41,10 @@ def sh_flops_per_object_step(degree: int) -> float:
 
 # DRAM bytes (read + write) of one step-kernel launch over 10^4 objects and 5
 # steps at eight lanes, from an ncu capture (dram__bytes_read.sum +
-# dram__bytes_write.sum); a longer launch reads one more 864-byte epoch record
+# dram__bytes_write.sum); a longer launch reads one more 896-byte epoch record
 # per added stage.
-NCU_BYTES_5_STEPS_1E4 = 1_581_824 + 3_914_496
-RECORD_BYTES = 864
+NCU_BYTES_5_STEPS_1E4 = 1_570_560 + 1_846_016
+RECORD_BYTES = 896
 
 
 def launch_traffic_bytes(objects: int, steps: int) -> float:
@@ -335,7 +335,7 @@ def main():
                          "frac": achieved / peak if peak > 0 else None,
                          "traffic": launch_traffic_bytes(n, int(round(span / step_s))),
                          "traffic_note": "DRAM bytes per launch: ncu capture of a 5-step launch of the same "
-                                         "10^4 objects at eight lanes (5.496 MB read+write) plus 864 B per further stage "
+                                         "10^4 objects at eight lanes (3.417 MB read+write) plus 896 B per further stage "
                                          "record",
                          "peak_source": "measured FP64 FMA throughput (phop_fma_peak) on this GPU",
                          "numerator": "29 FLOP x (N+1)(N+2)/2 SH terms x 13 stages per object-step, N = 70"},
