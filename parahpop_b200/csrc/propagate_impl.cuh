@@ -326,7 +326,23 @@ static __device__ __forceinline__ double shadowFactor(const double rS[3], const 
 // NRLMSISE-00 density (kg/km^3) at ITRF position f; the L lanes of a group
 // share the globe7 tables of the model and all return the same value.
 template <int L>
-static __device__ __noinline__ double nrlDensity(const DevEnv& e, const EpochRecord& r, const double f[3]) {
+static __device__ __forceinline__ double nrlDensityBody(const DevEnv& e, const EpochRecord& r, const double f[3]);
+
+// Out of line for eight and sixteen lanes, where the caller's live state is
+// small enough that the call's register saves cost less than the larger
+// inlined kernel; inline for one to four lanes (measured both ways).
+template <int L>
+static __device__ __noinline__ double nrlDensityCall(const DevEnv& e, const EpochRecord& r, const double f[3]) {
+    return nrlDensityBody<L>(e, r, f);
+}
+template <int L>
+static __device__ __forceinline__ double nrlDensity(const DevEnv& e, const EpochRecord& r, const double f[3]) {
+    if constexpr (L <= 4) return nrlDensityBody<L>(e, r, f);
+    else return nrlDensityCall<L>(e, r, f);
+}
+
+template <int L>
+static __device__ __forceinline__ double nrlDensityBody(const DevEnv& e, const EpochRecord& r, const double f[3]) {
     // geodetic latitude / longitude / altitude (Nrlmsise00.cu:243-266)
     const double rho2 = f[0] * f[0] + f[1] * f[1];
     if (!(rho2 + f[2] * f[2] > 0.0)) return NAN;
