@@ -202,6 +202,16 @@ int phop_fma_peak(int device, double* fp64_tflops, double* fp32_tflops);
  * Returns 0, or nonzero with the message in phop_last_error(NULL). */
 int phop_nrlmsise00_density(int device, int64_t n, const double* inputs, int lanes, double* out_rho);
 
+/* Reads a configuration and its environment files on the host, with the
+ * validation phop_create applies, and needs no device: a configuration check
+ * for machines without a GPU.  The files are read and parsed in parallel,
+ * one thread per file (errors are those a sequential load meets first).
+ * `digest` (optional) receives a 64-bit FNV-1a digest of everything loaded,
+ * `load_ms` (optional) the wall time of the load.  Returns 0, or nonzero with
+ * the message in phop_last_error(NULL).  The environment part of the
+ * reference's driver start-up (parahpop_gpu/driver.cpp:52-84). */
+int phop_load_environment(const char* config_path, uint64_t* digest, double* load_ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -57,6 +57,7 @@ def library() -> C.CDLL:
         lib.paraHPOP_setLogLevel.argtypes = [C.c_int]
         lib.phop_fma_peak.argtypes = [C.c_int, D, D]
         lib.phop_nrlmsise00_density.argtypes = [C.c_int, C.c_int64, D, C.c_int, D]
+        lib.phop_load_environment.argtypes = [C.c_char_p, C.POINTER(C.c_uint64), D]
         lib.phop_server_create.argtypes = [C.c_void_p, C.c_int64, C.c_double, C.POINTER(C.c_void_p)]
         lib.phop_server_destroy.argtypes = [C.c_void_p]
         lib.phop_server_last_error.argtypes = [C.c_void_p]
@@ -293,6 +294,19 @@ def nrlmsise00_density(inputs, lanes: int = 4, device: int = 0) -> np.ndarray:
     if lib.phop_nrlmsise00_density(device, len(a), _dp(a), lanes, _dp(out)) != 0:
         raise PhopError(lib.phop_last_error(None).decode())
     return out
+
+
+def load_environment(config) -> tuple:
+    """Reads a configuration and its environment files on the host (no device
+    needed), with the checks ``Propagator`` applies; returns (digest of
+    everything loaded, load wall time in ms).  Raises PhopError with the
+    loader's message."""
+    digest = C.c_uint64(0)
+    ms = C.c_double(0.0)
+    lib = library()
+    if lib.phop_load_environment(str(config).encode(), C.byref(digest), C.byref(ms)) != 0:
+        raise PhopError(lib.phop_last_error(None).decode())
+    return digest.value, ms.value
 
 
 def run(config, targets, output, backend="device") -> int:

@@ -151,6 +151,23 @@ int phop_create(const char* configPath, int device, phop_context** out) {
     }
 }
 
+int phop_load_environment(const char* configPath, uint64_t* digest, double* loadMs) {
+    try {
+        if (!configPath) throw std::runtime_error("phop_load_environment: null argument");
+        const auto t0 = std::chrono::steady_clock::now();
+        LoadedConfig lc = readConfig(fs::absolute(configPath), "device");
+        phop::HostEnvironment env;
+        phop::loadEnvironment(lc.config.at("model"), env);
+        const auto t1 = std::chrono::steady_clock::now();
+        if (digest) *digest = phop::environmentDigest(env);
+        if (loadMs) *loadMs = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        return 0;
+    } catch (const std::exception& e) {
+        g_createError = e.what();
+        return 1;
+    }
+}
+
 void phop_destroy(phop_context* ctx) { delete ctx; }
 
 const char* phop_last_error(const phop_context* ctx) { return ctx ? ctx->error.c_str() : g_createError.c_str(); }

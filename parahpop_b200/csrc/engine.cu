@@ -2,13 +2,19 @@
 // device residency, coefficient-tile construction and kernel launches.
 #include <algorithm>
 #include <array>
+#include <cerrno>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
+#include <exception>
+#include <functional>
 #include <numeric>
 #include <sstream>
 #include <stdexcept>
+#include <thread>
 
 #include <cub/device/device_radix_sort.cuh>
 
@@ -37,6 +43,86 @@ static int naifId(const std::string& name) {
 }
 
 // ---- loaders ------------------------------------------------------------------------------------------
+// Lines of a text file, as std::getline(…, '\n') yields them.
+class TextLines {
+public:
+    explicit TextLines(const std::string& text) : p_(text.data()), end_(text.data() + text.size()) {}
+    bool next(const char*& b, const char*& e) {
+        if (p_ >= end_) return false;
+        const char* nl = (const char*)std::memchr(p_, '\n', (size_t)(end_ - p_));
+        b = p_;
+        e = nl ? nl : end_;
+        p_ = nl ? nl + 1 : end_;
+        return true;
+    }
+
+private:
+    const char* p_;
+    const char* end_;
+};
+
+// Whitespace-separated fields of one line, read as std::istream's >> reads an
+// int or a double: after white space, the longest [sign]digits[.digits]
+// [e[sign]digits] prefix (an exponent only after a mantissa digit), which
+// must convert whole; an out-of-range int or an infinite double fails.
+class LineFields {
+public:
+    LineFields(const char* b, const char* e) : p_(b), end_(e) {}
+    bool readInt(int& v) {
+        const char* s = start();
+        if (p_ < end_ && (*p_ == '+' || *p_ == '-')) ++p_;
+        const char* d = p_;
+        digits();
+        if (p_ == d) return false;
+        errno = 0;
+        const long long x = std::strtoll(copy(s), nullptr, 10);
+        if (errno == ERANGE || x < INT32_MIN || x > INT32_MAX) return false;
+        v = (int)x;
+        return true;
+    }
+    bool readDouble(double& v) {
+        const char* s = start();
+        if (p_ < end_ && (*p_ == '+' || *p_ == '-')) ++p_;
+        const char* m = p_;
+        digits();
+        bool mantissa = p_ != m;
+        if (p_ < end_ && *p_ == '.') {
+            ++p_;
+            const char* f = p_;
+            digits();
+            mantissa = mantissa || p_ != f;
+        }
+        if (mantissa && p_ < end_ && (*p_ == 'e' || *p_ == 'E')) {
+            ++p_;
+            if (p_ < end_ && (*p_ == '+' || *p_ == '-')) ++p_;
+            digits();
+        }
+        if (p_ == s) return false;
+        char* stop = nullptr;
+        const double x = std::strtod(copy(s), &stop);
+        if (*stop != 0 || std::isinf(x)) return false;
+        v = x;
+        return true;
+    }
+
+private:
+    const char* start() {
+        while (p_ < end_ && std::isspace((unsigned char)*p_)) ++p_;
+        return p_;
+    }
+    void digits() {
+        while (p_ < end_ && *p_ >= '0' && *p_ <= '9') ++p_;
+    }
+    // the field [s, p_) as a C string
+    const char* copy(const char* s) {
+        field_.assign(s, (size_t)(p_ - s));
+        return field_.c_str();
+    }
+    const char* p_;
+    const char* end_;
+    std::string field_;
+};
+
 static void loadConstants(const std::string& path, HostEnvironment& env) {
     const Value c = parseJson(readTextFile(path));
     if (!c.isArray()) throw std::runtime_error("Constants file must hold a JSON array: " + path);
@@ -63,26 +149,33 @@ static void loadShTable(const Value& shape, HostEnvironment& env) {
     const int headerLines = shape.find("headerLines") ? (int)shape.at("headerLines").asInt() : 0;
     const int reqDeg = shape.find("degree") ? (int)shape.at("degree").asInt() : -1;
     const int reqOrd = shape.find("order") ? (int)shape.at("order").asInt() : -1;
-    std::istringstream in(readTextFile(path));
-    std::string line;
+    const std::string text = readTextFile(path);
+    TextLines lines(text);
+    const char *lb, *le;
     std::vector<std::vector<double>> rows;
+    std::string tok;
     int skip = headerLines;
-    while (std::getline(in, line)) {
+    while (lines.next(lb, le)) {
         if (skip > 0) {
             --skip;
             continue;
         }
+        // fields split at the delimiter, leading blanks dropped, blank fields skipped, read by std::stod
         std::vector<double> row;
-        std::string tok;
-        std::istringstream ls(line);
         bool any = false;
-        while (std::getline(ls, tok, delim)) {
-            size_t a = tok.find_first_not_of(" \t\r");
-            if (a == std::string::npos) continue;
-            row.push_back(std::stod(tok.substr(a)));
-            any = true;
+        for (const char* q = lb; q < le;) {
+            const char* te = (const char*)std::memchr(q, delim, (size_t)(le - q));
+            if (!te) te = le;
+            const char* a = q;
+            while (a < te && (*a == ' ' || *a == '\t' || *a == '\r')) ++a;
+            if (a < te) {
+                tok.assign(a, (size_t)(te - a));
+                row.push_back(std::stod(tok));
+                any = true;
+            }
+            q = te < le ? te + 1 : le;
         }
-        if (any) rows.push_back(row);
+        if (any) rows.push_back(std::move(row));
     }
     if (rows.empty()) throw std::runtime_error("No coefficients found in file: " + path);
     const auto& h = rows.front();
@@ -158,7 +251,7 @@ static std::vector<BrieUnit> brieUnits(const Value& file, const std::string& pat
                 if (kv.second.isNumber()) b.md[kv.first] = kv.second.asDouble();
             const Value& d = u.at("data");
             b.data.resize(d.size());
-            for (size_t k = 0; k < d.size(); ++k) b.data[k] = d[k].asDouble();
+            d.copyReals(0, d.size(), b.data.data());
             out.push_back(std::move(b));
         }
         return out;
@@ -186,13 +279,13 @@ static std::vector<BrieUnit> brieUnits(const Value& file, const std::string& pat
         if (off < 0 || size < 0 || off + size > (int64_t)data.size())
             throw std::runtime_error("BRIE layout-2 unit data out of range: " + path);
         b.data.resize((size_t)size);
-        for (int64_t k = 0; k < size; ++k) b.data[(size_t)k] = data[(size_t)(off + k)].asDouble();
+        data.copyReals((size_t)off, (size_t)size, b.data.data());
         out.push_back(std::move(b));
     }
     return out;
 }
 
-static void loadEphemeris(const std::string& path, HostEnvironment& env) {
+static void loadEphemeris(const std::string& path, std::vector<EphUnitHost>& out) {
     const Value root = parseCbor(readBinaryFile(path));
     // state units' integer members (brie/states/metadata/RefEphUnit.h:13-25)
     for (const BrieUnit& u : brieUnits(root, path, {"frame", "dtype", "target", "center", "nintervals", "pdeg",
@@ -218,7 +311,7 @@ static void loadEphemeris(const std::string& path, HostEnvironment& env) {
         if (e.data.size() != expected)
             throw std::runtime_error("Ephemeris unit size mismatch for target " + std::to_string(e.target));
         e.data.resize(positions);  // the velocity blocks of a Type-3 unit are not used
-        env.eph.push_back(std::move(e));
+        out.push_back(std::move(e));
     }
 }
 
@@ -427,19 +520,22 @@ static void loadSpaceWeather(const Value& nrl, HostEnvironment& env) {
         int ap[8];
     };
     std::vector<Rec> all;
-    std::istringstream in(readTextFile(path));
-    std::string line;
-    while (std::getline(in, line)) {
-        std::istringstream ls(line);
+    const std::string text = readTextFile(path);
+    TextLines lines(text);
+    const char *lb, *le;
+    while (lines.next(lb, le)) {
+        LineFields ls(lb, le);
         int y, mo, d, bsrn, nd, kp[8], sumKp, c9, isn, q, avg;
         double cp, adj, adjc, adjl, obs, obsc, obsl;
         Rec r{};
-        if (!(ls >> y >> mo >> d >> bsrn >> nd)) continue;
+        if (!(ls.readInt(y) && ls.readInt(mo) && ls.readInt(d) && ls.readInt(bsrn) && ls.readInt(nd))) continue;
         bool ok = true;
-        for (int& v : kp) ok = ok && (bool)(ls >> v);
-        ok = ok && (bool)(ls >> sumKp);
-        for (int& v : r.ap) ok = ok && (bool)(ls >> v);
-        ok = ok && (bool)(ls >> avg >> cp >> c9 >> isn >> adj >> q >> adjc >> adjl >> obs >> obsc >> obsl);
+        for (int& v : kp) ok = ok && ls.readInt(v);
+        ok = ok && ls.readInt(sumKp);
+        for (int& v : r.ap) ok = ok && ls.readInt(v);
+        ok = ok && ls.readInt(avg) && ls.readDouble(cp) && ls.readInt(c9) && ls.readInt(isn) && ls.readDouble(adj)
+             && ls.readInt(q) && ls.readDouble(adjc) && ls.readDouble(adjl) && ls.readDouble(obs)
+             && ls.readDouble(obsc) && ls.readDouble(obsl);
         if (!ok) continue;
         r.mjd = calendarMjd(y, mo, d);
         r.obs = obs;
@@ -479,14 +575,18 @@ static void loadSpaceWeather(const Value& nrl, HostEnvironment& env) {
 
 // HPOP EOP-All (earthcorrections/EarthCorrections.h:142-177)
 static void loadEop(const std::string& path, HostEnvironment& env) {
-    std::istringstream in(readTextFile(path));
-    std::string line;
+    const std::string text = readTextFile(path);
+    TextLines lines(text);
+    const char *lb, *le;
     std::vector<std::array<double, 5>> rec;
-    while (std::getline(in, line)) {
-        std::istringstream row(line);
+    while (lines.next(lb, le)) {
+        LineFields row(lb, le);
         int y, mo, d;
         double mjd, xp, yp, dut, lod, dpsi, deps, dx, dy, dat;
-        if (!(row >> y >> mo >> d >> mjd >> xp >> yp >> dut >> lod >> dpsi >> deps >> dx >> dy >> dat)) continue;
+        if (!(row.readInt(y) && row.readInt(mo) && row.readInt(d) && row.readDouble(mjd) && row.readDouble(xp)
+              && row.readDouble(yp) && row.readDouble(dut) && row.readDouble(lod) && row.readDouble(dpsi)
+              && row.readDouble(deps) && row.readDouble(dx) && row.readDouble(dy) && row.readDouble(dat)))
+            continue;
         if (!(y >= 1960 && mo >= 1 && mo <= 12 && d >= 1 && d <= 31 && std::isfinite(mjd) && std::isfinite(xp)
               && std::isfinite(yp) && std::isfinite(dut) && std::isfinite(dat) && mjd == std::floor(mjd)))
             throw std::runtime_error("Invalid Earth-tide EOP record in: " + path);
@@ -546,8 +646,72 @@ static void loadExponentialAtmosphere(const Value& v, HostEnvironment& env) {
     if (env.expSeg.size() > (size_t)kMaxExpBands) throw std::runtime_error("Too many atmosphere bands for this backend.");
 }
 
+// Environment files read and parsed on threads of their own, each into a part
+// of the environment that nothing else touches while it runs.  A job is
+// launched at the point where a sequential load would read its file, and
+// errors are reported as a sequential load meets them: a job's error, or a
+// synchronous step's, gives way to the error of any job launched before it.
+class FileJobs {
+public:
+    ~FileJobs() {
+        for (Job& j : jobs_)
+            if (j.thread.joinable()) j.thread.join();
+    }
+    size_t size() const { return jobs_.size(); }
+    void launch(std::function<void()> f) {
+        jobs_.emplace_back();
+        Job& j = jobs_.back();
+        j.thread = std::thread([&j, f = std::move(f)] {
+            try {
+                f();
+            } catch (...) {
+                j.error = std::current_exception();
+            }
+        });
+    }
+    // Waits for jobs [0, k) and rethrows the first error among them.
+    void joinUpTo(size_t k) { joinRange(0, k); }
+    // Waits for jobs [a, b); on an error there, the first error of [0, b).
+    void joinRange(size_t a, size_t b) {
+        for (size_t i = a; i < b; ++i) join(i);
+        for (size_t i = a; i < b; ++i)
+            if (jobs_[i].error) {
+                joinUpTo(a);
+                std::rethrow_exception(jobs_[i].error);
+            }
+    }
+    // A synchronous step failed: the first error of the jobs launched before it, else its own.
+    [[noreturn]] void rethrowAfter(std::exception_ptr own) {
+        joinUpTo(jobs_.size());
+        std::rethrow_exception(own);
+    }
+
+private:
+    struct Job {
+        std::thread thread;
+        std::exception_ptr error;
+    };
+    void join(size_t i) {
+        if (jobs_[i].thread.joinable()) jobs_[i].thread.join();
+    }
+    std::deque<Job> jobs_;  // stable addresses: each thread writes its own Job
+};
+
+static void loadEnvironmentFiles(const Value& e, HostEnvironment& env, FileJobs& jobs);
+
 void loadEnvironment(const Value& model, HostEnvironment& env) {
     const Value& e = model.at("environment");
+    FileJobs jobs;
+    try {
+        loadEnvironmentFiles(e, env, jobs);
+        jobs.joinUpTo(jobs.size());
+    } catch (...) {
+        jobs.rethrowAfter(std::current_exception());
+    }
+}
+
+static void loadEnvironmentFiles(const Value& e, HostEnvironment& env, FileJobs& jobs) {
+    int shapeJobs = 0;
     for (const auto& kv : e.members()) {
         const std::string& k = kv.first;
         if (k != "bodies" && k != "ephemeris" && k != "orientations" && k != "constants" && k != "preferSSB"
@@ -577,7 +741,10 @@ void loadEnvironment(const Value& model, HostEnvironment& env) {
                             if (b.id != 399)
                                 throw std::runtime_error("Spherical-harmonic gravity is supported for the Earth only.");
                             b.flags |= kShape;
-                            loadShTable(g.second, env);
+                            if (shapeJobs) jobs.joinUpTo(jobs.size());  // a second table replaces the first
+                            ++shapeJobs;
+                            const Value* shape = &g.second;
+                            jobs.launch([shape, &env] { loadShTable(*shape, env); });
                         } else if (gk == "oblateness") {
                             if (g.second.isBool() ? g.second.asBool() : !g.second.isNull()) {
                                 if (b.id != 399)
@@ -656,15 +823,34 @@ void loadEnvironment(const Value& model, HostEnvironment& env) {
     bool haveEarth = false;
     for (auto& b : env.bodies) haveEarth |= b.id == 399;
     if (!haveEarth) throw std::runtime_error("The Earth (center of integration) must be configured.");
-    if (const Value* eph = e.find("ephemeris"))
-        for (const Value& p : eph->items()) loadEphemeris(p.asString(), env);
+    // one part per file, merged in file order: a body's unit comes from the first file holding it
+    std::vector<std::vector<EphUnitHost>> ephParts;
+    if (const Value* eph = e.find("ephemeris")) {
+        ephParts.resize(eph->size());
+        for (size_t i = 0; i < ephParts.size(); ++i) {
+            const std::string path = eph->items()[i].asString();
+            std::vector<EphUnitHost>* part = &ephParts[i];
+            jobs.launch([path, part] { loadEphemeris(path, *part); });
+        }
+    }
     {
+        std::vector<std::vector<EarthFrameUnit>> oriParts;
+        const size_t first = jobs.size();
+        if (const Value* ori = e.find("orientations")) {
+            oriParts.resize(ori->size());
+            for (size_t i = 0; i < oriParts.size(); ++i) {
+                const std::string path = ori->items()[i].asString();
+                std::vector<EarthFrameUnit>* part = &oriParts[i];
+                jobs.launch([path, part] { loadOrientation(path, *part); });
+            }
+        }
+        jobs.joinRange(first, jobs.size());
         std::vector<EarthFrameUnit> earthFrames;
-        if (const Value* ori = e.find("orientations"))
-            for (const Value& p : ori->items()) loadOrientation(p.asString(), earthFrames);
+        for (auto& part : oriParts)
+            for (auto& f : part) earthFrames.push_back(std::move(f));
         selectEarthFrame(earthFrames, env);
     }
-    if (atmosphere) loadSpaceWeather(*atmosphere, env);
+    if (atmosphere) jobs.launch([atmosphere, &env] { loadSpaceWeather(*atmosphere, env); });
     if (const Value* ec = e.find("earthCorrections")) {
         env.solid = ec->find("solidEarthTides") && ec->at("solidEarthTides").asBool();
         env.ocean = ec->find("oceanTides") && ec->at("oceanTides").asBool();
@@ -672,11 +858,58 @@ void loadEnvironment(const Value& model, HostEnvironment& env) {
         const std::string sys = ec->find("tideSystem") ? ec->at("tideSystem").asString() : std::string("zero_tide");
         if (sys != "zero_tide" && sys != "tide_free") throw std::runtime_error("tideSystem must be zero_tide or tide_free.");
         env.zeroTide = sys == "zero_tide";
-        if (env.solid || env.ocean) loadEop(ec->at("eopFile").asString(), env);
+        if (env.solid || env.ocean) {
+            const std::string path = ec->at("eopFile").asString();
+            jobs.launch([path, &env] { loadEop(path, env); });
+        }
     }
+    jobs.joinUpTo(jobs.size());
+    for (auto& part : ephParts)
+        for (auto& u : part) env.eph.push_back(std::move(u));
     if ((env.hasShape || env.hasNrl || env.solid || env.ocean) && !env.hasRot)
         throw std::runtime_error("An Earth orientation unit (ITRF93 or IERS2000) is required for the configured "
                                  "forces.");
+}
+
+uint64_t environmentDigest(const HostEnvironment& e) {
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&h](const void* p, size_t n) {
+        const unsigned char* c = (const unsigned char*)p;
+        for (size_t i = 0; i < n; ++i) {
+            h ^= c[i];
+            h *= 1099511628211ull;
+        }
+    };
+    auto s = [&mix](const auto& x) { mix(&x, sizeof x); };
+    auto v = [&mix](const auto& x) {
+        const size_t n = x.size();
+        mix(&n, sizeof n);
+        if (n) mix(x.data(), n * sizeof(x[0]));
+    };
+    s(e.au);
+    for (const auto* m : {&e.constGm, &e.constRadius, &e.constJ2, &e.constSoi})
+        for (const auto& kv : *m) {
+            s(kv.first);
+            s(kv.second);
+        }
+    for (const auto& b : e.bodies) {
+        mix(b.name.data(), b.name.size());
+        s(b.id), s(b.flags), s(b.gm), s(b.radius), s(b.j2), s(b.gmConst), s(b.soi);
+    }
+    s(e.flattening), s(e.hasShape), s(e.shDegree), s(e.shOrder), s(e.shNormalized), s(e.shR), s(e.shGM);
+    v(e.shC), v(e.shS);
+    for (const auto& u : e.eph) {
+        s(u.target), s(u.center), s(u.nint), s(u.pdeg), s(u.startEpoch), s(u.finalEpoch);
+        v(u.data);
+    }
+    s(e.hasRot), s(e.rotKind), s(e.rotNnut), s(e.rotNerp), s(e.rotNint), s(e.rotPdeg), s(e.rotEcliptic);
+    s(e.iauDeg), s(e.iauNp), s(e.iauBaryOffset), s(e.iauNpDeg), s(e.iauNpAngles), s(e.rotStart), s(e.rotFinal);
+    v(e.rotData), v(e.expSeg);
+    s(e.hasNrl), s(e.nrlStartMjd), s(e.nrlHcutoff), s(e.nrlDensityScale), s(e.nrlNdays);
+    v(e.nrlWeather);
+    s(e.solid), s(e.ocean), s(e.relativity), s(e.zeroTide), s(e.eopFirstMjd), s(e.eopN);
+    v(e.eop);
+    return h;
 }
 
 // ---- engine --------------------------------------------------------------------------------------------

@@ -83,6 +83,9 @@ struct HostEnvironment {
 // interface::config::Model input); relative paths must already be resolved.
 void loadEnvironment(const Value& model, HostEnvironment& env);
 
+// 64-bit FNV-1a digest of every loaded field, for comparing loads.
+uint64_t environmentDigest(const HostEnvironment& env);
+
 // Per-object inputs in the reference's target schema (driver.cpp:97-123).
 struct TargetSet {
     std::vector<int64_t> ids;

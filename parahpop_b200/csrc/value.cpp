@@ -1,6 +1,8 @@
 #include "value.hpp"
 
+#include <algorithm>
 #include <cerrno>
+#include <cstddef>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -28,8 +30,26 @@ const std::string& Value::asString() const {
     throw std::runtime_error("JSON value is not a string");
 }
 const Value& Value::operator[](size_t i) const {
-    if (kind_ != Array || i >= arr_.size()) throw std::runtime_error("JSON array index out of range");
+    if (kind_ != Array || i >= size()) throw std::runtime_error("JSON array index out of range");
+    unpack();
     return arr_[i];
+}
+void Value::unpack() const {
+    if (!packed_) return;
+    arr_.reserve(reals_.size());
+    for (double d : reals_) arr_.push_back(Value::real(d));
+    reals_.clear();
+    reals_.shrink_to_fit();
+    packed_ = false;
+}
+void Value::copyReals(size_t off, size_t n, double* out) const {
+    if (n == 0) return;
+    if (kind_ != Array || off > size() || n > size() - off) throw std::runtime_error("JSON array index out of range");
+    if (packed_) {
+        std::copy(reals_.begin() + (std::ptrdiff_t)off, reals_.begin() + (std::ptrdiff_t)(off + n), out);
+        return;
+    }
+    for (size_t k = 0; k < n; ++k) out[k] = arr_[off + k].asDouble();
 }
 bool Value::has(const std::string& k) const { return find(k) != nullptr; }
 const Value* Value::find(const std::string& k) const {
@@ -121,6 +141,7 @@ void Value::dumpTo(std::string& out, int indent, int level) const {
         case Real: fmtDouble(out, d_); break;
         case String: escape(out, s_); break;
         case Array:
+            unpack();
             if (arr_.empty()) {
                 out += "[]";
                 break;
@@ -336,6 +357,26 @@ struct CborParser {
                 return Value::string(s);
             }
             case 4: {
+                if (info != 31) {
+                    // an array of float64 items (ephemeris and orientation data) is read packed
+                    const size_t save = i;
+                    const uint64_t n = arg(info);
+                    if (n > 0 && n <= (b.size() - i) / 9 && b[i] == 0xFB) {
+                        std::vector<double> r((size_t)n);
+                        size_t j = i;
+                        uint64_t k = 0;
+                        for (; k < n && b[j] == 0xFB; ++k, j += 9) {
+                            uint64_t u = 0;
+                            for (int q = 1; q <= 8; ++q) u = (u << 8) | b[j + q];
+                            std::memcpy(&r[(size_t)k], &u, 8);
+                        }
+                        if (k == n) {
+                            i = j;
+                            return Value::reals(std::move(r));
+                        }
+                    }
+                    i = save;
+                }
                 Value v = Value::array();
                 if (info == 31) {
                     while (i < b.size() && b[i] != 0xFF) v.push(parse());

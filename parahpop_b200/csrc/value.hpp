@@ -24,6 +24,9 @@ public:
     static Value string(std::string s) { Value v; v.kind_ = String; v.s_ = std::move(s); return v; }
     static Value array() { Value v; v.kind_ = Array; return v; }
     static Value object() { Value v; v.kind_ = Object; return v; }
+    // An array whose items are all reals, held packed (a CBOR array of
+    // float64 items, as ephemeris data is written); it reads like any array.
+    static Value reals(std::vector<double> r) { Value v; v.kind_ = Array; v.packed_ = true; v.reals_ = std::move(r); return v; }
 
     Kind kind() const { return kind_; }
     bool isNull() const { return kind_ == Null; }
@@ -40,11 +43,15 @@ public:
     const std::string& asString() const;
 
     // arrays
-    size_t size() const { return kind_ == Array ? arr_.size() : (kind_ == Object ? obj_.size() : 0); }
+    size_t size() const {
+        return kind_ == Array ? (packed_ ? reals_.size() : arr_.size()) : (kind_ == Object ? obj_.size() : 0);
+    }
     const Value& operator[](size_t i) const;
-    Value& push(Value v) { arr_.push_back(std::move(v)); return arr_.back(); }
-    const std::vector<Value>& items() const { return arr_; }
-    std::vector<Value>& items() { return arr_; }
+    Value& push(Value v) { unpack(); arr_.push_back(std::move(v)); return arr_.back(); }
+    const std::vector<Value>& items() const { unpack(); return arr_; }
+    std::vector<Value>& items() { unpack(); return arr_; }
+    // items [off, off + n) of an array of numbers as doubles (throws if out of range or not numbers)
+    void copyReals(size_t off, size_t n, double* out) const;
 
     // objects
     bool has(const std::string& k) const;
@@ -61,12 +68,15 @@ public:
 
 private:
     void dumpTo(std::string& out, int indent, int level) const;
+    void unpack() const;  // a packed real array turned into items, on first item access
     Kind kind_ = Null;
     bool b_ = false;
     int64_t i_ = 0;
     double d_ = 0.0;
     std::string s_;
-    std::vector<Value> arr_;
+    mutable bool packed_ = false;
+    mutable std::vector<double> reals_;
+    mutable std::vector<Value> arr_;
     std::vector<std::pair<std::string, Value>> obj_;
 };
 

@@ -1,0 +1,147 @@
+"""Host environment loading (phop_load_environment; no device needed).
+
+The loader reads every environment file on a thread of its own and parses
+CBOR float64 arrays packed; these tests hold it to what a sequential load
+gives:
+
+* the same files in CBOR layout 1 or 2, Type-2 or Type-3 units, and text
+  files with CRLF line ends or lines the readers skip (headers, truncated
+  rows, trailing fields) load to the same digest;
+* repeated loads agree (no order dependence between the file threads);
+* with several broken files, the error reported is the one a sequential load
+  meets first (field table, ephemerides, orientations, space weather, EOP,
+  in the order parahpop_gpu/driver.cpp:52-84 reads the environment).
+"""
+import json
+import shutil
+
+import pytest
+
+from parahpop_b200 import api, synthetic as S
+
+
+def _env(tmp_path, name, spec=None, **cfg):
+    d = tmp_path / name
+    d.mkdir()
+    S.write_environment(d, spec or S.EnvSpec())
+    (d / "config.json").write_text(json.dumps(S.make_config(d, 3600.0, 60.0, **cfg)))
+    return d
+
+
+def _variant(src, dst, transforms):
+    shutil.copytree(src, dst)
+    for name, f in transforms.items():
+        p = dst / name
+        p.write_bytes(f(p.read_bytes()))
+    # make_config writes paths relative to the configuration's directory
+    return dst / "config.json"
+
+
+def _digest(d):
+    return api.load_environment(d if str(d).endswith(".json") else d / "config.json")[0]
+
+
+def _crlf(b):
+    return b.replace(b"\n", b"\r\n")
+
+
+def _skipped_lines(b):
+    out = [b"# header", b"", b"   ", b"DATATYPE 123 abc"]
+    for i, line in enumerate(b.split(b"\n")):
+        if i % 9 == 4 and line.strip():
+            line += b"  1e  extra +"       # fields after the last one read are ignored
+        out.append(line)
+        if i % 50 == 7:
+            out.append(line[: len(line) // 2])  # a truncated row is skipped
+    out.append(b"END")
+    return b"\n".join(out)
+
+
+def _tab_spacing(b):
+    out = []
+    for i, line in enumerate(b.split(b"\n")):
+        if i % 5 == 1:
+            line = b"  " + line.replace(b",", b" , ") + b","
+        if i % 7 == 2:
+            line += b"\r"
+        out.append(line)
+    out.insert(3, b"")
+    out.insert(5, b" , ,")
+    return b"\n".join(out) + b"\n\n"
+
+
+def test_equivalent_files_load_alike(tmp_path):
+    base = _env(tmp_path, "base")
+    ref = _digest(base)
+    assert _digest(_env(tmp_path, "layout2", S.EnvSpec(brie_layout=2))) == ref
+    assert _digest(_env(tmp_path, "type3", S.EnvSpec(ephemeris_type=3))) == ref
+    assert _digest(_variant(base, tmp_path / "crlf", {"SW-All.txt": _crlf, "EOP-All.txt": _crlf,
+                                                       "gravity.tab": _crlf})) == ref
+    assert _digest(_variant(base, tmp_path / "junk", {"SW-All.txt": _skipped_lines,
+                                                       "EOP-All.txt": _skipped_lines})) == ref
+    assert _digest(_variant(base, tmp_path / "tab", {"gravity.tab": _tab_spacing})) == ref
+    # and a changed value is seen
+    sw = (base / "SW-All.txt").read_bytes()
+    changed = _variant(base, tmp_path / "changed", {})
+    lines = sw.split(b"\n")
+    k = next(i for i, line in enumerate(lines) if line.split()[:3] == [b"2011", b"1", b"10"])
+    fields = lines[k].split()
+    fields[14] = b"%d" % (int(fields[14]) + 12)  # the day's first 3-hour ap
+    lines[k] = b" ".join(fields)
+    (changed.parent / "SW-All.txt").write_bytes(b"\n".join(lines))
+    assert _digest(changed) != ref
+
+
+def test_repeated_loads_agree(tmp_path):
+    d = _env(tmp_path, "both", S.EnvSpec(earth_frame="both", brie_layout=2, ephemeris_files=2),
+             earth_orientation="ITRF93", ephemeris=["bodies.brie", "bodies2.brie"])
+    first = _digest(d)
+    assert all(_digest(d) == first for _ in range(10))
+    assert first != _digest(_env(tmp_path, "iers"))
+
+
+# Files that exist (paths are checked up front, in configuration order) but
+# do not parse; each loader names its file in its message.
+BROKEN = {"bad.tab": b"", "bad.brie": b"\xa0", "bad.brot2": b"\xa0", "bad_sw.txt": b"", "bad_eop.txt": b""}
+
+ERROR_CASES = {
+    # broken entries -> the message of the first one a sequential load reaches
+    "field_and_ephemeris": ({"shape": "bad.tab", "ephemeris": ["bad.brie"]}, "No coefficients found in file"),
+    "field_and_later_option": ({"shape": "bad.tab", "sun_option": True}, "No coefficients found in file"),
+    "field_and_orientation": ({"shape": "bad.tab", "orientations": ["bad.brot2"]}, "No coefficients found in file"),
+    "ephemeris_and_orientation": ({"ephemeris": ["bad.brie"], "orientations": ["bad.brot2"]},
+                                  "Unknown BRIE layout type: .*bad.brie"),
+    "second_ephemeris_and_weather": ({"ephemeris": ["bodies.brie", "bad.brie"], "sw": "bad_sw.txt"},
+                                     "Unknown BRIE layout type: .*bad.brie"),
+    "orientation_and_weather": ({"orientations": ["bad.brot2"], "sw": "bad_sw.txt"},
+                                "Unknown BRIE layout type: .*bad.brot2"),
+    "weather_and_eop": ({"sw": "bad_sw.txt", "eop": "bad_eop.txt"}, "No CelesTrak SW-All records found in"),
+    "eop_alone": ({"eop": "bad_eop.txt"}, "Earth tides require at least two HPOP EOP-All records in"),
+    "later_option_alone": ({"sun_option": True}, "Unsupported body option for Sun: bogus"),
+}
+
+
+@pytest.mark.parametrize("case", sorted(ERROR_CASES))
+def test_error_is_the_first_a_sequential_load_meets(tmp_path, case):
+    d = _env(tmp_path, "e")
+    for name, data in BROKEN.items():
+        (d / name).write_bytes(data)
+    cfg = json.loads((d / "config.json").read_text())
+    env = cfg["model"]["environment"]
+    change, expect = ERROR_CASES[case]
+    if "shape" in change:
+        env["bodies"]["Earth"]["gravity"]["shape"]["file"] = change["shape"]
+    if "ephemeris" in change:
+        env["ephemeris"] = change["ephemeris"]
+    if "orientations" in change:
+        env["orientations"] = change["orientations"]
+    if "sw" in change:
+        env["bodies"]["Earth"]["atmosphere"]["nrlmsise00"]["spaceWeatherFile"] = change["sw"]
+    if "eop" in change:
+        env["earthCorrections"]["eopFile"] = change["eop"]
+    if "sun_option" in change:
+        env["bodies"]["Sun"]["bogus"] = 1
+    (d / "bad.json").write_text(json.dumps(cfg))
+    for _ in range(3):  # whichever file thread finishes first
+        with pytest.raises(api.PhopError, match=expect):
+            api.load_environment(d / "bad.json")
