@@ -15,6 +15,7 @@ gives:
 import json
 import shutil
 
+import numpy as np
 import pytest
 
 from parahpop_b200 import api, synthetic as S
@@ -145,3 +146,53 @@ def test_error_is_the_first_a_sequential_load_meets(tmp_path, case):
     for _ in range(3):  # whichever file thread finishes first
         with pytest.raises(api.PhopError, match=expect):
             api.load_environment(d / "bad.json")
+
+
+def _encoder(floats):
+    """A CBOR writer like synthetic.cbor_dumps whose arrays of reals are
+    written another legal way: `floats` maps one real to its item bytes,
+    and a None result writes the array with indefinite length."""
+    import struct
+    scalar = S.cbor_dumps  # the module's own writer, for everything but arrays
+
+    def enc(obj):
+        if isinstance(obj, np.ndarray):
+            obj = obj.tolist()
+        if isinstance(obj, (list, tuple)) and obj and all(isinstance(x, float) for x in obj):
+            items = [floats(x) for x in obj]
+            if items[0] is None:
+                return b"\x9f" + b"".join(b"\xfb" + struct.pack(">d", x) for x in obj) + b"\xff"
+            return S._cbor_head(4, len(obj)) + b"".join(items)
+        if isinstance(obj, (list, tuple)):
+            return S._cbor_head(4, len(obj)) + b"".join(enc(x) for x in obj)
+        if isinstance(obj, dict):
+            return S._cbor_head(5, len(obj)) + b"".join(enc(k) + enc(v) for k, v in obj.items())
+        return scalar(obj)
+    return enc
+
+
+def _compact(x):
+    import struct
+    if x == int(x) and abs(x) < 2 ** 53:
+        v = int(x)
+        return S._cbor_head(0, v) if v >= 0 else S._cbor_head(1, -1 - v)
+    f32 = struct.pack(">f", x)
+    if struct.unpack(">f", f32)[0] == x:
+        return b"\xfa" + f32
+    return b"\xfb" + struct.pack(">d", x)
+
+
+@pytest.mark.parametrize("form", ["indefinite", "mixed"])
+def test_other_cbor_encodings_of_the_same_reals(tmp_path, monkeypatch, form):
+    """Ephemeris data arrays that are not all float64 items (indefinite
+    length; integers, single and double floats mixed) take the reader's
+    general path and load to the same values as the packed one."""
+    base = _env(tmp_path, "base")
+    ref = _digest(base)
+    other = _variant(base, tmp_path / form, {})
+    spec = S.EnvSpec()
+    monkeypatch.setattr(S, "cbor_dumps", _encoder((lambda x: None) if form == "indefinite" else _compact))
+    S.write_brie(other.parent / "bodies.brie", spec.start_mjd, spec.end_mjd)
+    monkeypatch.undo()
+    assert (other.parent / "bodies.brie").read_bytes() != (base / "bodies.brie").read_bytes()
+    assert _digest(other) == ref
