@@ -14,6 +14,7 @@
 #include <numeric>
 #include <sstream>
 #include <stdexcept>
+#include <system_error>
 #include <thread>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -661,13 +662,18 @@ public:
     void launch(std::function<void()> f) {
         jobs_.emplace_back();
         Job& j = jobs_.back();
-        j.thread = std::thread([&j, f = std::move(f)] {
+        auto run = [&j, f = std::move(f)] {
             try {
                 f();
             } catch (...) {
                 j.error = std::current_exception();
             }
-        });
+        };
+        try {
+            j.thread = std::thread(run);
+        } catch (const std::system_error&) {
+            run();  // no thread to be had (a process limit): load this file here
+        }
     }
     // Waits for jobs [0, k) and rethrows the first error among them.
     void joinUpTo(size_t k) { joinRange(0, k); }
