@@ -169,6 +169,68 @@ CASES["two_ephemeris_files_1h"] = (lambda: S.population_leo(16, 25), 3600.0, 60.
 CASES["truncated_120_to_70_1h"] = (lambda: S.population_leo(16, 18), 3600.0, 60.0, {"degree": 70}, {"degree": 120})
 
 
+def _concat(*pops):
+    """One population from several (ids renumbered 1..n)."""
+    cat = lambda k: None if getattr(pops[0], k) is None else np.concatenate([getattr(p, k) for p in pops])
+    n = sum(len(p) for p in pops)
+    return S.Population(np.arange(1, n + 1), cat("epochs"), cat("states"), cat("mass"), cat("drag_area"),
+                        cat("srp_area"), cat("cd"), cat("cr"), cat("duration"), cat("step"), seed=pops[0].seed,
+                        note=" + ".join(p.note for p in pops))
+
+
+# ---- the benchmark configurations at their own durations ------------------
+# C0: all 1,024 central-gravity objects, 600 s at 60 s
+CASES["c0_central_1024_600s"] = (lambda: S.population_central(1024, 0), 600.0, 60.0, {"force": "central"}, {})
+# C1: full force, degree/order 70, 24 h at 60 s: 48 objects over the
+# benchmark's 300-2000 km and 16 between 300 and 400 km, where drag is largest
+CASES["c1_full_24h"] = (lambda: _concat(S.population_leo(48, 41), S.population_leo(16, 42, alt=(300.0, 400.0))),
+                        86400.0, 60.0, {"threads": 8}, {})
+# C2: degree/order 120, 24 h at 60 s
+CASES["c2_deg120_24h"] = (lambda: _concat(S.population_leo(12, 43), S.population_leo(4, 44, alt=(300.0, 450.0))),
+                          86400.0, 60.0, {"degree": 120, "threads": 8}, {"degree": 120})
+
+
+def c3_group(kind: int, count: int, duration: float, seed: int, low: int = 0):
+    """Objects of one orbit class of the uneven C3 population (0 LEO at 30 s,
+    1 MEO at 120 s, 2 GEO/GTO at 300 s), with C3's per-object epochs spread
+    over +-10 days and one shared duration: the reference command line takes
+    one duration and one step per run, so the mixed population is pinned
+    group by group.  ``low`` of the objects are taken from the lowest
+    perigees (LEO: drag) or the largest eccentricities (GEO/GTO)."""
+    p = S.population_mixed(4000, seed)
+    step = {0: 30.0, 1: 120.0, 2: 300.0}[kind]
+    idx = np.flatnonzero(p.step == step)
+    r = np.linalg.norm(p.states[idx, :3], axis=1)
+    v2 = (p.states[idx, 3:] ** 2).sum(1)
+    a = 1.0 / (2.0 / r - v2 / S.MU_ELEMENTS)
+    h = np.linalg.norm(np.cross(p.states[idx, :3], p.states[idx, 3:]), axis=1)
+    e = np.sqrt(np.maximum(0.0, 1.0 - h * h / (S.MU_ELEMENTS * a)))
+    key = a * (1 - e) if kind == 0 else -e
+    pick = list(idx[np.argsort(key)[:low]])
+    pick += [i for i in idx if i not in pick][:count - low]
+    q = p.subset(np.array(pick))
+    q.duration = np.full(len(q), float(duration))
+    ai = np.array([a[list(idx).index(i)] for i in pick])
+    ei = np.array([e[list(idx).index(i)] for i in pick])
+    q.mass, q.drag_area, q.srp_area = S._screen_decay(np.random.default_rng(seed + 1), ai, ei, q.mass.copy(),
+                                                      q.drag_area.copy(), q.srp_area.copy(), q.cd, q.duration)
+    q.note = f"C3 orbit class {kind} ({step:g} s step), {duration:g} s, seed {seed}"
+    return q
+
+
+# C3 groups: a 7-day LEO run (two of the lowest perigees), a LEO run ending
+# with a shortened 17 s step, MEO over two days and GEO/GTO (eccentricities
+# up to 0.7) over three days, each with a shortened final step
+C3_GROUPS = {
+    "c3_leo_7d": (lambda: c3_group(0, 4, 7 * 86400.0, 51, low=2), 7 * 86400.0, 30.0),
+    "c3_leo_19h": (lambda: c3_group(0, 12, 19 * 3600.0 + 17.0, 52, low=4), 19 * 3600.0 + 17.0, 30.0),
+    "c3_meo_2d": (lambda: c3_group(1, 8, 2 * 86400.0 + 77.0, 53), 2 * 86400.0 + 77.0, 120.0),
+    "c3_geo_3d": (lambda: c3_group(2, 8, 3 * 86400.0 + 123.0, 54, low=4), 3 * 86400.0 + 123.0, 300.0),
+}
+for _name, (_fn, _dur, _step) in C3_GROUPS.items():
+    CASES[_name] = (_fn, _dur, _step, {"threads": 8}, {})
+
+
 def make_propagation_goldens(only=None):
     for name, (pop_fn, dur, step, ckw, ekw) in CASES.items():
         if only and name not in only:

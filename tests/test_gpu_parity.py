@@ -49,7 +49,7 @@ def test_every_lane_split_matches(golden, name, lanes):
     assert dpos <= POS_TOL_M and dvel <= VEL_TOL_M_S, (dpos, dvel)
 
 
-@pytest.mark.parametrize("name", ["full_1h", "deg120_1h"])
+@pytest.mark.parametrize("name", ["full_1h", "deg120_1h", "c1_full_24h", "c2_deg120_24h"])
 def test_split_precision_within_1cm(golden, name):
     case = golden(name)
     p = api.Propagator(case.config_path, split=True)
@@ -205,3 +205,45 @@ def test_split_floor_keeps_low_objects_in_fp64(tmp_path):
         assert np.linalg.norm(b[:, :3] - a[:, :3], axis=1).max() * 1e3 <= SPLIT_POS_TOL_M
     for p in (fp64, split, plain_split):
         p.close()
+
+
+C3_GROUPS = ["c3_leo_7d", "c3_leo_19h", "c3_meo_2d", "c3_geo_3d"]
+
+
+def merged_c3(golden):
+    """The C3 groups (each pinned by the reference with its own duration and
+    step, as the reference command line requires) as ONE uneven batch with
+    per-object epochs, durations and steps; ids renumbered."""
+    cases = [golden(n) for n in C3_GROUPS]
+    merged, refs, spans = [], [], []
+    for c in cases:
+        for t, ref in zip(c.targets["targets"], c.ref_states):
+            t = dict(t, id=len(merged) + 1)
+            t["duration_seconds"] = float(c.data["config"]["run"]["duration_seconds"])
+            t["step_seconds"] = float(c.data["config"]["execution"]["integration"]["initialStepSize"])
+            merged.append(t)
+            refs.append(ref)
+            spans.append(c.name)
+    return cases, {"targets": merged}, np.array(refs), np.array(spans)
+
+
+@pytest.mark.parametrize("split", [False, True])
+def test_c3_groups_in_one_mixed_batch(golden, split):
+    """LEO (30 s, up to 7 days), MEO (120 s) and GEO/GTO (300 s, e to 0.7)
+    objects with shortened final steps, in one persistent launch, against
+    the reference run of each group: 1 mm / 1e-6 m/s in FP64, 1 cm split."""
+    cases, tg, refs, groups = merged_c3(golden)
+    p = api.Propagator(cases[0].config_path, split=split)
+    ep, st = p.propagate_targets(tg)
+    assert p.stats()["shared_grid"] == 0
+    dpos = np.linalg.norm(st[:, :3] - refs[:, :3], axis=1) * 1e3
+    dvel = np.linalg.norm(st[:, 3:] - refs[:, 3:], axis=1) * 1e3
+    worst = {g: float(dpos[groups == g].max()) for g in C3_GROUPS}
+    if split:
+        assert dpos.max() <= SPLIT_POS_TOL_M, worst
+    else:
+        assert dpos.max() <= POS_TOL_M and dvel.max() <= VEL_TOL_M_S, (worst, dvel.max())
+    for c in cases:
+        m = groups == c.name
+        np.testing.assert_allclose(ep[m], c.ref_epochs, rtol=0, atol=1e-4 / 86400.0)
+    p.close()

@@ -17,11 +17,16 @@ def test_oracle_matches_reference_propagation(golden, name):
     ids, ep, st = O.propagate(env, case.targets, threads=4)
     assert list(ids) == list(case.ref_ids)
     # reference acceptance (example/compare.py:7-8): 1 mm, 1e-6 m/s; the
-    # restatement is far inside it
+    # restatement is ten times inside it up to a day.  Beyond a day (the
+    # week-long LEO run) rounding differences grow along track to a few
+    # 1e-4 m, and the bar is the acceptance itself.
     dpos = np.linalg.norm(st[:, :3] - case.ref_states[:, :3], axis=1) * 1e3
     dvel = np.linalg.norm(st[:, 3:] - case.ref_states[:, 3:], axis=1) * 1e3
-    assert dpos.max() < 1e-4, dpos.max()
-    assert dvel.max() < 1e-7, dvel.max()
+    longest = max([float(t.get("duration_seconds", 0.0)) for t in case.targets["targets"]]
+                  + [float(case.data["config"]["run"]["duration_seconds"])])
+    pos_tol, vel_tol = (1e-4, 1e-7) if longest <= 86400.0 else (1e-3, 1e-6)
+    assert dpos.max() < pos_tol, dpos.max()
+    assert dvel.max() < vel_tol, dvel.max()
     assert np.abs(ep - case.ref_epochs).max() * 86400 < 1e-9
 
 
