@@ -89,20 +89,26 @@ int phop_propagate_trajectory(phop_context* ctx, int64_t n, double epoch_mjd2000
                               const double* cd, const double* cr, double duration_s, double step_s, int64_t every,
                               int64_t max_records, double* out_epochs, double* out_states, int64_t* out_records);
 
-/* Allocation-free form of phop_propagate_device, for callers that cannot
- * call cudaMalloc while they propagate (inside a stream capture that must not
- * allocate, under a fixed memory budget, or as a plug-in in a process whose
- * allocator it does not own).  No counterpart in the reference.  Scratch
- * comes from one 4 MiB device array built into the library, held on every
- * GPU that loads it until the process exits; the call allocates nothing.
- * The caller passes device arrays: d_states_soa (6*n doubles, updated in
- * place), d_bc = cd * area / mass and d_ams = cr_eff * area / mass (area in
- * km^2, cr_eff = cr * srp_area / drag_area, n doubles each).  Limits: at most
- * 256 fixed steps per call and a coefficient tile of at most 512 KiB
- * (degree/order 120 in FP64); larger requests fail with an error.  All calls
- * share the array, so calls whose GPU work overlaps race on it: order them.
- * The first call on a device resolves the array's address and should come
- * before any stream capture. */
+/* Allocation-free form of phop_propagate_device.  No counterpart in the
+ * reference.  It is for callers that cannot call cudaMalloc while they
+ * propagate: a plug-in inside a host application whose own pool allocator
+ * has reserved the GPU's memory, a real-time loop that cannot take the
+ * device-wide synchronisation a cudaMalloc or cudaFree may imply, or a
+ * service that fixes its memory footprint at start-up.  Scratch comes from
+ * one 4 MiB device array built into the library, held on every GPU that
+ * loads it until the process exits; the call allocates nothing.  The caller
+ * passes device arrays: d_states_soa (6*n doubles, updated in place), d_bc =
+ * cd * area / mass and d_ams = cr_eff * area / mass (area in km^2, cr_eff =
+ * cr * srp_area / drag_area, n doubles each).  Limits: at most 256 fixed
+ * steps per call and a coefficient tile of at most 512 KiB (degree/order 120
+ * in FP64); larger requests fail with an error, and so does the context
+ * option "split_floor_km" (the split form here has the FP32 tile only).
+ * The call is synchronous: it returns when the propagation has finished on
+ * the GPU.  All calls share the array (the tile it holds is re-copied when a
+ * call needs another context's, lane count's or precision's), so calls
+ * whose GPU work overlaps race on it: order them.  The first call on a
+ * device resolves the array's address and should come before any stream
+ * capture. */
 int phop_propagate_device_noalloc(phop_context* ctx, int64_t n, double* d_states_soa, const double* d_bc,
                                   const double* d_ams, double epoch_mjd2000_tdb, double duration_s, double step_s,
                                   double* out_epoch_mjd2000_tdb);
@@ -209,7 +215,7 @@ int phop_nrlmsise00_density(int device, int64_t n, const double* inputs, int lan
  * `digest` (optional) receives a 64-bit FNV-1a digest of everything loaded,
  * `load_ms` (optional) the wall time of the load.  Returns 0, or nonzero with
  * the message in phop_last_error(NULL).  The environment part of the
- * reference's driver start-up (parahpop_gpu/driver.cpp:52-84). */
+ * reference's driver start-up (src/common/driver.cpp:132-135). */
 int phop_load_environment(const char* config_path, uint64_t* digest, double* load_ms);
 
 #ifdef __cplusplus

@@ -1,6 +1,7 @@
 // Host engine: environment loading (reference file formats and validation),
 // device residency, coefficient-tile construction and kernel launches.
 #include <algorithm>
+#include <atomic>
 #include <array>
 #include <cerrno>
 #include <climits>
@@ -985,7 +986,9 @@ static double factorC(int m, bool norm) {
     return (m == 1 || m == 0) ? 1.0 : (2.0 * m - 1.0);
 }
 
-Engine::Engine(const HostEnvironment& env, int device) : host_(env), device_(device) {
+static std::atomic<uint64_t> g_engineSerial{0};
+
+Engine::Engine(const HostEnvironment& env, int device) : host_(env), serial_(++g_engineSerial), device_(device) {
     PHOP_CUDA(cudaSetDevice(device_));
     PHOP_CUDA(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_));
     PHOP_CUDA(cudaDeviceGetAttribute(&maxSmem_, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));

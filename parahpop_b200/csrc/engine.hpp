@@ -227,6 +227,7 @@ private:
                    cudaStream_t stream, int64_t launchesBefore);
 
     HostEnvironment host_;
+    uint64_t serial_ = 0;  // unique per context in this process, never reused (1, 2, ...)
     int device_ = 0;
     int sms_ = 0;
     int maxSmem_ = 0;

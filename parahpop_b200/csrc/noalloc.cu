@@ -1,12 +1,13 @@
 // Propagation entry point that allocates no device memory.
 //
-// Some callers cannot call cudaMalloc at the moment they propagate: code
-// running inside a stream capture that must not allocate, callers with a
-// pre-reserved memory budget that forbids growth, or plug-ins that share a
-// process whose allocator they do not own.  For them this entry point runs
-// the same two kernels as phop_propagate_device (epoch records, then the
-// fused step kernel) but takes every scratch buffer from one file-scope
-// device array, kStaticScratchBytes large, carved as:
+// Some callers cannot call cudaMalloc at the moment they propagate: a
+// plug-in inside a host application whose own pool allocator has reserved
+// the GPU's memory, a real-time loop that cannot afford the device-wide
+// synchronisation a cudaMalloc or cudaFree may imply, or a service that
+// fixes its memory footprint at start-up and must not grow it.  For them
+// this entry point runs the same two kernels as phop_propagate_device (epoch
+// records, then the fused step kernel) but takes every scratch buffer from
+// one file-scope device array, kStaticScratchBytes large, carved as:
 //
 //   control words (work counter, error flag)     256 B
 //   coefficient tile + block table               kTileBytes + kBlockBytes
@@ -19,10 +20,13 @@
 // beyond them are rejected with an error.  Every GPU that loads the library
 // holds the array (4 MiB) until the process exits.  All calls share it: the
 // control words are cleared on every call, the tile is re-copied whenever a
-// call needs a different one, and calls whose work overlaps on the GPU race
-// on the array, so the caller must order them (one stream, or events).
-// The first call on a device resolves the array's device address; make that
-// first call before any stream capture.
+// call needs another one than the array holds (keyed by the context's
+// never-reused serial number, the lane count and the precision), and calls
+// whose work overlaps on the GPU race on the array, so the caller must order
+// them (one stream, or events).  The call is synchronous: it returns once
+// the propagation has finished on the GPU and its error flag has been read.
+// The first call on a device resolves the array's device address
+// (cudaGetSymbolAddress); make that first call before any stream capture.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -47,7 +51,7 @@ static __device__ __align__(256) unsigned char g_staticScratch[kStaticScratchByt
 namespace {
 struct DeviceScratch {
     unsigned char* base = nullptr;  // device address of g_staticScratch on this device
-    const void* tileOwner = nullptr;
+    uint64_t tileOwner = 0;         // serial number of the context whose tile the array holds (0: none)
     int tileKey = -1;
 };
 DeviceScratch g_scratch[64];
@@ -146,6 +150,11 @@ void Engine::propagateNoAlloc(int64_t n, double* dState, const double* dBc, cons
                               double duration, double step, int64_t maxSteps, const RunOptions& opt,
                               double* outEpochMjd, cudaStream_t stream) {
     if (cudaSetDevice(device_) != cudaSuccess) throw std::runtime_error("cannot select the context's device");
+    if (opt.lanes != 0 && opt.lanes != 1 && opt.lanes != 2 && opt.lanes != 4 && opt.lanes != 8 && opt.lanes != 16)
+        throw std::runtime_error("lanes must be 1, 2, 4, 8 or 16");
+    if (opt.split && opt.splitFloorKm > 0.0)
+        throw std::runtime_error("the allocation-free entry point does not take the split_floor_km option "
+                                 "(it would need the FP64 tile beside the FP32 one)");
     DeviceScratch& ds = scratchFor(device_);
     // shared time grid (FixedStep.h:7-37)
     const double start = std::fma(epochMjd, 86400.0, -43200.0);
@@ -197,12 +206,19 @@ void Engine::propagateNoAlloc(int64_t n, double* dState, const double* dBc, cons
     auto check = [](cudaError_t e) {
         if (e != cudaSuccess) throw std::runtime_error(std::string("CUDA error: ") + cudaGetErrorString(e));
     };
-    if (ds.tileOwner != (const void*)this || ds.tileKey != key) {
-        check(cudaMemcpyAsync(tileDst, ht.bytes.data(), ht.bytes.size(), cudaMemcpyHostToDevice, stream));
-        check(cudaMemcpyAsync(blocksDst, ht.blocks.data(), ht.blocks.size() * sizeof(int2), cudaMemcpyHostToDevice,
-                              stream));
-        ds.tileOwner = this;
-        ds.tileKey = key;
+    {
+        // the array's tile belongs to the last call's (context, lanes,
+        // precision); a context's serial number is never reused, so a new
+        // context at a freed one's address still gets its own tile
+        std::lock_guard<std::mutex> lock(g_scratchMutex);
+        if (ds.tileOwner != serial_ || ds.tileKey != key) {
+            ds.tileOwner = 0;
+            check(cudaMemcpyAsync(tileDst, ht.bytes.data(), ht.bytes.size(), cudaMemcpyHostToDevice, stream));
+            check(cudaMemcpyAsync(blocksDst, ht.blocks.data(), ht.blocks.size() * sizeof(int2),
+                                  cudaMemcpyHostToDevice, stream));
+            ds.tileOwner = serial_;
+            ds.tileKey = key;
+        }
     }
     check(cudaMemcpyAsync(dT0, t0, K * sizeof(double), cudaMemcpyHostToDevice, stream));
     check(cudaMemcpyAsync(dDt, dtv, K * sizeof(double), cudaMemcpyHostToDevice, stream));
@@ -232,7 +248,7 @@ void Engine::propagateNoAlloc(int64_t n, double* dState, const double* dBc, cons
     const int threadsReq = std::min(opt.threads > 0 ? opt.threads : 512, maxStepThreads(L));
     const int kPerThread = 13 * ((6 + L - 1) / L) * 8;
     int threads;
-    if ((int)ht.bytes.size() + 1024 + 64 * kPerThread <= maxSmem_) {
+    if (opt.tileSmem != 0 && (int)ht.bytes.size() + 1024 + 64 * kPerThread <= maxSmem_) {
         sp.useSmemTile = 1;
         threads = std::min(threadsReq, (maxSmem_ - (int)ht.bytes.size() - 1024) / kPerThread / 32 * 32);
     } else {
@@ -240,7 +256,7 @@ void Engine::propagateNoAlloc(int64_t n, double* dState, const double* dBc, cons
         threads = std::min(threadsReq, (maxSmem_ - 1024) / kPerThread / 32 * 32);
     }
     const int smem = propagateSmemBytes(sp, L, threads);
-    int perSm = propagateMaxCtasPerSm(L, opt.split, true, threads, smem);
+    int perSm = opt.ctasPerSm > 0 ? opt.ctasPerSm : propagateMaxCtasPerSm(L, opt.split, true, threads, smem);
     if (perSm <= 0) perSm = 1;
     const int64_t groups = (n + (32 / L) - 1) / (32 / L);
     const int64_t need = (groups + threads / 32 - 1) / (threads / 32);
