@@ -16,7 +16,7 @@ The numbers must be identical to the reference's (they are the physical
 model), so they are extracted rather than retyped.  Run here, where the
 reference tree is available; the output is committed:
 
-    python oracle/gen_model_tables.py /root/reference
+    python oracle/gen_model_tables.py <reference tree>
 """
 import re
 import sys
@@ -113,4 +113,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python oracle/gen_model_tables.py <reference tree>")
+    main(sys.argv[1])

@@ -34,15 +34,23 @@ NAIF = {"Sun": 10, "Moon": 301, "Earth": 399, "MercuryBarycenter": 1, "VenusBary
 F_GRAVITY, F_SHAPE, F_RADIATION, F_ATMOSPHERE, F_OCCULTING, F_OBLATENESS = 1, 2, 4, 8, 16, 32
 
 
+REF_MODELS = HERE / "_ref" / "ref_models.o"
+
+
 def build(force=False):
-    """Compile the oracle library (g++, OpenMP)."""
+    """Compile the oracle library (g++, OpenMP), linked with the reference's
+    NRLMSISE-00 and tide sources compiled into oracle/_ref/ref_models.o by
+    ``make -f oracle/Makefile.ref models REF=<reference tree>``."""
     src = HERE / "phop_oracle.cpp"
-    deps = [src, HERE.parent / "parahpop_b200/csrc/nrlmsise00.cuh", HERE.parent / "parahpop_b200/csrc/tides.cuh"]
+    if not REF_MODELS.exists():
+        raise RuntimeError(f"{REF_MODELS} is missing: build it from the reference sources with "
+                           "`make -f oracle/Makefile.ref models REF=<reference tree>`")
+    deps = [src, REF_MODELS]
     if LIB.exists() and not force and all(LIB.stat().st_mtime >= d.stat().st_mtime for d in deps):
         return LIB
     LIB.parent.mkdir(parents=True, exist_ok=True)
     cmd = ["g++", "-O3", "-march=x86-64-v3", "-std=c++17", "-fopenmp", "-shared", "-fPIC", "-w",
-           str(src), "-o", str(LIB)]
+           str(src), str(REF_MODELS), "-o", str(LIB)]
     subprocess.run(cmd, check=True)
     return LIB
 

@@ -26,9 +26,11 @@
 //                        LagrangeInterp.h:88-130, RotationModelUnit.h:96-148,
 //                        parm/interpolate/lagrange/Interpolator.h:61-104,416-432,812-833
 //
-// The empirical NRLMSISE-00 model and the epoch-only tide coefficient sets
-// come from the package's shared model headers, which the tests pin against
-// known answers produced by the reference's own sources (oracle/ref_kat.cpp).
+// The empirical NRLMSISE-00 model (gtd7d) and the epoch-only tide
+// coefficient sets are the reference's own sources, compiled unchanged into
+// oracle/_ref/ref_models.o (oracle/ref_models.cpp) and linked here; nothing
+// of the product is included, so every GPU-vs-oracle comparison checks the
+// product's drag and tide code against the reference's.
 #include <math.h>
 #include <stdint.h>
 #include <string.h>
@@ -36,8 +38,44 @@
 #include <algorithm>
 #include <vector>
 
-#include "../parahpop_b200/csrc/nrlmsise00.cuh"
-#include "../parahpop_b200/csrc/tides.cuh"
+extern "C" {
+double ref_nrl_density(int doy, double sec, double alt, double glat, double glong, double lst, double f107A,
+                       double f107, double ap, const double ap_a[7]);
+void ref_tide_coefficients(const double E[9], const double sun[3], const double moon[3], double mjdUtc, double ut1Utc,
+                           double ttUtc, double xp, double yp, int zeroTide, int solid, double C[49], double S[49]);
+}
+
+namespace tide {
+// epoch inputs of the tide model (HpopCorrections.h:19-23)
+struct Epoch {
+    double E[9];             // ICRF -> ITRF, row-major
+    double sun[3], moon[3];  // geocentric ICRF, m
+    double mjdUtc, ut1Utc, ttUtc, xpArcsec, ypArcsec;
+};
+struct Coeffs {
+    double C[7][7];
+    double S[7][7];
+};
+// constants of the tide and relativity model (HpopCorrections.h:25-31)
+constexpr double kMuEarth = 398600.4415e9;
+constexpr double kRadius = 6378.1363e3;
+constexpr double kLight = 299792457.999999984;
+
+inline void rotate(const double E[9], const double x[3], double out[3]) {
+    for (int i = 0; i < 3; ++i) out[i] = E[3 * i] * x[0] + E[3 * i + 1] * x[1] + E[3 * i + 2] * x[2];
+}
+// solid (zero-tide or tide-free) or ocean coefficient set of the reference
+inline void coefficients(const Epoch& ep, bool solid, bool zeroTide, Coeffs& out) {
+    double C[49], S[49];
+    ref_tide_coefficients(ep.E, ep.sun, ep.moon, ep.mjdUtc, ep.ut1Utc, ep.ttUtc, ep.xpArcsec, ep.ypArcsec,
+                          zeroTide ? 1 : 0, solid ? 1 : 0, C, S);
+    for (int n = 0; n < 7; ++n)
+        for (int m = 0; m < 7; ++m) {
+            out.C[n][m] = C[7 * n + m];
+            out.S[n][m] = S[7 * n + m];
+        }
+}
+}  // namespace tide
 
 extern "C" {
 
@@ -698,18 +736,8 @@ double nrlDensity(const OracleEnv& e, V3 fixed, double et, double Req) {
     calendarDate(mjdUtc, y, mo, d, h, mi, s);
     const double sec = h * 3600.0 + mi * 60.0 + s;
     const double kRad = 57.2957795130823208768;
-    phop::nrl::Input<double> in;
-    in.doy = dayOfYear(y, mo, d);
-    in.sec = sec;
-    in.alt = alt;
-    in.g_lat = lat * kRad;
-    in.g_long = lon * kRad;
-    in.lst = wrapHours(gastHours(mjdUtc) + lon * kRad / 15.0);
-    in.f107A = f107a;
-    in.f107 = f107;
-    in.ap = avgAp;
-    for (int k = 0; k < 7; ++k) in.ap_a[k] = ap[k];
-    const double rho = phop::nrl::density<double>(in);
+    const double rho = ref_nrl_density(dayOfYear(y, mo, d), sec, alt, lat * kRad, lon * kRad,
+                                       wrapHours(gastHours(mjdUtc) + lon * kRad / 15.0), f107a, f107, avgAp, ap);
     if (!isfinite(rho) || rho < 0.0) return NAN;
     return (rho * 1.0e9) * e.nrl_density_scale;
 }
@@ -723,7 +751,7 @@ double tdbMinusTt(double mjdTt) {
         + 0.000010 * sin(628.3076 * t + 4.2490);
 }
 
-bool eopTime(const OracleEnv& e, double et, phop::tides::Epoch& ep) {
+bool eopTime(const OracleEnv& e, double et, tide::Epoch& ep) {
     if (e.eop_n < 2 || !isfinite(et)) return false;
     const double* xp = e.eop;
     const double* yp = e.eop + e.eop_n;
@@ -779,11 +807,11 @@ void legendreWithDerivative(int nmax, double phi, double p[7][7], double dp[7][7
 }
 
 // gradient of a low-degree coefficient set, SI in / SI out (inertial axes)
-void tideGradient(const phop::tides::Epoch& ep, const double rin[3], const phop::tides::Coeffs& cf, int maxDeg,
+void tideGradient(const tide::Epoch& ep, const double rin[3], const tide::Coeffs& cf, int maxDeg,
                   double out[3]) {
-    const double mu = phop::tides::Consts::muEarth, R = phop::tides::Consts::radius;
+    const double mu = tide::kMuEarth, R = tide::kRadius;
     double r[3];
-    phop::tides::rotate(ep.E, rin, r);
+    tide::rotate(ep.E, rin, r);
     const double d = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
     const double phi = asin(r[2] / d), lon = atan2(r[1], r[0]);
     double p[7][7], dp[7][7];
@@ -820,24 +848,24 @@ V3 earthCorrections(const OracleEnv& e, V3 pos, V3 vel, double et) {
     double v[3] = {1000.0 * vel.x, 1000.0 * vel.y, 1000.0 * vel.z};
     double solid[3] = {0, 0, 0}, ocean[3] = {0, 0, 0}, rel[3] = {0, 0, 0};
     if (e.solid || e.ocean) {
-        phop::tides::Epoch ep;
+        tide::Epoch ep;
         if (!eopTime(e, et, ep)) return {NAN, NAN, NAN};
         const V3 sun = position(e, et, kSun, kEarth), moon = position(e, et, kMoon, kEarth);
         ep.sun[0] = 1000.0 * sun.x; ep.sun[1] = 1000.0 * sun.y; ep.sun[2] = 1000.0 * sun.z;
         ep.moon[0] = 1000.0 * moon.x; ep.moon[1] = 1000.0 * moon.y; ep.moon[2] = 1000.0 * moon.z;
         earthRotation(e, et, ep.E, nullptr);
-        phop::tides::Coeffs cf;
+        tide::Coeffs cf;
         if (e.solid) {
-            phop::tides::solid(ep, cf, e.zero_tide != 0);
+            tide::coefficients(ep, true, e.zero_tide != 0, cf);
             tideGradient(ep, r, cf, 4, solid);
         }
         if (e.ocean) {
-            phop::tides::ocean(ep, cf);
+            tide::coefficients(ep, false, false, cf);
             tideGradient(ep, r, cf, 6, ocean);
         }
     }
     if (e.relativity) {
-        const double mu = phop::tides::Consts::muEarth, c = phop::tides::Consts::c;
+        const double mu = tide::kMuEarth, c = tide::kLight;
         const double rr = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
         const double vv = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
         const double rv = r[0] * v[0] + r[1] * v[1] + r[2] * v[2];
@@ -1087,27 +1115,23 @@ void oracle_acceleration(const OracleEnv* env, const double pos[3], const double
 // Pieces exposed for the known-answer tests against the reference's sources.
 double oracle_nrl_density(int doy, double sec, double alt, double glat, double glong, double lst, double f107A,
                           double f107, double ap, const double ap_a[7]) {
-    phop::nrl::Input<double> in;
-    in.doy = doy; in.sec = sec; in.alt = alt; in.g_lat = glat; in.g_long = glong; in.lst = lst;
-    in.f107A = f107A; in.f107 = f107; in.ap = ap;
-    for (int k = 0; k < 7; ++k) in.ap_a[k] = ap_a[k];
-    return phop::nrl::density<double>(in);
+    return ref_nrl_density(doy, sec, alt, glat, glong, lst, f107A, f107, ap, ap_a);
 }
 
 void oracle_tides(const double r[3], const double v[3], const double sun[3], const double moon[3], const double E[9],
                   double mjdUtc, double ut1Utc, double ttUtc, double xp, double yp, double solidC[49],
                   double solidS[49], double oceanC[49], double oceanS[49], double acc_solid[3], double acc_ocean[3],
                   double acc_rel[3]) {
-    phop::tides::Epoch ep;
+    tide::Epoch ep;
     for (int k = 0; k < 3; ++k) {
         ep.sun[k] = sun[k];
         ep.moon[k] = moon[k];
     }
     for (int k = 0; k < 9; ++k) ep.E[k] = E[k];
     ep.mjdUtc = mjdUtc; ep.ut1Utc = ut1Utc; ep.ttUtc = ttUtc; ep.xpArcsec = xp; ep.ypArcsec = yp;
-    phop::tides::Coeffs cs, co;
-    phop::tides::solid(ep, cs, true);
-    phop::tides::ocean(ep, co);
+    tide::Coeffs cs, co;
+    tide::coefficients(ep, true, true, cs);
+    tide::coefficients(ep, false, false, co);
     for (int n = 0; n < 7; ++n)
         for (int m = 0; m < 7; ++m) {
             solidC[7 * n + m] = cs.C[n][m]; solidS[7 * n + m] = cs.S[n][m];
@@ -1115,7 +1139,7 @@ void oracle_tides(const double r[3], const double v[3], const double sun[3], con
         }
     tideGradient(ep, r, cs, 4, acc_solid);
     tideGradient(ep, r, co, 6, acc_ocean);
-    const double mu = phop::tides::Consts::muEarth, c = phop::tides::Consts::c;
+    const double mu = tide::kMuEarth, c = tide::kLight;
     const double rr = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
     const double vv = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
     const double rv = r[0] * v[0] + r[1] * v[1] + r[2] * v[2];
