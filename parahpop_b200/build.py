@@ -29,7 +29,7 @@ CU_SOURCES = ["propagate.cu", "engine.cu", "peak.cu", "noalloc.cu", "server.cu",
 INST = [("f64_grid", ["-DPHOP_T=double", "-DPHOP_SG=1"]), ("f64_mixed", ["-DPHOP_T=double", "-DPHOP_SG=0"]),
         ("f32_grid", ["-DPHOP_T=float", "-DPHOP_SG=1"]), ("f32_mixed", ["-DPHOP_T=float", "-DPHOP_SG=0"])]
 CPP_SOURCES = ["value.cpp", "capi.cpp"]
-HEADERS = ["propagate.cuh", "propagate_impl.cuh", "device_env.cuh", "nrlmsise00.cuh", "nrl_fast.cuh", "tides.cuh", "engine.hpp", "server.hpp", "value.hpp",
+HEADERS = ["propagate.cuh", "propagate_impl.cuh", "device_env.cuh", "nrlmsise00.cuh", "nrl_fast.cuh", "tide_field.cuh", "engine.hpp", "server.hpp", "value.hpp",
            "tables/nrlmsise00_coeffs.inc", "tables/tide_tables.inc"]
 
 

@@ -21,7 +21,7 @@
 #include <stdint.h>
 
 #include "nrl_fast.cuh"
-#include "tides.cuh"
+#include "tide_field.cuh"
 
 namespace phop {
 
@@ -81,6 +81,7 @@ struct DevEnv {
     // Earth corrections
     int solid, ocean, relativity, zeroTide;
     int tidesAlone;  // tides on without a gravity field: the deltas are summed on their own (degree <= 6)
+    const tidefield::OceanAmp* tideOcean;  // FES2004 amplitudes, slot-major (tide_field.cuh)
     int eopN;
     double eopFirstMjd;
     const double* eop;  // 4 x n component-major
@@ -429,7 +430,7 @@ static __device__ __forceinline__ double tdbMinusTt(double mjdTt) {
         + 0.000010 * sin(628.3076 * t + 4.2490);
 }
 
-static __device__ bool eopTime(const DevEnv& e, double et, tides::Epoch& ep) {
+static __device__ bool eopTime(const DevEnv& e, double et, tidefield::Epoch& ep) {
     if (e.eopN < 2 || !isfinite(et)) return false;
     const double* xp = e.eop;
     const double* yp = e.eop + e.eopN;
@@ -450,8 +451,8 @@ static __device__ bool eopTime(const DevEnv& e, double et, tides::Epoch& ep) {
     ep.mjdUtc = utc;
     ep.ut1Utc = dut[i] + f * (dut[i + 1] - dut[i]);
     ep.ttUtc = 32.184 + dat[i];
-    ep.xpArcsec = xp[i] + f * (xp[i + 1] - xp[i]);
-    ep.ypArcsec = yp[i] + f * (yp[i + 1] - yp[i]);
+    ep.xp = xp[i] + f * (xp[i + 1] - xp[i]);
+    ep.yp = yp[i] + f * (yp[i + 1] - yp[i]);
     return true;
 }
 
@@ -529,7 +530,13 @@ static __device__ void nrlEpoch(const DevEnv& e, double et, EpochRecord& r) {
 }
 
 // ---- full epoch record ------------------------------------------------------------------------
-static __device__ void evalEpochRecord(const DevEnv& e, double et, EpochRecord& r) {
+// Everything of a record but the tide corrections, one thread per record:
+// rotation, body positions, the epoch-only indirect third-body term, the
+// NRLMSISE-00 time inputs.  The tide deltas are left at zero (NaN with
+// tideValid = 0 when the EOP table does not cover the epoch) and `tin` gets
+// the tide model's inputs; returns whether the tide corrections are to be
+// formed (epochRecordsKernel does that one warp per record).
+static __device__ bool evalEpochRecordBase(const DevEnv& e, double et, EpochRecord& r, tidefield::Epoch& tin) {
     r.et = et;
     for (int i = 0; i < 9; ++i) r.R[i] = (i % 4 == 0) ? 1.0 : 0.0;
     r.w[0] = r.w[1] = r.w[2] = 0.0;
@@ -549,9 +556,9 @@ static __device__ void evalEpochRecord(const DevEnv& e, double et, EpochRecord& 
     }
     for (int k = 0; k < kTideTri; ++k) r.dC[k] = r.dS[k] = 0.0;
     r.tideValid = 1;
+    bool tides = false;
     if (e.solid || e.ocean) {
-        tides::Epoch ep;
-        if (!eopTime(e, et, ep)) {
+        if (!eopTime(e, et, tin)) {
             r.tideValid = 0;
             for (int k = 0; k < kTideTri; ++k) r.dC[k] = r.dS[k] = NAN;
         } else {
@@ -559,38 +566,18 @@ static __device__ void evalEpochRecord(const DevEnv& e, double et, EpochRecord& 
             chainPosition(e, e.sunUnitsPlus, e.sunUnitsMinus, et, sun);
             chainPosition(e, e.moonUnitsPlus, e.moonUnitsMinus, et, moon);
             for (int k = 0; k < 3; ++k) {
-                ep.sun[k] = 1000.0 * sun[k];
-                ep.moon[k] = 1000.0 * moon[k];
+                tin.sun[k] = 1000.0 * sun[k];
+                tin.moon[k] = 1000.0 * moon[k];
             }
-            for (int k = 0; k < 9; ++k) ep.E[k] = r.R[k];
-            tides::Coeffs cf;
-            if (e.solid) {
-                tides::solid(ep, cf, e.zeroTide != 0);
-                for (int n = 2; n <= 4; ++n)
-                    for (int m = 0; m <= n; ++m) {
-                        r.dC[n * (n + 1) / 2 + m] += cf.C[n][m];
-                        r.dS[n * (n + 1) / 2 + m] += cf.S[n][m];
-                    }
-            }
-            if (e.ocean) {
-                tides::ocean(ep, cf);
-                for (int n = 2; n <= 6; ++n)
-                    for (int m = 0; m <= n; ++m) {
-                        r.dC[n * (n + 1) / 2 + m] += cf.C[n][m];
-                        r.dS[n * (n + 1) / 2 + m] += cf.S[n][m];
-                    }
-            }
-            for (int n = 0; n <= 6; ++n)
-                for (int m = 0; m <= n; ++m) {
-                    r.dC[n * (n + 1) / 2 + m] *= e.tideScale[n];
-                    r.dS[n * (n + 1) / 2 + m] *= e.tideScale[n];
-                }
+            for (int k = 0; k < 9; ++k) tin.E[k] = r.R[k];
+            tides = true;
         }
     }
     if (e.hasNrl) nrlEpoch(e, et, r);
     else {
         r.nrlValid = 0;
     }
+    return tides;
 }
 
 #endif  // __CUDACC__

@@ -16,13 +16,48 @@ PHOP_DECL(f32_grid)
 PHOP_DECL(f32_mixed)
 #undef PHOP_DECL
 
-__global__ void epochRecordsKernel(const __grid_constant__ DevEnv env, const double* __restrict__ epochs, int count,
-                                   EpochRecord* __restrict__ out) {
+// One epoch record per thread; then the warp forms the tide corrections of
+// its records one after the other, the terms split across its lanes
+// (tidefield::tideDeltasWarp: lane s < 25 owns coefficient slot s).
+__global__ void __launch_bounds__(64) epochRecordsKernel(const __grid_constant__ DevEnv env,
+                                                         const double* __restrict__ epochs, int count,
+                                                         EpochRecord* __restrict__ out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= count) return;
-    EpochRecord r;
-    evalEpochRecord(env, epochs[i], r);
-    out[i] = r;
+    const bool live = i < count;
+    tidefield::Epoch tin;
+    bool tides = false;
+    if (live) {
+        EpochRecord r;
+        tides = evalEpochRecordBase(env, epochs[i], r, tin);
+        out[i] = r;
+    }
+    if (!(env.solid || env.ocean)) return;
+    __syncwarp();
+    const int lane = threadIdx.x & 31;
+    const int warpFirst = i - lane;
+    unsigned todo = __ballot_sync(0xffffffffu, tides);
+    while (todo) {
+        const int src = __ffs(todo) - 1;
+        todo &= todo - 1;
+        tidefield::Epoch ep;
+        for (int k = 0; k < 9; ++k) ep.E[k] = __shfl_sync(0xffffffffu, tin.E[k], src);
+        for (int k = 0; k < 3; ++k) {
+            ep.sun[k] = __shfl_sync(0xffffffffu, tin.sun[k], src);
+            ep.moon[k] = __shfl_sync(0xffffffffu, tin.moon[k], src);
+        }
+        ep.mjdUtc = __shfl_sync(0xffffffffu, tin.mjdUtc, src);
+        ep.ut1Utc = __shfl_sync(0xffffffffu, tin.ut1Utc, src);
+        ep.ttUtc = __shfl_sync(0xffffffffu, tin.ttUtc, src);
+        ep.xp = __shfl_sync(0xffffffffu, tin.xp, src);
+        ep.yp = __shfl_sync(0xffffffffu, tin.yp, src);
+        double dC, dS;
+        tidefield::tideDeltasWarp(ep, env.solid != 0, env.ocean != 0, env.zeroTide != 0, env.tideOcean,
+                                  env.tideScale, dC, dS);
+        if (lane < tidefield::kSlots) {
+            out[warpFirst + src].dC[lane + 3] = dC;
+            out[warpFirst + src].dS[lane + 3] = dS;
+        }
+    }
 }
 
 void launchEpochRecords(const DevEnv& env, const double* epochs, int count, EpochRecord* out, cudaStream_t stream) {
