@@ -717,7 +717,26 @@ void loadEnvironment(const Value& model, HostEnvironment& env) {
     }
 }
 
+static void loadEnvironmentFilesIn(const Value& e, HostEnvironment& env, FileJobs& jobs,
+                                   std::vector<std::vector<EphUnitHost>>& ephParts,
+                                   std::vector<std::vector<EarthFrameUnit>>& oriParts);
+
+// The per-file parts that jobs write into live here, outside the loading
+// steps, and every job is joined before they go: when a synchronous step
+// throws while jobs still run, the jobs never write into freed memory.
 static void loadEnvironmentFiles(const Value& e, HostEnvironment& env, FileJobs& jobs) {
+    std::vector<std::vector<EphUnitHost>> ephParts;
+    std::vector<std::vector<EarthFrameUnit>> oriParts;
+    try {
+        loadEnvironmentFilesIn(e, env, jobs, ephParts, oriParts);
+    } catch (...) {
+        jobs.rethrowAfter(std::current_exception());
+    }
+}
+
+static void loadEnvironmentFilesIn(const Value& e, HostEnvironment& env, FileJobs& jobs,
+                                   std::vector<std::vector<EphUnitHost>>& ephParts,
+                                   std::vector<std::vector<EarthFrameUnit>>& oriParts) {
     int shapeJobs = 0;
     for (const auto& kv : e.members()) {
         const std::string& k = kv.first;
@@ -831,7 +850,6 @@ static void loadEnvironmentFiles(const Value& e, HostEnvironment& env, FileJobs&
     for (auto& b : env.bodies) haveEarth |= b.id == 399;
     if (!haveEarth) throw std::runtime_error("The Earth (center of integration) must be configured.");
     // one part per file, merged in file order: a body's unit comes from the first file holding it
-    std::vector<std::vector<EphUnitHost>> ephParts;
     if (const Value* eph = e.find("ephemeris")) {
         ephParts.resize(eph->size());
         for (size_t i = 0; i < ephParts.size(); ++i) {
@@ -841,7 +859,6 @@ static void loadEnvironmentFiles(const Value& e, HostEnvironment& env, FileJobs&
         }
     }
     {
-        std::vector<std::vector<EarthFrameUnit>> oriParts;
         const size_t first = jobs.size();
         if (const Value* ori = e.find("orientations")) {
             oriParts.resize(ori->size());
@@ -1021,15 +1038,15 @@ void Engine::uploadEnvironment() {
     // join the field's low-degree block rescaled to its GM and radius, or are
     // summed on their own (scale 1) when the Earth has no gravity field file
     for (int n = 0; n <= 6; ++n)
-        e.tideScale[n] = h.hasShape ? (tides::Consts::muEarth * 1e-9 / h.shGM) * std::pow(tides::Consts::radius * 1e-3 / h.shR, (double)n) : 1.0;
+        e.tideScale[n] = h.hasShape ? (tidefield::kMuEarth * 1e-9 / h.shGM) * std::pow(tidefield::kRadius * 1e-3 / h.shR, (double)n) : 1.0;
     if (h.hasShape) {
         e.shC = upload(owned_, h.shC);
         e.shS = upload(owned_, h.shS);
         LowTable low{};
-        for (int n = 0; n <= kLowDeg + 1 && n <= h.shDegree; ++n)
+        for (int n = 0; n <= kLowMax + 1 && n <= h.shDegree; ++n)
             for (int m = 0; m <= n && m <= h.shOrder; ++m) {
                 const int ti = n * (n + 1) / 2 + m;
-                if (n <= kLowDeg) {
+                if (n <= kLowMax) {
                     low.C[ti] = h.shC[ti];
                     low.S[ti] = h.shS[ti];
                 }
@@ -1167,14 +1184,20 @@ void Engine::uploadEnvironment() {
     e.relativity = h.relativity;
     e.tidesAlone = (h.solid || h.ocean) && !h.hasShape;
     e.zeroTide = h.zeroTide;
+    e.tideOcean = nullptr;
+    if (h.ocean) {
+        std::vector<tidefield::OceanAmp> ocean(tidefield::kWaves * tidefield::kSlots);
+        tidefield::buildOceanTable(ocean.data());
+        e.tideOcean = upload(owned_, ocean);
+    }
     e.eopN = h.eopN;
     e.eopFirstMjd = h.eopFirstMjd;
     e.eop = upload(owned_, h.eop);
 }
 
 // Lane-interleaved coefficient tile for the n > 8 part (layout in propagate.cuh)
-const Engine::Tile& Engine::tileFor(int L, bool split) {
-    const int key = L * 2 + (split ? 1 : 0);
+const Engine::Tile& Engine::tileFor(int L, bool split, int lowDeg) {
+    const int key = (lowDeg * 32 + L) * 2 + (split ? 1 : 0);
     auto it = tiles_.find(key);
     if (it != tiles_.end()) return it->second;
     const HostEnvironment& h = host_;
@@ -1184,7 +1207,7 @@ const Engine::Tile& Engine::tileFor(int L, bool split) {
     std::vector<int2> blocks(nb > 0 ? nb : 1, int2{0, 0});
     std::vector<TileD> entries;
     for (int b = 0; b < nb; ++b) {
-        const int n0b = std::max(b * L, kLowDeg + 1);
+        const int n0b = std::max(b * L, lowDeg + 1);
         const int len = std::max(0, N - n0b + 1);
         blocks[b] = int2{(int)entries.size(), len};
         const size_t base = entries.size();
@@ -1192,7 +1215,7 @@ const Engine::Tile& Engine::tileFor(int L, bool split) {
         for (int j = 0; j < L; ++j) {
             const int m = b * L + j;
             if (m > M) continue;
-            const int n0 = std::max(m, kLowDeg + 1);
+            const int n0 = std::max(m, lowDeg + 1);
             for (int i = 0; i < len; ++i) {
                 const int n = n0 + i;
                 if (n > N) break;
@@ -1380,19 +1403,29 @@ void Engine::launchStepGraph(const StepParams& p, const LaunchShape& shape, cons
     PHOP_CUDA(cudaGraphLaunch(key.exec, stream));
 }
 
+// FP64 low part of each column: n <= 8 in the FP64 form, n <= the option's
+// degree (default 20) in split precision.
+int lowDegreeFor(const RunOptions& opt) {
+    if (!opt.split) return kLowDeg;
+    const int d = opt.splitFp64Degree;
+    return d < kLowDeg ? kLowDeg : (d > kLowMax ? kLowMax : d);
+}
+
 // Host side of a launch: coefficient tile, shared-memory split and grid.
 Engine::LaunchShape Engine::prepareStep(StepParams& p, int L, const RunOptions& opt, bool shared) {
     if (L != 1 && L != 2 && L != 4 && L != 8 && L != 16) throw std::runtime_error("lanes must be 1, 2, 4, 8 or 16");
-    const Tile& tile = tileFor(L, opt.split);
+    const int lowDeg = lowDegreeFor(opt);
+    const Tile& tile = tileFor(L, opt.split, lowDeg);
     p.tile = tile.dTile;
     p.tileBytes = tile.bytes;
     p.blocks = tile.dBlocks;
     p.nblocks = tile.nblocks;
     p.diagStep = tile.dDiagStep;
+    p.lowDeg = lowDeg;
     p.tile64 = nullptr;
     p.splitRadius = 0.0;
     if (opt.split && opt.splitFloorKm > 0.0) {
-        p.tile64 = tileFor(L, false).dTile;
+        p.tile64 = tileFor(L, false, lowDeg).dTile;
         p.splitRadius = host_.shR + opt.splitFloorKm;
     }
     // shared memory per CTA: the coefficient tile (when it fits) plus the

@@ -196,3 +196,15 @@ def test_other_cbor_encodings_of_the_same_reals(tmp_path, monkeypatch, form):
     monkeypatch.undo()
     assert (other.parent / "bodies.brie").read_bytes() != (base / "bodies.brie").read_bytes()
     assert _digest(other) == ref
+
+
+def test_refusal_while_file_jobs_run(tmp_path):
+    """A synchronous step that refuses the configuration (two high-precision
+    Earth frames loaded, none named) while the ephemeris files are still
+    being read on their own threads: every load ends with the refusal and no
+    job writes into the loader's freed per-file parts."""
+    d = S.write_environment(tmp_path / "both", S.EnvSpec(earth_frame="both"))
+    (d / "config.json").write_text(json.dumps(S.make_config(d, 600.0, 60.0, max_steps=1000)))
+    for _ in range(40):
+        with pytest.raises(api.PhopError, match="more than one loaded high-precision orientation frame"):
+            api.load_environment(d / "config.json")
