@@ -117,7 +117,11 @@ int phop_propagate_device_noalloc(phop_context* ctx, int64_t n, double* d_states
  * launch shapes):
  *   "lanes"    lanes per object, 0 = autotuned, else 1, 2, 4, 8 or 16
  *   "split"    0 = plain FP64, 1 = split precision (FP32 for geopotential
- *              degrees n > 8, FP64 elsewhere)
+ *              degrees above "split_fp64_degree", FP64 elsewhere)
+ *   "split_fp64_degree"  split precision: degrees n <= this (8 .. 24,
+ *              default 20) stay FP64; FP32 rounding in the recursion of the
+ *              strongest terms (n <= 20) costs more final-position error
+ *              than their FP32 speed gains
  *   "threads"  threads per CTA (multiple of 32, <= 512)
  *   "ctas_per_sm"  resident CTAs per SM, 0 = from occupancy
  *   "ordered"  1 (default) = hand objects to warps in order of geocentric
@@ -128,9 +132,8 @@ int phop_propagate_device_noalloc(phop_context* ctx, int64_t n, double* d_states
  *   "tile_smem"  1 (default) = stage the coefficient tile in shared memory
  *              when it fits, 0 = read it through L1 (more threads per SM)
  *   "split_floor_km"  split precision only: objects closer than this height
- *              (km) above the geopotential's reference radius keep the
- *              n > 8 harmonics in FP64, where FP32 rounding of the largest
- *              high-degree terms would exceed the 1 cm budget; 0 = none */
+ *              (km) above the geopotential's reference radius keep every
+ *              harmonic in FP64; 0 = none */
 int phop_set_option(phop_context* ctx, const char* key, double value);
 
 /* ---- serving loop (no counterpart in the reference, whose driver propagates

@@ -220,6 +220,14 @@ int phop_set_option(phop_context* ctx, const char* key, double value) {
             return 1;
         }
         ctx->opt.splitFloorKm = value;
+    } else if (k == "split_fp64_degree") {
+        const int d = (int)value;
+        if ((double)d != value || d < phop::kLowDeg || d > phop::kLowMax) {
+            ctx->error = "split_fp64_degree must be an integer in [" + std::to_string(phop::kLowDeg) + ", "
+                         + std::to_string(phop::kLowMax) + "]";
+            return 1;
+        }
+        ctx->opt.splitFp64Degree = d;
     } else {
         ctx->error = "Unknown option: " + k;
         return 1;

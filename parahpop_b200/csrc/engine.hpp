@@ -119,7 +119,8 @@ struct RunOptions {
     int ctasPerSm = 0; // 0: occupancy
     bool ordered = true;  // process objects in order of geocentric radius
     bool graph = true;    // launch the step as a cached CUDA graph
-    double splitFloorKm = 0.0;  // split precision: FP64 n > 8 below this height over the field radius
+    double splitFloorKm = 0.0;  // split precision: FP64 tile part below this height over the field radius
+    int splitFp64Degree = kSplitFp64Degree;  // split precision: degrees n <= this stay FP64 (8 .. kLowMax)
     int tileSmem = -1;    // coefficient tile in shared memory: -1 when it fits, 0 never (read through L1)
     int mixedOrder = 0;   // mixed batches inside a step-count bucket: 0 radius, 1 epoch, 2 drag band + epoch
     // trajectory records of a uniform batch: device buffer of
@@ -128,6 +129,9 @@ struct RunOptions {
     int trajEvery = 0;
     int trajRecords = 0;  // capacity of dTraj in records
 };
+
+// degrees n <= this of every column run in FP64 from the LowTable
+int lowDegreeFor(const RunOptions& opt);
 
 class Engine {
 public:
@@ -199,8 +203,8 @@ public:
 
 private:
     friend class Server;
-    const Tile& tileFor(int lanes, bool split);
-    const HostTile& hostTileFor(int lanes, bool split);
+    const Tile& tileFor(int lanes, bool split, int lowDeg);
+    const HostTile& hostTileFor(int lanes, bool split, int lowDeg);
     void uploadEnvironment();
     void* scratch(const std::string& name, size_t bytes);
     // device order of objects by increasing geocentric radius (SoA state of

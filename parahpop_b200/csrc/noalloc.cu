@@ -76,8 +76,8 @@ static double tileFactorB(int n, int m, bool norm) {
                 : (nn + mm - 1.0) / (nn - mm);
 }
 
-const Engine::HostTile& Engine::hostTileFor(int L, bool split) {
-    const int key = L * 2 + (split ? 1 : 0);
+const Engine::HostTile& Engine::hostTileFor(int L, bool split, int lowDeg) {
+    const int key = (lowDeg * 32 + L) * 2 + (split ? 1 : 0);
     auto it = hostTiles_.find(key);
     if (it != hostTiles_.end()) return it->second;
     const HostEnvironment& h = host_;
@@ -89,7 +89,7 @@ const Engine::HostTile& Engine::hostTileFor(int L, bool split) {
     out.blocks.assign(nb > 0 ? nb : 1, int2{0, 0});
     std::vector<TileD> entries;
     for (int b = 0; b < nb; ++b) {
-        const int n0b = std::max(b * L, kLowDeg + 1);
+        const int n0b = std::max(b * L, lowDeg + 1);
         const int len = std::max(0, N - n0b + 1);
         out.blocks[b] = int2{(int)entries.size(), len};
         const size_t base = entries.size();
@@ -97,7 +97,7 @@ const Engine::HostTile& Engine::hostTileFor(int L, bool split) {
         for (int j = 0; j < L; ++j) {
             const int m = b * L + j;
             if (m > M) continue;
-            const int n0 = std::max(m, kLowDeg + 1);
+            const int n0 = std::max(m, lowDeg + 1);
             for (int i = 0; i < len; ++i) {
                 const int n = n0 + i;
                 if (n > N) break;
@@ -199,10 +199,11 @@ void Engine::propagateNoAlloc(int64_t n, double* dState, const double* dBc, cons
     EpochRecord* dRec = (EpochRecord*)p;
     // coefficient tile (host copy kept by the engine) into the array
     const int L = opt.lanes > 0 ? opt.lanes : autoLanes(n);
-    const HostTile& ht = hostTileFor(L, opt.split);
+    const int lowDeg = lowDegreeFor(opt);
+    const HostTile& ht = hostTileFor(L, opt.split, lowDeg);
     if (ht.bytes.size() > kTileBytes || ht.blocks.size() * sizeof(int2) > kBlockBytes)
         throw std::runtime_error("coefficient tile exceeds the allocation-free entry point's 512 KiB limit");
-    const int key = L * 2 + (opt.split ? 1 : 0);
+    const int key = (lowDeg * 32 + L) * 2 + (opt.split ? 1 : 0);
     auto check = [](cudaError_t e) {
         if (e != cudaSuccess) throw std::runtime_error(std::string("CUDA error: ") + cudaGetErrorString(e));
     };
@@ -242,6 +243,7 @@ void Engine::propagateNoAlloc(int64_t n, double* dState, const double* dBc, cons
     sp.blocks = blocksDst;
     sp.nblocks = ht.nblocks;
     sp.low = dLow_;
+    sp.lowDeg = lowDeg;
     sp.diagC = dDiag_;
     sp.workCounter = ctl;
     sp.errorFlag = ctl + 1;

@@ -46,8 +46,14 @@
 
 namespace phop {
 
-constexpr int kLowDeg = 8;                          // n <= 8 stays FP64
-constexpr int kLowTri = (kLowDeg + 2) * (kLowDeg + 3) / 2;  // factor triangle up to n = 9
+// Each column's low degrees run in FP64 from the LowTable (with the epoch's
+// tide deltas for n <= 6); the tile holds the degrees above.  The FP64 form
+// starts its tile at n = 9; split precision keeps n <= splitFp64Degree
+// (default 20, at most kLowMax) in FP64 and runs the rest in FP32.
+constexpr int kLowDeg = 8;                                  // FP64 form: n <= 8 from the LowTable
+constexpr int kSplitFp64Degree = 20;                        // split form default
+constexpr int kLowMax = 24;                                 // largest FP64 low part
+constexpr int kLowTri = (kLowMax + 2) * (kLowMax + 3) / 2;  // factor triangle up to n = kLowMax + 1
 
 // coefficient tile entry for the n > 8 part: c, s, (n+1)c, (n+1)s and the
 // recursion factors a, b of the step n -> n+1
@@ -61,7 +67,7 @@ template <typename T> struct TileOf;
 template <> struct TileOf<double> { using type = TileD; };
 template <> struct TileOf<float> { using type = TileF; };
 
-// low-degree FP64 table (n <= 8 coefficients, factors to n = 9, diagonal c_m)
+// low-degree FP64 table (n <= kLowMax coefficients, factors to n = kLowMax + 1)
 struct LowTable {
     double C[kLowTri];
     double S[kLowTri];
@@ -110,8 +116,9 @@ struct StepParams {
     const LowTable* low;
     const double* diagC;    // c_m, m = 0..M
     const double2* diagStep;  // per m: (c_{m+1}...c_{m+L}, same x (m+L)/m), nullable
+    int lowDeg;             // n <= lowDeg of every column in FP64 from `low`; the tile starts at lowDeg + 1
     const void* tile64;     // split precision: the FP64 tile (global memory, same blocks)
-    double splitRadius;     // split precision: radius (km) below which n > 8 stays FP64; 0 = none
+    double splitRadius;     // split precision: radius (km) below which the tile part stays FP64; 0 = none
     int useSmemTile;
     // scheduling and errors
     int* workCounter;

@@ -115,6 +115,7 @@ static __device__ __forceinline__ void shAccel(const StepParams& p, const typena
     using Tile = typename TileOf<T>::type;
     const int j = (int)(threadIdx.x % L);
     const int N = p.env.shDegree, M = p.env.shOrder;
+    const int lowDeg = p.lowDeg;
     const LowTable* __restrict__ low = p.low;
     const double* __restrict__ diagC = p.diagC;
     const double rn = sqrt(x * x + y * y + z * z);
@@ -170,10 +171,10 @@ static __device__ __forceinline__ void shAccel(const StepParams& p, const typena
         const bool act = mcol <= M;
         double SA0 = 0, SA1 = 0, SA2 = 0, SA3 = 0, SA4 = 0, SA5 = 0;
         T P = T(0), P1 = T(0), dP = T(0), dP1 = T(0);
-        if (act && mcol <= kLowDeg) {
-            // n = mcol .. 8 in FP64 with the epoch's tide deltas (n <= 6)
+        if (act && mcol <= lowDeg) {
+            // n = mcol .. lowDeg in FP64 with the epoch's tide deltas (n <= 6)
             double Pn = Pmm, Pn1 = 0.0, dPn = dPmm, dPn1 = 0.0, an = am, anPrev = am;
-            const int nEnd = N < kLowDeg ? N : kLowDeg;
+            const int nEnd = N < lowDeg ? N : lowDeg;
             for (int n = mcol; n <= nEnd; ++n) {
                 const int ti = n * (n + 1) / 2 + mcol;
                 double c = low->C[ti], s = low->S[ti];
@@ -413,7 +414,7 @@ static __device__ __noinline__ void tideAloneAccel(const EpochRecord& r, const d
     const double x = R[0] * pos[0] + R[1] * pos[1] + R[2] * pos[2];
     const double y = R[3] * pos[0] + R[4] * pos[1] + R[5] * pos[2];
     const double z = R[6] * pos[0] + R[7] * pos[1] + R[8] * pos[2];
-    const double mu = tides::Consts::muEarth * 1e-9, Re = tides::Consts::radius * 1e-3;  // km^3/s^2, km
+    const double mu = tidefield::kMuEarth * 1e-9, Re = tidefield::kRadius * 1e-3;  // km^3/s^2, km
     const double xy2 = x * x + y * y, xy = sqrt(xy2);
     const double d = sqrt(xy2 + z * z);
     const double sphi = z / d, cphi = xy / d, tphi = z / xy;
@@ -604,7 +605,7 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
         az += t[2];
     }
     if (e.relativity) {
-        const double mu = tides::Consts::muEarth, c = tides::Consts::c;
+        const double mu = tidefield::kMuEarth, c = tidefield::kLight;
         const double r0 = 1000.0 * pos[0], r1 = 1000.0 * pos[1], r2 = 1000.0 * pos[2];
         const double v0 = 1000.0 * vel[0], v1 = 1000.0 * vel[1], v2 = 1000.0 * vel[2];
         const double irr = rsqrt(r0 * r0 + r1 * r1 + r2 * r2);
@@ -658,10 +659,6 @@ static __device__ __forceinline__ bool stageTile(void* dst, const void* src, int
 }
 
 // ---- the persistent step kernel ----------------------------------------------------------------
-static __device__ __noinline__ void epochRecordOutOfLine(const DevEnv& env, double et, EpochRecord& r) {
-    evalEpochRecord(env, et, r);
-}
-
 // Stage record of a mixed batch: 4-point Lagrange interpolation in the
 // batch's record grid (rotation, angular velocity, body positions, tide
 // deltas; a 30 s spacing keeps the interpolation error of the rotation below
@@ -725,6 +722,10 @@ __global__ void __launch_bounds__(maxStepThreads(L), 1) propagateKernel(const __
     extern __shared__ __align__(128) unsigned char smem[];
     const Tile* tile = (const Tile*)p.tile;
     int kOffset = 0;
+    if (!SHARED_GRID && !p.grid) {  // per-object time needs the batch's record grid
+        if (threadIdx.x == 0) atomicExch(p.errorFlag, 3);
+        return;
+    }
     if (p.useSmemTile) {
         if (!stageTile(smem, p.tile, p.tileBytes, p.errorFlag)) return;
         tile = (const Tile*)smem;
@@ -796,8 +797,7 @@ __global__ void __launch_bounds__(maxStepThreads(L), 1) propagateKernel(const __
                 } else {
                     EpochRecord rec;
                     const double ts = s == 0 ? t0 : t0 + dt * rkC(s - 1);
-                    if (p.grid) epochRecordFromGrid(p, ts, rec);
-                    else epochRecordOutOfLine(p.env, ts, rec);
+                    epochRecordFromGrid(p, ts, rec);
                     accelerations<L, T>(p, tile, rec, st, st + 3, bc, ams, acc);
                 }
 #pragma unroll
