@@ -76,6 +76,29 @@ int phop_propagate_device(phop_context* ctx, int64_t n, double* d_states_soa, do
                           const double* cd, const double* cr, double duration_s, double step_s,
                           double* out_epoch_mjd2000_tdb);
 
+/* An uneven batch resident in device memory, advanced in slices (the
+ * serving loop's pattern, for callers that keep their objects in HBM):
+ * phop_object_times fills, on the host, the per-object time arrays the
+ * step kernel works on from epochs (MJD2000 TDB), durations and steps (s)
+ * with the reference's fixed-step rules (FixedStep.h:7-28 per object:
+ * epochs in TDB seconds past J2000, the first step shortened to the span,
+ * the maxNumSteps refusal), as 4*n doubles: current epoch[n], end epoch[n],
+ * current step size[n] (0 once the end is reached), nominal step[n].
+ * phop_propagate_device_objects then advances every object that has not
+ * reached its end by at most max_steps fixed steps, on device arrays:
+ * d_states_soa (6*n), d_time (4*n, the layout above, updated in place),
+ * d_bc and d_ams as for phop_propagate_device_noalloc; *out_unfinished
+ * gets the objects still short of their end.  Slices continue exactly where
+ * the previous call stopped: any sequence of calls gives, bit for bit, the
+ * results of one phop_propagate call over the whole durations at the same
+ * lane count.  No reference counterpart (its driver propagates one batch to
+ * the end). */
+int phop_object_times(const phop_context* ctx, int64_t n, const double* epoch_mjd2000_tdb, const double* duration_s,
+                      const double* step_s, double* out_time);
+int phop_propagate_device_objects(phop_context* ctx, int64_t n, double* d_states_soa, double* d_time,
+                                  const double* d_bc, const double* d_ams, int64_t max_steps,
+                                  int64_t* out_unfinished);
+
 /* Trajectory of a batch that shares one epoch, duration and step: the
  * states (n x 6, km and km/s, host arrays in and out) after every
  * `every`-th fixed step, written by the step kernel as it goes.  out_states

@@ -51,6 +51,9 @@ def library() -> C.CDLL:
         lib.phop_propagate_device.restype = C.c_int
         lib.phop_propagate_trajectory.argtypes = [C.c_void_p, C.c_int64, C.c_double] + [D] * 6 + \
             [C.c_double, C.c_double, C.c_int64, C.c_int64, D, D, C.POINTER(C.c_int64)]
+        lib.phop_object_times.argtypes = [C.c_void_p, C.c_int64, D, D, D, D]
+        lib.phop_propagate_device_objects.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                      C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]
         lib.phop_set_option.argtypes = [C.c_void_p, C.c_char_p, C.c_double]
         lib.phop_last_stats.argtypes = [C.c_void_p, C.POINTER(PhopStats)]
         lib.paraHPOP_run.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.c_char_p]
@@ -160,6 +163,39 @@ class Propagator:
         if rc != 0:
             raise PhopError(library().phop_last_error(self._h).decode())
         return out.value
+
+    def object_times(self, epochs, durations, steps) -> np.ndarray:
+        """Per-object time arrays (4*n: current epoch, end epoch, current step
+        size, nominal step; TDB seconds past J2000) for
+        ``propagate_device_objects``."""
+        f = lambda a: np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+        ep, du, st = map(f, (epochs, durations, steps))
+        n = len(ep)
+        out = np.empty(4 * n)
+        if library().phop_object_times(self._h, n, _dp(ep), _dp(du), _dp(st), _dp(out)) != 0:
+            raise PhopError(library().phop_last_error(self._h).decode())
+        return out
+
+    def propagate_device_objects(self, n: int, d_state_ptr: int, d_time_ptr: int, d_bc_ptr: int, d_ams_ptr: int,
+                                 max_steps: int) -> int:
+        """Advance a resident uneven batch by at most ``max_steps`` steps per
+        object (device pointers); returns the objects still short of their end."""
+        left = C.c_int64()
+        rc = library().phop_propagate_device_objects(self._h, n, C.c_void_p(d_state_ptr), C.c_void_p(d_time_ptr),
+                                                     C.c_void_p(d_bc_ptr), C.c_void_p(d_ams_ptr), int(max_steps),
+                                                     C.byref(left))
+        if rc != 0:
+            raise PhopError(library().phop_last_error(self._h).decode())
+        return left.value
+
+    @staticmethod
+    def factors(mass, drag_area, srp_area, cd, cr):
+        """Per-object drag and SRP factors (bc, ams) as the library forms them
+        (driver.cpp:118-120, PrivateAccelerations.h:41-42): area in km^2,
+        cr scaled by srp_area / drag_area."""
+        area = np.asarray(drag_area, dtype=np.float64) * 1e-6
+        crf = np.asarray(cr, dtype=np.float64) * np.asarray(srp_area, dtype=np.float64) / np.asarray(drag_area)
+        return np.asarray(cd) * area / np.asarray(mass), crf * area / np.asarray(mass)
 
     def trajectory(self, epoch: float, states, mass, drag_area, srp_area, cd, cr, duration: float, step: float,
                    every: int = 1):

@@ -329,6 +329,58 @@ int phop_propagate_device(phop_context* ctx, int64_t n, double* dState, double e
     }
 }
 
+int phop_object_times(const phop_context* ctx, int64_t n, const double* epoch, const double* duration,
+                      const double* step, double* outTime) {
+    if (!ctx) return 1;
+    phop_context* c = const_cast<phop_context*>(ctx);
+    try {
+        if (n <= 0) throw std::runtime_error("targets must be a nonempty array.");
+        if (!epoch || !duration || !step || !outTime) throw std::runtime_error("phop_object_times: null argument");
+        double lo = epoch[0], hi = epoch[0];
+        for (int64_t i = 0; i < n; ++i) {
+            if (!(duration[i] > 0) || !std::isfinite(duration[i]))
+                throw std::runtime_error("duration_seconds must be finite and positive.");
+            if (!(step[i] > 0) || !std::isfinite(step[i]))
+                throw std::runtime_error("initialStepSize must be finite and positive.");
+            // FixedStep.h:7-28 per object: ET epochs, first step, step count
+            const double cur = std::fma(epoch[i], 86400.0, -43200.0);
+            const double end = std::fma(epoch[i] + duration[i] / 86400.0, 86400.0, -43200.0);
+            const double span = end - cur;
+            if (!(span > 0) || !std::isfinite(span))
+                throw std::runtime_error("Duration/step cannot be represented by the integration time/index types.");
+            if (std::ceil(span / step[i]) > (double)c->maxSteps)
+                throw std::runtime_error("A target stopped without reaching the requested end of simulation.");
+            outTime[i] = cur;
+            outTime[n + i] = end;
+            outTime[2 * n + i] = std::min(step[i], span);
+            outTime[3 * n + i] = step[i];
+            lo = std::min(lo, epoch[i]);
+            hi = std::max(hi, epoch[i] + duration[i] / 86400.0);
+        }
+        c->engine->assertCoverage(lo, hi);
+        return 0;
+    } catch (const std::exception& e) {
+        c->error = e.what();
+        return 1;
+    }
+}
+
+int phop_propagate_device_objects(phop_context* ctx, int64_t n, double* dState, double* dTime, const double* dBc,
+                                  const double* dAms, int64_t maxSteps, int64_t* outUnfinished) {
+    if (!ctx) return 1;
+    try {
+        if (n <= 0) throw std::runtime_error("targets must be a nonempty array.");
+        if (!dState || !dTime || !dBc || !dAms) throw std::runtime_error("device arrays must not be null");
+        ctx->stats = phop::RunStats{};
+        const int64_t left = ctx->engine->advanceObjects(n, dState, dTime, dBc, dAms, maxSteps, ctx->opt, &ctx->stats);
+        if (outUnfinished) *outUnfinished = left;
+        return 0;
+    } catch (const std::exception& e) {
+        ctx->error = e.what();
+        return 1;
+    }
+}
+
 int phop_propagate_trajectory(phop_context* ctx, int64_t n, double epoch, const double* states, const double* mass,
                               const double* dragArea, const double* srpArea, const double* cd, const double* cr,
                               double duration, double step, int64_t every, int64_t maxRecords, double* outEpochs,

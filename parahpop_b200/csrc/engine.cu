@@ -1786,6 +1786,96 @@ void Engine::propagate(const TargetSet& t, int64_t maxSteps, const RunOptions& o
         for (int d = 0; d < 6; ++d) outState[(size_t)6 * i + d] = soa[(size_t)d * n + i];
 }
 
+// Per-object time of a sliced batch: over the unfinished objects (step
+// size > 0) the earliest epoch and the latest epoch the next `maxSteps`
+// steps can reach, per block; the unfinished count and the steps they will
+// take (min(maxSteps, ceil(remaining / step)) each) by atomics.
+__global__ void objectSpanKernel(const double* __restrict__ cur, const double* __restrict__ end,
+                                 const double* __restrict__ dt, const double* __restrict__ step, int64_t n,
+                                 int64_t maxSteps, double* __restrict__ blockLo, double* __restrict__ blockHi,
+                                 unsigned long long* __restrict__ counts) {
+    __shared__ double sLo[256], sHi[256];
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double lo = INFINITY, hi = -INFINITY;
+    if (i < n && dt[i] > 0.0) {
+        const double c = cur[i], e = end[i], h = step[i];
+        const double steps = fmin((double)maxSteps, ceil((e - c) / h));
+        lo = c;
+        hi = fmin(e, c + steps * h);
+        atomicAdd(&counts[0], 1ull);
+        atomicAdd(&counts[1], (unsigned long long)steps);
+    }
+    sLo[threadIdx.x] = lo;
+    sHi[threadIdx.x] = hi;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+        if ((int)threadIdx.x < k) {
+            sLo[threadIdx.x] = fmin(sLo[threadIdx.x], sLo[threadIdx.x + k]);
+            sHi[threadIdx.x] = fmax(sHi[threadIdx.x], sHi[threadIdx.x + k]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        blockLo[blockIdx.x] = sLo[0];
+        blockHi[blockIdx.x] = sHi[0];
+    }
+}
+
+int64_t Engine::advanceObjects(int64_t n, double* dState, double* dTime, const double* dBc, const double* dAms,
+                               int64_t maxSteps, const RunOptions& opt, RunStats* stats, cudaStream_t stream) {
+    PHOP_CUDA(cudaSetDevice(device_));
+    if (maxSteps <= 0) throw std::runtime_error("max_steps must be positive.");
+    double* cur = dTime;
+    double* end = dTime + n;
+    double* dtv = dTime + 2 * n;
+    double* stp = dTime + 3 * n;
+    RunStats local;
+    RunStats* st = stats ? stats : &local;
+    const int threads = 256;
+    const int blocks = (int)((n + threads - 1) / threads);
+    double* dLo = (double*)scratch("spanLo", (size_t)blocks * 8);
+    double* dHi = (double*)scratch("spanHi", (size_t)blocks * 8);
+    unsigned long long* dCounts = (unsigned long long*)scratch("spanCounts", 16);
+    auto span = [&](double& lo, double& hi, int64_t& unfinished, int64_t& steps) {
+        PHOP_CUDA(cudaMemsetAsync(dCounts, 0, 16, stream));
+        objectSpanKernel<<<blocks, threads, 0, stream>>>(cur, end, dtv, stp, n, maxSteps, dLo, dHi, dCounts);
+        PHOP_CUDA(cudaGetLastError());
+        std::vector<double> l(blocks), h(blocks);
+        unsigned long long c[2];
+        PHOP_CUDA(cudaMemcpyAsync(l.data(), dLo, (size_t)blocks * 8, cudaMemcpyDeviceToHost, stream));
+        PHOP_CUDA(cudaMemcpyAsync(h.data(), dHi, (size_t)blocks * 8, cudaMemcpyDeviceToHost, stream));
+        PHOP_CUDA(cudaMemcpyAsync(c, dCounts, 16, cudaMemcpyDeviceToHost, stream));
+        PHOP_CUDA(cudaStreamSynchronize(stream));
+        lo = INFINITY;
+        hi = -INFINITY;
+        for (int b = 0; b < blocks; ++b) {
+            lo = std::min(lo, l[b]);
+            hi = std::max(hi, h[b]);
+        }
+        unfinished = (int64_t)c[0];
+        steps = (int64_t)c[1];
+    };
+    double lo, hi;
+    int64_t unfinished, steps;
+    span(lo, hi, unfinished, steps);
+    if (unfinished == 0) return 0;
+    TimeGrid g;
+    g.shared = false;
+    g.cur = cur;
+    g.end = end;
+    g.dt1 = dtv;
+    g.step = stp;
+    g.unfinished = (int*)scratch("unfinished", (size_t)n * 4);
+    int64_t launches = 2;  // span kernel; counts
+    buildRecordGrid(lo, hi, g, stream, &launches);
+    const int64_t* dOrder = opt.ordered ? orderByRadius(n, dState, stream, &launches) : nullptr;
+    runKernel(n, dState, dBc, dAms, g, dOrder, maxSteps, opt, st, stream, launches);
+    st->objectSteps += steps;
+    span(lo, hi, unfinished, steps);
+    st->launches += 1;
+    return unfinished;
+}
+
 void Engine::propagateResident(int64_t n, double* dState, const double* epochMjd, const double* bc, const double* ams,
                                double duration, double step, int64_t maxSteps, const RunOptions& opt,
                                std::vector<double>& outEpochMjd, RunStats* stats, cudaStream_t stream) {

@@ -157,6 +157,14 @@ public:
                            double duration, double step, int64_t maxSteps, const RunOptions& opt,
                            std::vector<double>& outEpochMjd, RunStats* stats, cudaStream_t stream = 0);
 
+    // Sliced per-object-time batch resident in device memory: dTime holds
+    // cur[n], end[n], dt[n], step[n] (TDB seconds past J2000; dt = 0 once an
+    // object has reached its end), updated in place; every unfinished
+    // object advances by at most maxSteps fixed steps.  Returns the number
+    // of objects still short of their end.
+    int64_t advanceObjects(int64_t n, double* dState, double* dTime, const double* dBc, const double* dAms,
+                           int64_t maxSteps, const RunOptions& opt, RunStats* stats, cudaStream_t stream = 0);
+
     int device() const { return device_; }
     int smCount() const { return sms_; }
     int autoLanes(int64_t n) const;

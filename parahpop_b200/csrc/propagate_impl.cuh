@@ -770,7 +770,7 @@ __global__ void __launch_bounds__(maxStepThreads(L), 1) propagateKernel(const __
             dtv = p.dt[oi];
             endv = p.end[oi];
             stepv = p.step[oi];
-            done = !valid;
+            done = !valid || !(dtv > 0.0);  // a resident batch keeps objects that have reached their end
         }
         const int64_t nsteps = SHARED_GRID ? (int64_t)p.nsteps : p.maxSteps;
         for (int64_t kstep = 0; kstep < nsteps; ++kstep) {
