@@ -1018,6 +1018,7 @@ Engine::~Engine() {
     for (auto& kv : scratch_) cudaFree(kv.second.first);
     for (GraphEntry& g : graphs_) cudaGraphExecDestroy(g.exec);
     if (captureStream_) cudaStreamDestroy(captureStream_);
+    if (gridCache_) cudaFree(gridCache_);
     for (auto& kv : tiles_) {
         cudaFree(kv.second.dTile);
         cudaFree(kv.second.dBlocks);
@@ -1329,25 +1330,65 @@ const int64_t* Engine::orderByRadius(int64_t n, const double* dState, cudaStream
 }
 
 // Epoch records at TDB seconds k * 30 for every k whose 4-point stencil an
-// epoch in [lo, hi] can reach, for the per-object time path.
+// epoch in [lo, hi] can reach, for the per-object time path.  Records depend
+// on the absolute epoch alone, so the context keeps them: a request inside
+// the kept range reuses it, one beyond it extends the range (with a margin of
+// a quarter of the span, at least a day, so that slices that advance a batch
+// step by step rarely extend it again) and computes only the new records.
 void Engine::buildRecordGrid(double lo, double hi, TimeGrid& g, cudaStream_t stream, int64_t* launches) {
     const double H = kRecordGridSeconds;
     const int64_t kLo = (int64_t)std::floor(lo / H) - 1;
     const int64_t kHi = (int64_t)std::ceil(hi / H) + 2;
-    const int64_t G = kHi - kLo + 1;
-    if (G > (int64_t)1 << 26) throw std::runtime_error("the batch spans too long a time interval");
-    std::vector<double> ts(G);
-    for (int64_t k = 0; k < G; ++k) ts[k] = (double)(kLo + k) * H;
-    double* dT = (double*)scratch("gridT", (size_t)G * 8);
-    EpochRecord* dRec = (EpochRecord*)scratch("gridRecords", (size_t)G * sizeof(EpochRecord));
-    PHOP_CUDA(cudaMemcpyAsync(dT, ts.data(), (size_t)G * 8, cudaMemcpyHostToDevice, stream));
-    launchEpochRecords(denv_, dT, (int)G, dRec, stream);
-    PHOP_CUDA(cudaGetLastError());
-    if (launches) *launches += 1;
-    g.grid = dRec;
+    if (kHi - kLo + 1 > (int64_t)1 << 26) throw std::runtime_error("the batch spans too long a time interval");
+    if (!(gridCache_ && kLo >= gridKLo_ && kHi <= gridKHi_)) {
+        const int64_t margin = std::max<int64_t>(2880, (kHi - kLo) / 4);
+        int64_t a = kLo, b = kHi + margin;
+        if (gridCache_ && gridKHi_ >= a - 1 && gridKLo_ <= b + 1) {  // overlapping or adjacent: keep the old records
+            a = std::min(a, gridKLo_);
+            b = std::max(b, gridKHi_);
+        }
+        const int64_t G = b - a + 1;
+        if (G > (int64_t)1 << 26) throw std::runtime_error("the batch spans too long a time interval");
+        EpochRecord* fresh = nullptr;
+        PHOP_CUDA(cudaMalloc(&fresh, (size_t)G * sizeof(EpochRecord)));
+        std::vector<double> ts;
+        std::vector<int64_t> at;  // grid indices to compute
+        const bool keep = gridCache_ && gridKLo_ >= a && gridKHi_ <= b;
+        for (int64_t k = a; k <= b; ++k)
+            if (!(keep && k >= gridKLo_ && k <= gridKHi_)) at.push_back(k);
+        if (keep) {
+            PHOP_CUDA(cudaMemcpyAsync(fresh + (gridKLo_ - a), gridCache_,
+                                      (size_t)(gridKHi_ - gridKLo_ + 1) * sizeof(EpochRecord),
+                                      cudaMemcpyDeviceToDevice, stream));
+        }
+        // the new records come in at most two contiguous runs (below and above the kept range)
+        size_t i = 0;
+        while (i < at.size()) {
+            size_t j = i;
+            while (j + 1 < at.size() && at[j + 1] == at[j] + 1) ++j;
+            const int64_t count = (int64_t)(j - i + 1);
+            ts.resize(count);
+            for (int64_t q = 0; q < count; ++q) ts[q] = (double)(at[i] + q) * H;
+            double* dT = (double*)scratch("gridT", (size_t)count * 8);
+            PHOP_CUDA(cudaMemcpyAsync(dT, ts.data(), (size_t)count * 8, cudaMemcpyHostToDevice, stream));
+            launchEpochRecords(denv_, dT, (int)count, fresh + (at[i] - a), stream);
+            PHOP_CUDA(cudaGetLastError());
+            PHOP_CUDA(cudaStreamSynchronize(stream));  // ts is reused by the next run
+            if (launches) *launches += 1;
+            i = j + 1;
+        }
+        if (gridCache_) {
+            PHOP_CUDA(cudaStreamSynchronize(stream));
+            cudaFree(gridCache_);
+        }
+        gridCache_ = fresh;
+        gridKLo_ = a;
+        gridKHi_ = b;
+    }
+    g.grid = gridCache_;
     g.gridH = H;
-    g.gridBase = kLo;
-    g.gridN = (int)G;
+    g.gridBase = gridKLo_;
+    g.gridN = (int)(gridKHi_ - gridKLo_ + 1);
 }
 
 Engine::LaunchShape Engine::launchStep(StepParams p, int L, const RunOptions& opt, bool shared, cudaStream_t stream) {
@@ -1866,10 +1907,12 @@ int64_t Engine::advanceObjects(int64_t n, double* dState, double* dTime, const d
     g.dt1 = dtv;
     g.step = stp;
     g.unfinished = (int*)scratch("unfinished", (size_t)n * 4);
-    int64_t launches = 2;  // span kernel; counts
+    int64_t launches = 1;  // the span kernel
     buildRecordGrid(lo, hi, g, stream, &launches);
     const int64_t* dOrder = opt.ordered ? orderByRadius(n, dState, stream, &launches) : nullptr;
-    runKernel(n, dState, dBc, dAms, g, dOrder, maxSteps, opt, st, stream, launches);
+    RunOptions o = opt;
+    o.graph = false;  // every slice's launch parameters differ: nothing to replay
+    runKernel(n, dState, dBc, dAms, g, dOrder, maxSteps, o, st, stream, launches);
     st->objectSteps += steps;
     span(lo, hi, unfinished, steps);
     st->launches += 1;

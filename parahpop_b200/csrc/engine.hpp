@@ -232,6 +232,9 @@ private:
         cudaGraphExec_t exec = nullptr;
     };
     std::vector<GraphEntry> graphs_;
+    // epoch records of the per-object-time path at grid indices [gridKLo_, gridKHi_]
+    EpochRecord* gridCache_ = nullptr;
+    int64_t gridKLo_ = 0, gridKHi_ = -1;
     cudaStream_t captureStream_ = nullptr;
     int tunedLanes(const StepParams& base, const RunOptions& opt, bool shared, cudaStream_t stream, int64_t* launches);
     void runKernel(int64_t n, double* dState, const double* dBc, const double* dAms, const TimeGrid& g,

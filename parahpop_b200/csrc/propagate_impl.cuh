@@ -107,15 +107,76 @@ static __device__ __forceinline__ void finalUpdate(double (&y)[CPL], const Stage
     }
 }
 
+// ---- epoch records as the force model reads them -----------------------------------------
+// A shared-grid batch reads the precomputed record of its (step, stage) in
+// place.  A per-object-time batch interpolates each field where the force
+// model reads it (4-point Lagrange in the batch's record grid, weights
+// depending on the epoch alone), so no record is copied into the thread's
+// local memory.
+struct RecordRef {
+    const EpochRecord* r;
+    __device__ __forceinline__ double R(int i) const { return r->R[i]; }
+    __device__ __forceinline__ double W(int i) const { return r->w[i]; }
+    __device__ __forceinline__ double body(int b, int i) const { return r->body[b][i]; }
+    __device__ __forceinline__ double indirect(int i) const { return r->indirect[i]; }
+    __device__ __forceinline__ double dC(int k) const { return r->dC[k]; }
+    __device__ __forceinline__ double dS(int k) const { return r->dS[k]; }
+    // NRLMSISE-00 time inputs; valid = -1 (evaluate at the epoch in `sec`
+    // when an object below the cut-off needs them) when the record has none
+    __device__ __forceinline__ NrlTime nrlDeferred() const {
+        NrlTime t{r->nrlSec, r->nrlGast, r->nrlBlock, r->nrlValid};
+        if (t.valid < 0) t.sec = r->et;
+        return t;
+    }
+};
+
+struct RecordInterp {
+    const double* g;  // first record of the 4-point stencil, as doubles
+    double w0, w1, w2, w3;
+    double et;        // the stage epoch (TDB s past J2000)
+    static constexpr int kStride = (int)(sizeof(EpochRecord) / sizeof(double));
+    __device__ __forceinline__ double at(int off) const {
+        const double* b = g + off;
+        return w0 * b[0] + w1 * b[kStride] + w2 * b[2 * kStride] + w3 * b[3 * kStride];
+    }
+    __device__ __forceinline__ double R(int i) const { return at((int)(offsetof(EpochRecord, R) / 8) + i); }
+    __device__ __forceinline__ double W(int i) const { return at((int)(offsetof(EpochRecord, w) / 8) + i); }
+    __device__ __forceinline__ double body(int b, int i) const {
+        return at((int)(offsetof(EpochRecord, body) / 8) + 3 * b + i);
+    }
+    __device__ __forceinline__ double indirect(int i) const {
+        return at((int)(offsetof(EpochRecord, indirect) / 8) + i);
+    }
+    __device__ __forceinline__ double dC(int k) const { return at((int)(offsetof(EpochRecord, dC) / 8) + k); }
+    __device__ __forceinline__ double dS(int k) const { return at((int)(offsetof(EpochRecord, dS) / 8) + k); }
+    // NRLMSISE-00 time inputs: evaluated exactly at the stage epoch by the
+    // drag model, only for objects below the density cut-off
+    __device__ __forceinline__ NrlTime nrlDeferred() const { return NrlTime{et, 0.0, 0, -1}; }
+};
+
+// body-fixed (ITRF) components of an inertial vector, and back
+template <class Rec>
+static __device__ __forceinline__ void toBody(const Rec& r, const double v[3], double out[3]) {
+    out[0] = r.R(0) * v[0] + r.R(1) * v[1] + r.R(2) * v[2];
+    out[1] = r.R(3) * v[0] + r.R(4) * v[1] + r.R(5) * v[2];
+    out[2] = r.R(6) * v[0] + r.R(7) * v[1] + r.R(8) * v[2];
+}
+template <class Rec>
+static __device__ __forceinline__ void fromBody(const Rec& r, const double a[3], double out[3]) {
+    out[0] = r.R(0) * a[0] + r.R(3) * a[1] + r.R(6) * a[2];
+    out[1] = r.R(1) * a[0] + r.R(4) * a[1] + r.R(7) * a[2];
+    out[2] = r.R(2) * a[0] + r.R(5) * a[1] + r.R(8) * a[2];
+}
+
 // ---- spherical harmonics, lane-split over orders --------------------------------------------
-template <int L, typename T>
+template <int L, typename T, class Rec>
 static __device__ __forceinline__ void shAccel(const StepParams& p, const typename TileOf<T>::type* __restrict__ tile,
-                                        const double* __restrict__ dC, const double* __restrict__ dS, double x,
-                                        double y, double z, double out[3]) {
+                                        const Rec& rec, double x, double y, double z, double out[3]) {
     using Tile = typename TileOf<T>::type;
     const int j = (int)(threadIdx.x % L);
     const int N = p.env.shDegree, M = p.env.shOrder;
     const int lowDeg = p.lowDeg;
+    const bool tides = p.env.solid || p.env.ocean;
     const LowTable* __restrict__ low = p.low;
     const double* __restrict__ diagC = p.diagC;
     const double rn = sqrt(x * x + y * y + z * z);
@@ -178,9 +239,9 @@ static __device__ __forceinline__ void shAccel(const StepParams& p, const typena
             for (int n = mcol; n <= nEnd; ++n) {
                 const int ti = n * (n + 1) / 2 + mcol;
                 double c = low->C[ti], s = low->S[ti];
-                if (n <= 6) {
-                    c += dC[ti];
-                    s += dS[ti];
+                if (n <= 6 && tides) {
+                    c += rec.dC(ti);
+                    s += rec.dS(ti);
                 }
                 if (mcol == 0) s = 0.0;
                 const double q = an * Pn, qd = an * dPn, np1 = (double)(n + 1);
@@ -275,7 +336,7 @@ static __device__ __forceinline__ void shAccel(const StepParams& p, const typena
         for (int n = 1; n <= N; ++n) {
             const int ti = n * (n + 1) / 2 + 1;
             double s = p.env.shS[ti];
-            if (n <= 6) s += dS[ti];
+            if (n <= 6 && tides) s += rec.dS(ti);
             const double sign = sinPhi > 0.0 ? 1.0 : ((n & 1) ? 1.0 : -1.0);
             double lim = 0.5 * (double)n * (n + 1.0);
             if (p.env.shNormalized) lim *= sqrt(2.0 * (2.0 * n + 1.0) / ((double)n * (n + 1.0)));
@@ -327,23 +388,23 @@ static __device__ __forceinline__ double shadowFactor(const double rS[3], const 
 // NRLMSISE-00 density (kg/km^3) at ITRF position f; the L lanes of a group
 // share the globe7 tables of the model and all return the same value.
 template <int L>
-static __device__ __forceinline__ double nrlDensityBody(const DevEnv& e, const EpochRecord& r, const double f[3]);
+static __device__ __forceinline__ double nrlDensityBody(const DevEnv& e, NrlTime t, const double f[3]);
 
 // Out of line for eight and sixteen lanes, where the caller's live state is
 // small enough that the call's register saves cost less than the larger
 // inlined kernel; inline for one to four lanes (measured both ways).
 template <int L>
-static __device__ __noinline__ double nrlDensityCall(const DevEnv& e, const EpochRecord& r, const double f[3]) {
-    return nrlDensityBody<L>(e, r, f);
+static __device__ __noinline__ double nrlDensityCall(const DevEnv& e, NrlTime t, const double f[3]) {
+    return nrlDensityBody<L>(e, t, f);
 }
 template <int L>
-static __device__ __forceinline__ double nrlDensity(const DevEnv& e, const EpochRecord& r, const double f[3]) {
-    if constexpr (L <= 4) return nrlDensityBody<L>(e, r, f);
-    else return nrlDensityCall<L>(e, r, f);
+static __device__ __forceinline__ double nrlDensity(const DevEnv& e, NrlTime t, const double f[3]) {
+    if constexpr (L <= 4) return nrlDensityBody<L>(e, t, f);
+    else return nrlDensityCall<L>(e, t, f);
 }
 
 template <int L>
-static __device__ __forceinline__ double nrlDensityBody(const DevEnv& e, const EpochRecord& r, const double f[3]) {
+static __device__ __forceinline__ double nrlDensityBody(const DevEnv& e, NrlTime t, const double f[3]) {
     // geodetic latitude / longitude / altitude (Nrlmsise00.cu:243-266)
     const double rho2 = f[0] * f[0] + f[1] * f[1];
     if (!(rho2 + f[2] * f[2] > 0.0)) return NAN;
@@ -368,8 +429,7 @@ static __device__ __forceinline__ double nrlDensityBody(const DevEnv& e, const E
     const double alt = nh - nn;
     if (!(isfinite(lat) && isfinite(lon) && isfinite(alt))) return NAN;
     if (alt > e.nrlHcutoff) return 0.0;
-    NrlTime t{r.nrlSec, r.nrlGast, r.nrlBlock, r.nrlValid};
-    if (t.valid < 0) t = nrlTime(e, r.et);
+    if (t.valid < 0) t = nrlTime(e, t.sec);  // deferred: `sec` holds the stage epoch (TDB s past J2000)
     if (!t.valid) return NAN;
     const double kRad = 57.2957795130823208768;
     nrlf::Fast<double> model(e.nrlBlocks[t.block], t.sec);
@@ -409,11 +469,11 @@ static __device__ __forceinline__ double geodeticHeight(const double r[3], const
 // Legendre functions by the column recurrences and their latitude
 // derivatives in closed form (the reference recurses them alongside,
 // HpopCorrections.h:121-145).
-static __device__ __noinline__ void tideAloneAccel(const EpochRecord& r, const double pos[3], double acc[3]) {
-    const double* R = r.R;
-    const double x = R[0] * pos[0] + R[1] * pos[1] + R[2] * pos[2];
-    const double y = R[3] * pos[0] + R[4] * pos[1] + R[5] * pos[2];
-    const double z = R[6] * pos[0] + R[7] * pos[1] + R[8] * pos[2];
+template <class Rec>
+static __device__ __noinline__ void tideAloneAccel(const Rec r, const double pos[3], double acc[3]) {
+    double b[3];
+    toBody(r, pos, b);
+    const double x = b[0], y = b[1], z = b[2];
     const double mu = tidefield::kMuEarth * 1e-9, Re = tidefield::kRadius * 1e-3;  // km^3/s^2, km
     const double xy2 = x * x + y * y, xy = sqrt(xy2);
     const double d = sqrt(xy2 + z * z);
@@ -452,7 +512,7 @@ static __device__ __noinline__ void tideAloneAccel(const EpochRecord& r, const d
         double q1 = 0.0, q2 = 0.0, q3 = 0.0;
         for (int m = 0; m <= n; ++m) {
             const int ti = n * (n + 1) / 2 + m;
-            const double c = r.dC[ti], s = r.dS[ti];
+            const double c = r.dC(ti), s = r.dS(ti);
             const double v = c * cm[m] + s * sm[m];
             q1 += p[n][m] * v;
             q2 += dp[n][m] * v;
@@ -466,15 +526,18 @@ static __device__ __noinline__ void tideAloneAccel(const EpochRecord& r, const d
     const double q = dUdr / d - z / (d * d * xy) * dUdlat;
     const double bf0 = q * x - (dUdlon / xy2) * y, bf1 = q * y + (dUdlon / xy2) * x;
     const double bf2 = dUdr / d * z + xy / (d * d) * dUdlat;
-    acc[0] += R[0] * bf0 + R[3] * bf1 + R[6] * bf2;
-    acc[1] += R[1] * bf0 + R[4] * bf1 + R[7] * bf2;
-    acc[2] += R[2] * bf0 + R[5] * bf1 + R[8] * bf2;
+    const double bf[3] = {bf0, bf1, bf2};
+    double a[3];
+    fromBody(r, bf, a);
+    acc[0] += a[0];
+    acc[1] += a[1];
+    acc[2] += a[2];
 }
 
 // full right-hand side acceleration (km/s^2); every lane of the group calls it
-template <int L, typename T>
+template <int L, typename T, class Rec>
 static __device__ __forceinline__ void accelerations(const StepParams& p, const typename TileOf<T>::type* tile,
-                                              const EpochRecord& r, const double pos[3], const double vel[3],
+                                              const Rec& r, const double pos[3], const double vel[3],
                                               double bc, double ams, double acc[3]) {
     const DevEnv& e = p.env;
     double ax = 0.0, ay = 0.0, az = 0.0;
@@ -492,7 +555,7 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
             } else {
                 // direct part per object; the indirect part (epoch-only) is
                 // the record's sum, added after the loop
-                const double* rb = r.body[bi];
+                const double rb[3] = {r.body(bi, 0), r.body(bi, 1), r.body(bi, 2)};
                 const double d0 = pos[0] - rb[0], d1 = pos[1] - rb[1], d2 = pos[2] - rb[2];
                 const double ird = rsqrt(d0 * d0 + d1 * d1 + d2 * d2);
                 const double f1 = -gm * (ird * ird * ird);
@@ -502,54 +565,55 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
             }
         }
         if (fl & kShape) {
-            const double* R = r.R;
-            const double bx = R[0] * pos[0] + R[1] * pos[1] + R[2] * pos[2];
-            const double by = R[3] * pos[0] + R[4] * pos[1] + R[5] * pos[2];
-            const double bz = R[6] * pos[0] + R[7] * pos[1] + R[8] * pos[2];
+            double b[3];
+            toBody(r, pos, b);
+            const double bx = b[0], by = b[1], bz = b[2];
             double a[3];
             if constexpr (!std::is_same<T, double>::value) {
                 // split precision: objects below the split radius keep the
-                // n > 8 part in FP64 (from the FP64 tile in global memory)
+                // tile part in FP64 (from the FP64 tile in global memory)
                 if (p.splitRadius > 0.0 && bx * bx + by * by + bz * bz < p.splitRadius * p.splitRadius)
-                    shAccel<L, double>(p, (const TileD*)p.tile64, r.dC, r.dS, bx, by, bz, a);
+                    shAccel<L, double>(p, (const TileD*)p.tile64, r, bx, by, bz, a);
                 else
-                    shAccel<L, T>(p, tile, r.dC, r.dS, bx, by, bz, a);
+                    shAccel<L, T>(p, tile, r, bx, by, bz, a);
             } else {
-                shAccel<L, T>(p, tile, r.dC, r.dS, bx, by, bz, a);
+                shAccel<L, T>(p, tile, r, bx, by, bz, a);
             }
-            ax += R[0] * a[0] + R[3] * a[1] + R[6] * a[2];
-            ay += R[1] * a[0] + R[4] * a[1] + R[7] * a[2];
-            az += R[2] * a[0] + R[5] * a[1] + R[8] * a[2];
+            double ai[3];
+            fromBody(r, a, ai);
+            ax += ai[0];
+            ay += ai[1];
+            az += ai[2];
         }
         if ((fl & kOblateness) && !(fl & kShape)) {
             // J2 model in the body frame (J2.h:17-33,63-78), inside the sphere of influence
-            const double* R = r.R;
             const double rr = sqrt(pos[0] * pos[0] + pos[1] * pos[1] + pos[2] * pos[2]);
             if (rr <= e.bodySoi[bi]) {
-                const double bx = R[0] * pos[0] + R[1] * pos[1] + R[2] * pos[2];
-                const double by = R[3] * pos[0] + R[4] * pos[1] + R[5] * pos[2];
-                const double bz = R[6] * pos[0] + R[7] * pos[1] + R[8] * pos[2];
+                double b[3];
+                toBody(r, pos, b);
+                const double bx = b[0], by = b[1], bz = b[2];
                 const double invr = 1.0 / sqrt(bx * bx + by * by + bz * bz);
                 const double invr2 = invr * invr;
                 const double invr5 = invr2 * invr2 * invr;
                 const double base = 1.0 - 5.0 * (bz * bz) * invr2;
                 const double c = -1.5 * e.bodyGmConst[bi] * e.bodyJ2[bi] * invr5 * e.bodyRadius[bi] * e.bodyRadius[bi];
-                const double a0 = c * bx * base, a1 = c * by * base, a2 = c * bz * (base + 2.0);
-                ax += R[0] * a0 + R[3] * a1 + R[6] * a2;
-                ay += R[1] * a0 + R[4] * a1 + R[7] * a2;
-                az += R[2] * a0 + R[5] * a1 + R[8] * a2;
+                const double aj[3] = {c * bx * base, c * by * base, c * bz * (base + 2.0)};
+                double ai[3];
+                fromBody(r, aj, ai);
+                ax += ai[0];
+                ay += ai[1];
+                az += ai[2];
             }
         }
         if (fl & kRadiation) {
-            const double* rb = r.body[bi];
+            const double rb[3] = {r.body(bi, 0), r.body(bi, 1), r.body(bi, 2)};
             const double dp[3] = {pos[0] - rb[0], pos[1] - rb[1], pos[2] - rb[2]};
             const double ird = rsqrt(dp[0] * dp[0] + dp[1] * dp[1] + dp[2] * dp[2]);
             double occ = 1.0;
             if (e.anyOcculter) {
                 for (int oj = 0; oj < e.nbodies; ++oj) {
                     if (!(e.bodyFlags[oj] & kOcculting) || oj == e.sunIndex) continue;
-                    const double* op = r.body[oj];
-                    const double rB[3] = {pos[0] - op[0], pos[1] - op[1], pos[2] - op[2]};
+                    const double rB[3] = {pos[0] - r.body(oj, 0), pos[1] - r.body(oj, 1), pos[2] - r.body(oj, 2)};
                     occ *= shadowFactor(dp, rB, e.bodyRadius[bi], e.bodyRadius[oj]);
                 }
             }
@@ -562,13 +626,13 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
             // piecewise exponential drag (PrivateAccelerations.h:137-206,
             // PiecewiseExponentialAtmosphere.h:40-90): band = bands above the
             // first whose base h0 <= h; no drag above the band's cut-off
-            const double pole[3] = {r.R[6], r.R[7], r.R[8]};  // body z axis in inertial axes
+            const double pole[3] = {r.R(6), r.R(7), r.R(8)};  // body z axis in inertial axes
             const double h = geodeticHeight(pos, pole, e.bodyRadius[bi], e.flattening);
             int band = 0;
             for (int sgi = 1; sgi < e.nExp; ++sgi) band += e.expSeg[sgi][1] <= h ? 1 : 0;
             if (h <= e.expSeg[band][3]) {
                 const double rho = e.expSeg[band][0] * exp(-(h - e.expSeg[band][1]) / e.expSeg[band][2]);
-                const double* w = r.w;
+                const double w[3] = {r.W(0), r.W(1), r.W(2)};
                 const double vr0 = vel[0] - (w[1] * pos[2] - w[2] * pos[1]);
                 const double vr1 = vel[1] - (w[2] * pos[0] - w[0] * pos[2]);
                 const double vr2 = vel[2] - (w[0] * pos[1] - w[1] * pos[0]);
@@ -579,12 +643,10 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
             }
         }
         if ((fl & kAtmosphere) && e.hasNrl) {
-            const double* R = r.R;
-            const double fx[3] = {R[0] * pos[0] + R[1] * pos[1] + R[2] * pos[2],
-                                  R[3] * pos[0] + R[4] * pos[1] + R[5] * pos[2],
-                                  R[6] * pos[0] + R[7] * pos[1] + R[8] * pos[2]};
-            const double rho = nrlDensity<L>(e, r, fx);
-            const double* w = r.w;
+            double fx[3];
+            toBody(r, pos, fx);
+            const double rho = nrlDensity<L>(e, r.nrlDeferred(), fx);
+            const double w[3] = {r.W(0), r.W(1), r.W(2)};
             const double vr0 = vel[0] - (w[1] * pos[2] - w[2] * pos[1]);
             const double vr1 = vel[1] - (w[2] * pos[0] - w[0] * pos[2]);
             const double vr2 = vel[2] - (w[0] * pos[1] - w[1] * pos[0]);
@@ -594,9 +656,9 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
             az += f * vr2;
         }
     }
-    ax += r.indirect[0];
-    ay += r.indirect[1];
-    az += r.indirect[2];
+    ax += r.indirect(0);
+    ay += r.indirect(1);
+    az += r.indirect(2);
     if (e.tidesAlone) {
         double t[3] = {0.0, 0.0, 0.0};
         tideAloneAccel(r, pos, t);
@@ -659,12 +721,13 @@ static __device__ __forceinline__ bool stageTile(void* dst, const void* src, int
 }
 
 // ---- the persistent step kernel ----------------------------------------------------------------
-// Stage record of a mixed batch: 4-point Lagrange interpolation in the
+// Stage record of a per-object-time batch: 4-point Lagrange weights in the
 // batch's record grid (rotation, angular velocity, body positions, tide
 // deltas; a 30 s spacing keeps the interpolation error of the rotation below
-// 1e-12 relative); the NRLMSISE-00 time inputs are evaluated exactly at the
-// stage epoch by the drag model when it needs them.
-static __device__ __noinline__ void epochRecordFromGrid(const StepParams& p, double et, EpochRecord& r) {
+// 1e-12 relative), read field by field by the force model; the NRLMSISE-00
+// time inputs are evaluated exactly at the stage epoch by the drag model
+// when it needs them.
+static __device__ __forceinline__ RecordInterp recordFromGrid(const StepParams& p, double et) {
     // stencil k0 - 1 .. k0 + 2 around the absolute grid index k0 = floor(et / H);
     // q depends on et alone, so the weights are the same in every batch
     const double u = et / p.gridH;
@@ -684,35 +747,7 @@ static __device__ __noinline__ void epochRecordFromGrid(const StepParams& p, dou
             }
         w[j] = num / den;
     }
-    const EpochRecord* g = p.grid + i0;
-    auto interp = [&](const double* f0, size_t off) {
-        const double* b = f0 + off;
-        constexpr size_t stride = sizeof(EpochRecord) / sizeof(double);
-        return w[0] * b[0] + w[1] * b[stride] + w[2] * b[2 * stride] + w[3] * b[3 * stride];
-    };
-    const double* f0 = (const double*)g;
-#pragma unroll
-    for (int i = 0; i < 9; ++i) r.R[i] = interp(f0, offsetof(EpochRecord, R) / 8 + i);
-#pragma unroll
-    for (int i = 0; i < 3; ++i) r.w[i] = interp(f0, offsetof(EpochRecord, w) / 8 + i);
-    for (int b = 0; b < p.env.nbodies; ++b)
-#pragma unroll
-        for (int i = 0; i < 3; ++i) r.body[b][i] = interp(f0, offsetof(EpochRecord, body) / 8 + 3 * b + i);
-#pragma unroll
-    for (int i = 0; i < 3; ++i) r.indirect[i] = interp(f0, offsetof(EpochRecord, indirect) / 8 + i);
-    r.tideValid = g[0].tideValid & g[1].tideValid & g[2].tideValid & g[3].tideValid;
-    if (p.env.solid || p.env.ocean) {
-        for (int k = 0; k < kTideTri; ++k) {
-            r.dC[k] = interp(f0, offsetof(EpochRecord, dC) / 8 + k);
-            r.dS[k] = interp(f0, offsetof(EpochRecord, dS) / 8 + k);
-        }
-    } else {
-        for (int k = 0; k < kTideTri; ++k) r.dC[k] = r.dS[k] = 0.0;
-    }
-    // NRLMSISE-00 time inputs: evaluated at the first drag evaluation below
-    // the density cut-off (objects above it never need them)
-    r.et = et;
-    r.nrlValid = p.env.hasNrl ? -1 : 0;
+    return RecordInterp{(const double*)(p.grid + i0), w[0], w[1], w[2], w[3], et};
 }
 
 template <int L, typename T, bool SHARED_GRID>
@@ -792,12 +827,11 @@ __global__ void __launch_bounds__(maxStepThreads(L), 1) propagateKernel(const __
                 }
                 double acc[3];
                 if (SHARED_GRID) {
-                    const EpochRecord& rec = p.records[kstep * 13 + s];
+                    const RecordRef rec{p.records + kstep * 13 + s};
                     accelerations<L, T>(p, tile, rec, st, st + 3, bc, ams, acc);
                 } else {
-                    EpochRecord rec;
                     const double ts = s == 0 ? t0 : t0 + dt * rkC(s - 1);
-                    epochRecordFromGrid(p, ts, rec);
+                    const RecordInterp rec = recordFromGrid(p, ts);
                     accelerations<L, T>(p, tile, rec, st, st + 3, bc, ams, acc);
                 }
 #pragma unroll
