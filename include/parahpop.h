@@ -154,6 +154,10 @@ int phop_propagate_device_noalloc(phop_context* ctx, int64_t n, double* d_states
  *              launches
  *   "tile_smem"  1 (default) = stage the coefficient tile in shared memory
  *              when it fits, 0 = read it through L1 (more threads per SM)
+ *   "tile_wait_test"  1 = test of the tile-staging time-out: the staging
+ *              barrier is armed but no copy issued, so every CTA's bounded
+ *              wait runs out and the CTA reads the tile from global memory
+ *              (counted in phop_stats.tile_fallbacks); 0 (default) = off
  *   "split_floor_km"  split precision only: objects closer than this height
  *              (km) above the geopotential's reference radius keep every
  *              harmonic in FP64; 0 = none */
@@ -215,6 +219,8 @@ typedef struct {
     int64_t launches;        /* kernels launched by the last call */
     int lanes, ctas, threads, split, shared_grid, tile_in_smem;
     double tune_ms;          /* lane-count autotuner probes of the last call (first batch of a size class) */
+    int64_t tile_fallbacks;  /* CTAs whose shared-memory staging of the coefficient tile timed out and that
+                                read the tile from global memory instead (results are the same) */
 } phop_stats;
 
 int phop_last_stats(const phop_context* ctx, phop_stats* out);

@@ -220,6 +220,8 @@ int phop_set_option(phop_context* ctx, const char* key, double value) {
             return 1;
         }
         ctx->opt.splitFloorKm = value;
+    } else if (k == "tile_wait_test") {
+        ctx->opt.tileWaitTest = value != 0.0 ? 1 : 0;
     } else if (k == "split_fp64_degree") {
         const int d = (int)value;
         if ((double)d != value || d < phop::kLowDeg || d > phop::kLowMax) {
@@ -577,6 +579,7 @@ int phop_last_stats(const phop_context* ctx, phop_stats* out) {
     out->split = ctx->stats.split;
     out->shared_grid = ctx->stats.sharedGrid;
     out->tile_in_smem = ctx->stats.tileInSmem;
+    out->tile_fallbacks = ctx->stats.tileFallbacks;
     return 0;
 }
 

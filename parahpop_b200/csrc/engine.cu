@@ -1633,10 +1633,12 @@ void Engine::runKernel(int64_t n, double* dState, const double* dBc, const doubl
     }
     if (opt.dTraj && (!shared || opt.trajEvery <= 0))
         throw std::runtime_error("Trajectory records need a batch with one epoch, duration and step.");
-    int* dCtl = (int*)scratch("ctl", 2 * sizeof(int));
+    int* dCtl = (int*)scratch("ctl", 4 * sizeof(int));
     p.workCounter = dCtl;
     p.errorFlag = dCtl + 1;
-    PHOP_CUDA(cudaMemsetAsync(dCtl, 0, 2 * sizeof(int), stream));
+    p.tileFallbacks = dCtl + 2;
+    p.tileWaitTest = opt.tileWaitTest;
+    PHOP_CUDA(cudaMemsetAsync(dCtl, 0, 4 * sizeof(int), stream));
     PHOP_CUDA(cudaEventRecord(eTuned, stream));  // end of the epoch records
     const int L = opt.lanes > 0 ? opt.lanes : tunedLanes(p, opt, shared, stream, &launches);
     if (opt.dTraj) {  // after the autotuner's probes, which must not write records
@@ -1651,10 +1653,12 @@ void Engine::runKernel(int64_t n, double* dState, const double* dBc, const doubl
     ++launches;
     PHOP_CUDA(cudaEventRecord(e2, stream));
     PHOP_CUDA(cudaEventSynchronize(e2));
-    int err = 0;
-    PHOP_CUDA(cudaMemcpy(&err, dCtl + 1, sizeof(int), cudaMemcpyDeviceToHost));
+    int ctl[3] = {0, 0, 0};
+    PHOP_CUDA(cudaMemcpy(ctl, dCtl, 3 * sizeof(int), cudaMemcpyDeviceToHost));
+    const int err = ctl[1];
     if (err) throw std::runtime_error("Propagation kernel reported error " + std::to_string(err) + ".");
     if (stats) {
+        stats->tileFallbacks += ctl[2];
         float a = 0, b = 0, c = 0;
         cudaEventElapsedTime(&a, e0, eTuned);
         cudaEventElapsedTime(&c, eTuned, e1);

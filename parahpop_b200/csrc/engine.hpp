@@ -110,6 +110,7 @@ struct RunStats {
     bool split = false;
     bool sharedGrid = false;
     bool tileInSmem = false;
+    int64_t tileFallbacks = 0;     // CTAs that read the tile from global memory after a staging time-out
 };
 
 struct RunOptions {
@@ -123,6 +124,7 @@ struct RunOptions {
     int splitFp64Degree = kSplitFp64Degree;  // split precision: degrees n <= this stay FP64 (8 .. kLowMax)
     int tileSmem = -1;    // coefficient tile in shared memory: -1 when it fits, 0 never (read through L1)
     int mixedOrder = 0;   // mixed batches inside a step-count bucket: 0 radius, 1 epoch, 2 drag band + epoch
+    int tileWaitTest = 0; // test of the tile-staging time-out: the barrier is armed, no copy issued
     // trajectory records of a uniform batch: device buffer of
     // (steps / trajEvery) x 6 x n doubles, null for none
     double* dTraj = nullptr;

@@ -120,9 +120,11 @@ struct StepParams {
     const void* tile64;     // split precision: the FP64 tile (global memory, same blocks)
     double splitRadius;     // split precision: radius (km) below which the tile part stays FP64; 0 = none
     int useSmemTile;
+    int tileWaitTest;       // test of the staging time-out: arm the barrier, issue no copy
     // scheduling and errors
     int* workCounter;
     int* errorFlag;
+    int* tileFallbacks;     // CTAs whose tile staging timed out (read the tile from global memory); nullable
 };
 
 // Threads per CTA the step kernel is compiled for: narrow lane splits run one

@@ -685,7 +685,14 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
 }
 
 // ---- TMA bulk staging of the coefficient tile --------------------------------------------------
-static __device__ __forceinline__ bool stageTile(void* dst, const void* src, int bytes, int* errorFlag) {
+// Stages the tile with bulk copies (32 KB chunks) on one mbarrier and waits
+// for them with a bounded poll.  Returns whether the whole CTA saw the copies
+// land; on a time-out the CTA reads the tile from global memory instead (the
+// copies, should any still be in flight, only write the tile's region of
+// shared memory, which the CTA then leaves alone).  `issue` = false arms the
+// barrier without any copy (a test of the time-out path: nothing is in
+// flight when the wait gives up).
+static __device__ __forceinline__ bool stageTile(void* dst, const void* src, int bytes, bool issue, long polls) {
     __shared__ __align__(8) uint64_t bar;
     const uint32_t barAddr = (uint32_t)__cvta_generic_to_shared(&bar);
     const uint32_t dstAddr = (uint32_t)__cvta_generic_to_shared(dst);
@@ -694,7 +701,7 @@ static __device__ __forceinline__ bool stageTile(void* dst, const void* src, int
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(barAddr), "r"(bytes) : "memory");
         const int chunk = 32768;
-        for (int off = 0; off < bytes; off += chunk) {
+        for (int off = 0; issue && off < bytes; off += chunk) {
             const int sz = (bytes - off) < chunk ? (bytes - off) : chunk;
             asm volatile(
                 "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
@@ -706,18 +713,14 @@ static __device__ __forceinline__ bool stageTile(void* dst, const void* src, int
     __syncthreads();
     // bounded wait on phase 0
     uint32_t done = 0;
-    for (long it = 0; it < (1L << 24) && !done; ++it) {
+    for (long it = 0; it < polls && !done; ++it) {
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
             : "=r"(done)
             : "r"(barAddr), "r"(0)
             : "memory");
     }
-    if (!done) {
-        if (threadIdx.x == 0) atomicExch(errorFlag, 2);
-        return false;
-    }
-    return true;
+    return __syncthreads_and((int)done) != 0;
 }
 
 // ---- the persistent step kernel ----------------------------------------------------------------
@@ -762,8 +765,11 @@ __global__ void __launch_bounds__(maxStepThreads(L), 1) propagateKernel(const __
         return;
     }
     if (p.useSmemTile) {
-        if (!stageTile(smem, p.tile, p.tileBytes, p.errorFlag)) return;
-        tile = (const Tile*)smem;
+        const bool test = p.tileWaitTest != 0;
+        if (stageTile(smem, p.tile, p.tileBytes, !test, test ? 4096L : (1L << 24)))
+            tile = (const Tile*)smem;
+        else if (threadIdx.x == 0 && p.tileFallbacks)
+            atomicAdd(p.tileFallbacks, 1);  // this CTA reads the tile from global memory
         kOffset = p.tileBytes;
     }
     StageStore<CPL> kst{(double*)(smem + kOffset), (int)blockDim.x};

@@ -288,3 +288,26 @@ def test_sliced_resident_batch_equals_one_call(tmp_path):
     np.testing.assert_array_equal(t[:n], t[n:2 * n])      # every object at its end epoch
     np.testing.assert_array_equal(t[2 * n:3 * n], 0.0)   # and finished
     p.close()
+
+
+def test_tile_staging_timeout_falls_back_to_global_memory(golden):
+    """The bounded wait on the tile's bulk copies: with the test switch the
+    barrier is armed but no copy issued, every CTA's wait runs out, the CTAs
+    read the tile from global memory (counted, not an error), and the
+    results are those of the staged tile."""
+    case = golden("full_600s")
+    ref = api.Propagator(case.config_path, lanes=2)
+    _, st_ref = ref.propagate_targets(case.targets)
+    assert ref.stats()["tile_in_smem"] == 1 and ref.stats()["tile_fallbacks"] == 0
+    t = api.Propagator(case.config_path, lanes=2)
+    t.set_option("tile_wait_test", 1)
+    _, st = t.propagate_targets(case.targets)
+    s = t.stats()
+    assert s["tile_in_smem"] == 1 and s["tile_fallbacks"] == s["ctas"] > 0
+    np.testing.assert_array_equal(st, st_ref)
+    t.set_option("tile_wait_test", 0)
+    _, st2 = t.propagate_targets(case.targets)
+    assert t.stats()["tile_fallbacks"] == 0
+    np.testing.assert_array_equal(st2, st_ref)
+    ref.close()
+    t.close()
