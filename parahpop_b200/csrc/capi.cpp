@@ -220,6 +220,8 @@ int phop_set_option(phop_context* ctx, const char* key, double value) {
             return 1;
         }
         ctx->opt.splitFloorKm = value;
+    } else if (k == "pair_sh") {
+        ctx->opt.pairSh = value != 0.0;
     } else if (k == "tile_wait_test") {
         ctx->opt.tileWaitTest = value != 0.0 ? 1 : 0;
     } else if (k == "split_fp64_degree") {

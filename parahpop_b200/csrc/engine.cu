@@ -1456,7 +1456,10 @@ int lowDegreeFor(const RunOptions& opt) {
 Engine::LaunchShape Engine::prepareStep(StepParams& p, int L, const RunOptions& opt, bool shared) {
     if (L != 1 && L != 2 && L != 4 && L != 8 && L != 16) throw std::runtime_error("lanes must be 1, 2, 4, 8 or 16");
     const int lowDeg = lowDegreeFor(opt);
-    const Tile& tile = tileFor(L, opt.split, lowDeg);
+    // lane-group pairs share the tile (built for 2L lanes); not with the
+    // split form's FP64 floor, whose low objects take the FP64 tile of L lanes
+    p.pairSh = (opt.pairSh && L <= 16 && !(opt.split && opt.splitFloorKm > 0.0)) ? 1 : 0;
+    const Tile& tile = tileFor(p.pairSh ? 2 * L : L, opt.split, lowDeg);
     p.tile = tile.dTile;
     p.tileBytes = tile.bytes;
     p.blocks = tile.dBlocks;

@@ -125,6 +125,7 @@ struct RunOptions {
     int tileSmem = -1;    // coefficient tile in shared memory: -1 when it fits, 0 never (read through L1)
     int mixedOrder = 0;   // mixed batches inside a step-count bucket: 0 radius, 1 epoch, 2 drag band + epoch
     int tileWaitTest = 0; // test of the tile-staging time-out: the barrier is armed, no copy issued
+    bool pairSh = true;   // split precision: geopotential of lane-group pairs in packed FP32
     // trajectory records of a uniform batch: device buffer of
     // (steps / trajEvery) x 6 x n doubles, null for none
     double* dTraj = nullptr;

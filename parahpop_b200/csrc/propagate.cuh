@@ -120,6 +120,7 @@ struct StepParams {
     const void* tile64;     // split precision: the FP64 tile (global memory, same blocks)
     double splitRadius;     // split precision: radius (km) below which the tile part stays FP64; 0 = none
     int useSmemTile;
+    int pairSh;             // split precision: the geopotential of lane-group pairs (tile built for 2L lanes)
     int tileWaitTest;       // test of the staging time-out: arm the barrier, issue no copy
     // scheduling and errors
     int* workCounter;

@@ -115,6 +115,11 @@ static __device__ __forceinline__ void finalUpdate(double (&y)[CPL], const Stage
 // local memory.
 struct RecordRef {
     const EpochRecord* r;
+    // the record of the object held by lane (lane ^ delta)
+    __device__ __forceinline__ RecordRef partner(unsigned mask, int delta) const {
+        const unsigned long long q = __shfl_xor_sync(mask, (unsigned long long)r, delta);
+        return RecordRef{(const EpochRecord*)q};
+    }
     __device__ __forceinline__ double R(int i) const { return r->R[i]; }
     __device__ __forceinline__ double W(int i) const { return r->w[i]; }
     __device__ __forceinline__ double body(int b, int i) const { return r->body[b][i]; }
@@ -135,6 +140,16 @@ struct RecordInterp {
     double w0, w1, w2, w3;
     double et;        // the stage epoch (TDB s past J2000)
     static constexpr int kStride = (int)(sizeof(EpochRecord) / sizeof(double));
+    __device__ __forceinline__ RecordInterp partner(unsigned mask, int delta) const {
+        RecordInterp o;
+        o.g = (const double*)__shfl_xor_sync(mask, (unsigned long long)g, delta);
+        o.w0 = __shfl_xor_sync(mask, w0, delta);
+        o.w1 = __shfl_xor_sync(mask, w1, delta);
+        o.w2 = __shfl_xor_sync(mask, w2, delta);
+        o.w3 = __shfl_xor_sync(mask, w3, delta);
+        o.et = __shfl_xor_sync(mask, et, delta);
+        return o;
+    }
     __device__ __forceinline__ double at(int off) const {
         const double* b = g + off;
         return w0 * b[0] + w1 * b[kStride] + w2 * b[2 * kStride] + w3 * b[3 * kStride];
@@ -354,6 +369,309 @@ static __device__ __forceinline__ void shAccel(const StepParams& p, const typena
     out[2] = sinPhi * ar + cosPhi * aphi;
 }
 
+// ---- spherical harmonics for a pair of objects, packed FP32 ---------------------------------
+// Two FP32 values in one 64-bit register pair, operated on by the packed
+// f32x2 instructions of sm_100.
+struct F2 {
+    unsigned long long v;
+};
+static __device__ __forceinline__ F2 f2(float lo, float hi) {
+    F2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(lo), "f"(hi));
+    return r;
+}
+static __device__ __forceinline__ F2 f2fma(F2 a, F2 b, F2 c) {
+    F2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+    return d;
+}
+static __device__ __forceinline__ F2 f2mul(F2 a, F2 b) {
+    F2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+    return d;
+}
+static __device__ __forceinline__ void f2split(F2 a, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a.v));
+}
+// The FP64 form of the same pair: two doubles, operated on one by one.
+struct D2 {
+    double lo, hi;
+};
+template <typename T> struct PairOf;
+template <> struct PairOf<float> {
+    using type = F2;
+    static __device__ __forceinline__ F2 make(float a, float b) { return f2(a, b); }
+    static __device__ __forceinline__ F2 fma(F2 a, F2 b, F2 c) { return f2fma(a, b, c); }
+    static __device__ __forceinline__ F2 mul(F2 a, F2 b) { return f2mul(a, b); }
+    static __device__ __forceinline__ void split(F2 a, float& lo, float& hi) { f2split(a, lo, hi); }
+};
+template <> struct PairOf<double> {
+    using type = D2;
+    static __device__ __forceinline__ D2 make(double a, double b) { return D2{a, b}; }
+    static __device__ __forceinline__ D2 fma(D2 a, D2 b, D2 c) { return D2{::fma(a.lo, b.lo, c.lo), ::fma(a.hi, b.hi, c.hi)}; }
+    static __device__ __forceinline__ D2 mul(D2 a, D2 b) { return D2{a.lo * b.lo, a.hi * b.hi}; }
+    static __device__ __forceinline__ void split(D2 a, double& lo, double& hi) {
+        lo = a.lo;
+        hi = a.hi;
+    }
+};
+
+// Per-object quantities of the column recursion.
+struct ShGeo {
+    double sinPhi, cosPhi, sinL, cosL, alpha, invCos;
+};
+static __device__ __forceinline__ ShGeo shGeo(double x, double y, double z, double R) {
+    ShGeo g;
+    const double rn = sqrt(x * x + y * y + z * z);
+    const double rho = sqrt(x * x + y * y);
+    g.sinPhi = z / rn;
+    g.cosPhi = rho / rn;
+    g.sinL = rho > 1e-14 ? y / rho : 0.0;
+    g.cosL = rho > 1e-14 ? x / rho : 1.0;
+    g.alpha = R / rn;
+    g.invCos = g.cosPhi == 0.0 ? 0.0 : 1.0 / g.cosPhi;
+    return g;
+}
+
+// Diagonal of one object: P_mm, dP_mm, cos / sin m lambda, alpha^m, and the
+// closed-form step by W orders (P_{m+W} = D_m cos^W P_m, the phasor rotated
+// by W lambda, alpha^W), as shAccel forms them.
+struct ShDiag {
+    double Pmm, dPmm, cML, sML, am;
+    double cosW1, cLam, sLam, aW;  // cos^(W-1) phi, cos / sin W lambda, alpha^W
+};
+
+// FP64 low part of column `mcol` of one object (n = mcol .. lowDeg, tide
+// deltas for n <= 6): the six column sums and the FP32 start values of the
+// tile rows (degrees lowDeg + 1 and lowDeg).
+template <typename T, class Rec>
+static __device__ __forceinline__ void shLowColumn(const StepParams& p, const Rec& rec, const ShGeo& g,
+                                                   const ShDiag& d, int mcol, double S[6], T& P, T& P1, T& dP,
+                                                   T& dP1) {
+    const LowTable* __restrict__ low = p.low;
+    const int N = p.env.shDegree, lowDeg = p.lowDeg;
+    const bool tides = p.env.solid || p.env.ocean;
+    double Pn = d.Pmm, Pn1 = 0.0, dPn = d.dPmm, dPn1 = 0.0, an = d.am, anPrev = d.am;
+    const int nEnd = N < lowDeg ? N : lowDeg;
+    for (int k = 0; k < 6; ++k) S[k] = 0.0;
+    for (int n = mcol; n <= nEnd; ++n) {
+        const int ti = n * (n + 1) / 2 + mcol;
+        double c = low->C[ti], s = low->S[ti];
+        if (n <= 6 && tides) {
+            c += rec.dC(ti);
+            s += rec.dS(ti);
+        }
+        if (mcol == 0) s = 0.0;
+        const double q = an * Pn, qd = an * dPn, np1 = (double)(n + 1);
+        S[0] = fma(np1 * c, q, S[0]);
+        S[1] = fma(np1 * s, q, S[1]);
+        S[2] = fma(c, qd, S[2]);
+        S[3] = fma(s, qd, S[3]);
+        S[4] = fma(c, q, S[4]);
+        S[5] = fma(s, q, S[5]);
+        if (n < N) {
+            const int tn = (n + 1) * (n + 2) / 2 + mcol;
+            const double fa = low->a[tn], fb = low->b[tn];
+            const double P2 = Pn1;
+            Pn1 = Pn;
+            Pn = fa * g.sinPhi * Pn1 - fb * P2;
+            const double dP2 = dPn1;
+            dPn1 = dPn;
+            dPn = fa * (g.sinPhi * dPn1 + g.cosPhi * Pn1) - fb * dP2;
+            anPrev = an;
+            an *= g.alpha;
+        }
+    }
+    P = (T)(an * Pn);
+    P1 = (T)(anPrev * Pn1);
+    dP = (T)(an * dPn);
+    dP1 = (T)(anPrev * dPn1);
+}
+
+static __device__ __forceinline__ void shDiagStart(const StepParams& p, const ShGeo& g, int first, int W,
+                                                   ShDiag& d) {
+    const double* __restrict__ diagC = p.diagC;
+    const int M = p.env.shOrder;
+    d.Pmm = 1.0;
+    d.dPmm = 0.0;
+    d.cML = 1.0;
+    d.sML = 0.0;
+    d.am = 1.0;
+    for (int m = 0; m < first && m < M; ++m) {
+        const double ns = g.cosL * d.sML + g.sinL * d.cML;
+        const double nc = g.cosL * d.cML - g.sinL * d.sML;
+        d.sML = ns;
+        d.cML = nc;
+        const double cm = diagC[m + 1];
+        const double nP = cm * g.cosPhi * d.Pmm;
+        const double ndP = cm * (g.cosPhi * d.dPmm - g.sinPhi * d.Pmm);
+        d.Pmm = nP;
+        d.dPmm = ndP;
+        d.am *= g.alpha;
+    }
+    d.cosW1 = 1.0;
+    d.cLam = 1.0;
+    d.sLam = 0.0;
+    d.aW = 1.0;
+    for (int t = 0; t < W - 1; ++t) d.cosW1 *= g.cosPhi;
+    for (int t = 0; t < W; ++t) {
+        const double ns = g.cosL * d.sLam + g.sinL * d.cLam;
+        const double nc = g.cosL * d.cLam - g.sinL * d.sLam;
+        d.sLam = ns;
+        d.cLam = nc;
+        d.aW *= g.alpha;
+    }
+}
+
+// advance the diagonal from order m to m + W (shAccel's block step)
+static __device__ __forceinline__ void shDiagStep(const double2* __restrict__ diagStep, const ShGeo& g, int m, int W,
+                                                  ShDiag& d) {
+    const double2 f = diagStep[m];
+    const double cosWp = d.cosW1 * g.cosPhi;
+    const double nP = f.x * cosWp * d.Pmm;
+    const double ndP = m == 0 ? -(double)W * g.sinPhi * d.cosW1 * f.x : f.y * cosWp * d.dPmm;
+    d.Pmm = nP;
+    d.dPmm = ndP;
+    const double ns = d.cLam * d.sML + d.sLam * d.cML;
+    const double nc = d.cLam * d.cML - d.sLam * d.sML;
+    d.sML = ns;
+    d.cML = nc;
+    d.am *= d.aW;
+}
+
+// Geopotential of the two objects of a pair of lane groups: the 2L lanes of
+// groups 2k and 2k+1 split the orders (lane pj of the pair takes
+// m = b 2L + pj, from the tile built for 2L lanes) and every lane runs its
+// columns for both objects (object of the first group, object of the
+// second), so each coefficient loaded from shared memory serves two objects
+// -- the column loop is bound by shared-memory bandwidth, not arithmetic.
+// Split precision runs the tile part as packed FP32 pairs (f32x2); FP64
+// runs it as two interleaved columns.  The low part and the diagonal stay
+// FP64 per object.  Returns the calling lane's own object's acceleration
+// (body frame, km/s^2), the same on every lane of its group.
+template <int L, typename T, class Rec>
+static __device__ __forceinline__ void shAccelPair(const StepParams& p, const typename TileOf<T>::type* __restrict__ tile,
+                                                   const Rec& rec, double x, double y, double z, double out[3]) {
+    using Pr = PairOf<T>;
+    using V = typename Pr::type;
+    using Tile = typename TileOf<T>::type;
+    constexpr int W = 2 * L;
+    const int lane = (int)(threadIdx.x & 31);
+    const int pj = lane % W;
+    const bool second = pj >= L;
+    const unsigned pairMask = W >= 32 ? 0xffffffffu : (((1u << W) - 1u) << (lane - pj));
+    const int N = p.env.shDegree, M = p.env.shOrder;
+    const int lowDeg = p.lowDeg;
+    const double ox = __shfl_xor_sync(pairMask, x, L), oy = __shfl_xor_sync(pairMask, y, L),
+                 oz = __shfl_xor_sync(pairMask, z, L);
+    const Rec orec = rec.partner(pairMask, L);
+    const ShGeo g0 = second ? shGeo(ox, oy, oz, p.env.shR) : shGeo(x, y, z, p.env.shR);
+    const ShGeo g1 = second ? shGeo(x, y, z, p.env.shR) : shGeo(ox, oy, oz, p.env.shR);
+    const Rec& r0 = second ? orec : rec;
+    const Rec& r1 = second ? rec : orec;
+    ShDiag d0, d1;
+    shDiagStart(p, g0, pj, W, d0);
+    shDiagStart(p, g1, pj, W, d1);
+    const V u = Pr::make((T)(g0.alpha * g0.sinPhi), (T)(g1.alpha * g1.sinPhi));
+    const V v = Pr::make((T)(g0.alpha * g0.cosPhi), (T)(g1.alpha * g1.cosPhi));
+    const V a2 = Pr::make((T)(g0.alpha * g0.alpha), (T)(g1.alpha * g1.alpha));
+    double acc0[3] = {0.0, 0.0, 0.0}, acc1[3] = {0.0, 0.0, 0.0};  // ar, aphi, alam
+    const double2* __restrict__ diagStep = p.diagStep;
+    const int nblocks = p.nblocks;
+    for (int b = 0; b < nblocks; ++b) {
+        const int mcol = b * W + pj;
+        const bool act = mcol <= M;
+        double S0[6] = {0, 0, 0, 0, 0, 0}, S1[6] = {0, 0, 0, 0, 0, 0};
+        T P0 = T(0), P10 = T(0), dP0 = T(0), dP10 = T(0), P1_ = T(0), P11 = T(0), dP1_ = T(0), dP11 = T(0);
+        if (act && mcol <= lowDeg) {
+            shLowColumn<T>(p, r0, g0, d0, mcol, S0, P0, P10, dP0, dP10);
+            shLowColumn<T>(p, r1, g1, d1, mcol, S1, P1_, P11, dP1_, dP11);
+        } else if (act) {
+            P0 = (T)(d0.am * d0.Pmm);
+            dP0 = (T)(d0.am * d0.dPmm);
+            P1_ = (T)(d1.am * d1.Pmm);
+            dP1_ = (T)(d1.am * d1.dPmm);
+        }
+        V P = Pr::make(P0, P1_), Pm1 = Pr::make(P10, P11), dP = Pr::make(dP0, dP1_), dPm1 = Pr::make(dP10, dP11);
+        V Scc = Pr::make(T(0), T(0)), Ssc = Scc, Spc = Scc, Sps = Scc, Sdc = Scc, Sds = Scc;
+        const int2 blk = p.blocks[b];
+        const Tile* tp = tile + blk.x + pj;
+        for (int i = 0; i < blk.y; ++i, tp += W) {
+            const Tile e = *tp;
+            const V c = Pr::make(T(e.c), T(e.c)), s = Pr::make(T(e.s), T(e.s));
+            const V cp = Pr::make(T(e.cp), T(e.cp)), sp = Pr::make(T(e.sp), T(e.sp));
+            const V fa = Pr::make(T(e.a), T(e.a)), nb = Pr::make(-T(e.b), -T(e.b));
+            Scc = Pr::fma(cp, P, Scc);
+            Ssc = Pr::fma(sp, P, Ssc);
+            Spc = Pr::fma(c, P, Spc);
+            Sps = Pr::fma(s, P, Sps);
+            Sdc = Pr::fma(c, dP, Sdc);
+            Sds = Pr::fma(s, dP, Sds);
+            const V Pn = Pr::fma(fa, Pr::mul(u, P), Pr::mul(nb, Pr::mul(a2, Pm1)));
+            const V dPn = Pr::fma(fa, Pr::fma(u, dP, Pr::mul(v, P)), Pr::mul(nb, Pr::mul(a2, dPm1)));
+            Pm1 = P;
+            P = Pn;
+            dPm1 = dP;
+            dP = dPn;
+        }
+        if (act) {
+            T t0[6], t1[6];
+            Pr::split(Scc, t0[0], t1[0]);
+            Pr::split(Ssc, t0[1], t1[1]);
+            Pr::split(Sdc, t0[2], t1[2]);
+            Pr::split(Sds, t0[3], t1[3]);
+            Pr::split(Spc, t0[4], t1[4]);
+            Pr::split(Sps, t0[5], t1[5]);
+            const double mInv0 = (double)mcol * g0.invCos, mInv1 = (double)mcol * g1.invCos;
+            acc0[0] -= d0.cML * (S0[0] + (double)t0[0]) + d0.sML * (S0[1] + (double)t0[1]);
+            acc0[1] += d0.cML * (S0[2] + (double)t0[2]) + d0.sML * (S0[3] + (double)t0[3]);
+            acc0[2] -= mInv0 * (d0.sML * (S0[4] + (double)t0[4]) - d0.cML * (S0[5] + (double)t0[5]));
+            acc1[0] -= d1.cML * (S1[0] + (double)t1[0]) + d1.sML * (S1[1] + (double)t1[1]);
+            acc1[1] += d1.cML * (S1[2] + (double)t1[2]) + d1.sML * (S1[3] + (double)t1[3]);
+            acc1[2] -= mInv1 * (d1.sML * (S1[4] + (double)t1[4]) - d1.cML * (S1[5] + (double)t1[5]));
+        }
+        const int m = b * W + pj;
+        if (m + W <= M) {
+            shDiagStep(diagStep, g0, m, W, d0);
+            shDiagStep(diagStep, g1, m, W, d1);
+        }
+    }
+    // fold the pair's lanes: both objects' partial sums over all 2L lanes
+#pragma unroll
+    for (int off = W / 2; off > 0; off >>= 1)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            acc0[k] += __shfl_xor_sync(pairMask, acc0[k], off);
+            acc1[k] += __shfl_xor_sync(pairMask, acc1[k], off);
+        }
+    const ShGeo& g = second ? g1 : g0;
+    double ar = second ? acc1[0] : acc0[0], aphi = second ? acc1[1] : acc0[1], alam = second ? acc1[2] : acc0[2];
+    if (g.cosPhi == 0.0 && M >= 1) {
+        // exact pole: the m = 1 longitudinal term's analytical limit (as shAccel)
+        const bool tides = p.env.solid || p.env.ocean;
+        double an = g.alpha;
+        for (int n = 1; n <= N; ++n) {
+            const int ti = n * (n + 1) / 2 + 1;
+            double s = p.env.shS[ti];
+            if (n <= 6 && tides) s += rec.dS(ti);
+            const double sign = g.sinPhi > 0.0 ? 1.0 : ((n & 1) ? 1.0 : -1.0);
+            double lim = 0.5 * (double)n * (n + 1.0);
+            if (p.env.shNormalized) lim *= sqrt(2.0 * (2.0 * n + 1.0) / ((double)n * (n + 1.0)));
+            alam -= an * (sign * lim) * (-s);
+            an *= g.alpha;
+        }
+    }
+    (void)lowDeg;
+    const double rn = p.env.shR / g.alpha;
+    const double gm = p.env.shGM / (rn * rn);
+    ar *= gm;
+    aphi *= gm;
+    alam *= gm;
+    out[0] = g.cosPhi * g.cosL * ar - g.sinPhi * g.cosL * aphi - g.sinL * alam;
+    out[1] = g.cosPhi * g.sinL * ar - g.sinPhi * g.sinL * aphi + g.cosL * alam;
+    out[2] = g.sinPhi * ar + g.cosPhi * aphi;
+}
+
 // ---- the remaining forces ------------------------------------------------------------------
 static __device__ __forceinline__ double shadowFactor(const double rS[3], const double rB[3], double RSun, double RBody) {
     const double s2 = rS[0] * rS[0] + rS[1] * rS[1] + rS[2] * rS[2];
@@ -397,9 +715,13 @@ template <int L>
 static __device__ __noinline__ double nrlDensityCall(const DevEnv& e, NrlTime t, const double f[3]) {
     return nrlDensityBody<L>(e, t, f);
 }
-template <int L>
+#ifndef PHOP_NRL_INLINE_LANES_F32
+#define PHOP_NRL_INLINE_LANES_F32 4
+#endif
+template <int L, typename T>
 static __device__ __forceinline__ double nrlDensity(const DevEnv& e, NrlTime t, const double f[3]) {
-    if constexpr (L <= 4) return nrlDensityBody<L>(e, t, f);
+    constexpr int inlineLanes = std::is_same<T, double>::value ? 4 : PHOP_NRL_INLINE_LANES_F32;
+    if constexpr (L <= inlineLanes) return nrlDensityBody<L>(e, t, f);
     else return nrlDensityCall<L>(e, t, f);
 }
 
@@ -572,12 +894,17 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
             if constexpr (!std::is_same<T, double>::value) {
                 // split precision: objects below the split radius keep the
                 // tile part in FP64 (from the FP64 tile in global memory)
-                if (p.splitRadius > 0.0 && bx * bx + by * by + bz * bz < p.splitRadius * p.splitRadius)
+                if (p.pairSh)
+                    shAccelPair<L, T>(p, tile, r, bx, by, bz, a);
+                else if (p.splitRadius > 0.0 && bx * bx + by * by + bz * bz < p.splitRadius * p.splitRadius)
                     shAccel<L, double>(p, (const TileD*)p.tile64, r, bx, by, bz, a);
                 else
                     shAccel<L, T>(p, tile, r, bx, by, bz, a);
             } else {
-                shAccel<L, T>(p, tile, r, bx, by, bz, a);
+                if (p.pairSh)
+                    shAccelPair<L, T>(p, tile, r, bx, by, bz, a);
+                else
+                    shAccel<L, T>(p, tile, r, bx, by, bz, a);
             }
             double ai[3];
             fromBody(r, a, ai);
@@ -645,7 +972,7 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
         if ((fl & kAtmosphere) && e.hasNrl) {
             double fx[3];
             toBody(r, pos, fx);
-            const double rho = nrlDensity<L>(e, r.nrlDeferred(), fx);
+            const double rho = nrlDensity<L, T>(e, r.nrlDeferred(), fx);
             const double w[3] = {r.W(0), r.W(1), r.W(2)};
             const double vr0 = vel[0] - (w[1] * pos[2] - w[2] * pos[1]);
             const double vr1 = vel[1] - (w[2] * pos[0] - w[0] * pos[2]);
