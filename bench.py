@@ -54,10 +54,12 @@ def sh_flops_per_object_step(degree: int) -> float:
 
 
 # DRAM bytes (read + write) per object-step of the step kernel, from ncu
-# captures of the workloads' kernels (profiles/): the state is read once and
-# written once per launch, the rest is epoch records, the coefficient tile
-# and local-memory traffic.
-NCU_BYTES_PER_OBJECT_STEP = {"c1": (1_570_560 + 1_846_016) / (1e4 * 5), "c3": None, "c2": None}
+# captures (profiles/): the state is read once and written once per launch
+# (~100 B per object); the rest is local memory (register spills) evicted
+# from L2.  c3: the split form's kernel at two lanes, 10^5 objects x 24 steps
+# (7.60 + 12.10 GB over 2,391,620 object-steps); the other workloads have no
+# capture of the current kernel (null).
+NCU_BYTES_PER_OBJECT_STEP = {"c3": (7.604360e9 + 12.100122e9) / 2_391_620, "c1": None, "c2": None}
 
 
 def dist_env():
@@ -599,6 +601,9 @@ def main():
             "roofline": {"bound": "fp64+fp32" if head == "split" else "fp64", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak if peak > 0 else None,
                          "traffic": per_os * steps_per_launch if per_os else None,
+                         "traffic_note": "DRAM read+write bytes per launch: ncu capture of the split kernel at two "
+                                         "lanes (8.2 KB per object-step, almost all local-memory spill traffic) "
+                                         "times the object-steps of one timed launch" if per_os else None,
                          "peak_source": peak_note,
                          "numerator": f"29 FLOP x (N+1)(N+2)/2 SH terms x 13 stages per object-step, N = {degree}"},
             "cpu_baseline": cpu,
