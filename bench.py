@@ -392,8 +392,10 @@ def c3_run(prop, pop, slices: int, warmup: int, steps_per_slice: int, flush, e2e
         obj_steps += st["object_steps"]
         launches += st["launches"]
         lanes = st["lanes"]
+        pairs = st["pair_sh"]
     return {"ms": timer.ms, "kernel_ms": kernel_ms, "records_ms": records_ms, "object_steps": obj_steps,
-            "launches": launches, "lanes": lanes, "state": d_state.cpu().numpy().reshape(6, n).T.copy(),
+            "launches": launches, "lanes": lanes, "pairs": pairs,
+            "state": d_state.cpu().numpy().reshape(6, n).T.copy(),
             "h2d_bytes": n * (6 + 4 + 2) * 8, "d2h_bytes": n * (6 + 4) * 8}
 
 
@@ -499,6 +501,7 @@ def main():
                 for key in ("kernel_ms", "records_ms", "object_steps", "launches"):
                     r[key] += st[key]
                 r["lanes"] = st["lanes"]
+                r["pairs"] = st["pair_sh"]
             sync_barrier()
             r["ms"] = timer.ms
             r["state"] = d_state.cpu().numpy().reshape(6, -1).T.copy()
@@ -527,6 +530,7 @@ def main():
         forms[name] = {"value": r["object_steps"] * ws / (t_ms * 1e-3), "ms_per_step": t_ms / K,
                        "e2e_value": r["e2e"]["object_steps"] * ws / (e_ms * 1e-3),
                        "kernel_ms": r["kernel_ms"], "records_ms": r["records_ms"], "lanes": r["lanes"],
+                       "objects_per_lane_in_geopotential": 2 if r["pairs"] else 1,
                        "object_steps_per_gpu": r["object_steps"], "launches": r["launches"]}
     prefix_diff = np.linalg.norm(runs["split"]["state"][:, :3] - runs["fp64"]["state"][:, :3], axis=1)
 

@@ -154,6 +154,14 @@ int phop_propagate_device_noalloc(phop_context* ctx, int64_t n, double* d_states
  *              launches
  *   "tile_smem"  1 (default) = stage the coefficient tile in shared memory
  *              when it fits, 0 = read it through L1 (more threads per SM)
+ *   "pair_sh"  geopotential of lane-group pairs, two objects per lane
+ *              (each coefficient loaded from shared memory serves both;
+ *              packed FP32 in split precision; at one, two or four lanes
+ *              only): -1 (default) = chosen by the autotuner with the lane
+ *              count (pinned lanes: pairs up to four lanes), 0 = off, 1 = on
+ *   "split_drag_fp32_km"  split precision: NRLMSISE-00 in FP32 for objects
+ *              above this height (km); 0 (default) = never (measured slower
+ *              and above 1 cm at 500 km)
  *   "tile_wait_test"  1 = test of the tile-staging time-out: the staging
  *              barrier is armed but no copy issued, so every CTA's bounded
  *              wait runs out and the CTA reads the tile from global memory
@@ -221,6 +229,7 @@ typedef struct {
     double tune_ms;          /* lane-count autotuner probes of the last call (first batch of a size class) */
     int64_t tile_fallbacks;  /* CTAs whose shared-memory staging of the coefficient tile timed out and that
                                 read the tile from global memory instead (results are the same) */
+    int pair_sh;             /* the geopotential ran for lane-group pairs (two objects per lane) */
 } phop_stats;
 
 int phop_last_stats(const phop_context* ctx, phop_stats* out);

@@ -1458,7 +1458,8 @@ Engine::LaunchShape Engine::prepareStep(StepParams& p, int L, const RunOptions& 
     const int lowDeg = lowDegreeFor(opt);
     // lane-group pairs share the tile (built for 2L lanes); not with the
     // split form's FP64 floor, whose low objects take the FP64 tile of L lanes
-    p.pairSh = (opt.pairSh && L <= 16 && !(opt.split && opt.splitFloorKm > 0.0)) ? 1 : 0;
+    const bool pair = opt.pairSh < 0 ? L <= 4 : opt.pairSh != 0;
+    p.pairSh = (pair && L <= 4 && !(opt.split && opt.splitFloorKm > 0.0)) ? 1 : 0;
     const Tile& tile = tileFor(p.pairSh ? 2 * L : L, opt.split, lowDeg);
     p.tile = tile.dTile;
     p.tileBytes = tile.bytes;
@@ -1466,6 +1467,7 @@ Engine::LaunchShape Engine::prepareStep(StepParams& p, int L, const RunOptions& 
     p.nblocks = tile.nblocks;
     p.diagStep = tile.dDiagStep;
     p.lowDeg = lowDeg;
+    p.dragF32AboveKm = opt.split ? opt.splitDragF32Km : 0.0;
     p.tile64 = nullptr;
     p.splitRadius = 0.0;
     if (opt.split && opt.splitFloorKm > 0.0) {
@@ -1487,9 +1489,11 @@ Engine::LaunchShape Engine::prepareStep(StepParams& p, int L, const RunOptions& 
     int perSm = opt.ctasPerSm;
     if (perSm <= 0) {
         const int smem = propagateSmemBytes(p, L, threads);
-        const int64_t key = (((int64_t)smem * 1024 + threads) * 32 + L) * 4 + (opt.split ? 2 : 0) + (shared ? 1 : 0);
+        const int64_t key = ((((int64_t)smem * 1024 + threads) * 32 + L) * 4 + (opt.split ? 2 : 0) + (shared ? 1 : 0)) * 2
+                            + p.pairSh;
         auto it = occupancy_.find(key);
-        if (it == occupancy_.end()) it = occupancy_.emplace(key, propagateMaxCtasPerSm(L, opt.split, shared, threads, smem)).first;
+        if (it == occupancy_.end())
+            it = occupancy_.emplace(key, propagateMaxCtasPerSm(L, opt.split, shared, p.pairSh, threads, smem)).first;
         perSm = it->second;
     }
     if (perSm <= 0) perSm = 1;
@@ -1511,27 +1515,33 @@ Engine::LaunchShape Engine::prepareStep(StepParams& p, int L, const RunOptions& 
     return shape;
 }
 
-// Project autotuner for the lane split.  The first batch of each class
-// (log2 of the batch size, time-grid mode, precision) times a short probe
-// (up to eight steps, best of two after an untimed warm-up launch) of every lane count on
-// scratch copies of the inputs and keeps the fastest; later batches of the
-// class reuse the choice.  PARAHPOP_B200_TUNE_LOG=1 prints the probe times.
-int Engine::tunedLanes(const StepParams& base, const RunOptions& opt, bool shared, cudaStream_t stream,
+// Project autotuner for the launch shape: lanes per object (1, 2, 4, 8, 16)
+// and objects per lane in the geopotential (one, or two for lane-group pairs
+// at up to four lanes).  The first batch of each class (log2 of the batch
+// size, time-grid mode, precision, pairing option) times a short probe (up
+// to twelve steps, best of three after an untimed warm-up launch) of every
+// shape on scratch copies of the inputs and keeps the fastest; later batches
+// of the class reuse the choice.  PARAHPOP_B200_TUNE_LOG=1 prints the probe
+// times.
+int Engine::tunedShape(const StepParams& base, const RunOptions& opt, bool shared, cudaStream_t stream,
                        int64_t* launches) {
     int bucket = 0;
     while (bucket < 40 && (int64_t(1) << bucket) < base.n) ++bucket;
-    const int key = bucket * 4 + (shared ? 2 : 0) + (opt.split ? 1 : 0);
+    const int key = (bucket * 4 + (shared ? 2 : 0) + (opt.split ? 1 : 0)) * 4 + (opt.pairSh + 1);
     auto it = tuned_.find(key);
     if (it != tuned_.end()) return it->second;
-    if (base.stride != 0 && base.stride != base.n) return autoLanes(base.n);  // pools pin their lane count
+    if (base.stride != 0 && base.stride != base.n) {  // pools pin their lane count
+        const int L = autoLanes(base.n);
+        return L * 2 + (opt.pairSh < 0 ? (L <= 4 ? 1 : 0) : opt.pairSh);
+    }
     const int64_t n = base.n;
     StepParams p = base;
     double* st = (double*)scratch("probeState", (size_t)6 * n * 8);
     p.state = st;
     if (shared) {
-        p.nsteps = std::min(p.nsteps, 8);
+        p.nsteps = std::min(p.nsteps, 12);
     } else {
-        p.maxSteps = 8;
+        p.maxSteps = 12;
         p.cur = (double*)scratch("probeCur", (size_t)n * 8);
         p.dt = (double*)scratch("probeDt", (size_t)n * 8);
         p.unfinished = (int*)scratch("probeUnf", (size_t)n * 4);
@@ -1539,25 +1549,31 @@ int Engine::tunedLanes(const StepParams& base, const RunOptions& opt, bool share
     cudaEvent_t e0, e1;
     PHOP_CUDA(cudaEventCreate(&e0));
     PHOP_CUDA(cudaEventCreate(&e1));
-    int best = autoLanes(n);
+    int best = autoLanes(n) * 2 + (opt.pairSh > 0 ? 1 : 0);
     float bestMs = 1e30f;
     const char* logEnv = std::getenv("PARAHPOP_B200_TUNE_LOG");
     const bool tuneLog = logEnv && std::atoi(logEnv) != 0;
-    for (int L : {1, 2, 4, 8, 16}) {
+    for (int code = 2; code < 34; ++code) {
+        const int L = code >> 1, pair = code & 1;
+        if (L != 1 && L != 2 && L != 4 && L != 8 && L != 16) continue;
+        if (opt.pairSh >= 0 && pair != opt.pairSh) continue;
+        if (opt.pairSh < 0 && pair && L >= 8) continue;  // pairs at 8 and 16 lanes measured slower on every workload
         if (L >= 8 && n >= (int64_t)sms_ * 512 * 4) continue;  // enough objects to fill the GPU with narrow groups
+        RunOptions o = opt;
+        o.pairSh = pair;
         // an untimed launch first (module loading, attribute set-up), then the
-        // fastest of two timed probes
+        // fastest of three timed probes
         float ms = 1e30f;
-        for (int rep = 0; rep < 3; ++rep) {
+        for (int rep = 0; rep < 4; ++rep) {
             PHOP_CUDA(cudaMemcpyAsync(st, base.state, (size_t)6 * n * 8, cudaMemcpyDeviceToDevice, stream));
             if (!shared) {
                 PHOP_CUDA(cudaMemcpyAsync(p.cur, base.cur, (size_t)n * 8, cudaMemcpyDeviceToDevice, stream));
                 PHOP_CUDA(cudaMemcpyAsync(p.dt, base.dt, (size_t)n * 8, cudaMemcpyDeviceToDevice, stream));
             }
             StepParams q = p;
-            const LaunchShape shape = prepareStep(q, L, opt, shared);
+            const LaunchShape shape = prepareStep(q, L, o, shared);
             PHOP_CUDA(cudaEventRecord(e0, stream));
-            enqueueStep(q, shape, opt, shared, stream);
+            enqueueStep(q, shape, o, shared, stream);
             PHOP_CUDA(cudaEventRecord(e1, stream));
             PHOP_CUDA(cudaEventSynchronize(e1));
             if (launches) ++*launches;
@@ -1568,11 +1584,12 @@ int Engine::tunedLanes(const StepParams& base, const RunOptions& opt, bool share
         int err = 0;
         PHOP_CUDA(cudaMemcpy(&err, p.errorFlag, sizeof(int), cudaMemcpyDeviceToHost));
         if (err) throw std::runtime_error("Propagation kernel reported error " + std::to_string(err) + ".");
-        if (tuneLog) std::fprintf(stderr, "parahpop-b200 tune: n=%lld shared=%d split=%d lanes=%d probe_ms=%.3f\n",
-                                  (long long)n, shared ? 1 : 0, opt.split ? 1 : 0, L, ms);
+        if (tuneLog)
+            std::fprintf(stderr, "parahpop-b200 tune: n=%lld shared=%d split=%d lanes=%d pairs=%d probe_ms=%.3f\n",
+                         (long long)n, shared ? 1 : 0, opt.split ? 1 : 0, L, pair, ms);
         if (ms < bestMs) {
             bestMs = ms;
-            best = L;
+            best = code;
         }
     }
     cudaEventDestroy(e0);
@@ -1643,16 +1660,22 @@ void Engine::runKernel(int64_t n, double* dState, const double* dBc, const doubl
     p.tileWaitTest = opt.tileWaitTest;
     PHOP_CUDA(cudaMemsetAsync(dCtl, 0, 4 * sizeof(int), stream));
     PHOP_CUDA(cudaEventRecord(eTuned, stream));  // end of the epoch records
-    const int L = opt.lanes > 0 ? opt.lanes : tunedLanes(p, opt, shared, stream, &launches);
+    RunOptions o = opt;
+    int L = opt.lanes;
+    if (L <= 0) {
+        const int code = tunedShape(p, opt, shared, stream, &launches);
+        L = code >> 1;
+        o.pairSh = code & 1;
+    }
     if (opt.dTraj) {  // after the autotuner's probes, which must not write records
         p.traj = opt.dTraj;
         p.trajEvery = opt.trajEvery;
         p.trajRecords = opt.trajRecords;
     }
-    const LaunchShape shape = prepareStep(p, L, opt, shared);
+    const LaunchShape shape = prepareStep(p, L, o, shared);
     PHOP_CUDA(cudaEventRecord(e1, stream));
-    if (opt.graph) launchStepGraph(p, shape, opt, shared, stream);
-    else enqueueStep(p, shape, opt, shared, stream);
+    if (opt.graph) launchStepGraph(p, shape, o, shared, stream);
+    else enqueueStep(p, shape, o, shared, stream);
     ++launches;
     PHOP_CUDA(cudaEventRecord(e2, stream));
     PHOP_CUDA(cudaEventSynchronize(e2));
@@ -1676,6 +1699,7 @@ void Engine::runKernel(int64_t n, double* dState, const double* dBc, const doubl
         stats->split = opt.split;
         stats->sharedGrid = shared;
         stats->tileInSmem = shape.smemTile;
+        stats->pairSh = p.pairSh != 0;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

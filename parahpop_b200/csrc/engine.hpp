@@ -110,6 +110,7 @@ struct RunStats {
     bool split = false;
     bool sharedGrid = false;
     bool tileInSmem = false;
+    bool pairSh = false;           // the geopotential of lane-group pairs was used
     int64_t tileFallbacks = 0;     // CTAs that read the tile from global memory after a staging time-out
 };
 
@@ -125,7 +126,9 @@ struct RunOptions {
     int tileSmem = -1;    // coefficient tile in shared memory: -1 when it fits, 0 never (read through L1)
     int mixedOrder = 0;   // mixed batches inside a step-count bucket: 0 radius, 1 epoch, 2 drag band + epoch
     int tileWaitTest = 0; // test of the tile-staging time-out: the barrier is armed, no copy issued
-    bool pairSh = true;   // split precision: geopotential of lane-group pairs in packed FP32
+    int pairSh = -1;      // geopotential of lane-group pairs (packed FP32 in split precision): 1 on, 0 off,
+                          // -1 autotuned with the lane count (pinned lanes: on up to 4 lanes)
+    double splitDragF32Km = 0.0;  // split precision: NRLMSISE-00 in FP32 above this height; 0 = never
     // trajectory records of a uniform batch: device buffer of
     // (steps / trajEvery) x 6 x n doubles, null for none
     double* dTraj = nullptr;
@@ -239,7 +242,8 @@ private:
     EpochRecord* gridCache_ = nullptr;
     int64_t gridKLo_ = 0, gridKHi_ = -1;
     cudaStream_t captureStream_ = nullptr;
-    int tunedLanes(const StepParams& base, const RunOptions& opt, bool shared, cudaStream_t stream, int64_t* launches);
+    // autotuned launch shape of a batch class: lanes * 2 + (pairs ? 1 : 0)
+    int tunedShape(const StepParams& base, const RunOptions& opt, bool shared, cudaStream_t stream, int64_t* launches);
     void runKernel(int64_t n, double* dState, const double* dBc, const double* dAms, const TimeGrid& g,
                    const int64_t* dOrder, int64_t maxSteps, const RunOptions& opt, RunStats* stats,
                    cudaStream_t stream, int64_t launchesBefore);

@@ -818,11 +818,13 @@ struct Fast {
 #pragma unroll
         for (int r = 0; r < R; ++r) acc[r] = acc2[r] = T(0.0);
 #if PHOP_NRL_ROLLED_GLOBE
+        if constexpr (L <= 4) {
         // the monomials formed once into a small local array, then a rolled
         // dot-product loop: a short instruction stream (the step kernel
         // alternates this model with the geopotential loop, and both compete
         // for the instruction cache; measured 1-2 % faster on the uneven
-        // population than the fully unrolled form below)
+        // population at two lanes than the fully unrolled form, which the
+        // eight- and sixteen-lane kernels keep: they call the model out of line)
         T mono[kGlobeBasis + 1];
 #pragma unroll
         for (int i = 0; i <= kGlobeBasis; ++i) mono[i] = globeMonomial(i, x, x2, U1, U2);
@@ -835,6 +837,18 @@ struct Fast {
                 acc[r] = fma(T(c.x), b0, acc[r]);
                 acc2[r] = fma(T(c.y), b1, acc2[r]);
             }
+        }
+        } else {
+#pragma unroll
+        for (int i = 0; i < kGlobeBasis; i += 2) {
+            const T b0 = globeMonomial(i, x, x2, U1, U2), b1 = globeMonomial(i + 1, x, x2, U1, U2);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const double2 c = __ldg(rows + (i / 2) * kGlobeRows + r * L + j);
+                acc[r] = fma(T(c.x), b0, acc[r]);
+                acc2[r] = fma(T(c.y), b1, acc2[r]);
+            }
+        }
         }
 #else
 #pragma unroll

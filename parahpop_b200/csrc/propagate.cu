@@ -9,7 +9,7 @@ namespace phop {
 #define PHOP_DECL(sfx)                                                                                     \
     cudaError_t launchPropagate_##sfx(const StepParams& p, size_t paramsBytes, int lanes, int ctas, int threads, \
                                       int smem, cudaStream_t stream);                                       \
-    int occupancy_##sfx(int lanes, int threads, int smem);
+    int occupancy_##sfx(int lanes, int pair, int threads, int smem);
 PHOP_DECL(f64_grid)
 PHOP_DECL(f64_mixed)
 PHOP_DECL(f32_grid)
@@ -71,9 +71,10 @@ int propagateSmemBytes(const StepParams& p, int lanes, int threads) {
     return (p.useSmemTile ? p.tileBytes : 0) + 13 * cpl * threads * (int)sizeof(double);
 }
 
-int propagateMaxCtasPerSm(int lanes, bool split, bool shared, int threads, int smem) {
-    if (split) return shared ? occupancy_f32_grid(lanes, threads, smem) : occupancy_f32_mixed(lanes, threads, smem);
-    return shared ? occupancy_f64_grid(lanes, threads, smem) : occupancy_f64_mixed(lanes, threads, smem);
+int propagateMaxCtasPerSm(int lanes, bool split, bool shared, int pair, int threads, int smem) {
+    if (split)
+        return shared ? occupancy_f32_grid(lanes, pair, threads, smem) : occupancy_f32_mixed(lanes, pair, threads, smem);
+    return shared ? occupancy_f64_grid(lanes, pair, threads, smem) : occupancy_f64_mixed(lanes, pair, threads, smem);
 }
 
 cudaError_t launchPropagate(const StepParams& p, int lanes, bool split, bool shared, int ctas, int threads,

@@ -120,7 +120,8 @@ struct StepParams {
     const void* tile64;     // split precision: the FP64 tile (global memory, same blocks)
     double splitRadius;     // split precision: radius (km) below which the tile part stays FP64; 0 = none
     int useSmemTile;
-    int pairSh;             // split precision: the geopotential of lane-group pairs (tile built for 2L lanes)
+    int pairSh;             // the geopotential of lane-group pairs (tile built for 2L lanes)
+    double dragF32AboveKm;  // split precision: NRLMSISE-00 in FP32 above this height (km); 0 = never
     int tileWaitTest;       // test of the staging time-out: arm the barrier, issue no copy
     // scheduling and errors
     int* workCounter;
@@ -139,6 +140,6 @@ void launchEpochRecords(const DevEnv& env, const double* epochs, int count, Epoc
 cudaError_t launchPropagate(const StepParams& p, int lanes, bool split, bool shared, int ctas, int threads,
                             cudaStream_t stream);
 int propagateSmemBytes(const StepParams& p, int lanes, int threads);
-int propagateMaxCtasPerSm(int lanes, bool split, bool shared, int threads, int smem);
+int propagateMaxCtasPerSm(int lanes, bool split, bool shared, int pair, int threads, int smem);
 
 }  // namespace phop

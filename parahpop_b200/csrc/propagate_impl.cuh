@@ -705,28 +705,33 @@ static __device__ __forceinline__ double shadowFactor(const double rS[3], const 
 
 // NRLMSISE-00 density (kg/km^3) at ITRF position f; the L lanes of a group
 // share the globe7 tables of the model and all return the same value.
-template <int L>
-static __device__ __forceinline__ double nrlDensityBody(const DevEnv& e, NrlTime t, const double f[3]);
+template <int L, typename M = double>
+static __device__ __forceinline__ double nrlDensityBody(const DevEnv& e, NrlTime t, const double f[3],
+                                                        double f32AboveKm = 0.0);
 
 // Out of line for eight and sixteen lanes, where the caller's live state is
 // small enough that the call's register saves cost less than the larger
 // inlined kernel; inline for one to four lanes (measured both ways).
-template <int L>
-static __device__ __noinline__ double nrlDensityCall(const DevEnv& e, NrlTime t, const double f[3]) {
-    return nrlDensityBody<L>(e, t, f);
+template <int L, typename M>
+static __device__ __noinline__ double nrlDensityCall(const DevEnv& e, NrlTime t, const double f[3], double f32AboveKm) {
+    return nrlDensityBody<L, M>(e, t, f, f32AboveKm);
 }
 #ifndef PHOP_NRL_INLINE_LANES_F32
 #define PHOP_NRL_INLINE_LANES_F32 4
 #endif
+// T = float (split precision) also instantiates the FP32 per-object model,
+// used above `f32AboveKm` when that is positive.
 template <int L, typename T>
-static __device__ __forceinline__ double nrlDensity(const DevEnv& e, NrlTime t, const double f[3]) {
+static __device__ __forceinline__ double nrlDensity(const DevEnv& e, NrlTime t, const double f[3],
+                                                    double f32AboveKm) {
     constexpr int inlineLanes = std::is_same<T, double>::value ? 4 : PHOP_NRL_INLINE_LANES_F32;
-    if constexpr (L <= inlineLanes) return nrlDensityBody<L>(e, t, f);
-    else return nrlDensityCall<L>(e, t, f);
+    if constexpr (L <= inlineLanes) return nrlDensityBody<L, T>(e, t, f, f32AboveKm);
+    else return nrlDensityCall<L, T>(e, t, f, f32AboveKm);
 }
 
-template <int L>
-static __device__ __forceinline__ double nrlDensityBody(const DevEnv& e, NrlTime t, const double f[3]) {
+template <int L, typename M>
+static __device__ __forceinline__ double nrlDensityBody(const DevEnv& e, NrlTime t, const double f[3],
+                                                        double f32AboveKm) {
     // geodetic latitude / longitude / altitude (Nrlmsise00.cu:243-266)
     const double rho2 = f[0] * f[0] + f[1] * f[1];
     if (!(rho2 + f[2] * f[2] > 0.0)) return NAN;
@@ -754,10 +759,17 @@ static __device__ __forceinline__ double nrlDensityBody(const DevEnv& e, NrlTime
     if (t.valid < 0) t = nrlTime(e, t.sec);  // deferred: `sec` holds the stage epoch (TDB s past J2000)
     if (!t.valid) return NAN;
     const double kRad = 57.2957795130823208768;
-    nrlf::Fast<double> model(e.nrlBlocks[t.block], t.sec);
     const double lst = wrapHours(t.gast + lon * kRad / 15.0);
     const int lane = (int)(threadIdx.x & 31);
-    const double rhoSi = model.template density<L>(lat * kRad, lon * kRad, alt, lst, lane % L, lane - lane % L);
+    double rhoSi;
+    if (!std::is_same<M, double>::value && f32AboveKm > 0.0 && alt > f32AboveKm) {
+        nrlf::Fast<float> model(e.nrlBlocks[t.block], t.sec);
+        rhoSi = (double)model.template density<L>((float)(lat * kRad), (float)(lon * kRad), (float)alt, (float)lst,
+                                                  lane % L, lane - lane % L);
+    } else {
+        nrlf::Fast<double> model(e.nrlBlocks[t.block], t.sec);
+        rhoSi = model.template density<L>(lat * kRad, lon * kRad, alt, lst, lane % L, lane - lane % L);
+    }
     if (!isfinite(rhoSi) || rhoSi < 0.0) return NAN;
     return (rhoSi * 1.0e9) * e.nrlDensityScale;
 }
@@ -856,8 +868,10 @@ static __device__ __noinline__ void tideAloneAccel(const Rec r, const double pos
     acc[2] += a[2];
 }
 
-// full right-hand side acceleration (km/s^2); every lane of the group calls it
-template <int L, typename T, class Rec>
+// full right-hand side acceleration (km/s^2); every lane of the group calls it.
+// PAIR: the geopotential of lane-group pairs (a separate kernel instantiation,
+// so the one-object-per-lane kernel keeps its own register allocation).
+template <int L, typename T, bool PAIR, class Rec>
 static __device__ __forceinline__ void accelerations(const StepParams& p, const typename TileOf<T>::type* tile,
                                               const Rec& r, const double pos[3], const double vel[3],
                                               double bc, double ams, double acc[3]) {
@@ -894,14 +908,14 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
             if constexpr (!std::is_same<T, double>::value) {
                 // split precision: objects below the split radius keep the
                 // tile part in FP64 (from the FP64 tile in global memory)
-                if (p.pairSh)
+                if constexpr (PAIR)
                     shAccelPair<L, T>(p, tile, r, bx, by, bz, a);
                 else if (p.splitRadius > 0.0 && bx * bx + by * by + bz * bz < p.splitRadius * p.splitRadius)
                     shAccel<L, double>(p, (const TileD*)p.tile64, r, bx, by, bz, a);
                 else
                     shAccel<L, T>(p, tile, r, bx, by, bz, a);
             } else {
-                if (p.pairSh)
+                if constexpr (PAIR)
                     shAccelPair<L, T>(p, tile, r, bx, by, bz, a);
                 else
                     shAccel<L, T>(p, tile, r, bx, by, bz, a);
@@ -972,7 +986,7 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
         if ((fl & kAtmosphere) && e.hasNrl) {
             double fx[3];
             toBody(r, pos, fx);
-            const double rho = nrlDensity<L, T>(e, r.nrlDeferred(), fx);
+            const double rho = nrlDensity<L, T>(e, r.nrlDeferred(), fx, p.dragF32AboveKm);
             const double w[3] = {r.W(0), r.W(1), r.W(2)};
             const double vr0 = vel[0] - (w[1] * pos[2] - w[2] * pos[1]);
             const double vr1 = vel[1] - (w[2] * pos[0] - w[0] * pos[2]);
@@ -1080,7 +1094,7 @@ static __device__ __forceinline__ RecordInterp recordFromGrid(const StepParams& 
     return RecordInterp{(const double*)(p.grid + i0), w[0], w[1], w[2], w[3], et};
 }
 
-template <int L, typename T, bool SHARED_GRID>
+template <int L, typename T, bool SHARED_GRID, bool PAIR>
 __global__ void __launch_bounds__(maxStepThreads(L), 1) propagateKernel(const __grid_constant__ StepParams p) {
     using Tile = typename TileOf<T>::type;
     constexpr int CPL = (6 + L - 1) / L;
@@ -1161,11 +1175,11 @@ __global__ void __launch_bounds__(maxStepThreads(L), 1) propagateKernel(const __
                 double acc[3];
                 if (SHARED_GRID) {
                     const RecordRef rec{p.records + kstep * 13 + s};
-                    accelerations<L, T>(p, tile, rec, st, st + 3, bc, ams, acc);
+                    accelerations<L, T, PAIR>(p, tile, rec, st, st + 3, bc, ams, acc);
                 } else {
                     const double ts = s == 0 ? t0 : t0 + dt * rkC(s - 1);
                     const RecordInterp rec = recordFromGrid(p, ts);
-                    accelerations<L, T>(p, tile, rec, st, st + 3, bc, ams, acc);
+                    accelerations<L, T, PAIR>(p, tile, rec, st, st + 3, bc, ams, acc);
                 }
 #pragma unroll
                 for (int c = 0; c < CPL; ++c) {
