@@ -134,29 +134,34 @@ def _reference_env():
     return env
 
 
-def run_reference_cli(env_dir: Path, pop, duration: float, step: float, threads: int, degree: int = 70) -> dict:
-    """One run of the reference CPU backend (oracle/_ref/bin/parahpop_cpu,
-    built from the reference sources): its command line takes one duration
-    and one step for all targets."""
+def run_reference_cli(env_dir: Path, pop, duration: float, step: float, threads: int, degree: int = 70,
+                      backend: str = "cpu") -> dict:
+    """One run of a reference backend (oracle/_ref/bin/parahpop_cpu or
+    parahpop_gpu, built from the reference sources): its command line takes
+    one duration and one step for all targets.  `seconds` is the
+    `propagation_seconds` of its summary.json (model and cache set-up,
+    transfers, graph construction and replay; not the environment load)."""
     from parahpop_b200 import synthetic as S
-    binary = ROOT / "oracle" / "_ref" / "bin" / "parahpop_cpu"
+    binary = ROOT / "oracle" / "_ref" / "bin" / f"parahpop_{backend}"
     if not binary.exists():
         return {"unavailable": f"{binary.relative_to(ROOT)} not built"}
     cfg = S.make_config(env_dir, duration, step, max_steps=10 ** 6, threads=threads, degree=degree)
     tag = f"{len(pop)}_{int(duration)}_{int(step)}"
-    cfgp, tgp = env_dir / f"cpu_config_{tag}.json", env_dir / f"cpu_targets_{tag}.json"
+    cfgp, tgp = env_dir / f"{backend}_config_{tag}.json", env_dir / f"{backend}_targets_{tag}.json"
     cfgp.write_text(json.dumps(cfg))
     tg = pop.targets_json()
     for t in tg["targets"]:  # one duration and step per run
         t.pop("duration_seconds", None)
         t.pop("step_seconds", None)
     tgp.write_text(json.dumps(tg))
-    out = Path(tempfile.mkdtemp(prefix="cpu_ref_", dir=env_dir))
+    out = Path(tempfile.mkdtemp(prefix=f"{backend}_ref_", dir=env_dir))
     shutil.rmtree(out)
-    r = subprocess.run([str(binary), str(cfgp), str(tgp), str(out)], cwd=env_dir, env=_reference_env(),
+    env = _reference_env() if backend == "cpu" else dict(os.environ)
+    r = subprocess.run([str(binary), str(cfgp), str(tgp), str(out)], cwd=env_dir, env=env,
                        capture_output=True, text=True)
     if r.returncode != 0:
-        return {"unavailable": "reference CPU run failed: " + (r.stderr.strip().splitlines() or ["?"])[-1]}
+        return {"unavailable": f"reference {backend.upper()} run failed: "
+                               + (r.stderr.strip().splitlines() or ["?"])[-1]}
     summ = json.loads((out / "summary.json").read_text())
     shutil.rmtree(out, ignore_errors=True)
     steps = int(np.ceil(duration / step))
@@ -201,6 +206,33 @@ def time_reference_c1(work: Path, threads: int) -> dict:
     return {"value": r["object_steps"] / r["seconds"], "seconds": r["seconds"], "object_steps": r["object_steps"],
             "sample": f"{n} objects x 1 h (60 steps) of the 10^4-object LEO workload, {r['seconds']:.2f} s on "
                       f"{threads} threads"}
+
+
+def time_reference_gpu(work: Path, workload: str) -> dict:
+    """The reference's own GPU backend (oracle/_ref/bin/parahpop_gpu, built
+    from the reference sources for sm_100a) on the same GPU: for C1 the whole
+    10^4-object population for 1 h, for C3 each orbit class of a 10^5-object
+    draw of the population for 1 h, one run per (step, duration) group as its
+    command line requires.  Throughput = object-steps / propagation_seconds
+    (its summary.json), the timing scope of the reference's
+    scripts/benchmark_gpu.py."""
+    from parahpop_b200 import synthetic as S
+    if workload == "c3":
+        pop = S.population_mixed(100000, seed=91)
+        groups = [(pop.subset(np.flatnonzero(pop.step == st)), 3600.0, st) for st in (30.0, 120.0, 300.0)]
+    else:
+        groups = [(S.population_leo(10000 if workload == "c1" else 100000, 11), 3600.0, 60.0)]
+    secs, obj = 0.0, 0
+    for pop, dur, step in groups:
+        r = run_reference_cli(work, pop, dur, step, 1, degree=120 if workload == "c2" else 70, backend="gpu")
+        if "unavailable" in r:
+            return r
+        secs += r["seconds"]
+        obj += r["object_steps"]
+    sample = ", ".join(f"{len(p)} objects at {s:g} s" for p, _, s in groups)
+    return {"value": obj / secs, "unit": "object-steps/s", "seconds": secs, "object_steps": obj,
+            "kind": "reference GPU backend (parahpop_gpu built from the reference sources for sm_100a)",
+            "sample": f"1 h per group ({sample}), propagation_seconds summed: {secs:.2f} s"}
 
 
 def run_reference_arm(args):
@@ -413,6 +445,7 @@ def main():
     ap.add_argument("--lanes", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--no-parity", action="store_true", help="skip the parity leg")
+    ap.add_argument("--no-reference-gpu", action="store_true", help="skip timing the reference's GPU backend")
     ap.add_argument("--serving-seconds", type=float, default=8.0,
                     help="arrival window of the serving trace (C4 shape) per precision form (0: skip)")
     args = ap.parse_args()
@@ -536,6 +569,7 @@ def main():
 
     parity = None
     cpu = None
+    ref_gpu = None
     serving = None
     if rank == 0:
         if not args.no_parity:
@@ -549,6 +583,8 @@ def main():
             else:
                 cpu = {"value": r["value"], "unit": "object-steps/s", "cores": threads, "kind": "reference",
                        "sample": r["sample"]}
+        if not args.no_reference_gpu:
+            ref_gpu = time_reference_gpu(work, args.workload)
         if args.serving_seconds > 0:
             from parahpop_b200 import serving as SV
             serving = {}
@@ -611,6 +647,7 @@ def main():
                          "peak_source": peak_note,
                          "numerator": f"29 FLOP x (N+1)(N+2)/2 SH terms x 13 stages per object-step, N = {degree}"},
             "cpu_baseline": cpu,
+            "reference_gpu": ref_gpu,
             "e2e": {"value": h["e2e_value"], "unit": "object-steps/s", "h2d_bytes_per_step": r["e2e"]["h2d_bytes"],
                     "d2h_bytes_per_step": r["e2e"]["d2h_bytes"]},
             "parity": parity,

@@ -145,7 +145,10 @@ int phop_propagate_device_noalloc(phop_context* ctx, int64_t n, double* d_states
  *              default 20) stay FP64; FP32 rounding in the recursion of the
  *              strongest terms (n <= 20) costs more final-position error
  *              than their FP32 speed gains
- *   "threads"  threads per CTA (multiple of 32, <= 512)
+ *   "threads"  threads per CTA (multiple of 32, <= 512); a launch uses at
+ *              most what the chosen kernel instantiation accepts (its
+ *              maxThreadsPerBlock: 256 at 1 lane, 320 at 2, 384 above) and
+ *              what shared memory allows
  *   "ctas_per_sm"  resident CTAs per SM, 0 = from occupancy
  *   "ordered"  1 (default) = hand objects to warps in order of geocentric
  *              radius, 0 = in input order; results are identical either way
@@ -159,9 +162,10 @@ int phop_propagate_device_noalloc(phop_context* ctx, int64_t n, double* d_states
  *              packed FP32 in split precision; at one, two or four lanes
  *              only): -1 (default) = chosen by the autotuner with the lane
  *              count (pinned lanes: pairs up to four lanes), 0 = off, 1 = on
- *   "split_drag_fp32_km"  split precision: NRLMSISE-00 in FP32 for objects
- *              above this height (km); 0 (default) = never (measured slower
- *              and above 1 cm at 500 km)
+ *   "deep_registers"  thread bound of the step kernel at two and four lanes:
+ *              1 = 256 threads a CTA with up to 255 registers a thread, 0 =
+ *              320 (two lanes) or 384 (four lanes) threads with up to 168;
+ *              -1 (default) = chosen by the autotuner (pinned lanes: 0)
  *   "tile_wait_test"  1 = test of the tile-staging time-out: the staging
  *              barrier is armed but no copy issued, so every CTA's bounded
  *              wait runs out and the CTA reads the tile from global memory
@@ -230,6 +234,8 @@ typedef struct {
     int64_t tile_fallbacks;  /* CTAs whose shared-memory staging of the coefficient tile timed out and that
                                 read the tile from global memory instead (results are the same) */
     int pair_sh;             /* the geopotential ran for lane-group pairs (two objects per lane) */
+    int deep_registers;      /* the step kernel ran at its deep thread bound (256 threads, <= 255 registers) */
+    int registers;           /* registers a thread of the step kernel instantiation used */
 } phop_stats;
 
 int phop_last_stats(const phop_context* ctx, phop_stats* out);

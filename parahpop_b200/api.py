@@ -27,7 +27,8 @@ class PhopStats(C.Structure):
     _fields_ = [("kernel_ms", C.c_double), ("records_ms", C.c_double), ("total_ms", C.c_double),
                 ("object_steps", C.c_int64), ("launches", C.c_int64), ("lanes", C.c_int), ("ctas", C.c_int),
                 ("threads", C.c_int), ("split", C.c_int), ("shared_grid", C.c_int), ("tile_in_smem", C.c_int),
-                ("tune_ms", C.c_double), ("tile_fallbacks", C.c_int64), ("pair_sh", C.c_int)]
+                ("tune_ms", C.c_double), ("tile_fallbacks", C.c_int64), ("pair_sh", C.c_int),
+                ("deep_registers", C.c_int), ("registers", C.c_int)]
 
 
 def library() -> C.CDLL:

@@ -220,18 +220,18 @@ int phop_set_option(phop_context* ctx, const char* key, double value) {
             return 1;
         }
         ctx->opt.splitFloorKm = value;
-    } else if (k == "split_drag_fp32_km") {
-        if (!(value >= 0.0) || !std::isfinite(value)) {
-            ctx->error = "split_drag_fp32_km must be finite and non-negative";
-            return 1;
-        }
-        ctx->opt.splitDragF32Km = value;
     } else if (k == "pair_sh") {
         if (value != -1.0 && value != 0.0 && value != 1.0) {
             ctx->error = "pair_sh must be -1 (autotuned), 0 or 1";
             return 1;
         }
         ctx->opt.pairSh = (int)value;
+    } else if (k == "deep_registers") {
+        if (value != -1.0 && value != 0.0 && value != 1.0) {
+            ctx->error = "deep_registers must be -1 (autotuned), 0 or 1";
+            return 1;
+        }
+        ctx->opt.deepRegs = (int)value;
     } else if (k == "tile_wait_test") {
         ctx->opt.tileWaitTest = value != 0.0 ? 1 : 0;
     } else if (k == "split_fp64_degree") {
@@ -593,6 +593,8 @@ int phop_last_stats(const phop_context* ctx, phop_stats* out) {
     out->tile_in_smem = ctx->stats.tileInSmem;
     out->tile_fallbacks = ctx->stats.tileFallbacks;
     out->pair_sh = ctx->stats.pairSh ? 1 : 0;
+    out->deep_registers = ctx->stats.deepRegs ? 1 : 0;
+    out->registers = ctx->stats.registers;
     return 0;
 }
 

@@ -1460,6 +1460,7 @@ Engine::LaunchShape Engine::prepareStep(StepParams& p, int L, const RunOptions& 
     // split form's FP64 floor, whose low objects take the FP64 tile of L lanes
     const bool pair = opt.pairSh < 0 ? L <= 4 : opt.pairSh != 0;
     p.pairSh = (pair && L <= 4 && !(opt.split && opt.splitFloorKm > 0.0)) ? 1 : 0;
+    p.deepRegs = (opt.deepRegs > 0 && hasDeepShape(L)) ? 1 : 0;
     const Tile& tile = tileFor(p.pairSh ? 2 * L : L, opt.split, lowDeg);
     p.tile = tile.dTile;
     p.tileBytes = tile.bytes;
@@ -1467,7 +1468,6 @@ Engine::LaunchShape Engine::prepareStep(StepParams& p, int L, const RunOptions& 
     p.nblocks = tile.nblocks;
     p.diagStep = tile.dDiagStep;
     p.lowDeg = lowDeg;
-    p.dragF32AboveKm = opt.split ? opt.splitDragF32Km : 0.0;
     p.tile64 = nullptr;
     p.splitRadius = 0.0;
     if (opt.split && opt.splitFloorKm > 0.0) {
@@ -1476,7 +1476,21 @@ Engine::LaunchShape Engine::prepareStep(StepParams& p, int L, const RunOptions& 
     }
     // shared memory per CTA: the coefficient tile (when it fits) plus the
     // stage derivatives, 13 x ceil(6/L) doubles per thread
-    const int threadsReq = std::min(opt.threads > 0 ? opt.threads : 512, maxStepThreads(L));
+    int registers = 0;
+    int threadsReq = std::min(opt.threads > 0 ? opt.threads : 512, stepThreadBound(L, p.deepRegs));
+    {
+        // never more threads than the compiled instantiation accepts (its
+        // register count times the threads must fit the SM's register file)
+        const int akey = (((L * 2 + (opt.split ? 1 : 0)) * 2 + (shared ? 1 : 0)) * 2 + p.pairSh) * 2 + p.deepRegs;
+        auto at = attrs_.find(akey);
+        if (at == attrs_.end()) {
+            cudaFuncAttributes a{};
+            PHOP_CUDA(propagateAttributes(L, opt.split, shared, p.pairSh, p.deepRegs, &a));
+            at = attrs_.emplace(akey, std::make_pair(a.maxThreadsPerBlock, a.numRegs)).first;
+        }
+        threadsReq = std::max(32, std::min(threadsReq, at->second.first / 32 * 32));
+        registers = at->second.second;
+    }
     const int kPerThread = 13 * ((6 + L - 1) / L) * 8;
     int threads = threadsReq;
     if (opt.tileSmem != 0 && tile.bytes + 1024 + 64 * kPerThread <= maxSmem_) {
@@ -1489,11 +1503,13 @@ Engine::LaunchShape Engine::prepareStep(StepParams& p, int L, const RunOptions& 
     int perSm = opt.ctasPerSm;
     if (perSm <= 0) {
         const int smem = propagateSmemBytes(p, L, threads);
-        const int64_t key = ((((int64_t)smem * 1024 + threads) * 32 + L) * 4 + (opt.split ? 2 : 0) + (shared ? 1 : 0)) * 2
-                            + p.pairSh;
+        const int64_t key = (((((int64_t)smem * 1024 + threads) * 32 + L) * 4 + (opt.split ? 2 : 0) + (shared ? 1 : 0)) * 2
+                             + p.pairSh) * 2 + p.deepRegs;
         auto it = occupancy_.find(key);
         if (it == occupancy_.end())
-            it = occupancy_.emplace(key, propagateMaxCtasPerSm(L, opt.split, shared, p.pairSh, threads, smem)).first;
+            it = occupancy_
+                     .emplace(key, propagateMaxCtasPerSm(L, opt.split, shared, p.pairSh, p.deepRegs, threads, smem))
+                     .first;
         perSm = it->second;
     }
     if (perSm <= 0) perSm = 1;
@@ -1512,36 +1528,47 @@ Engine::LaunchShape Engine::prepareStep(StepParams& p, int L, const RunOptions& 
     shape.threads = threads;
     shape.ctas = (int)std::max<int64_t>(1, std::min<int64_t>(slots, need));
     shape.smemTile = p.useSmemTile != 0;
+    shape.registers = registers;
     return shape;
 }
 
-// Project autotuner for the launch shape: lanes per object (1, 2, 4, 8, 16)
-// and objects per lane in the geopotential (one, or two for lane-group pairs
-// at up to four lanes).  The first batch of each class (log2 of the batch
-// size, time-grid mode, precision, pairing option) times a short probe (up
-// to twelve steps, best of three after an untimed warm-up launch) of every
-// shape on scratch copies of the inputs and keeps the fastest; later batches
-// of the class reuse the choice.  PARAHPOP_B200_TUNE_LOG=1 prints the probe
-// times.
+// Project autotuner for the launch shape: lanes per object (1, 2, 4, 8, 16),
+// objects per lane in the geopotential (one, or two for lane-group pairs at
+// up to four lanes) and, at two and four lanes, the thread bound the kernel
+// is compiled for (wide: 320 / 384 threads at 168 registers; deep: 256
+// threads at 255 registers).  Threads per CTA follow from the bound, shared
+// memory and the batch size (prepareStep).  The first batch of each class
+// (log2 of the batch size, time-grid mode, precision, pairing and bound
+// options) times a short probe of
+// every shape on scratch copies of the inputs and keeps the fastest; later
+// batches of the class reuse the choice.  A probe launch advances every
+// object by up to twelve steps, fewer for large batches so that one launch
+// stays near kProbeObjectSteps object-steps (at least one step); the
+// fastest of two timed launches after an untimed warm-up counts.
+// PARAHPOP_B200_TUNE_LOG=1 prints the probe times.
+static constexpr int64_t kProbeObjectSteps = int64_t(1) << 17;
 int Engine::tunedShape(const StepParams& base, const RunOptions& opt, bool shared, cudaStream_t stream,
                        int64_t* launches) {
     int bucket = 0;
     while (bucket < 40 && (int64_t(1) << bucket) < base.n) ++bucket;
-    const int key = (bucket * 4 + (shared ? 2 : 0) + (opt.split ? 1 : 0)) * 4 + (opt.pairSh + 1);
+    const int key = ((bucket * 4 + (shared ? 2 : 0) + (opt.split ? 1 : 0)) * 4 + (opt.pairSh + 1)) * 4
+                    + (opt.deepRegs + 1);
     auto it = tuned_.find(key);
     if (it != tuned_.end()) return it->second;
     if (base.stride != 0 && base.stride != base.n) {  // pools pin their lane count
         const int L = autoLanes(base.n);
-        return L * 2 + (opt.pairSh < 0 ? (L <= 4 ? 1 : 0) : opt.pairSh);
+        const int pair = opt.pairSh < 0 ? (L <= 4 ? 1 : 0) : opt.pairSh;
+        return (L * 2 + pair) * 2 + (opt.deepRegs > 0 && hasDeepShape(L) ? 1 : 0);
     }
     const int64_t n = base.n;
     StepParams p = base;
     double* st = (double*)scratch("probeState", (size_t)6 * n * 8);
     p.state = st;
+    const int probeSteps = (int)std::max<int64_t>(1, std::min<int64_t>(12, kProbeObjectSteps / std::max<int64_t>(1, n)));
     if (shared) {
-        p.nsteps = std::min(p.nsteps, 12);
+        p.nsteps = std::min(p.nsteps, probeSteps);
     } else {
-        p.maxSteps = 12;
+        p.maxSteps = probeSteps;
         p.cur = (double*)scratch("probeCur", (size_t)n * 8);
         p.dt = (double*)scratch("probeDt", (size_t)n * 8);
         p.unfinished = (int*)scratch("probeUnf", (size_t)n * 4);
@@ -1549,22 +1576,26 @@ int Engine::tunedShape(const StepParams& base, const RunOptions& opt, bool share
     cudaEvent_t e0, e1;
     PHOP_CUDA(cudaEventCreate(&e0));
     PHOP_CUDA(cudaEventCreate(&e1));
-    int best = autoLanes(n) * 2 + (opt.pairSh > 0 ? 1 : 0);
+    int best = (autoLanes(n) * 2 + (opt.pairSh > 0 ? 1 : 0)) * 2;
     float bestMs = 1e30f;
     const char* logEnv = std::getenv("PARAHPOP_B200_TUNE_LOG");
     const bool tuneLog = logEnv && std::atoi(logEnv) != 0;
-    for (int code = 2; code < 34; ++code) {
-        const int L = code >> 1, pair = code & 1;
+    // shape code: ((lanes * 2 + pairs) * 2 + deep thread bound)
+    for (int code = 4; code < 68; ++code) {
+        const int L = code >> 2, pair = (code >> 1) & 1, deep = code & 1;
         if (L != 1 && L != 2 && L != 4 && L != 8 && L != 16) continue;
         if (opt.pairSh >= 0 && pair != opt.pairSh) continue;
         if (opt.pairSh < 0 && pair && L >= 8) continue;  // pairs at 8 and 16 lanes measured slower on every workload
+        if (deep && !hasDeepShape(L)) continue;
+        if (opt.deepRegs >= 0 && deep != (opt.deepRegs && hasDeepShape(L) ? 1 : 0)) continue;
         if (L >= 8 && n >= (int64_t)sms_ * 512 * 4) continue;  // enough objects to fill the GPU with narrow groups
         RunOptions o = opt;
         o.pairSh = pair;
+        o.deepRegs = deep;
         // an untimed launch first (module loading, attribute set-up), then the
-        // fastest of three timed probes
+        // fastest of two timed probes
         float ms = 1e30f;
-        for (int rep = 0; rep < 4; ++rep) {
+        for (int rep = 0; rep < 3; ++rep) {
             PHOP_CUDA(cudaMemcpyAsync(st, base.state, (size_t)6 * n * 8, cudaMemcpyDeviceToDevice, stream));
             if (!shared) {
                 PHOP_CUDA(cudaMemcpyAsync(p.cur, base.cur, (size_t)n * 8, cudaMemcpyDeviceToDevice, stream));
@@ -1585,8 +1616,10 @@ int Engine::tunedShape(const StepParams& base, const RunOptions& opt, bool share
         PHOP_CUDA(cudaMemcpy(&err, p.errorFlag, sizeof(int), cudaMemcpyDeviceToHost));
         if (err) throw std::runtime_error("Propagation kernel reported error " + std::to_string(err) + ".");
         if (tuneLog)
-            std::fprintf(stderr, "parahpop-b200 tune: n=%lld shared=%d split=%d lanes=%d pairs=%d probe_ms=%.3f\n",
-                         (long long)n, shared ? 1 : 0, opt.split ? 1 : 0, L, pair, ms);
+            std::fprintf(stderr,
+                         "parahpop-b200 tune: n=%lld shared=%d split=%d lanes=%d pairs=%d deep=%d probe_steps=%d "
+                         "probe_ms=%.3f\n",
+                         (long long)n, shared ? 1 : 0, opt.split ? 1 : 0, L, pair, deep, probeSteps, ms);
         if (ms < bestMs) {
             bestMs = ms;
             best = code;
@@ -1664,8 +1697,9 @@ void Engine::runKernel(int64_t n, double* dState, const double* dBc, const doubl
     int L = opt.lanes;
     if (L <= 0) {
         const int code = tunedShape(p, opt, shared, stream, &launches);
-        L = code >> 1;
-        o.pairSh = code & 1;
+        L = code >> 2;
+        o.pairSh = (code >> 1) & 1;
+        o.deepRegs = code & 1;
     }
     if (opt.dTraj) {  // after the autotuner's probes, which must not write records
         p.traj = opt.dTraj;
@@ -1700,6 +1734,8 @@ void Engine::runKernel(int64_t n, double* dState, const double* dBc, const doubl
         stats->sharedGrid = shared;
         stats->tileInSmem = shape.smemTile;
         stats->pairSh = p.pairSh != 0;
+        stats->deepRegs = p.deepRegs != 0;
+        stats->registers = shape.registers;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -111,6 +111,8 @@ struct RunStats {
     bool sharedGrid = false;
     bool tileInSmem = false;
     bool pairSh = false;           // the geopotential of lane-group pairs was used
+    bool deepRegs = false;         // the deep thread bound (256 threads, 255 registers) was used
+    int registers = 0;             // registers a thread of the step kernel used
     int64_t tileFallbacks = 0;     // CTAs that read the tile from global memory after a staging time-out
 };
 
@@ -128,7 +130,8 @@ struct RunOptions {
     int tileWaitTest = 0; // test of the tile-staging time-out: the barrier is armed, no copy issued
     int pairSh = -1;      // geopotential of lane-group pairs (packed FP32 in split precision): 1 on, 0 off,
                           // -1 autotuned with the lane count (pinned lanes: on up to 4 lanes)
-    double splitDragF32Km = 0.0;  // split precision: NRLMSISE-00 in FP32 above this height; 0 = never
+    int deepRegs = -1;    // thread bound at 2 and 4 lanes: 1 deep (256 threads, 255 registers), 0 wide
+                          // (320 / 384 threads, 168 registers), -1 autotuned (pinned lanes: wide)
     // trajectory records of a uniform batch: device buffer of
     // (steps / trajEvery) x 6 x n doubles, null for none
     double* dTraj = nullptr;
@@ -198,6 +201,7 @@ public:
     // Launch geometry of one step-kernel launch.
     struct LaunchShape {
         int lanes = 0, threads = 0, ctas = 0;
+        int registers = 0;  // registers a thread of the chosen instantiation
         bool smemTile = false;
     };
     // Per-batch time description handed to the step kernel.
@@ -262,6 +266,7 @@ private:
     double* dDiag_ = nullptr;
     std::map<int, int> tuned_;  // autotuned lane count per batch class
     std::map<int64_t, int> occupancy_;  // resident CTAs per SM by launch configuration
+    std::map<int, std::pair<int, int>> attrs_;  // maxThreadsPerBlock, numRegs of each step-kernel instantiation
 };
 
 }  // namespace phop

@@ -258,7 +258,7 @@ void Engine::propagateNoAlloc(int64_t n, double* dState, const double* dBc, cons
         threads = std::min(threadsReq, (maxSmem_ - 1024) / kPerThread / 32 * 32);
     }
     const int smem = propagateSmemBytes(sp, L, threads);
-    int perSm = opt.ctasPerSm > 0 ? opt.ctasPerSm : propagateMaxCtasPerSm(L, opt.split, true, 0, threads, smem);
+    int perSm = opt.ctasPerSm > 0 ? opt.ctasPerSm : propagateMaxCtasPerSm(L, opt.split, true, 0, 0, threads, smem);
     if (perSm <= 0) perSm = 1;
     const int64_t groups = (n + (32 / L) - 1) / (32 / L);
     const int64_t need = (groups + threads / 32 - 1) / (threads / 32);

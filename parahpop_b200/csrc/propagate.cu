@@ -9,7 +9,8 @@ namespace phop {
 #define PHOP_DECL(sfx)                                                                                     \
     cudaError_t launchPropagate_##sfx(const StepParams& p, size_t paramsBytes, int lanes, int ctas, int threads, \
                                       int smem, cudaStream_t stream);                                       \
-    int occupancy_##sfx(int lanes, int pair, int threads, int smem);
+    int occupancy_##sfx(int lanes, int pair, int deep, int threads, int smem);                            \
+    cudaError_t attributes_##sfx(int lanes, int pair, int deep, cudaFuncAttributes* a);
 PHOP_DECL(f64_grid)
 PHOP_DECL(f64_mixed)
 PHOP_DECL(f32_grid)
@@ -71,10 +72,17 @@ int propagateSmemBytes(const StepParams& p, int lanes, int threads) {
     return (p.useSmemTile ? p.tileBytes : 0) + 13 * cpl * threads * (int)sizeof(double);
 }
 
-int propagateMaxCtasPerSm(int lanes, bool split, bool shared, int pair, int threads, int smem) {
+int propagateMaxCtasPerSm(int lanes, bool split, bool shared, int pair, int deep, int threads, int smem) {
     if (split)
-        return shared ? occupancy_f32_grid(lanes, pair, threads, smem) : occupancy_f32_mixed(lanes, pair, threads, smem);
-    return shared ? occupancy_f64_grid(lanes, pair, threads, smem) : occupancy_f64_mixed(lanes, pair, threads, smem);
+        return shared ? occupancy_f32_grid(lanes, pair, deep, threads, smem)
+                      : occupancy_f32_mixed(lanes, pair, deep, threads, smem);
+    return shared ? occupancy_f64_grid(lanes, pair, deep, threads, smem)
+                  : occupancy_f64_mixed(lanes, pair, deep, threads, smem);
+}
+
+cudaError_t propagateAttributes(int lanes, bool split, bool shared, int pair, int deep, cudaFuncAttributes* a) {
+    if (split) return shared ? attributes_f32_grid(lanes, pair, deep, a) : attributes_f32_mixed(lanes, pair, deep, a);
+    return shared ? attributes_f64_grid(lanes, pair, deep, a) : attributes_f64_mixed(lanes, pair, deep, a);
 }
 
 cudaError_t launchPropagate(const StepParams& p, int lanes, bool split, bool shared, int ctas, int threads,

@@ -121,7 +121,7 @@ struct StepParams {
     double splitRadius;     // split precision: radius (km) below which the tile part stays FP64; 0 = none
     int useSmemTile;
     int pairSh;             // the geopotential of lane-group pairs (tile built for 2L lanes)
-    double dragF32AboveKm;  // split precision: NRLMSISE-00 in FP32 above this height (km); 0 = never
+    int deepRegs;           // host-side choice of the kernel's thread bound (stepThreadBound)
     int tileWaitTest;       // test of the staging time-out: arm the barrier, issue no copy
     // scheduling and errors
     int* workCounter;
@@ -131,15 +131,27 @@ struct StepParams {
 
 // Threads per CTA the step kernel is compiled for: narrow lane splits run one
 // CTA of few threads per SM (the coefficient tile fills shared memory), so
-// they get up to 255 registers per thread instead of spilling at 128.
+// they get up to 255 registers per thread instead of spilling at 128.  The
+// "wide" shape below, and at two and four lanes also a "deep" one of
+// kDeepThreads threads: 255 registers a thread instead of 168 (fewer warps,
+// fewer spills; the autotuner times both).
 __host__ __device__ constexpr int maxStepThreads(int lanes) {
     return lanes == 1 ? 256 : lanes == 2 ? 320 : 384;
+}
+constexpr int kDeepThreads = 256;
+__host__ __device__ constexpr bool hasDeepShape(int lanes) { return lanes == 2 || lanes == 4; }
+__host__ __device__ constexpr int stepThreadBound(int lanes, int deep) {
+    return deep && hasDeepShape(lanes) ? kDeepThreads : maxStepThreads(lanes);
 }
 
 void launchEpochRecords(const DevEnv& env, const double* epochs, int count, EpochRecord* out, cudaStream_t stream);
 cudaError_t launchPropagate(const StepParams& p, int lanes, bool split, bool shared, int ctas, int threads,
                             cudaStream_t stream);
 int propagateSmemBytes(const StepParams& p, int lanes, int threads);
-int propagateMaxCtasPerSm(int lanes, bool split, bool shared, int pair, int threads, int smem);
+int propagateMaxCtasPerSm(int lanes, bool split, bool shared, int pair, int deep, int threads, int smem);
+// The compiled instantiation's attributes (maxThreadsPerBlock, numRegs,
+// localSizeBytes): the launch shape never asks for more threads than the
+// instantiation accepts.
+cudaError_t propagateAttributes(int lanes, bool split, bool shared, int pair, int deep, cudaFuncAttributes* a);
 
 }  // namespace phop

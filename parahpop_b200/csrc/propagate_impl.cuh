@@ -705,33 +705,27 @@ static __device__ __forceinline__ double shadowFactor(const double rS[3], const 
 
 // NRLMSISE-00 density (kg/km^3) at ITRF position f; the L lanes of a group
 // share the globe7 tables of the model and all return the same value.
-template <int L, typename M = double>
-static __device__ __forceinline__ double nrlDensityBody(const DevEnv& e, NrlTime t, const double f[3],
-                                                        double f32AboveKm = 0.0);
+template <int L>
+static __device__ __forceinline__ double nrlDensityBody(const DevEnv& e, NrlTime t, const double f[3]);
 
 // Out of line for eight and sixteen lanes, where the caller's live state is
 // small enough that the call's register saves cost less than the larger
 // inlined kernel; inline for one to four lanes (measured both ways).
-template <int L, typename M>
-static __device__ __noinline__ double nrlDensityCall(const DevEnv& e, NrlTime t, const double f[3], double f32AboveKm) {
-    return nrlDensityBody<L, M>(e, t, f, f32AboveKm);
+template <int L>
+static __device__ __noinline__ double nrlDensityCall(const DevEnv& e, NrlTime t, const double f[3]) {
+    return nrlDensityBody<L>(e, t, f);
 }
-#ifndef PHOP_NRL_INLINE_LANES_F32
-#define PHOP_NRL_INLINE_LANES_F32 4
-#endif
-// T = float (split precision) also instantiates the FP32 per-object model,
-// used above `f32AboveKm` when that is positive.
-template <int L, typename T>
-static __device__ __forceinline__ double nrlDensity(const DevEnv& e, NrlTime t, const double f[3],
-                                                    double f32AboveKm) {
-    constexpr int inlineLanes = std::is_same<T, double>::value ? 4 : PHOP_NRL_INLINE_LANES_F32;
-    if constexpr (L <= inlineLanes) return nrlDensityBody<L, T>(e, t, f, f32AboveKm);
-    else return nrlDensityCall<L, T>(e, t, f, f32AboveKm);
+// FP64 in both precision forms: an FP32 per-object model (the split form's
+// option at one time) was slower and moved 500 km objects by more than 1 cm
+// in 24 h.
+template <int L>
+static __device__ __forceinline__ double nrlDensity(const DevEnv& e, NrlTime t, const double f[3]) {
+    if constexpr (L <= 4) return nrlDensityBody<L>(e, t, f);
+    else return nrlDensityCall<L>(e, t, f);
 }
 
-template <int L, typename M>
-static __device__ __forceinline__ double nrlDensityBody(const DevEnv& e, NrlTime t, const double f[3],
-                                                        double f32AboveKm) {
+template <int L>
+static __device__ __forceinline__ double nrlDensityBody(const DevEnv& e, NrlTime t, const double f[3]) {
     // geodetic latitude / longitude / altitude (Nrlmsise00.cu:243-266)
     const double rho2 = f[0] * f[0] + f[1] * f[1];
     if (!(rho2 + f[2] * f[2] > 0.0)) return NAN;
@@ -761,15 +755,8 @@ static __device__ __forceinline__ double nrlDensityBody(const DevEnv& e, NrlTime
     const double kRad = 57.2957795130823208768;
     const double lst = wrapHours(t.gast + lon * kRad / 15.0);
     const int lane = (int)(threadIdx.x & 31);
-    double rhoSi;
-    if (!std::is_same<M, double>::value && f32AboveKm > 0.0 && alt > f32AboveKm) {
-        nrlf::Fast<float> model(e.nrlBlocks[t.block], t.sec);
-        rhoSi = (double)model.template density<L>((float)(lat * kRad), (float)(lon * kRad), (float)alt, (float)lst,
-                                                  lane % L, lane - lane % L);
-    } else {
-        nrlf::Fast<double> model(e.nrlBlocks[t.block], t.sec);
-        rhoSi = model.template density<L>(lat * kRad, lon * kRad, alt, lst, lane % L, lane - lane % L);
-    }
+    nrlf::Fast<double> model(e.nrlBlocks[t.block], t.sec);
+    const double rhoSi = model.template density<L>(lat * kRad, lon * kRad, alt, lst, lane % L, lane - lane % L);
     if (!isfinite(rhoSi) || rhoSi < 0.0) return NAN;
     return (rhoSi * 1.0e9) * e.nrlDensityScale;
 }
@@ -986,7 +973,7 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
         if ((fl & kAtmosphere) && e.hasNrl) {
             double fx[3];
             toBody(r, pos, fx);
-            const double rho = nrlDensity<L, T>(e, r.nrlDeferred(), fx, p.dragF32AboveKm);
+            const double rho = nrlDensity<L>(e, r.nrlDeferred(), fx);
             const double w[3] = {r.W(0), r.W(1), r.W(2)};
             const double vr0 = vel[0] - (w[1] * pos[2] - w[2] * pos[1]);
             const double vr1 = vel[1] - (w[2] * pos[0] - w[0] * pos[2]);
@@ -1094,8 +1081,11 @@ static __device__ __forceinline__ RecordInterp recordFromGrid(const StepParams& 
     return RecordInterp{(const double*)(p.grid + i0), w[0], w[1], w[2], w[3], et};
 }
 
-template <int L, typename T, bool SHARED_GRID, bool PAIR>
-__global__ void __launch_bounds__(maxStepThreads(L), 1) propagateKernel(const __grid_constant__ StepParams p) {
+// MAXT: the thread bound the kernel is compiled for, which sets its register
+// budget (the register file is split over the SM's four sub-partitions, so
+// 320 or 384 threads leave 168 registers a thread and 256 threads leave 255).
+template <int L, typename T, bool SHARED_GRID, bool PAIR, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1) propagateKernel(const __grid_constant__ StepParams p) {
     using Tile = typename TileOf<T>::type;
     constexpr int CPL = (6 + L - 1) / L;
     extern __shared__ __align__(128) unsigned char smem[];

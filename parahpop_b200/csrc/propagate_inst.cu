@@ -21,65 +21,75 @@
 
 namespace phop {
 
-template <int L, bool PAIR>
-static cudaError_t launchOne(const StepParams& p, int ctas, int threads, int smem, cudaStream_t stream) {
-    auto k = propagateKernel<L, PHOP_T, (bool)PHOP_SG, PAIR>;
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return e;
+// one compiled step-kernel shape: lanes per object, lane-group pairs, thread bound
+template <int L_, bool PAIR_, int MAXT_>
+struct Shape {
+    static constexpr int L = L_;
+    static constexpr bool PAIR = PAIR_;
+    static constexpr int MAXT = MAXT_;
+};
+
+// The instantiated shapes: 1, 2, 4, 8, 16 lanes at the wide thread bound;
+// pairs at 1, 2, 4 lanes (slower at 8 and 16); the deep bound at 2 and 4
+// lanes, paired or not.  Anything else returns `bad`.
+template <class R, class F>
+static R dispatch(int lanes, int pair, int deep, R bad, F&& f) {
+    if (deep && hasDeepShape(lanes)) {
+        if (lanes == 2) return pair ? f(Shape<2, true, kDeepThreads>{}) : f(Shape<2, false, kDeepThreads>{});
+        return pair ? f(Shape<4, true, kDeepThreads>{}) : f(Shape<4, false, kDeepThreads>{});
     }
-    k<<<ctas, threads, smem, stream>>>(p);
-    return cudaGetLastError();
+    if (deep) return bad;
+    if (pair) {
+        switch (lanes) {
+            case 1: return f(Shape<1, true, maxStepThreads(1)>{});
+            case 2: return f(Shape<2, true, maxStepThreads(2)>{});
+            case 4: return f(Shape<4, true, maxStepThreads(4)>{});
+            default: return bad;
+        }
+    }
+    switch (lanes) {
+        case 1: return f(Shape<1, false, maxStepThreads(1)>{});
+        case 2: return f(Shape<2, false, maxStepThreads(2)>{});
+        case 4: return f(Shape<4, false, maxStepThreads(4)>{});
+        case 8: return f(Shape<8, false, maxStepThreads(8)>{});
+        case 16: return f(Shape<16, false, maxStepThreads(16)>{});
+        default: return bad;
+    }
 }
 
-template <int L, bool PAIR>
-static int occupancyOne(int threads, int smem) {
-    int n = 0;
-    auto k = propagateKernel<L, PHOP_T, (bool)PHOP_SG, PAIR>;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, threads, smem);
-    return n;
+template <class S>
+static auto kernelOf() {
+    return propagateKernel<S::L, PHOP_T, (bool)PHOP_SG, S::PAIR, S::MAXT>;
 }
 
 cudaError_t PHOP_CAT(launchPropagate_, PHOP_SUFFIX)(const StepParams& p, size_t paramsBytes, int lanes, int ctas,
                                                     int threads, int smem, cudaStream_t stream) {
     if (paramsBytes != sizeof(StepParams)) return cudaErrorInvalidValue;  // objects built from different headers
-    // lane-group pairs at up to four lanes only (slower at eight and sixteen)
-    if (p.pairSh) {
-        switch (lanes) {
-            case 1: return launchOne<1, true>(p, ctas, threads, smem, stream);
-            case 2: return launchOne<2, true>(p, ctas, threads, smem, stream);
-            case 4: return launchOne<4, true>(p, ctas, threads, smem, stream);
-            default: return cudaErrorInvalidValue;
+    return dispatch(lanes, p.pairSh, p.deepRegs, cudaErrorInvalidValue, [&](auto shape) -> cudaError_t {
+        auto k = kernelOf<decltype(shape)>();
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            if (e != cudaSuccess) return e;
         }
-    }
-    switch (lanes) {
-        case 1: return launchOne<1, false>(p, ctas, threads, smem, stream);
-        case 2: return launchOne<2, false>(p, ctas, threads, smem, stream);
-        case 4: return launchOne<4, false>(p, ctas, threads, smem, stream);
-        case 8: return launchOne<8, false>(p, ctas, threads, smem, stream);
-        case 16: return launchOne<16, false>(p, ctas, threads, smem, stream);
-        default: return cudaErrorInvalidValue;
-    }
+        k<<<ctas, threads, smem, stream>>>(p);
+        return cudaGetLastError();
+    });
 }
 
-int PHOP_CAT(occupancy_, PHOP_SUFFIX)(int lanes, int pair, int threads, int smem) {
-    if (pair) {
-        switch (lanes) {
-            case 1: return occupancyOne<1, true>(threads, smem);
-            case 2: return occupancyOne<2, true>(threads, smem);
-            case 4: return occupancyOne<4, true>(threads, smem);
-            default: return 0;
-        }
-    }
-    switch (lanes) {
-        case 1: return occupancyOne<1, false>(threads, smem);
-        case 2: return occupancyOne<2, false>(threads, smem);
-        case 4: return occupancyOne<4, false>(threads, smem);
-        case 8: return occupancyOne<8, false>(threads, smem);
-        case 16: return occupancyOne<16, false>(threads, smem);
-        default: return 0;
-    }
+int PHOP_CAT(occupancy_, PHOP_SUFFIX)(int lanes, int pair, int deep, int threads, int smem) {
+    return dispatch(lanes, pair, deep, 0, [&](auto shape) -> int {
+        auto k = kernelOf<decltype(shape)>();
+        if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        int n = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, threads, smem);
+        return n;
+    });
+}
+
+cudaError_t PHOP_CAT(attributes_, PHOP_SUFFIX)(int lanes, int pair, int deep, cudaFuncAttributes* a) {
+    return dispatch(lanes, pair, deep, cudaErrorInvalidValue, [&](auto shape) -> cudaError_t {
+        return cudaFuncGetAttributes(a, kernelOf<decltype(shape)>());
+    });
 }
 
 }  // namespace phop

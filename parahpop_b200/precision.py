@@ -43,8 +43,6 @@ def main(argv=None):
                     help="split precision: FP64 harmonics below this height (km); default: the library's")
     ap.add_argument("--split-degree", type=int, default=None,
                     help="split precision: degrees n <= this stay FP64 (default: the library's, 20)")
-    ap.add_argument("--split-drag-fp32-km", type=float, default=None,
-                    help="split precision: NRLMSISE-00 in FP32 above this height (km); default: never")
     ap.add_argument("--no-pair", action="store_true", help="one object per lane in the geopotential")
     args = ap.parse_args(argv)
 
@@ -68,8 +66,6 @@ def main(argv=None):
             p.set_option("split_floor_km", args.split_floor_km)
         if split and args.split_degree is not None:
             p.set_option("split_fp64_degree", args.split_degree)
-        if split and args.split_drag_fp32_km is not None:
-            p.set_option("split_drag_fp32_km", args.split_drag_fp32_km)
         if args.no_pair:
             p.set_option("pair_sh", 0)
         warm = pop.subset(np.arange(min(n, 4096)))
@@ -88,7 +84,7 @@ def main(argv=None):
     out = {"workload": ("mixed LEO/MEO/GEO" if args.mixed else "LEO") + f", {n} objects, degree {args.degree}, "
                        f"{args.hours:g} h", "object_steps": int(res["fp64"]["object_steps"]),
            "split_floor_km": args.split_floor_km, "split_degree": args.split_degree,
-           "split_drag_fp32_km": args.split_drag_fp32_km, "pair": not args.no_pair}
+           "pair": not args.no_pair}
     for name in ("fp64", "split"):
         r = res[name]
         out[name] = {"object_steps_per_s": r["object_steps"] / ((r["kernel_ms"] + r["records_ms"]) * 1e-3),
