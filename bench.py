@@ -443,6 +443,10 @@ def main():
     ap.add_argument("--hours", type=float, default=24.0, help="c1/c2: span covered by the K timed steps")
     ap.add_argument("--split-degree", type=int, default=None, help="split precision: FP64 up to this degree")
     ap.add_argument("--lanes", type=int, default=0)
+    ap.add_argument("--pair-sh", type=int, default=-1, choices=[-1, 0, 1],
+                    help="geopotential of lane-group pairs: -1 autotuned (pinned lanes: on up to 4 lanes)")
+    ap.add_argument("--deep-registers", type=int, default=-1, choices=[-1, 0, 1],
+                    help="thread bound at 2 and 4 lanes: 1 deep (256 threads, 255 registers), 0 wide, -1 autotuned")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--no-parity", action="store_true", help="skip the parity leg")
     ap.add_argument("--no-reference-gpu", action="store_true", help="skip timing the reference's GPU backend")
@@ -491,6 +495,8 @@ def main():
             prop = api.Propagator(work / "config.json", device=local, lanes=args.lanes or None, split=split)
             if split and args.split_degree is not None:
                 prop.set_option("split_fp64_degree", args.split_degree)
+            prop.set_option("pair_sh", args.pair_sh)
+            prop.set_option("deep_registers", args.deep_registers)
             sync_barrier()
             if name == "fp64":
                 clocks.start()
@@ -512,6 +518,8 @@ def main():
             prop = api.Propagator(work / "config.json", device=local, lanes=args.lanes or None, split=split)
             if split and args.split_degree is not None:
                 prop.set_option("split_fp64_degree", args.split_degree)
+            prop.set_option("pair_sh", args.pair_sh)
+            prop.set_option("deep_registers", args.deep_registers)
             soa = np.ascontiguousarray(pop.states.T).reshape(-1)
             d_state = torch.from_numpy(soa.copy()).cuda()
             scratch = d_state.clone()

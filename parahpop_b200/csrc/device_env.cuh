@@ -5,8 +5,8 @@
 // the time and space-weather inputs of NRLMSISE-00) is evaluated once per
 // stage epoch into an EpochRecord.  Batches whose objects share one time grid
 // evaluate the records ahead of the step kernel (one per step and stage);
-// mixed batches evaluate them per object inside the step kernel with the same
-// device functions.
+// mixed batches (per-object time) interpolate them in time from a grid of
+// records at 30 s spacing.
 //
 // Reference behaviour restated (paths relative to the reference tree):
 //   Chebyshev ephemeris    third_party/parm/parm/interpolate/chebyshev/Interpolator.h:71-86,
@@ -19,6 +19,7 @@
 #pragma once
 #include <math.h>
 #include <stdint.h>
+#include <stddef.h>
 
 #include "nrl_fast.cuh"
 #include "tide_field.cuh"
@@ -99,6 +100,9 @@ struct EpochRecord {
     int nrlBlock, nrlValid;      // nrlValid: 1 / 0, or -1 = time inputs not evaluated yet (from et)
     int tideValid, pad;
 };
+// Fields 0 .. kInterpFields - 1 of a record (rotation to tide deltas) are the
+// ones the per-object-time force model interpolates in time.
+constexpr int kInterpFields = (int)(offsetof(EpochRecord, nrlSec) / sizeof(double));
 
 // NRLMSISE-00 time inputs of one epoch
 struct NrlTime {

@@ -1019,6 +1019,7 @@ Engine::~Engine() {
     for (GraphEntry& g : graphs_) cudaGraphExecDestroy(g.exec);
     if (captureStream_) cudaStreamDestroy(captureStream_);
     if (gridCache_) cudaFree(gridCache_);
+    if (pairCache_) cudaFree(pairCache_);
     for (auto& kv : tiles_) {
         cudaFree(kv.second.dTile);
         cudaFree(kv.second.dBlocks);
@@ -1384,8 +1385,15 @@ void Engine::buildRecordGrid(double lo, double hi, TimeGrid& g, cudaStream_t str
         gridCache_ = fresh;
         gridKLo_ = a;
         gridKHi_ = b;
+        if (pairCache_) cudaFree(pairCache_);
+        pairCache_ = nullptr;
+        PHOP_CUDA(cudaMalloc(&pairCache_, (size_t)(G - 1) * kInterpFields * sizeof(double2)));
+        launchRecordPairs(gridCache_, G, pairCache_, stream);
+        PHOP_CUDA(cudaGetLastError());
+        if (launches) *launches += 1;
     }
     g.grid = gridCache_;
+    g.gridPairs = pairCache_;
     g.gridH = H;
     g.gridBase = gridKLo_;
     g.gridN = (int)(gridKHi_ - gridKLo_ + 1);
@@ -1650,6 +1658,7 @@ void Engine::runKernel(int64_t n, double* dState, const double* dBc, const doubl
     p.step = g.step;
     p.unfinished = g.unfinished;
     p.grid = g.grid;
+    p.gridPairs = g.gridPairs;
     p.gridH = g.gridH;
     p.gridBase = g.gridBase;
     p.gridN = g.gridN;

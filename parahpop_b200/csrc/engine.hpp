@@ -213,6 +213,7 @@ public:
         double *cur = nullptr, *end = nullptr, *dt1 = nullptr, *step = nullptr;
         int* unfinished = nullptr;
         const EpochRecord* grid = nullptr;
+        const double2* gridPairs = nullptr;
         double gridH = 0.0;
         int64_t gridBase = 0;
         int gridN = 0;
@@ -244,6 +245,7 @@ private:
     std::vector<GraphEntry> graphs_;
     // epoch records of the per-object-time path at grid indices [gridKLo_, gridKHi_]
     EpochRecord* gridCache_ = nullptr;
+    double2* pairCache_ = nullptr;  // gridCache_ as value pairs (StepParams::gridPairs)
     int64_t gridKLo_ = 0, gridKHi_ = -1;
     cudaStream_t captureStream_ = nullptr;
     // autotuned launch shape of a batch class: lanes * 2 + (pairs ? 1 : 0)

@@ -67,6 +67,23 @@ void launchEpochRecords(const DevEnv& env, const double* epochs, int count, Epoc
     epochRecordsKernel<<<(count + threads - 1) / threads, threads, 0, stream>>>(env, epochs, count, out);
 }
 
+static __global__ void recordPairsKernel(const EpochRecord* __restrict__ grid, int64_t total, double2* __restrict__ pairs) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const int64_t k = i / kInterpFields;
+    const int f = (int)(i - k * kInterpFields);
+    const double* a = (const double*)(grid + k);
+    const double* b = (const double*)(grid + k + 1);
+    pairs[i] = make_double2(a[f], b[f]);
+}
+
+void launchRecordPairs(const EpochRecord* grid, int64_t count, double2* pairs, cudaStream_t stream) {
+    if (count < 2) return;
+    const int64_t total = (count - 1) * kInterpFields;
+    const int threads = 256;
+    recordPairsKernel<<<(unsigned)((total + threads - 1) / threads), threads, 0, stream>>>(grid, total, pairs);
+}
+
 int propagateSmemBytes(const StepParams& p, int lanes, int threads) {
     const int cpl = (6 + lanes - 1) / lanes;
     return (p.useSmemTile ? p.tileBytes : 0) + 13 * cpl * threads * (int)sizeof(double);

@@ -104,6 +104,10 @@ struct StepParams {
     // at multiples of gridH, so an object's interpolated records do not depend
     // on which other objects share its batch.
     const EpochRecord* grid;
+    // the same grid as value pairs: gridPairs[k * kInterpFields + f] = field f
+    // of records k and k + 1, so that a 4-point stencil reads each field with
+    // two 16-byte loads from two records instead of four 8-byte loads
+    const double2* gridPairs;
     double gridH;
     int64_t gridBase;
     int gridN;
@@ -145,6 +149,8 @@ __host__ __device__ constexpr int stepThreadBound(int lanes, int deep) {
 }
 
 void launchEpochRecords(const DevEnv& env, const double* epochs, int count, EpochRecord* out, cudaStream_t stream);
+// pairs[(k * kInterpFields + f)] = {field f of grid[k], of grid[k + 1]}, k < count - 1
+void launchRecordPairs(const EpochRecord* grid, int64_t count, double2* pairs, cudaStream_t stream);
 cudaError_t launchPropagate(const StepParams& p, int lanes, bool split, bool shared, int ctas, int threads,
                             cudaStream_t stream);
 int propagateSmemBytes(const StepParams& p, int lanes, int threads);

@@ -136,13 +136,14 @@ struct RecordRef {
 };
 
 struct RecordInterp {
-    const double* g;  // first record of the 4-point stencil, as doubles
+    // value pairs of the stencil's records i0, i0 + 1 (field f at g[f]); those
+    // of records i0 + 2, i0 + 3 follow 2 kInterpFields pairs later
+    const double2* g;
     double w0, w1, w2, w3;
     double et;        // the stage epoch (TDB s past J2000)
-    static constexpr int kStride = (int)(sizeof(EpochRecord) / sizeof(double));
     __device__ __forceinline__ RecordInterp partner(unsigned mask, int delta) const {
         RecordInterp o;
-        o.g = (const double*)__shfl_xor_sync(mask, (unsigned long long)g, delta);
+        o.g = (const double2*)__shfl_xor_sync(mask, (unsigned long long)g, delta);
         o.w0 = __shfl_xor_sync(mask, w0, delta);
         o.w1 = __shfl_xor_sync(mask, w1, delta);
         o.w2 = __shfl_xor_sync(mask, w2, delta);
@@ -151,8 +152,8 @@ struct RecordInterp {
         return o;
     }
     __device__ __forceinline__ double at(int off) const {
-        const double* b = g + off;
-        return w0 * b[0] + w1 * b[kStride] + w2 * b[2 * kStride] + w3 * b[3 * kStride];
+        const double2 x = g[off], y = g[2 * kInterpFields + off];
+        return w0 * x.x + w1 * x.y + w2 * y.x + w3 * y.y;
     }
     __device__ __forceinline__ double R(int i) const { return at((int)(offsetof(EpochRecord, R) / 8) + i); }
     __device__ __forceinline__ double W(int i) const { return at((int)(offsetof(EpochRecord, w) / 8) + i); }
@@ -1078,7 +1079,7 @@ static __device__ __forceinline__ RecordInterp recordFromGrid(const StepParams& 
             }
         w[j] = num / den;
     }
-    return RecordInterp{(const double*)(p.grid + i0), w[0], w[1], w[2], w[3], et};
+    return RecordInterp{p.gridPairs + i0 * kInterpFields, w[0], w[1], w[2], w[3], et};
 }
 
 // MAXT: the thread bound the kernel is compiled for, which sets its register
@@ -1091,7 +1092,7 @@ __global__ void __launch_bounds__(MAXT, 1) propagateKernel(const __grid_constant
     extern __shared__ __align__(128) unsigned char smem[];
     const Tile* tile = (const Tile*)p.tile;
     int kOffset = 0;
-    if (!SHARED_GRID && !p.grid) {  // per-object time needs the batch's record grid
+    if (!SHARED_GRID && !p.gridPairs) {  // per-object time needs the batch's record grid
         if (threadIdx.x == 0) atomicExch(p.errorFlag, 3);
         return;
     }

@@ -55,7 +55,7 @@ Server::~Server() {
     cudaSetDevice(engine_.device());
     if (stream_) cudaStreamSynchronize(stream_);
     for (void* p : {(void*)state_, (void*)bc_, (void*)ams_, (void*)cur_, (void*)end_, (void*)dt_, (void*)step_,
-                    (void*)unfinished_, (void*)active_, (void*)ctl_, (void*)grid_.grid})
+                    (void*)unfinished_, (void*)active_, (void*)ctl_, (void*)grid_.grid, (void*)grid_.gridPairs})
         if (p) cudaFree(p);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
@@ -193,16 +193,24 @@ void Server::ensureGrid(double lo, double hi) {
     EpochRecord* rec = nullptr;
     PHOP_SCUDA(cudaStreamSynchronize(stream_));
     if (grid_.grid) cudaFree((void*)grid_.grid);
+    if (grid_.gridPairs) cudaFree((void*)grid_.gridPairs);
     grid_.grid = nullptr;
+    grid_.gridPairs = nullptr;
     PHOP_SCUDA(cudaMalloc(&dT, (size_t)G * sizeof(double)));
     PHOP_SCUDA(cudaMalloc(&rec, (size_t)G * sizeof(EpochRecord)));
     PHOP_SCUDA(cudaMemcpyAsync(dT, ts.data(), (size_t)G * sizeof(double), cudaMemcpyHostToDevice, stream_));
     launchEpochRecords(engine_.denv_, dT, (int)G, rec, stream_);
     PHOP_SCUDA(cudaGetLastError());
+    double2* pairs = nullptr;
+    PHOP_SCUDA(cudaMalloc(&pairs, (size_t)(G - 1) * kInterpFields * sizeof(double2)));
+    launchRecordPairs(rec, G, pairs, stream_);
+    PHOP_SCUDA(cudaGetLastError());
+    ++stats_.launches;
     PHOP_SCUDA(cudaStreamSynchronize(stream_));
     cudaFree(dT);
     ++stats_.launches;
     grid_.grid = rec;
+    grid_.gridPairs = pairs;
     grid_.gridH = H;
     grid_.gridBase = a;
     grid_.gridN = (int)G;
@@ -282,6 +290,7 @@ int Server::step() {
         p.step = step_;
         p.unfinished = unfinished_;
         p.grid = grid_.grid;
+        p.gridPairs = grid_.gridPairs;
         p.gridH = grid_.gridH;
         p.gridBase = grid_.gridBase;
         p.gridN = grid_.gridN;
