@@ -151,9 +151,11 @@ struct RecordInterp {
         o.et = __shfl_xor_sync(mask, et, delta);
         return o;
     }
+    // explicit roundings: every copy of this code gives the same bits (the
+    // geopotential of lane-group pairs evaluates it for both objects)
     __device__ __forceinline__ double at(int off) const {
         const double2 x = g[off], y = g[2 * kInterpFields + off];
-        return w0 * x.x + w1 * x.y + w2 * y.x + w3 * y.y;
+        return __fma_rn(w3, y.y, __fma_rn(w2, y.x, __fma_rn(w1, x.y, __dmul_rn(w0, x.x))));
     }
     __device__ __forceinline__ double R(int i) const { return at((int)(offsetof(EpochRecord, R) / 8) + i); }
     __device__ __forceinline__ double W(int i) const { return at((int)(offsetof(EpochRecord, w) / 8) + i); }
@@ -410,7 +412,7 @@ template <> struct PairOf<double> {
     using type = D2;
     static __device__ __forceinline__ D2 make(double a, double b) { return D2{a, b}; }
     static __device__ __forceinline__ D2 fma(D2 a, D2 b, D2 c) { return D2{::fma(a.lo, b.lo, c.lo), ::fma(a.hi, b.hi, c.hi)}; }
-    static __device__ __forceinline__ D2 mul(D2 a, D2 b) { return D2{a.lo * b.lo, a.hi * b.hi}; }
+    static __device__ __forceinline__ D2 mul(D2 a, D2 b) { return D2{__dmul_rn(a.lo, b.lo), __dmul_rn(a.hi, b.hi)}; }
     static __device__ __forceinline__ void split(D2 a, double& lo, double& hi) {
         lo = a.lo;
         hi = a.hi;
@@ -421,16 +423,24 @@ template <> struct PairOf<double> {
 struct ShGeo {
     double sinPhi, cosPhi, sinL, cosL, alpha, invCos;
 };
+// The per-object parts of the pair geopotential (shGeo, shDiagStart,
+// shDiagStep, shLowColumn and the column sums) are written with explicit
+// roundings (__fma_rn, __dmul_rn, ...): each lane evaluates them for both
+// objects of its pair, in two copies of the code, and an object's result must
+// not depend on whether it is the pair's first or second object (that is, on
+// which other object shares its warp).  Plain expressions would leave each
+// copy's multiply-add contraction to the compiler.
 static __device__ __forceinline__ ShGeo shGeo(double x, double y, double z, double R) {
     ShGeo g;
-    const double rn = sqrt(x * x + y * y + z * z);
-    const double rho = sqrt(x * x + y * y);
-    g.sinPhi = z / rn;
-    g.cosPhi = rho / rn;
-    g.sinL = rho > 1e-14 ? y / rho : 0.0;
-    g.cosL = rho > 1e-14 ? x / rho : 1.0;
-    g.alpha = R / rn;
-    g.invCos = g.cosPhi == 0.0 ? 0.0 : 1.0 / g.cosPhi;
+    const double rho2 = __fma_rn(y, y, __dmul_rn(x, x));
+    const double rn = __dsqrt_rn(__fma_rn(z, z, rho2));
+    const double rho = __dsqrt_rn(rho2);
+    g.sinPhi = __ddiv_rn(z, rn);
+    g.cosPhi = __ddiv_rn(rho, rn);
+    g.sinL = rho > 1e-14 ? __ddiv_rn(y, rho) : 0.0;
+    g.cosL = rho > 1e-14 ? __ddiv_rn(x, rho) : 1.0;
+    g.alpha = __ddiv_rn(R, rn);
+    g.invCos = g.cosPhi == 0.0 ? 0.0 : __drcp_rn(g.cosPhi);
     return g;
 }
 
@@ -459,34 +469,34 @@ static __device__ __forceinline__ void shLowColumn(const StepParams& p, const Re
         const int ti = n * (n + 1) / 2 + mcol;
         double c = low->C[ti], s = low->S[ti];
         if (n <= 6 && tides) {
-            c += rec.dC(ti);
-            s += rec.dS(ti);
+            c = __dadd_rn(c, rec.dC(ti));
+            s = __dadd_rn(s, rec.dS(ti));
         }
         if (mcol == 0) s = 0.0;
-        const double q = an * Pn, qd = an * dPn, np1 = (double)(n + 1);
-        S[0] = fma(np1 * c, q, S[0]);
-        S[1] = fma(np1 * s, q, S[1]);
-        S[2] = fma(c, qd, S[2]);
-        S[3] = fma(s, qd, S[3]);
-        S[4] = fma(c, q, S[4]);
-        S[5] = fma(s, q, S[5]);
+        const double q = __dmul_rn(an, Pn), qd = __dmul_rn(an, dPn), np1 = (double)(n + 1);
+        S[0] = __fma_rn(__dmul_rn(np1, c), q, S[0]);
+        S[1] = __fma_rn(__dmul_rn(np1, s), q, S[1]);
+        S[2] = __fma_rn(c, qd, S[2]);
+        S[3] = __fma_rn(s, qd, S[3]);
+        S[4] = __fma_rn(c, q, S[4]);
+        S[5] = __fma_rn(s, q, S[5]);
         if (n < N) {
             const int tn = (n + 1) * (n + 2) / 2 + mcol;
             const double fa = low->a[tn], fb = low->b[tn];
             const double P2 = Pn1;
             Pn1 = Pn;
-            Pn = fa * g.sinPhi * Pn1 - fb * P2;
+            Pn = __fma_rn(__dmul_rn(fa, g.sinPhi), Pn1, -__dmul_rn(fb, P2));
             const double dP2 = dPn1;
             dPn1 = dPn;
-            dPn = fa * (g.sinPhi * dPn1 + g.cosPhi * Pn1) - fb * dP2;
+            dPn = __fma_rn(fa, __fma_rn(g.sinPhi, dPn1, __dmul_rn(g.cosPhi, Pn1)), -__dmul_rn(fb, dP2));
             anPrev = an;
-            an *= g.alpha;
+            an = __dmul_rn(an, g.alpha);
         }
     }
-    P = (T)(an * Pn);
-    P1 = (T)(anPrev * Pn1);
-    dP = (T)(an * dPn);
-    dP1 = (T)(anPrev * dPn1);
+    P = (T)__dmul_rn(an, Pn);
+    P1 = (T)__dmul_rn(anPrev, Pn1);
+    dP = (T)__dmul_rn(an, dPn);
+    dP1 = (T)__dmul_rn(anPrev, dPn1);
 }
 
 static __device__ __forceinline__ void shDiagStart(const StepParams& p, const ShGeo& g, int first, int W,
@@ -499,28 +509,28 @@ static __device__ __forceinline__ void shDiagStart(const StepParams& p, const Sh
     d.sML = 0.0;
     d.am = 1.0;
     for (int m = 0; m < first && m < M; ++m) {
-        const double ns = g.cosL * d.sML + g.sinL * d.cML;
-        const double nc = g.cosL * d.cML - g.sinL * d.sML;
+        const double ns = __fma_rn(g.cosL, d.sML, __dmul_rn(g.sinL, d.cML));
+        const double nc = __fma_rn(g.cosL, d.cML, -__dmul_rn(g.sinL, d.sML));
         d.sML = ns;
         d.cML = nc;
         const double cm = diagC[m + 1];
-        const double nP = cm * g.cosPhi * d.Pmm;
-        const double ndP = cm * (g.cosPhi * d.dPmm - g.sinPhi * d.Pmm);
+        const double nP = __dmul_rn(__dmul_rn(cm, g.cosPhi), d.Pmm);
+        const double ndP = __dmul_rn(cm, __fma_rn(g.cosPhi, d.dPmm, -__dmul_rn(g.sinPhi, d.Pmm)));
         d.Pmm = nP;
         d.dPmm = ndP;
-        d.am *= g.alpha;
+        d.am = __dmul_rn(d.am, g.alpha);
     }
     d.cosW1 = 1.0;
     d.cLam = 1.0;
     d.sLam = 0.0;
     d.aW = 1.0;
-    for (int t = 0; t < W - 1; ++t) d.cosW1 *= g.cosPhi;
+    for (int t = 0; t < W - 1; ++t) d.cosW1 = __dmul_rn(d.cosW1, g.cosPhi);
     for (int t = 0; t < W; ++t) {
-        const double ns = g.cosL * d.sLam + g.sinL * d.cLam;
-        const double nc = g.cosL * d.cLam - g.sinL * d.sLam;
+        const double ns = __fma_rn(g.cosL, d.sLam, __dmul_rn(g.sinL, d.cLam));
+        const double nc = __fma_rn(g.cosL, d.cLam, -__dmul_rn(g.sinL, d.sLam));
         d.sLam = ns;
         d.cLam = nc;
-        d.aW *= g.alpha;
+        d.aW = __dmul_rn(d.aW, g.alpha);
     }
 }
 
@@ -528,16 +538,31 @@ static __device__ __forceinline__ void shDiagStart(const StepParams& p, const Sh
 static __device__ __forceinline__ void shDiagStep(const double2* __restrict__ diagStep, const ShGeo& g, int m, int W,
                                                   ShDiag& d) {
     const double2 f = diagStep[m];
-    const double cosWp = d.cosW1 * g.cosPhi;
-    const double nP = f.x * cosWp * d.Pmm;
-    const double ndP = m == 0 ? -(double)W * g.sinPhi * d.cosW1 * f.x : f.y * cosWp * d.dPmm;
+    const double cosWp = __dmul_rn(d.cosW1, g.cosPhi);
+    const double nP = __dmul_rn(__dmul_rn(f.x, cosWp), d.Pmm);
+    const double ndP = m == 0 ? __dmul_rn(__dmul_rn(__dmul_rn(-(double)W, g.sinPhi), d.cosW1), f.x)
+                              : __dmul_rn(__dmul_rn(f.y, cosWp), d.dPmm);
     d.Pmm = nP;
     d.dPmm = ndP;
-    const double ns = d.cLam * d.sML + d.sLam * d.cML;
-    const double nc = d.cLam * d.cML - d.sLam * d.sML;
+    const double ns = __fma_rn(d.cLam, d.sML, __dmul_rn(d.sLam, d.cML));
+    const double nc = __fma_rn(d.cLam, d.cML, -__dmul_rn(d.sLam, d.sML));
     d.sML = ns;
     d.cML = nc;
-    d.am *= d.aW;
+    d.am = __dmul_rn(d.am, d.aW);
+}
+
+// one column's contribution (FP64 low sums S plus the tile part t) to an
+// object's (ar, aphi, alam) partial sums
+template <typename T>
+static __device__ __forceinline__ void columnSums(int mcol, const ShGeo& g, const ShDiag& d, const double S[6],
+                                                  const T t[6], double acc[3]) {
+    double c[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) c[k] = __dadd_rn(S[k], (double)t[k]);
+    const double mInv = __dmul_rn((double)mcol, g.invCos);
+    acc[0] = __dsub_rn(acc[0], __fma_rn(d.cML, c[0], __dmul_rn(d.sML, c[1])));
+    acc[1] = __dadd_rn(acc[1], __fma_rn(d.cML, c[2], __dmul_rn(d.sML, c[3])));
+    acc[2] = __dsub_rn(acc[2], __dmul_rn(mInv, __fma_rn(d.sML, c[4], -__dmul_rn(d.cML, c[5]))));
 }
 
 // Geopotential of the two objects of a pair of lane groups: the 2L lanes of
@@ -623,13 +648,8 @@ static __device__ __forceinline__ void shAccelPair(const StepParams& p, const ty
             Pr::split(Sds, t0[3], t1[3]);
             Pr::split(Spc, t0[4], t1[4]);
             Pr::split(Sps, t0[5], t1[5]);
-            const double mInv0 = (double)mcol * g0.invCos, mInv1 = (double)mcol * g1.invCos;
-            acc0[0] -= d0.cML * (S0[0] + (double)t0[0]) + d0.sML * (S0[1] + (double)t0[1]);
-            acc0[1] += d0.cML * (S0[2] + (double)t0[2]) + d0.sML * (S0[3] + (double)t0[3]);
-            acc0[2] -= mInv0 * (d0.sML * (S0[4] + (double)t0[4]) - d0.cML * (S0[5] + (double)t0[5]));
-            acc1[0] -= d1.cML * (S1[0] + (double)t1[0]) + d1.sML * (S1[1] + (double)t1[1]);
-            acc1[1] += d1.cML * (S1[2] + (double)t1[2]) + d1.sML * (S1[3] + (double)t1[3]);
-            acc1[2] -= mInv1 * (d1.sML * (S1[4] + (double)t1[4]) - d1.cML * (S1[5] + (double)t1[5]));
+            columnSums<T>(mcol, g0, d0, S0, t0, acc0);
+            columnSums<T>(mcol, g1, d1, S1, t1, acc1);
         }
         const int m = b * W + pj;
         if (m + W <= M) {
@@ -868,6 +888,16 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
     for (int bi = 0; bi < e.nbodies; ++bi) {
         const int fl = e.bodyFlags[bi];
         const bool isEarth = (bi == e.earthIndex);
+        // the body-fixed position (field, J2 and NRLMSISE-00 terms) and the
+        // body's position (direct attraction and radiation pressure), each
+        // read from the record once
+        double fb[3] = {0.0, 0.0, 0.0}, rb[3] = {0.0, 0.0, 0.0};
+        if ((fl & (kShape | kOblateness)) || ((fl & kAtmosphere) && e.hasNrl)) toBody(r, pos, fb);
+        if (((fl & kGravity) && !isEarth) || (fl & kRadiation)) {
+            rb[0] = r.body(bi, 0);
+            rb[1] = r.body(bi, 1);
+            rb[2] = r.body(bi, 2);
+        }
         if (fl & kGravity) {
             const double gm = e.bodyGm[bi];
             if (isEarth) {
@@ -879,7 +909,6 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
             } else {
                 // direct part per object; the indirect part (epoch-only) is
                 // the record's sum, added after the loop
-                const double rb[3] = {r.body(bi, 0), r.body(bi, 1), r.body(bi, 2)};
                 const double d0 = pos[0] - rb[0], d1 = pos[1] - rb[1], d2 = pos[2] - rb[2];
                 const double ird = rsqrt(d0 * d0 + d1 * d1 + d2 * d2);
                 const double f1 = -gm * (ird * ird * ird);
@@ -889,9 +918,7 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
             }
         }
         if (fl & kShape) {
-            double b[3];
-            toBody(r, pos, b);
-            const double bx = b[0], by = b[1], bz = b[2];
+            const double bx = fb[0], by = fb[1], bz = fb[2];
             double a[3];
             if constexpr (!std::is_same<T, double>::value) {
                 // split precision: objects below the split radius keep the
@@ -918,9 +945,7 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
             // J2 model in the body frame (J2.h:17-33,63-78), inside the sphere of influence
             const double rr = sqrt(pos[0] * pos[0] + pos[1] * pos[1] + pos[2] * pos[2]);
             if (rr <= e.bodySoi[bi]) {
-                double b[3];
-                toBody(r, pos, b);
-                const double bx = b[0], by = b[1], bz = b[2];
+                const double bx = fb[0], by = fb[1], bz = fb[2];
                 const double invr = 1.0 / sqrt(bx * bx + by * by + bz * bz);
                 const double invr2 = invr * invr;
                 const double invr5 = invr2 * invr2 * invr;
@@ -935,7 +960,6 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
             }
         }
         if (fl & kRadiation) {
-            const double rb[3] = {r.body(bi, 0), r.body(bi, 1), r.body(bi, 2)};
             const double dp[3] = {pos[0] - rb[0], pos[1] - rb[1], pos[2] - rb[2]};
             const double ird = rsqrt(dp[0] * dp[0] + dp[1] * dp[1] + dp[2] * dp[2]);
             double occ = 1.0;
@@ -972,9 +996,7 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
             }
         }
         if ((fl & kAtmosphere) && e.hasNrl) {
-            double fx[3];
-            toBody(r, pos, fx);
-            const double rho = nrlDensity<L>(e, r.nrlDeferred(), fx);
+            const double rho = nrlDensity<L>(e, r.nrlDeferred(), fb);
             const double w[3] = {r.W(0), r.W(1), r.W(2)};
             const double vr0 = vel[0] - (w[1] * pos[2] - w[2] * pos[1]);
             const double vr1 = vel[1] - (w[2] * pos[0] - w[0] * pos[2]);
