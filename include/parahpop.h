@@ -37,6 +37,29 @@ void paraHPOP_setLogLevel(int level);
  * reported in summary.json ("device" for parahpop_gpu). */
 int paraHPOP_run(int argc, char** argv, const char* backend);
 
+/* ---- resident environment across command-line runs (no counterpart in the
+ * reference, whose driver loads and uploads the environment in every run,
+ * src/common/driver.cpp:132-135) ------------------------------------------
+ * phop_resident_serve listens on the Unix-domain socket `socket_path` and
+ * serves command-line runs one at a time until phop_resident_stop: a run of
+ * paraHPOP_run with PARAHPOP_B200_SERVER=<socket_path> in its environment
+ * (CONFIG TARGETS OUTPUT form) sends its absolute paths and the
+ * PARAHPOP_B200_SPLIT / PARAHPOP_B200_LANES settings to the server, which
+ * runs the driver there -- same checks, outputs and messages -- with an
+ * environment kept on the device from an earlier run when the
+ * configuration's model section and the size and modification time of every
+ * data file it names are unchanged (up to four are kept, least recently used
+ * evicted), and answers with the exit status and the standard output and
+ * error text, which the client prints.  summary.json's environment_seconds
+ * is then the look-up.  A client that finds no server fails with
+ * "ParaHPOP: no resident environment server answers at <path>: <reason>".
+ * After a device error the server answers and stops (returns 1); it also
+ * returns 1 when another server answers at the path or it cannot listen.
+ * The command line: parahpop_gpu --serve SOCKET, parahpop_gpu --stop SOCKET. */
+int phop_resident_serve(const char* socket_path, const char* backend);
+/* Asks the server at `socket_path` to stop; 0 when it acknowledged. */
+int phop_resident_stop(const char* socket_path);
+
 /* Loads the configuration file's "model" section and its environment files
  * and makes them resident on `device` (the reference's
  * interface::config::Model + Environment::load + model upload,

@@ -3,19 +3,28 @@
 // The driver restates src/common/driver.cpp:57-186: the same arguments,
 // validation order, error texts, exit codes and output files.
 #include <cuda_runtime.h>
+#include <sys/socket.h>
+#include <sys/time.h>
+#include <sys/un.h>
+#include <unistd.h>
 
 #include <algorithm>
+#include <cerrno>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <filesystem>
 #include <fstream>
+#include <functional>
 #include <iomanip>
 #include <iostream>
 #include <limits>
 #include <memory>
 #include <set>
+#include <sstream>
 #include <string>
+#include <vector>
 
 #include "../../include/parahpop.h"
 #include "engine.hpp"
@@ -93,6 +102,22 @@ struct LoadedConfig {
     int64_t maxSteps = 0;
     int threads = 1;
 };
+
+// PARAHPOP_B200_SPLIT / PARAHPOP_B200_LANES: precision and lane count of the
+// command-line driver's propagation
+struct DriverOverrides {
+    int split = -1;  // -1: library default
+    int lanes = 0;   // 0: autotuned
+};
+
+DriverOverrides driverOverridesFromEnv() {
+    DriverOverrides ov;
+    if (const char* s = std::getenv("PARAHPOP_B200_SPLIT")) ov.split = std::atoi(s) != 0 ? 1 : 0;
+    if (const char* s = std::getenv("PARAHPOP_B200_LANES")) ov.lanes = std::atoi(s);
+    return ov;
+}
+
+using EngineSource = std::function<phop::Engine&(const LoadedConfig&)>;
 
 LoadedConfig readConfig(const fs::path& configPath, const char* backend) {
     LoadedConfig lc;
@@ -598,17 +623,26 @@ int phop_last_stats(const phop_context* ctx, phop_stats* out) {
     return 0;
 }
 
-int paraHPOP_run(int argc, char** argv, const char* backend) {
+}  // extern "C"
+
+namespace {
+
+// The driver proper, writing to `out` / `err`; `engineFor` supplies the
+// device-resident environment of the loaded configuration (a fresh load for
+// the in-process command line, a kept one for the resident server).
+int runDriver(const std::vector<std::string>& args, const char* backend, std::ostream& out, std::ostream& err,
+              const DriverOverrides& ov, const EngineSource& engineFor) {
     try {
-        if (argc == 2 && std::string(argv[1]) == "--help") {
-            std::cout << "Usage: " << argv[0] << " CONFIG.json TARGETS.json OUTPUT_DIRECTORY\n"
-                      << "Backend: " << backend << "; integrator: RKF78 fixed step\n";
+        const int argc = (int)args.size();
+        if (argc == 2 && args[1] == "--help") {
+            out << "Usage: " << args[0] << " CONFIG.json TARGETS.json OUTPUT_DIRECTORY\n"
+                << "Backend: " << backend << "; integrator: RKF78 fixed step\n";
             return 0;
         }
         if (argc != 4) throw std::runtime_error("Expected CONFIG.json TARGETS.json OUTPUT_DIRECTORY (or --help).");
-        const fs::path configPath = fs::absolute(argv[1]);
-        const fs::path inputPath = fs::absolute(argv[2]);
-        const fs::path outputPath = fs::absolute(argv[3]);
+        const fs::path configPath = fs::absolute(args[1]);
+        const fs::path inputPath = fs::absolute(args[2]);
+        const fs::path outputPath = fs::absolute(args[3]);
         for (const char* f : {"final_states.csv", "summary.json", "configuration_resolved.json"})
             if (fs::exists(outputPath / f))
                 throw std::runtime_error("Output exists; use a new directory: " + outputPath.string());
@@ -666,15 +700,13 @@ int paraHPOP_run(int argc, char** argv, const char* backend) {
                 throw std::runtime_error(std::string("No usable CUDA device: ") + cudaGetErrorString(status));
         }
         const auto environmentStart = std::chrono::steady_clock::now();
-        phop::HostEnvironment env;
-        phop::loadEnvironment(lc.config.at("model"), env);
-        phop::Engine engine(env, 0);
+        phop::Engine& engine = engineFor(lc);
         engine.assertCoverage(earliest, latest);
         const auto integrationStart = std::chrono::steady_clock::now();
         std::vector<double> finalEpoch, finalState;
         phop::RunOptions opt;
-        if (const char* s = std::getenv("PARAHPOP_B200_SPLIT")) opt.split = std::atoi(s) != 0;
-        if (const char* s = std::getenv("PARAHPOP_B200_LANES")) opt.lanes = std::atoi(s);
+        if (ov.split >= 0) opt.split = ov.split != 0;
+        opt.lanes = ov.lanes;
         engine.propagate(t, lc.maxSteps, opt, finalEpoch, finalState, nullptr);
         {
             const cudaError_t status = cudaDeviceSynchronize();
@@ -721,13 +753,275 @@ int paraHPOP_run(int argc, char** argv, const char* backend) {
         ss << sj << '\n';
         ss.close();
         if (!ss) throw std::runtime_error("Failed to write summary.");
-        std::cout << sj << '\n';
+        out << sj << '\n';
         return 0;
     } catch (const std::exception& e) {
-        std::cerr << "ParaHPOP: " << e.what() << '\n';
+        err << "ParaHPOP: " << e.what() << '\n';
         return 1;
     }
 }
+
+
+// ---- resident environment server -------------------------------------------
+// `parahpop_gpu --serve SOCKET` keeps environments resident on the device
+// between command-line runs: a client run (PARAHPOP_B200_SERVER=SOCKET
+// parahpop_gpu CONFIG TARGETS OUTPUT) sends its three absolute paths over a
+// Unix-domain socket, the server runs the driver with a kept environment
+// when the configuration's model section and the size and modification time
+// of every file it names are unchanged (a fresh load otherwise), writes the
+// output files itself and returns the exit status and the text of standard
+// output and error, which the client prints.  Requests are served one at a
+// time.  Messages: a 4-byte little-endian length, then JSON.
+
+constexpr size_t kResidentMaxMessage = size_t(64) << 20;
+constexpr size_t kResidentKeep = 4;  // environments kept (least recently used evicted)
+
+bool ioAll(int fd, void* buf, size_t n, bool writing) {
+    char* p = (char*)buf;
+    while (n > 0) {
+        const ssize_t k = writing ? ::send(fd, p, n, MSG_NOSIGNAL) : ::recv(fd, p, n, 0);
+        if (k < 0 && errno == EINTR) continue;
+        if (k <= 0) return false;
+        p += k;
+        n -= (size_t)k;
+    }
+    return true;
+}
+
+bool sendMessage(int fd, const std::string& text) {
+    if (text.size() > kResidentMaxMessage) return false;
+    unsigned char len[4];
+    for (int i = 0; i < 4; ++i) len[i] = (unsigned char)((text.size() >> (8 * i)) & 0xff);
+    return ioAll(fd, len, 4, true) && ioAll(fd, (void*)text.data(), text.size(), true);
+}
+
+bool receiveMessage(int fd, std::string& text) {
+    unsigned char len[4];
+    if (!ioAll(fd, len, 4, false)) return false;
+    size_t n = 0;
+    for (int i = 0; i < 4; ++i) n |= (size_t)len[i] << (8 * i);
+    if (n > kResidentMaxMessage) return false;
+    text.assign(n, '\0');
+    return n == 0 || ioAll(fd, &text[0], n, false);
+}
+
+// socket address of `path`; false when the path does not fit
+bool socketAddress(const std::string& path, sockaddr_un& addr) {
+    std::memset(&addr, 0, sizeof(addr));
+    addr.sun_family = AF_UNIX;
+    if (path.empty() || path.size() >= sizeof(addr.sun_path)) return false;
+    std::memcpy(addr.sun_path, path.c_str(), path.size());
+    return true;
+}
+
+int connectTo(const std::string& path, std::string& why) {
+    sockaddr_un addr;
+    if (!socketAddress(path, addr)) {
+        why = "socket path is empty or too long";
+        return -1;
+    }
+    const int fd = ::socket(AF_UNIX, SOCK_STREAM, 0);
+    if (fd < 0) {
+        why = std::strerror(errno);
+        return -1;
+    }
+    if (::connect(fd, (const sockaddr*)&addr, sizeof(addr)) != 0) {
+        why = std::strerror(errno);
+        ::close(fd);
+        return -1;
+    }
+    return fd;
+}
+
+// The data files a resolved model section names, with size and modification
+// time: part of the key under which the server keeps its environment.
+void fileStamps(const Value& v, std::string& key) {
+    if (v.isString()) {
+        std::error_code ec;
+        const fs::path p(v.asString());
+        if (p.is_absolute() && fs::is_regular_file(p, ec)) {
+            const auto size = fs::file_size(p, ec);
+            const auto mtime = fs::last_write_time(p, ec).time_since_epoch().count();
+            key += "\n" + p.string() + "|" + std::to_string(size) + "|" + std::to_string((long long)mtime);
+        }
+    } else if (v.isObject()) {
+        for (const auto& kv : v.members()) fileStamps(kv.second, key);
+    } else if (v.isArray()) {
+        for (const auto& item : v.items()) fileStamps(item, key);
+    }
+}
+
+struct KeptEnvironment {
+    std::string key;
+    std::unique_ptr<phop::Engine> engine;
+    uint64_t lastUse = 0;
+};
+
+int residentServe(const std::string& path, const char* backend) {
+    sockaddr_un addr;
+    if (!socketAddress(path, addr)) {
+        std::cerr << "ParaHPOP: socket path is empty or too long: " << path << '\n';
+        return 1;
+    }
+    {
+        std::string why;
+        const int probe = connectTo(path, why);
+        if (probe >= 0) {
+            ::close(probe);
+            std::cerr << "ParaHPOP: a server already answers at " << path << '\n';
+            return 1;
+        }
+    }
+    std::error_code ec;
+    if (fs::is_socket(path, ec)) fs::remove(path, ec);  // left behind by a server that did not stop cleanly
+    const int lfd = ::socket(AF_UNIX, SOCK_STREAM, 0);
+    if (lfd < 0 || ::bind(lfd, (const sockaddr*)&addr, sizeof(addr)) != 0 || ::listen(lfd, 16) != 0) {
+        std::cerr << "ParaHPOP: cannot listen at " << path << ": " << std::strerror(errno) << '\n';
+        if (lfd >= 0) ::close(lfd);
+        return 1;
+    }
+    std::cout << "ParaHPOP: resident environment server listening at " << path << std::endl;
+    std::vector<KeptEnvironment> kept;
+    uint64_t clock = 0;
+    int status = 0;
+    for (bool serving = true; serving;) {
+        const int fd = ::accept(lfd, nullptr, nullptr);
+        if (fd < 0) {
+            if (errno == EINTR) continue;
+            std::cerr << "ParaHPOP: accept failed: " << std::strerror(errno) << '\n';
+            status = 1;
+            break;
+        }
+        timeval tv{30, 0};  // a client that stops talking does not hold the server
+        ::setsockopt(fd, SOL_SOCKET, SO_RCVTIMEO, &tv, sizeof(tv));
+        std::string request;
+        Value reply = Value::object();
+        try {
+            if (!receiveMessage(fd, request)) throw std::runtime_error("incomplete request");
+            const Value req = phop::parseJson(request);
+            if (const Value* stop = req.find("stop"); stop && stop->asBool()) {
+                reply.set("status", Value::integer(0));
+                reply.set("stdout", Value::string(""));
+                reply.set("stderr", Value::string(""));
+                serving = false;
+            } else {
+                std::vector<std::string> args{"parahpop_gpu"};
+                for (const Value& a : req.at("args").items()) args.push_back(a.asString());
+                DriverOverrides ov;
+                ov.split = (int)req.at("split").asInt();
+                ov.lanes = (int)req.at("lanes").asInt();
+                std::ostringstream out, err;
+                const int rc = runDriver(args, backend, out, err, ov, [&](const LoadedConfig& lc) -> phop::Engine& {
+                    const Value& model = lc.config.at("model");
+                    std::string key = model.dump();
+                    fileStamps(model, key);
+                    for (auto& k : kept)
+                        if (k.key == key) {
+                            k.lastUse = ++clock;
+                            return *k.engine;
+                        }
+                    phop::HostEnvironment env;
+                    phop::loadEnvironment(model, env);
+                    if (kept.size() >= kResidentKeep) {
+                        auto lru = std::min_element(kept.begin(), kept.end(),
+                                                    [](const auto& a, const auto& b) { return a.lastUse < b.lastUse; });
+                        kept.erase(lru);
+                    }
+                    kept.push_back(KeptEnvironment{key, std::make_unique<phop::Engine>(env, 0), ++clock});
+                    return *kept.back().engine;
+                });
+                reply.set("status", Value::integer(rc));
+                reply.set("stdout", Value::string(out.str()));
+                reply.set("stderr", Value::string(err.str()));
+                // a device error leaves the context unusable: answer, then stop
+                const cudaError_t dev = cudaDeviceSynchronize();
+                if (dev != cudaSuccess && dev != cudaErrorNoDevice && dev != cudaErrorInsufficientDriver) {
+                    std::cerr << "ParaHPOP: device error, server stops: " << cudaGetErrorString(dev) << '\n';
+                    status = 1;
+                    serving = false;
+                }
+            }
+        } catch (const std::exception& e) {
+            reply.set("status", Value::integer(1));
+            reply.set("stdout", Value::string(""));
+            reply.set("stderr", Value::string(std::string("ParaHPOP: ") + e.what() + "\n"));
+        }
+        sendMessage(fd, reply.dump());
+        ::close(fd);
+    }
+    ::close(lfd);
+    fs::remove(path, ec);
+    kept.clear();
+    return status;
+}
+
+int residentClient(const std::string& path, const std::vector<std::string>& args, const DriverOverrides& ov) {
+    std::string why;
+    const int fd = connectTo(path, why);
+    if (fd < 0) {
+        std::cerr << "ParaHPOP: no resident environment server answers at " << path << ": " << why << '\n';
+        return 1;
+    }
+    Value req = Value::object();
+    Value a = Value::array();
+    for (size_t i = 1; i < args.size(); ++i) a.push(Value::string(fs::absolute(args[i]).string()));
+    req.set("args", a);
+    req.set("split", Value::integer(ov.split));
+    req.set("lanes", Value::integer(ov.lanes));
+    std::string text;
+    const bool ok = sendMessage(fd, req.dump()) && receiveMessage(fd, text);
+    ::close(fd);
+    if (!ok) {
+        std::cerr << "ParaHPOP: the resident environment server at " << path << " did not answer.\n";
+        return 1;
+    }
+    try {
+        const Value reply = phop::parseJson(text);
+        std::cout << reply.at("stdout").asString();
+        std::cerr << reply.at("stderr").asString();
+        return (int)reply.at("status").asInt();
+    } catch (const std::exception& e) {
+        std::cerr << "ParaHPOP: malformed answer from the resident environment server: " << e.what() << '\n';
+        return 1;
+    }
+}
+
+int residentStop(const std::string& path) {
+    std::string why;
+    const int fd = connectTo(path, why);
+    if (fd < 0) return 1;
+    Value req = Value::object();
+    req.set("stop", Value::boolean(true));
+    std::string text;
+    const bool ok = sendMessage(fd, req.dump()) && receiveMessage(fd, text);
+    ::close(fd);
+    return ok ? 0 : 1;
+}
+
+
+}  // namespace
+
+extern "C" {
+
+int paraHPOP_run(int argc, char** argv, const char* backend) {
+    std::vector<std::string> args(argv, argv + argc);
+    const DriverOverrides ov = driverOverridesFromEnv();
+    const char* server = std::getenv("PARAHPOP_B200_SERVER");
+    if (server && *server && argc == 4) return residentClient(server, args, ov);
+    std::unique_ptr<phop::Engine> engine;
+    return runDriver(args, backend, std::cout, std::cerr, ov, [&](const LoadedConfig& lc) -> phop::Engine& {
+        phop::HostEnvironment env;
+        phop::loadEnvironment(lc.config.at("model"), env);
+        engine = std::make_unique<phop::Engine>(env, 0);
+        return *engine;
+    });
+}
+
+int phop_resident_serve(const char* socket_path, const char* backend) {
+    return residentServe(socket_path ? socket_path : "", backend ? backend : "device");
+}
+
+int phop_resident_stop(const char* socket_path) { return residentStop(socket_path ? socket_path : ""); }
 
 int phop_nrlmsise00_density(int device, int64_t n, const double* inputs, int lanes, double* out_rho) {
     try {
