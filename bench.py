@@ -55,11 +55,12 @@ def sh_flops_per_object_step(degree: int) -> float:
 
 # DRAM bytes (read + write) per object-step of the step kernel, from ncu
 # captures (profiles/): the state is read once and written once per launch
-# (~100 B per object); the rest is local memory (register spills) evicted
-# from L2.  c3: the split form's kernel at two lanes, 10^5 objects x 24 steps
-# (7.60 + 12.10 GB over 2,391,620 object-steps); the other workloads have no
-# capture of the current kernel (null).
-NCU_BYTES_PER_OBJECT_STEP = {"c3": (7.604360e9 + 12.100122e9) / 2_391_620, "c1": None, "c2": None}
+# (~100 B per object); the rest is local memory written back from L2 and the
+# epoch-record grid.  c3: the split form's kernel at two lanes with lane-group
+# pairs and the 256-thread bound, 10^5 objects x 24 steps (8.77 + 5.82 GB over
+# 2,391,620 object-steps); the other workloads have no capture of the current
+# kernel (null).
+NCU_BYTES_PER_OBJECT_STEP = {"c3": (8.769621e9 + 5.815049e9) / 2_391_620, "c1": None, "c2": None}
 
 
 def dist_env():
@@ -650,8 +651,9 @@ def main():
                          "unit": "TFLOP/s", "frac": achieved / peak if peak > 0 else None,
                          "traffic": per_os * steps_per_launch if per_os else None,
                          "traffic_note": "DRAM read+write bytes per launch: ncu capture of the split kernel at two "
-                                         "lanes (8.2 KB per object-step, almost all local-memory spill traffic) "
-                                         "times the object-steps of one timed launch" if per_os else None,
+                                         "lanes, lane-group pairs, 256-thread bound (6.1 KB per object-step: "
+                                         "local-memory write-back and epoch-record reads) times the object-steps of "
+                                         "one timed launch" if per_os else None,
                          "peak_source": peak_note,
                          "numerator": f"29 FLOP x (N+1)(N+2)/2 SH terms x 13 stages per object-step, N = {degree}"},
             "cpu_baseline": cpu,
