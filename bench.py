@@ -621,7 +621,7 @@ def main():
         flops = sh_flops_per_object_step(degree) * r["object_steps"]
         achieved = flops / (r["kernel_ms"] * 1e-3) * 1e-12
         if head == "split":
-            low = args.split_degree or 20
+            low = args.split_degree or (24 if degree > 80 else 20)  # the library's default by field degree
             f64 = 13.0 * SH_FLOP_PER_TERM * sh_terms(low)
             f32 = sh_flops_per_object_step(degree) - f64
             peak = sh_flops_per_object_step(degree) / (f64 / fp64_peak + f32 / fp32_peak)
@@ -641,7 +641,7 @@ def main():
                 f"steps (the K timed steps cover each object's first {K * args.slice_steps} steps)"
                 if args.workload == "c3" else f"; {K} steps of {args.hours / K:.2f} h"),
                        "objects_per_gpu": n_obj, "degree": degree, "precision": head,
-                       "split_fp64_degree": args.split_degree or 20, "lanes": h["lanes"],
+                       "split_fp64_degree": args.split_degree or (24 if degree > 80 else 20), "lanes": h["lanes"],
                        "l2": "flushed (256 MiB write) before every timed step",
                        "parallelism": f"object sharding x{ws}, no collective"},
             "forms": {"fp64": forms["fp64"], "split": forms["split"],

@@ -164,10 +164,10 @@ int phop_propagate_device_noalloc(phop_context* ctx, int64_t n, double* d_states
  *   "lanes"    lanes per object, 0 = autotuned, else 1, 2, 4, 8 or 16
  *   "split"    0 = plain FP64, 1 = split precision (FP32 for geopotential
  *              degrees above "split_fp64_degree", FP64 elsewhere)
- *   "split_fp64_degree"  split precision: degrees n <= this (8 .. 24,
- *              default 20) stay FP64; FP32 rounding in the recursion of the
- *              strongest terms (n <= 20) costs more final-position error
- *              than their FP32 speed gains
+ *   "split_fp64_degree"  split precision: degrees n <= this (8 .. 24)
+ *              stay FP64; default 20, or 24 for fields above degree 80
+ *              (FP32 rounding in the recursion of the strongest terms costs
+ *              more final-position error than their FP32 speed gains)
  *   "threads"  threads per CTA (multiple of 32, <= 512); a launch uses at
  *              most what the chosen kernel instantiation accepts (its
  *              maxThreadsPerBlock: 256 at 1 lane, 320 at 2, 384 above) and

@@ -1453,17 +1453,21 @@ void Engine::launchStepGraph(const StepParams& p, const LaunchShape& shape, cons
 }
 
 // FP64 low part of each column: n <= 8 in the FP64 form, n <= the option's
-// degree (default 20) in split precision.
-int lowDegreeFor(const RunOptions& opt) {
+// degree in split precision.  Its default follows the field's degree: the
+// FP32 rounding of the recursion accumulates over more terms in a larger
+// field (24 h, 10^5 LEO objects at degree 120: 11.5 mm max with n <= 20 in
+// FP64, 8.3 mm with n <= 24; degree 70: 6.4 mm with n <= 20).
+int lowDegreeFor(const RunOptions& opt, int fieldDegree) {
     if (!opt.split) return kLowDeg;
-    const int d = opt.splitFp64Degree;
+    const int d = opt.splitFp64Degree > 0 ? opt.splitFp64Degree
+                                          : (fieldDegree > 80 ? kSplitFp64DegreeHigh : kSplitFp64Degree);
     return d < kLowDeg ? kLowDeg : (d > kLowMax ? kLowMax : d);
 }
 
 // Host side of a launch: coefficient tile, shared-memory split and grid.
 Engine::LaunchShape Engine::prepareStep(StepParams& p, int L, const RunOptions& opt, bool shared) {
     if (L != 1 && L != 2 && L != 4 && L != 8 && L != 16) throw std::runtime_error("lanes must be 1, 2, 4, 8 or 16");
-    const int lowDeg = lowDegreeFor(opt);
+    const int lowDeg = lowDegreeFor(opt, host_.shDegree);
     // lane-group pairs share the tile (built for 2L lanes); not with the
     // split form's FP64 floor, whose low objects take the FP64 tile of L lanes
     const bool pair = opt.pairSh < 0 ? L <= 4 : opt.pairSh != 0;

@@ -124,7 +124,7 @@ struct RunOptions {
     bool ordered = true;  // process objects in order of geocentric radius
     bool graph = true;    // launch the step as a cached CUDA graph
     double splitFloorKm = 0.0;  // split precision: FP64 tile part below this height over the field radius
-    int splitFp64Degree = kSplitFp64Degree;  // split precision: degrees n <= this stay FP64 (8 .. kLowMax)
+    int splitFp64Degree = 0;  // split precision: degrees n <= this stay FP64 (8 .. kLowMax); 0 = by field degree
     int tileSmem = -1;    // coefficient tile in shared memory: -1 when it fits, 0 never (read through L1)
     int mixedOrder = 0;   // mixed batches inside a step-count bucket: 0 radius, 1 epoch, 2 drag band + epoch
     int tileWaitTest = 0; // test of the tile-staging time-out: the barrier is armed, no copy issued
@@ -140,7 +140,7 @@ struct RunOptions {
 };
 
 // degrees n <= this of every column run in FP64 from the LowTable
-int lowDegreeFor(const RunOptions& opt);
+int lowDegreeFor(const RunOptions& opt, int fieldDegree);
 
 class Engine {
 public:

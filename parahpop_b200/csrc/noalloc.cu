@@ -199,7 +199,7 @@ void Engine::propagateNoAlloc(int64_t n, double* dState, const double* dBc, cons
     EpochRecord* dRec = (EpochRecord*)p;
     // coefficient tile (host copy kept by the engine) into the array
     const int L = opt.lanes > 0 ? opt.lanes : autoLanes(n);
-    const int lowDeg = lowDegreeFor(opt);
+    const int lowDeg = lowDegreeFor(opt, host_.shDegree);
     const HostTile& ht = hostTileFor(L, opt.split, lowDeg);
     if (ht.bytes.size() > kTileBytes || ht.blocks.size() * sizeof(int2) > kBlockBytes)
         throw std::runtime_error("coefficient tile exceeds the allocation-free entry point's 512 KiB limit");

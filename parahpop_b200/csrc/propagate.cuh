@@ -49,9 +49,11 @@ namespace phop {
 // Each column's low degrees run in FP64 from the LowTable (with the epoch's
 // tide deltas for n <= 6); the tile holds the degrees above.  The FP64 form
 // starts its tile at n = 9; split precision keeps n <= splitFp64Degree
-// (default 20, at most kLowMax) in FP64 and runs the rest in FP32.
+// (by default 20, or 24 for fields above degree 80; at most kLowMax) in FP64
+// and runs the rest in FP32.
 constexpr int kLowDeg = 8;                                  // FP64 form: n <= 8 from the LowTable
-constexpr int kSplitFp64Degree = 20;                        // split form default
+constexpr int kSplitFp64Degree = 20;                        // split form default up to degree 80
+constexpr int kSplitFp64DegreeHigh = 24;                    // split form default above degree 80
 constexpr int kLowMax = 24;                                 // largest FP64 low part
 constexpr int kLowTri = (kLowMax + 2) * (kLowMax + 3) / 2;  // factor triangle up to n = kLowMax + 1
 

@@ -256,12 +256,12 @@ static __device__ __forceinline__ void shAccel(const StepParams& p, const typena
             const int nEnd = N < lowDeg ? N : lowDeg;
             for (int n = mcol; n <= nEnd; ++n) {
                 const int ti = n * (n + 1) / 2 + mcol;
-                double c = low->C[ti], s = low->S[ti];
+                // order 0 has no sine term: nothing to read for it
+                double c = low->C[ti], s = mcol == 0 ? 0.0 : low->S[ti];
                 if (n <= 6 && tides) {
                     c += rec.dC(ti);
-                    s += rec.dS(ti);
+                    if (mcol != 0) s += rec.dS(ti);
                 }
-                if (mcol == 0) s = 0.0;
                 const double q = an * Pn, qd = an * dPn, np1 = (double)(n + 1);
                 SA0 = fma(np1 * c, q, SA0);
                 SA1 = fma(np1 * s, q, SA1);
@@ -467,12 +467,12 @@ static __device__ __forceinline__ void shLowColumn(const StepParams& p, const Re
     for (int k = 0; k < 6; ++k) S[k] = 0.0;
     for (int n = mcol; n <= nEnd; ++n) {
         const int ti = n * (n + 1) / 2 + mcol;
-        double c = low->C[ti], s = low->S[ti];
+        // order 0 has no sine term: nothing to read for it
+        double c = low->C[ti], s = mcol == 0 ? 0.0 : low->S[ti];
         if (n <= 6 && tides) {
             c = __dadd_rn(c, rec.dC(ti));
-            s = __dadd_rn(s, rec.dS(ti));
+            if (mcol != 0) s = __dadd_rn(s, rec.dS(ti));
         }
-        if (mcol == 0) s = 0.0;
         const double q = __dmul_rn(an, Pn), qd = __dmul_rn(an, dPn), np1 = (double)(n + 1);
         S[0] = __fma_rn(__dmul_rn(np1, c), q, S[0]);
         S[1] = __fma_rn(__dmul_rn(np1, s), q, S[1]);
