@@ -130,6 +130,8 @@ class _Env(C.Structure):
         ("rot_kind", C.c_int), ("rot_nint", C.c_int), ("rot_pdeg", C.c_int), ("rot_ecliptic", C.c_int),
         ("iau_deg", C.c_int * 3), ("iau_np", C.c_int * 3), ("iau_bary_offset", C.c_int), ("iau_np_deg", C.c_int),
         ("iau_np_angles", C.c_int),
+        ("frame_data", C.POINTER(C.c_double) * 12), ("frame_deg", (C.c_int * 3) * 12),
+        ("frame_np", (C.c_int * 3) * 12), ("frame_bary_offset", C.c_int * 12), ("frame_np_deg", C.c_int * 12),
     ]
 
 
@@ -313,7 +315,7 @@ def load_environment(config_path) -> Environment:
     # Earth frames: ITRF93 (binary Chebyshev angles, target 3000) and the
     # IERS2000 model unit (3001); bodies.Earth.orientation picks one, else
     # the unique loaded one (interface naming/orientations Resolver.h)
-    frames, barys = {}, {}
+    frames, barys, other_iau = {}, {}, {}
     for f in envc.get("orientations", []):
         for u in brie_units(cbor_loads(P(f).read_bytes()), ORIENTATION_INT_KEYS):
             md = u["metadata"]
@@ -328,6 +330,8 @@ def load_environment(config_path) -> Environment:
             target = md["frameClassID"] if kind == 3 else md["target"]
             if target in (3000, 3001, 399):
                 frames[target] = (kind, md, u["data"])
+            elif kind == 1:
+                other_iau.setdefault(target, (md, u["data"]))
     want = {"ITRF93": 3000, "ITRF": 3000, "EARTH_FIXED": 3000, "ITRF_IERS2000": 3001, "ITRF_IPF": 3001,
             "ITRF_NATIVE": 3001, "EARTH_BODY_FIXED": 399, "IAU_EARTH": 399}.get(
                 str(earth_orientation).upper()) if earth_orientation else None
@@ -357,6 +361,22 @@ def load_environment(config_path) -> Environment:
                 e.iau_bary_offset = len(data)
                 e.iau_np_deg, e.iau_np_angles = bmd["pdeg_np"] + 1, bmd["num_np_angles"]
                 e.rot_data = _dp(hold(np.array(list(data) + list(bdata), dtype=np.float64)))
+    # bodies other than the Earth with the J2 model: their IAU body models
+    for bi, r in enumerate(rows):
+        e.frame_bary_offset[bi] = -1
+        if r[0] == 399 or not (r[3] & F_OBLATENESS) or r[0] not in other_iau:
+            continue
+        md, data = other_iau[r[0]]
+        vals = list(data)
+        for k, name in enumerate(("ra", "dec", "pm")):
+            e.frame_deg[bi][k] = md["pdeg_" + name] + 1
+            e.frame_np[bi][k] = md["num_np_terms_" + name]
+        if max(md["num_np_terms_" + n] for n in ("ra", "dec", "pm")) > 0 and md["barycenter"] in barys:
+            bmd, bdata = barys[md["barycenter"]]
+            e.frame_bary_offset[bi] = len(vals)
+            e.frame_np_deg[bi] = bmd["pdeg_np"] + 1
+            vals += list(bdata)
+        e.frame_data[bi] = _dp(hold(np.array(vals, dtype=np.float64)))
     # atmosphere
     if atm is not None:
         recs = []

@@ -129,6 +129,11 @@ typedef struct {
     // polynomials appended to rot_data (offset -1: none)
     int iau_deg[3], iau_np[3];
     int iau_bary_offset, iau_np_deg, iau_np_angles;
+    // per body (index as body_id): the IAU body model of a body other than
+    // the Earth, for its J2 model (data NULL: none), laid out as rot_data of
+    // kind 1 with its barycentric angles at frame_bary_offset (-1: none)
+    const double* frame_data[12];
+    int frame_deg[12][3], frame_np[12][3], frame_bary_offset[12], frame_np_deg[12];
 } OracleEnv;
 
 }  // extern "C"
@@ -334,8 +339,8 @@ void binaryEarthRotation(const OracleEnv& e, double t, double R[9], V3* w) {
 // polynomials in Julian centuries, PM in days (degrees), with the
 // nutation-precession series over the barycentric angle polynomials; angles
 // mod 360, then as for a binary unit.
-void iauEarthRotation(const OracleEnv& e, double t, double R[9], V3* w) {
-    const double* d = e.rot_data;
+void iauRotation(const double* d, const int* degs, const int* nps, int baryOffset, int npDeg, double t, double R[9],
+                 V3* w) {
     const double cy = 3155760000.0, dy = 86400.0, deg = M_PI / 180.0;
     const double T = t / cy, D = t / dy;
     auto poly = [](const double* c, int n, double x, double* der) {
@@ -349,16 +354,16 @@ void iauEarthRotation(const OracleEnv& e, double t, double R[9], V3* w) {
         *der = dv;
         return v;
     };
-    const int n0 = e.iau_deg[0], n1 = e.iau_deg[1], n2 = e.iau_deg[2];
+    const int n0 = degs[0], n1 = degs[1], n2 = degs[2];
     double r0, r1, r2;
     double ang[3] = {poly(d, n0, T, &r0), poly(d + n0, n1, T, &r1), poly(d + n0 + n1, n2, D, &r2)};
     double rate[3] = {r0 / cy, r1 / cy, r2 / dy};
-    if (e.iau_bary_offset >= 0) {
+    if (baryOffset >= 0) {
         const double* amp = d + n0 + n1 + n2;
         for (int comp = 0; comp < 3; ++comp) {
-            for (int i = 0; i < e.iau_np[comp]; ++i) {
+            for (int i = 0; i < nps[comp]; ++i) {
                 double dp;
-                const double a = poly(d + e.iau_bary_offset + (int64_t)i * e.iau_np_deg, e.iau_np_deg, T, &dp);
+                const double a = poly(d + baryOffset + (int64_t)i * npDeg, npDeg, T, &dp);
                 if (comp == 1) {
                     ang[comp] += amp[i] * cos(a * deg);
                     rate[comp] += -amp[i] * sin(a * deg) * dp * deg / cy;
@@ -367,11 +372,15 @@ void iauEarthRotation(const OracleEnv& e, double t, double R[9], V3* w) {
                     rate[comp] += amp[i] * cos(a * deg) * dp * deg / cy;
                 }
             }
-            amp += e.iau_np[comp];
+            amp += nps[comp];
         }
     }
     eulerRotation(fmod(ang[0], 360.0) * deg, fmod(ang[1], 360.0) * deg, fmod(ang[2], 360.0) * deg, rate[0] * deg,
                   rate[1] * deg, rate[2] * deg, false, R, w);
+}
+
+void iauEarthRotation(const OracleEnv& e, double t, double R[9], V3* w) {
+    iauRotation(e.rot_data, e.iau_deg, e.iau_np, e.iau_bary_offset, e.iau_np_deg, t, R, w);
 }
 
 // passive Z-X-Z rotation (pi/2 + RA, pi/2 - Dec, PM) [then the ICRF ->
@@ -947,14 +956,25 @@ V3 acceleration(const OracleEnv& e, const ShFactors& F, V3 pos, V3 vel, double e
             acc = acc + matT(R, shBodyFixed(e, F, mat(R, dp)));
         }
         if ((fl & F_OBLATENESS) && !(fl & F_SHAPE)) {
-            // J2 model (PrivateAccelerations.h:88-97, J2.h:63-78)
+            // J2 model (PrivateAccelerations.h:88-97, J2.h:63-78), in the
+            // body's own frame: the Earth's, or another body's IAU model
             const V3 dp = (body != kEarth) ? pos - bodyPos : pos;
             if (norm(dp) <= e.body_soi[bi]) {
-                if (!haveRot) {
-                    earthRotation(e, et, R, &w);
-                    haveRot = true;
+                if (body != kEarth) {
+                    double Rb[9];
+                    V3 wb;
+                    iauRotation(e.frame_data[bi], e.frame_deg[bi], e.frame_np[bi], e.frame_bary_offset[bi],
+                                e.frame_np_deg[bi], et, Rb, &wb);
+                    acc = acc + matT(Rb, j2BodyFixed(mat(Rb, dp), e.body_gm_const[bi], e.body_j2[bi],
+                                                     e.body_radius[bi]));
+                } else {
+                    if (!haveRot) {
+                        earthRotation(e, et, R, &w);
+                        haveRot = true;
+                    }
+                    acc = acc + matT(R, j2BodyFixed(mat(R, dp), e.body_gm_const[bi], e.body_j2[bi],
+                                                    e.body_radius[bi]));
                 }
-                acc = acc + matT(R, j2BodyFixed(mat(R, dp), e.body_gm_const[bi], e.body_j2[bi], e.body_radius[bi]));
             }
         }
         if (fl & F_RADIATION) {

@@ -28,6 +28,7 @@ namespace phop {
 
 constexpr int kMaxBodies = 12;
 constexpr int kMaxChain = 4;
+constexpr int kMaxPoles = 2;  // bodies other than the Earth with the J2 model
 constexpr int kTideTri = 28;  // n <= 6 triangle, index n(n+1)/2 + m
 
 constexpr int kMaxExpBands = 16;
@@ -86,6 +87,16 @@ struct DevEnv {
     int eopN;
     double eopFirstMjd;
     const double* eop;  // 4 x n component-major
+    // bodies other than the Earth with the J2 model: each body's record
+    // slot for its polar axis (-1: none) and its IAU body model (the
+    // reference's default orientation target, the body's own NAIF id)
+    int poleSlot[kMaxBodies];
+    int nPoles;
+    int poleDeg[kMaxPoles][3], poleNp[kMaxPoles][3];
+    int poleData[kMaxPoles];    // offset of the model's coefficients in poleCoef
+    int poleBary[kMaxPoles];    // offset of its barycentric angle polynomials from there (-1: none)
+    int poleNpDeg[kMaxPoles];
+    const double* poleCoef;
 };
 
 struct EpochRecord {
@@ -95,6 +106,7 @@ struct EpochRecord {
     double indirect[3];          // sum over third bodies of -gm rb / |rb|^3 (km/s^2): epoch-only
     double dC[kTideTri];         // tide coefficient deltas, field units
     double dS[kTideTri];
+    double pole[kMaxPoles][3];   // polar (body z) axes of the J2 bodies other than the Earth, inertial
     double nrlSec, nrlGast;      // UTC seconds of day, apparent sidereal time (h)
     double et;                   // the record's epoch, TDB seconds past J2000
     int nrlBlock, nrlValid;      // nrlValid: 1 / 0, or -1 = time inputs not evaluated yet (from et)
@@ -300,8 +312,8 @@ static __device__ void binaryEarthRotation(const DevEnv& e, double t, double R[9
 // plus sum_i a_i sin(p_i(T)) (RA, PM) / a_i cos(p_i(T)) (Dec) over the
 // body's barycentric angle polynomials p_i (degrees, centuries); the angles
 // reduced mod 360, then the rotation and rate as for a binary unit.
-static __device__ void iauEarthRotation(const DevEnv& e, double t, double R[9], double w[3]) {
-    const double* d = e.rotData;
+static __device__ void iauRotation(const double* d, const int degs[3], const int nps[3], int baryOffset, int npDeg,
+                                   double t, double R[9], double w[3]) {
     const double secToCenturies = 3155760000.0, secToDays = 86400.0, deg = M_PI / 180.0;
     const double T = t / secToCenturies, D = t / secToDays;
     auto horner = [](const double* c, int n, double x) {
@@ -314,22 +326,22 @@ static __device__ void iauEarthRotation(const DevEnv& e, double t, double R[9], 
         for (int i = 0; i + 1 < n; ++i) r = fma(r, x, c[n - 1 - i] * (double)(n - 1 - i));
         return r;
     };
-    const int nRa = e.iauDeg[0], nDec = e.iauDeg[1], nPm = e.iauDeg[2];
+    const int nRa = degs[0], nDec = degs[1], nPm = degs[2];
     double ang[3] = {horner(d, nRa, T), horner(d + nRa, nDec, T), horner(d + nRa + nDec, nPm, D)};
     double rate[3] = {hornerRate(d, nRa, T) / secToCenturies, hornerRate(d + nRa, nDec, T) / secToCenturies,
                       hornerRate(d + nRa + nDec, nPm, D) / secToDays};
-    if (e.iauBaryOffset >= 0) {
+    if (baryOffset >= 0) {
         const double* amp = d + nRa + nDec + nPm;
-        const double* bary = d + e.iauBaryOffset;
+        const double* bary = d + baryOffset;
         for (int comp = 0; comp < 3; ++comp) {
             const bool isSin = comp != 1;
             double sum = 0.0, dsum = 0.0;
-            for (int i = 0; i < e.iauNp[comp]; ++i) {
-                const double* p = bary + (int64_t)i * e.iauNpDeg;
+            for (int i = 0; i < nps[comp]; ++i) {
+                const double* p = bary + (int64_t)i * npDeg;
                 double v = 0.0, dv = 0.0, tp = 1.0;
-                for (int j = 0; j < e.iauNpDeg; ++j) {
+                for (int j = 0; j < npDeg; ++j) {
                     v = fma(p[j], tp, v);
-                    if (j + 1 < e.iauNpDeg) dv = fma(p[j + 1] * (double)(j + 1), tp, dv);
+                    if (j + 1 < npDeg) dv = fma(p[j + 1] * (double)(j + 1), tp, dv);
                     tp *= T;
                 }
                 double sv, cv;
@@ -339,13 +351,17 @@ static __device__ void iauEarthRotation(const DevEnv& e, double t, double R[9], 
             }
             ang[comp] += sum;
             rate[comp] += dsum / secToCenturies;
-            amp += e.iauNp[comp];
+            amp += nps[comp];
         }
     }
     eulerBodyRotation(fmod(ang[0], 360.0) * deg, fmod(ang[1], 360.0) * deg, fmod(ang[2], 360.0) * deg,
                       rate[0] * deg, rate[1] * deg, rate[2] * deg, false, R, w);
 }
 
+
+static __device__ void iauEarthRotation(const DevEnv& e, double t, double R[9], double w[3]) {
+    iauRotation(e.rotData, e.iauDeg, e.iauNp, e.iauBaryOffset, e.iauNpDeg, t, R, w);
+}
 
 // ICRF -> ITRF rotation and inertial angular velocity of the IERS2000 unit
 static __device__ void earthRotation(const DevEnv& e, double t, double R[9], double w[3]) {
@@ -545,6 +561,16 @@ static __device__ bool evalEpochRecordBase(const DevEnv& e, double et, EpochReco
     for (int i = 0; i < 9; ++i) r.R[i] = (i % 4 == 0) ? 1.0 : 0.0;
     r.w[0] = r.w[1] = r.w[2] = 0.0;
     if (e.hasRot) earthRotation(e, et, r.R, r.w);
+    for (int k = 0; k < kMaxPoles; ++k) {
+        r.pole[k][0] = r.pole[k][1] = r.pole[k][2] = 0.0;
+        if (k >= e.nPoles) continue;
+        // the body's z axis in inertial axes: the third row of its ICRF -> body rotation
+        double Rb[9], wb[3];
+        iauRotation(e.poleCoef + e.poleData[k], e.poleDeg[k], e.poleNp[k], e.poleBary[k], e.poleNpDeg[k], et, Rb, wb);
+        r.pole[k][0] = Rb[6];
+        r.pole[k][1] = Rb[7];
+        r.pole[k][2] = Rb[8];
+    }
     for (int b = 0; b < e.nbodies; ++b) chainPosition(e, e.chainPlus[b], e.chainMinus[b], et, r.body[b]);
     // the indirect part of the third-body attraction (PointGravity.h:76-105):
     // the Earth's acceleration towards each body, the same for every object

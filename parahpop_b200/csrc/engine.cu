@@ -408,7 +408,8 @@ static void loadOrientation(const std::string& path, std::vector<EarthFrameUnit>
         } else {
             throw std::runtime_error("Orientation unit type " + std::to_string(type) + " is not supported: " + path);
         }
-        if (f.target != 3000 && f.target != 3001 && f.target != 399) continue;
+        // other bodies' IAU models are kept for their J2 model
+        if (f.target != 3000 && f.target != 3001 && f.target != 399 && type != 1) continue;
         if (type != 1) {
             f.start = u.at("startEpoch");
             f.final = u.at("finalEpoch");
@@ -444,6 +445,7 @@ static void selectEarthFrame(const std::vector<EarthFrameUnit>& earth, HostEnvir
     if (!want && !anyBinary) want = 399;
     for (const EarthFrameUnit& f : earth) {
         if (f.kind == 2) continue;
+        if (f.kind == 1 && f.target != 399) continue;  // another body's IAU model
         if (want && f.target != want) continue;
         if (!want && f.target == 399) continue;
         if (pick && pick->target != f.target)
@@ -488,6 +490,52 @@ static void selectEarthFrame(const std::vector<EarthFrameUnit>& earth, HostEnvir
                 env.rotData.insert(env.rotData.end(), b.data.begin(), b.data.end());
                 break;
             }
+    }
+}
+
+// The frames of the bodies other than the Earth that carry the J2 model:
+// the IAU body model of the body's own NAIF id, the reference's default
+// orientation target (interface/naming/orientations/Resolver.h:40-88), with
+// the barycentric angles its nutation-precession terms name.
+static void selectPoleFrames(const std::vector<EarthFrameUnit>& units, HostEnvironment& env) {
+    env.poles.clear();
+    for (size_t bi = 0; bi < env.bodies.size(); ++bi) {
+        const auto& b = env.bodies[bi];
+        if (b.id == 399 || !(b.flags & kOblateness) || (b.flags & kShape)) continue;
+        const EarthFrameUnit* pick = nullptr;
+        for (const EarthFrameUnit& f : units)
+            if (f.kind == 1 && f.target == b.id) {
+                pick = &f;
+                break;
+            }
+        if (!pick)
+            throw std::runtime_error("The oblateness (J2) model of " + b.name + " needs its body-fixed orientation: an "
+                                     "IAU body model unit for NAIF id " + std::to_string(b.id)
+                                     + " among the environment's orientations.");
+        if (env.poles.size() >= (size_t)kMaxPoles)
+            throw std::runtime_error("This backend takes the J2 model on at most " + std::to_string(kMaxPoles)
+                                     + " bodies besides the Earth.");
+        HostEnvironment::PoleBody pb;
+        pb.bodyIndex = (int)bi;
+        pb.data = pick->data;
+        int need = 0;
+        for (int k = 0; k < 3; ++k) {
+            pb.deg[k] = pick->deg[k];
+            pb.np[k] = pick->np[k];
+            need = std::max(need, pick->np[k]);
+        }
+        if (need > 0)
+            for (const EarthFrameUnit& u : units)
+                if (u.kind == 2 && u.target == pick->barycenter) {
+                    if (need > u.npAngles)
+                        throw std::runtime_error("The barycentric orientation unit has fewer angles than the IAU "
+                                                 "model's nutation-precession terms.");
+                    pb.baryOffset = (int)pb.data.size();
+                    pb.npDeg = u.npDeg;
+                    pb.data.insert(pb.data.end(), u.data.begin(), u.data.end());
+                    break;
+                }
+        env.poles.push_back(std::move(pb));
     }
 }
 
@@ -772,11 +820,7 @@ static void loadEnvironmentFilesIn(const Value& e, HostEnvironment& env, FileJob
                             const Value* shape = &g.second;
                             jobs.launch([shape, &env] { loadShTable(*shape, env); });
                         } else if (gk == "oblateness") {
-                            if (g.second.isBool() ? g.second.asBool() : !g.second.isNull()) {
-                                if (b.id != 399)
-                                    throw std::runtime_error("The oblateness (J2) model is supported for the Earth only.");
-                                b.flags |= kOblateness;
-                            }
+                            if (g.second.isBool() ? g.second.asBool() : !g.second.isNull()) b.flags |= kOblateness;
                         } else {
                             throw std::runtime_error("Unsupported gravity feature for " + b.name + ": " + g.first);
                         }
@@ -788,7 +832,6 @@ static void loadEnvironmentFilesIn(const Value& e, HostEnvironment& env, FileJob
                         std::transform(gk.begin(), gk.end(), gk.begin(), ::tolower);
                         if (gk != "oblateness")
                             throw std::runtime_error("Unsupported gravity feature for " + b.name + ": " + g.asString());
-                        if (b.id != 399) throw std::runtime_error("The oblateness (J2) model is supported for the Earth only.");
                         b.flags |= kOblateness;
                     }
                 } else {
@@ -873,6 +916,7 @@ static void loadEnvironmentFilesIn(const Value& e, HostEnvironment& env, FileJob
         for (auto& part : oriParts)
             for (auto& f : part) earthFrames.push_back(std::move(f));
         selectEarthFrame(earthFrames, env);
+        selectPoleFrames(earthFrames, env);
     }
     if (atmosphere) jobs.launch([atmosphere, &env] { loadSpaceWeather(*atmosphere, env); });
     if (const Value* ec = e.find("earthCorrections")) {
@@ -933,6 +977,10 @@ uint64_t environmentDigest(const HostEnvironment& e) {
     v(e.nrlWeather);
     s(e.solid), s(e.ocean), s(e.relativity), s(e.zeroTide), s(e.eopFirstMjd), s(e.eopN);
     v(e.eop);
+    for (const auto& pb : e.poles) {
+        s(pb.bodyIndex), s(pb.deg), s(pb.np), s(pb.baryOffset), s(pb.npDeg);
+        v(pb.data);
+    }
     return h;
 }
 
@@ -1121,6 +1169,24 @@ void Engine::uploadEnvironment() {
     e.iauNpDeg = h.iauNpDeg;
     e.iauNpAngles = h.iauNpAngles;
     e.rotData = upload(owned_, h.rotData);
+    for (int b = 0; b < kMaxBodies; ++b) e.poleSlot[b] = -1;
+    e.nPoles = (int)h.poles.size();
+    {
+        std::vector<double> coef;
+        for (int k = 0; k < e.nPoles; ++k) {
+            const auto& pb = h.poles[k];
+            e.poleSlot[pb.bodyIndex] = k;
+            for (int c = 0; c < 3; ++c) {
+                e.poleDeg[k][c] = pb.deg[c];
+                e.poleNp[k][c] = pb.np[c];
+            }
+            e.poleData[k] = (int)coef.size();
+            e.poleBary[k] = pb.baryOffset;
+            e.poleNpDeg[k] = pb.npDeg;
+            coef.insert(coef.end(), pb.data.begin(), pb.data.end());
+        }
+        e.poleCoef = coef.empty() ? nullptr : upload(owned_, coef);
+    }
     e.hasNrl = h.hasNrl;
     e.nrlNdays = h.nrlNdays;
     e.nrlStartMjd = h.nrlStartMjd;

@@ -77,6 +77,15 @@ struct HostEnvironment {
     double eopFirstMjd = 0.0;
     std::vector<double> eop;  // 4 x n
     int eopN = 0;
+    // bodies other than the Earth with the J2 model, each with its IAU body
+    // model (coefficients, then its barycentric angle polynomials)
+    struct PoleBody {
+        int bodyIndex = -1;
+        int deg[3] = {0, 0, 0}, np[3] = {0, 0, 0};
+        int baryOffset = -1, npDeg = 0;
+        std::vector<double> data;
+    };
+    std::vector<PoleBody> poles;
 };
 
 // Loads the environment of a `model` configuration object (the reference's

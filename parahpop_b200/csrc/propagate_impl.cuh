@@ -126,6 +126,7 @@ struct RecordRef {
     __device__ __forceinline__ double indirect(int i) const { return r->indirect[i]; }
     __device__ __forceinline__ double dC(int k) const { return r->dC[k]; }
     __device__ __forceinline__ double dS(int k) const { return r->dS[k]; }
+    __device__ __forceinline__ double pole(int k, int i) const { return r->pole[k][i]; }
     // NRLMSISE-00 time inputs; valid = -1 (evaluate at the epoch in `sec`
     // when an object below the cut-off needs them) when the record has none
     __device__ __forceinline__ NrlTime nrlDeferred() const {
@@ -167,6 +168,9 @@ struct RecordInterp {
     }
     __device__ __forceinline__ double dC(int k) const { return at((int)(offsetof(EpochRecord, dC) / 8) + k); }
     __device__ __forceinline__ double dS(int k) const { return at((int)(offsetof(EpochRecord, dS) / 8) + k); }
+    __device__ __forceinline__ double pole(int k, int i) const {
+        return at((int)(offsetof(EpochRecord, pole) / 8) + 3 * k + i);
+    }
     // NRLMSISE-00 time inputs: evaluated exactly at the stage epoch by the
     // drag model, only for objects below the density cut-off
     __device__ __forceinline__ NrlTime nrlDeferred() const { return NrlTime{et, 0.0, 0, -1}; }
@@ -892,7 +896,7 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
         // body's position (direct attraction and radiation pressure), each
         // read from the record once
         double fb[3] = {0.0, 0.0, 0.0}, rb[3] = {0.0, 0.0, 0.0};
-        if ((fl & (kShape | kOblateness)) || ((fl & kAtmosphere) && e.hasNrl)) toBody(r, pos, fb);
+        if (isEarth && ((fl & (kShape | kOblateness)) || ((fl & kAtmosphere) && e.hasNrl))) toBody(r, pos, fb);
         if (((fl & kGravity) && !isEarth) || (fl & kRadiation)) {
             rb[0] = r.body(bi, 0);
             rb[1] = r.body(bi, 1);
@@ -941,7 +945,28 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
             ay += ai[1];
             az += ai[2];
         }
-        if ((fl & kOblateness) && !(fl & kShape)) {
+        if ((fl & kOblateness) && !(fl & kShape) && !isEarth) {
+            // J2 model of another body (J2.h:17-33,63-78, PrivateAccelerations.h:88-97):
+            // position relative to the body, inside its sphere of influence;
+            // the model is axisymmetric, so the body frame enters through its
+            // polar axis u alone: a = c (d (1 - 5 z^2 / r^2) + 2 z u), z = u . d
+            const double d0 = pos[0] - rb[0], d1 = pos[1] - rb[1], d2 = pos[2] - rb[2];
+            const double rr2 = d0 * d0 + d1 * d1 + d2 * d2;
+            const int slot = e.poleSlot[bi];
+            if (slot >= 0 && rr2 <= e.bodySoi[bi] * e.bodySoi[bi]) {
+                const double u0 = r.pole(slot, 0), u1 = r.pole(slot, 1), u2 = r.pole(slot, 2);
+                const double invr = rsqrt(rr2);
+                const double invr2 = invr * invr;
+                const double z = u0 * d0 + u1 * d1 + u2 * d2;
+                const double base = 1.0 - 5.0 * (z * z) * invr2;
+                const double c = -1.5 * e.bodyGmConst[bi] * e.bodyJ2[bi] * (invr2 * invr2 * invr) * e.bodyRadius[bi]
+                                 * e.bodyRadius[bi];
+                ax += c * (d0 * base + 2.0 * z * u0);
+                ay += c * (d1 * base + 2.0 * z * u1);
+                az += c * (d2 * base + 2.0 * z * u2);
+            }
+        }
+        if ((fl & kOblateness) && !(fl & kShape) && isEarth) {
             // J2 model in the body frame (J2.h:17-33,63-78), inside the sphere of influence
             const double rr = sqrt(pos[0] * pos[0] + pos[1] * pos[1] + pos[2] * pos[2]);
             if (rr <= e.bodySoi[bi]) {

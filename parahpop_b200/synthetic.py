@@ -268,6 +268,31 @@ def population_leo(n=10000, seed=1, alt=(300.0, 2000.0), screen_duration=86400.0
                       note=f"full-force LEO population, n={n}, seed={seed}")
 
 
+def population_lunar(n=16, seed=17, epoch=4035.0):
+    """Objects on low lunar orbits (1,900-2,600 km from the Moon's centre,
+    circular about the Moon, random planes), as geocentric states at one
+    epoch from the synthetic Moon path."""
+    rng = np.random.default_rng(seed)
+    fns = body_functions()
+    h = 1e-3
+    moon = fns["moon"](epoch)
+    moon_v = (fns["moon"](epoch + h) - fns["moon"](epoch - h)) / (2 * h * SECONDS_PER_DAY)
+    gm_moon = 4902.800192171393
+    states = np.zeros((n, 6))
+    for i in range(n):
+        r = rng.uniform(1900.0, 2600.0)
+        u = rng.normal(size=3)
+        u /= np.linalg.norm(u)
+        w = np.cross(u, rng.normal(size=3))
+        w /= np.linalg.norm(w)
+        states[i, :3] = moon + r * u
+        states[i, 3:] = moon_v + math.sqrt(gm_moon / r) * np.cross(w, u)
+    ids = np.arange(1, n + 1)
+    return Population(ids, np.full(n, epoch), states, rng.uniform(500.0, 2000.0, n), rng.uniform(2.0, 10.0, n),
+                      rng.uniform(2.0, 10.0, n), np.full(n, 2.2), np.full(n, 1.3), seed=seed,
+                      note="low lunar orbits, geocentric states")
+
+
 def population_mixed(n=1000000, seed=3):
     """Uneven population: 70% LEO (30 s), 20% MEO (120 s), 10% GEO/GTO (300 s);
     epochs U(-10,+10) d around MJD2000 4035; durations log-uniform 1 h - 7 d."""
@@ -321,6 +346,7 @@ class EnvSpec:
     earth_frame: str = "iers"     # earth.brot2 holds: "iers" the IERS2000 model unit (3001), "itrf93" a binary
                                   # Chebyshev Euler-angle unit (3000, ECLIPJ2000-based), "both" the two, "iau"
                                   # an IAU body model (399) with barycentric nutation-precession terms
+    moon_frame: bool = False      # earth.brot2 also holds an IAU body model of the Moon (301)
 
 
 def kaula_field(degree, seed, zonal_only=False):
@@ -528,7 +554,18 @@ def iau_earth_units(start_mjd, end_mjd):
     return [body, bary]
 
 
-def write_brot2(path, start_mjd, end_mjd, layout=1, frame="iers"):
+def iau_moon_unit(start_mjd, end_mjd):
+    """IAU body model of the Moon (RA = 269.9949 + 0.0031 T, Dec = 66.5392 +
+    0.0130 T, W = 38.3213 + 13.17635815 d, degrees; the IAU WG's leading
+    terms) without nutation-precession terms."""
+    t0, t1 = mjd2000_to_et(start_mjd), mjd2000_to_et(end_mjd)
+    return {"metadata": {"unit_type": 1, "target": 301, "pdeg_ra": 1, "pdeg_dec": 1, "pdeg_pm": 1,
+                         "num_dims_radii": 0, "barycenter": 3, "num_np_terms_ra": 0, "num_np_terms_dec": 0,
+                         "num_np_terms_pm": 0, "startEpoch": t0, "finalEpoch": t1},
+            "data": [269.9949, 0.0031, 66.5392, 0.0130, 38.3213, 13.17635815]}
+
+
+def write_brot2(path, start_mjd, end_mjd, layout=1, frame="iers", moon=False):
     """IERS2000 unit: X, Y, s (rad) on a 1-day TT grid, ERP on daily keys.
     Constant EOP: xp = yp = 0, UT1-UTC = 0.3 s, TAI-UTC = 34 s."""
     t0 = start_mjd - 3.0
@@ -556,6 +593,8 @@ def write_brot2(path, start_mjd, end_mjd, layout=1, frame="iers"):
             units.append(itrf93_unit(start_mjd - 2.0, end_mjd + 2.0))
         if frame == "iau":
             units += iau_earth_units(start_mjd - 2.0, end_mjd + 2.0)
+        if moon:
+            units.append(iau_moon_unit(start_mjd - 2.0, end_mjd + 2.0))
         fh.write(cbor_dumps(brie_layout2(units, ORIENTATION_INT_KEYS) if layout == 2
                             else {"layout": 1, "core": units}))
 
@@ -606,7 +645,8 @@ def write_environment(directory, spec: EnvSpec = EnvSpec()) -> Path:
     else:
         write_brie(d / "bodies.brie", spec.start_mjd, spec.end_mjd, spec.ephemeris_type, spec.ephemeris_chain,
                    spec.brie_layout)
-    write_brot2(d / "earth.brot2", spec.start_mjd, spec.end_mjd, spec.brie_layout, spec.earth_frame)
+    write_brot2(d / "earth.brot2", spec.start_mjd, spec.end_mjd, spec.brie_layout, spec.earth_frame,
+                spec.moon_frame)
     write_space_weather(d / "SW-All.txt", spec.start_mjd, spec.end_mjd)
     write_eop(d / "EOP-All.txt", spec.start_mjd, spec.end_mjd)
     (d / "constants.json").write_text(json.dumps(CONSTANTS, indent=2) + "\n")
@@ -626,12 +666,14 @@ def make_config(env_dir, duration, step, max_steps=1000000, threads=1, force="fu
                 degree=70, bodies=("Sun", "Moon", "JupiterBarycenter"), tides=True,
                 relativity=True, drag=True, srp=True, start_mjd=4016.0, end_mjd=4064.0,
                 gravity="shape", atmosphere="nrlmsise00", tide_system="zero_tide",
-                occulting=("Earth",), earth_orientation=None, ephemeris=("bodies.brie",)) -> dict:
+                occulting=("Earth",), earth_orientation=None, ephemeris=("bodies.brie",),
+                moon_gravity="point") -> dict:
     """Run configuration in the reference schema (``example/config/envisat_full.json``).
     Paths are relative to ``env_dir`` (where the config file is written).
     ``gravity``: "shape" (the spherical-harmonic file) or "oblateness" (the
     J2 model from the constants file); ``atmosphere``: "nrlmsise00",
-    "exponential" (one band) or "piecewise" (three bands)."""
+    "exponential" (one band) or "piecewise" (three bands); ``moon_gravity``:
+    "point" or "oblateness" (the Moon's J2 model in its IAU frame)."""
     earth: dict = {}
     if force == "central":
         earth = {"gravity": True}
@@ -660,7 +702,9 @@ def make_config(env_dir, duration, step, max_steps=1000000, threads=1, force="fu
             if b == "Sun":
                 bodies_cfg["Sun"] = {"gravity": True, "radiation": bool(srp)}
             elif b == "Moon":
-                bodies_cfg["Moon"] = {"gravity": True, "occulting": True} if "Moon" in occulting else {"gravity": True}
+                grav_m = {"oblateness": True} if moon_gravity == "oblateness" else True
+                bodies_cfg["Moon"] = ({"gravity": grav_m, "occulting": True} if "Moon" in occulting
+                                      else {"gravity": grav_m})
             elif b == "JupiterBarycenter":
                 bodies_cfg["JupiterBarycenter"] = {"gm": 126712764.1, "gravity": True}
     env = {"bodies": bodies_cfg, "ephemeris": list(ephemeris), "constants": "constants.json", "preferSSB": True}

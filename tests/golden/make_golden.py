@@ -104,6 +104,11 @@ CASES["j2_exponential_2h"] = (lambda: S.population_leo(16, 13, alt=(300.0, 1200.
                               {"gravity": "oblateness", "atmosphere": "exponential"}, {})
 CASES["piecewise_drag_3h"] = (lambda: S.population_leo(24, 14, alt=(300.0, 1100.0)), 10800.0, 60.0,
                               {"atmosphere": "piecewise"}, {})
+# the J2 model on a body other than the Earth, in its own IAU frame: low
+# lunar orbits (1,900-2,600 km from the Moon's centre) integrated about the
+# Earth; the Moon's J2 moves them by 0.5-4.5 km in 2 h
+CASES["moon_j2_2h"] = (lambda: S.population_lunar(12, 17), 7200.0, 60.0, {"moon_gravity": "oblateness"},
+                       {"moon_frame": True})
 
 
 def lunar_penumbra():

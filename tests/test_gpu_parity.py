@@ -49,6 +49,50 @@ def test_every_lane_split_matches(golden, name, lanes):
     assert dpos <= POS_TOL_M and dvel <= VEL_TOL_M_S, (dpos, dvel)
 
 
+@pytest.mark.parametrize("lanes,pair,deep", [(1, 1, 0), (2, 1, 0), (2, 0, 1), (2, 1, 1), (4, 0, 1), (4, 1, 1)])
+@pytest.mark.parametrize("split", [False, True])
+@pytest.mark.parametrize("name", ["batch_33", "c3_leo_19h"])
+def test_every_launch_shape_matches(golden, name, split, lanes, pair, deep):
+    """Lane-group pairs and the deep thread bound (256 threads, up to 255
+    registers), pinned one shape at a time, on a shared time grid and on
+    per-object epochs: each holds the reference bar (FP64 1 mm / 1e-6 m/s,
+    split 1 cm), and the statistics report the shape that ran."""
+    case = golden(name)
+    p = api.Propagator(case.config_path, lanes=lanes, split=split)
+    p.set_option("pair_sh", pair)
+    p.set_option("deep_registers", deep)
+    ep, st = p.propagate_targets(case.targets)
+    s = p.stats()
+    assert (s["lanes"], s["pair_sh"], s["deep_registers"]) == (lanes, pair, deep)
+    assert s["threads"] <= (256 if deep or lanes == 1 else {2: 320, 4: 384}[lanes])
+    assert (s["registers"] > 168) == (deep == 1 or lanes == 1), s["registers"]
+    dpos, dvel = errors(st, case.ref_states)
+    if split:
+        assert dpos <= SPLIT_POS_TOL_M, dpos
+    else:
+        assert dpos <= POS_TOL_M and dvel <= VEL_TOL_M_S, (dpos, dvel)
+    p.close()
+
+
+def test_option_refusals(golden):
+    """Out-of-range execution options are refused with a message naming
+    them, and leave the context usable."""
+    case = golden("full_600s")
+    p = api.Propagator(case.config_path)
+    for key, bad in (("deep_registers", 2), ("pair_sh", 3), ("split_fp64_degree", 30), ("split_fp64_degree", 7),
+                     ("threads", 48), ("threads", 1024), ("lanes", 3), ("split_floor_km", -1.0)):
+        with pytest.raises(api.PhopError) as e:
+            p.set_option(key, bad)
+        assert key in str(e.value), (key, str(e.value))
+    with pytest.raises(api.PhopError) as e:
+        p.set_option("split_drag_fp32_km", 500.0)
+    assert "Unknown option" in str(e.value)
+    ep, st = p.propagate_targets(case.targets)
+    dpos, dvel = errors(st, case.ref_states)
+    assert dpos <= POS_TOL_M and dvel <= VEL_TOL_M_S
+    p.close()
+
+
 @pytest.mark.parametrize("name", ["full_1h", "deg120_1h", "c1_full_24h", "c2_deg120_24h"])
 def test_split_precision_within_1cm(golden, name):
     case = golden(name)
