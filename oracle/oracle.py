@@ -361,10 +361,10 @@ def load_environment(config_path) -> Environment:
                 e.iau_bary_offset = len(data)
                 e.iau_np_deg, e.iau_np_angles = bmd["pdeg_np"] + 1, bmd["num_np_angles"]
                 e.rot_data = _dp(hold(np.array(list(data) + list(bdata), dtype=np.float64)))
-    # bodies other than the Earth with the J2 model: their IAU body models
+    # bodies other than the Earth with the J2 model or the field: their IAU body models
     for bi, r in enumerate(rows):
         e.frame_bary_offset[bi] = -1
-        if r[0] == 399 or not (r[3] & F_OBLATENESS) or r[0] not in other_iau:
+        if r[0] == 399 or not (r[3] & (F_OBLATENESS | F_SHAPE)) or r[0] not in other_iau:
             continue
         md, data = other_iau[r[0]]
         vals = list(data)

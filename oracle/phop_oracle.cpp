@@ -948,12 +948,21 @@ V3 acceleration(const OracleEnv& e, const ShFactors& F, V3 pos, V3 vel, double e
             }
         }
         if (fl & F_SHAPE) {
+            // the field in its body's frame: the Earth's, or another body's IAU model
             const V3 dp = (body != kEarth) ? pos - bodyPos : pos;
-            if (!haveRot) {
-                earthRotation(e, et, R, &w);
-                haveRot = true;
+            if (body != kEarth) {
+                double Rb[9];
+                V3 wb;
+                iauRotation(e.frame_data[bi], e.frame_deg[bi], e.frame_np[bi], e.frame_bary_offset[bi],
+                            e.frame_np_deg[bi], et, Rb, &wb);
+                acc = acc + matT(Rb, shBodyFixed(e, F, mat(Rb, dp)));
+            } else {
+                if (!haveRot) {
+                    earthRotation(e, et, R, &w);
+                    haveRot = true;
+                }
+                acc = acc + matT(R, shBodyFixed(e, F, mat(R, dp)));
             }
-            acc = acc + matT(R, shBodyFixed(e, F, mat(R, dp)));
         }
         if ((fl & F_OBLATENESS) && !(fl & F_SHAPE)) {
             // J2 model (PrivateAccelerations.h:88-97, J2.h:63-78), in the

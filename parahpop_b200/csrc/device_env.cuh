@@ -97,6 +97,12 @@ struct DevEnv {
     int poleBary[kMaxPoles];    // offset of its barycentric angle polynomials from there (-1: none)
     int poleNpDeg[kMaxPoles];
     const double* poleCoef;
+    // a field on a body other than the Earth (shFrame = 1): the IAU body
+    // model of its frame (coefficients at poleCoef + shFrameData); shTides:
+    // the Earth's tide deltas join the field (the field is the Earth's)
+    int shFrame, shTides;
+    int shFrameDeg[3], shFrameNp[3];
+    int shFrameData, shFrameBary, shFrameNpDeg;
 };
 
 struct EpochRecord {
@@ -107,6 +113,7 @@ struct EpochRecord {
     double dC[kTideTri];         // tide coefficient deltas, field units
     double dS[kTideTri];
     double pole[kMaxPoles][3];   // polar (body z) axes of the J2 bodies other than the Earth, inertial
+    double fieldR[9];            // ICRF -> body rotation of a field on a body other than the Earth
     double nrlSec, nrlGast;      // UTC seconds of day, apparent sidereal time (h)
     double et;                   // the record's epoch, TDB seconds past J2000
     int nrlBlock, nrlValid;      // nrlValid: 1 / 0, or -1 = time inputs not evaluated yet (from et)
@@ -570,6 +577,12 @@ static __device__ bool evalEpochRecordBase(const DevEnv& e, double et, EpochReco
         r.pole[k][0] = Rb[6];
         r.pole[k][1] = Rb[7];
         r.pole[k][2] = Rb[8];
+    }
+    for (int i = 0; i < 9; ++i) r.fieldR[i] = (i % 4 == 0) ? 1.0 : 0.0;
+    if (e.shFrame) {
+        double wb[3];
+        iauRotation(e.poleCoef + e.shFrameData, e.shFrameDeg, e.shFrameNp, e.shFrameBary, e.shFrameNpDeg, et, r.fieldR,
+                    wb);
     }
     for (int b = 0; b < e.nbodies; ++b) chainPosition(e, e.chainPlus[b], e.chainMinus[b], et, r.body[b]);
     // the indirect part of the third-body attraction (PointGravity.h:76-105):

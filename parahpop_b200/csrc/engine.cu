@@ -499,9 +499,11 @@ static void selectEarthFrame(const std::vector<EarthFrameUnit>& earth, HostEnvir
 // the barycentric angles its nutation-precession terms name.
 static void selectPoleFrames(const std::vector<EarthFrameUnit>& units, HostEnvironment& env) {
     env.poles.clear();
+    env.shFrame = HostEnvironment::PoleBody();
     for (size_t bi = 0; bi < env.bodies.size(); ++bi) {
         const auto& b = env.bodies[bi];
-        if (b.id == 399 || !(b.flags & kOblateness) || (b.flags & kShape)) continue;
+        const bool field = (b.flags & kShape) != 0;
+        if (b.id == 399 || !((b.flags & kOblateness) || field)) continue;
         const EarthFrameUnit* pick = nullptr;
         for (const EarthFrameUnit& f : units)
             if (f.kind == 1 && f.target == b.id) {
@@ -509,10 +511,10 @@ static void selectPoleFrames(const std::vector<EarthFrameUnit>& units, HostEnvir
                 break;
             }
         if (!pick)
-            throw std::runtime_error("The oblateness (J2) model of " + b.name + " needs its body-fixed orientation: an "
-                                     "IAU body model unit for NAIF id " + std::to_string(b.id)
-                                     + " among the environment's orientations.");
-        if (env.poles.size() >= (size_t)kMaxPoles)
+            throw std::runtime_error(std::string(field ? "The spherical-harmonic field" : "The oblateness (J2) model")
+                                     + " of " + b.name + " needs its body-fixed orientation: an IAU body model unit "
+                                     "for NAIF id " + std::to_string(b.id) + " among the environment's orientations.");
+        if (!field && env.poles.size() >= (size_t)kMaxPoles)
             throw std::runtime_error("This backend takes the J2 model on at most " + std::to_string(kMaxPoles)
                                      + " bodies besides the Earth.");
         HostEnvironment::PoleBody pb;
@@ -535,7 +537,8 @@ static void selectPoleFrames(const std::vector<EarthFrameUnit>& units, HostEnvir
                     pb.data.insert(pb.data.end(), u.data.begin(), u.data.end());
                     break;
                 }
-        env.poles.push_back(std::move(pb));
+        if (field) env.shFrame = std::move(pb);
+        else env.poles.push_back(std::move(pb));
     }
 }
 
@@ -812,8 +815,10 @@ static void loadEnvironmentFilesIn(const Value& e, HostEnvironment& env, FileJob
                         std::string gk = g.first;
                         std::transform(gk.begin(), gk.end(), gk.begin(), ::tolower);
                         if (gk == "shape") {
-                            if (b.id != 399)
-                                throw std::runtime_error("Spherical-harmonic gravity is supported for the Earth only.");
+                            if (shapeJobs && env.shBodyId != b.id)
+                                throw std::runtime_error("This backend takes one spherical-harmonic field per "
+                                                         "configuration; " + b.name + " would hold a second.");
+                            env.shBodyId = b.id;
                             b.flags |= kShape;
                             if (shapeJobs) jobs.joinUpTo(jobs.size());  // a second table replaces the first
                             ++shapeJobs;
@@ -934,7 +939,7 @@ static void loadEnvironmentFilesIn(const Value& e, HostEnvironment& env, FileJob
     jobs.joinUpTo(jobs.size());
     for (auto& part : ephParts)
         for (auto& u : part) env.eph.push_back(std::move(u));
-    if ((env.hasShape || env.hasNrl || env.solid || env.ocean) && !env.hasRot)
+    if (((env.hasShape && env.shBodyId == 399) || env.hasNrl || env.solid || env.ocean) && !env.hasRot)
         throw std::runtime_error("An Earth orientation unit (ITRF93 or IERS2000) is required for the configured "
                                  "forces.");
 }
@@ -981,6 +986,8 @@ uint64_t environmentDigest(const HostEnvironment& e) {
         s(pb.bodyIndex), s(pb.deg), s(pb.np), s(pb.baryOffset), s(pb.npDeg);
         v(pb.data);
     }
+    s(e.shBodyId), s(e.shFrame.bodyIndex), s(e.shFrame.deg), s(e.shFrame.np), s(e.shFrame.baryOffset);
+    s(e.shFrame.npDeg), v(e.shFrame.data);
     return h;
 }
 
@@ -1185,8 +1192,22 @@ void Engine::uploadEnvironment() {
             e.poleNpDeg[k] = pb.npDeg;
             coef.insert(coef.end(), pb.data.begin(), pb.data.end());
         }
+        // a field on a body other than the Earth: its frame in every record
+        e.shFrame = h.shFrame.bodyIndex >= 0 ? 1 : 0;
+        if (e.shFrame) {
+            for (int c = 0; c < 3; ++c) {
+                e.shFrameDeg[c] = h.shFrame.deg[c];
+                e.shFrameNp[c] = h.shFrame.np[c];
+            }
+            e.shFrameData = (int)coef.size();
+            e.shFrameBary = h.shFrame.baryOffset;
+            e.shFrameNpDeg = h.shFrame.npDeg;
+            coef.insert(coef.end(), h.shFrame.data.begin(), h.shFrame.data.end());
+        }
         e.poleCoef = coef.empty() ? nullptr : upload(owned_, coef);
     }
+    // the Earth's tide deltas join the field only when it is the Earth's
+    e.shTides = (h.solid || h.ocean) && h.hasShape && h.shBodyId == 399;
     e.hasNrl = h.hasNrl;
     e.nrlNdays = h.nrlNdays;
     e.nrlStartMjd = h.nrlStartMjd;
@@ -1250,7 +1271,7 @@ void Engine::uploadEnvironment() {
     e.solid = h.solid;
     e.ocean = h.ocean;
     e.relativity = h.relativity;
-    e.tidesAlone = (h.solid || h.ocean) && !h.hasShape;
+    e.tidesAlone = (h.solid || h.ocean) && !(h.hasShape && h.shBodyId == 399);
     e.zeroTide = h.zeroTide;
     e.tideOcean = nullptr;
     if (h.ocean) {

@@ -86,6 +86,10 @@ struct HostEnvironment {
         std::vector<double> data;
     };
     std::vector<PoleBody> poles;
+    // the body whose field the geopotential is (one per configuration) and,
+    // for a body other than the Earth, its IAU body model
+    int shBodyId = 399;
+    PoleBody shFrame;
 };
 
 // Loads the environment of a `model` configuration object (the reference's

@@ -127,6 +127,7 @@ struct RecordRef {
     __device__ __forceinline__ double dC(int k) const { return r->dC[k]; }
     __device__ __forceinline__ double dS(int k) const { return r->dS[k]; }
     __device__ __forceinline__ double pole(int k, int i) const { return r->pole[k][i]; }
+    __device__ __forceinline__ double SR(int i) const { return r->fieldR[i]; }
     // NRLMSISE-00 time inputs; valid = -1 (evaluate at the epoch in `sec`
     // when an object below the cut-off needs them) when the record has none
     __device__ __forceinline__ NrlTime nrlDeferred() const {
@@ -171,6 +172,7 @@ struct RecordInterp {
     __device__ __forceinline__ double pole(int k, int i) const {
         return at((int)(offsetof(EpochRecord, pole) / 8) + 3 * k + i);
     }
+    __device__ __forceinline__ double SR(int i) const { return at((int)(offsetof(EpochRecord, fieldR) / 8) + i); }
     // NRLMSISE-00 time inputs: evaluated exactly at the stage epoch by the
     // drag model, only for objects below the density cut-off
     __device__ __forceinline__ NrlTime nrlDeferred() const { return NrlTime{et, 0.0, 0, -1}; }
@@ -198,7 +200,7 @@ static __device__ __forceinline__ void shAccel(const StepParams& p, const typena
     const int j = (int)(threadIdx.x % L);
     const int N = p.env.shDegree, M = p.env.shOrder;
     const int lowDeg = p.lowDeg;
-    const bool tides = p.env.solid || p.env.ocean;
+    const bool tides = p.env.shTides != 0;
     const LowTable* __restrict__ low = p.low;
     const double* __restrict__ diagC = p.diagC;
     const double rn = sqrt(x * x + y * y + z * z);
@@ -465,7 +467,7 @@ static __device__ __forceinline__ void shLowColumn(const StepParams& p, const Re
                                                    T& dP1) {
     const LowTable* __restrict__ low = p.low;
     const int N = p.env.shDegree, lowDeg = p.lowDeg;
-    const bool tides = p.env.solid || p.env.ocean;
+    const bool tides = p.env.shTides != 0;
     double Pn = d.Pmm, Pn1 = 0.0, dPn = d.dPmm, dPn1 = 0.0, an = d.am, anPrev = d.am;
     const int nEnd = N < lowDeg ? N : lowDeg;
     for (int k = 0; k < 6; ++k) S[k] = 0.0;
@@ -673,7 +675,7 @@ static __device__ __forceinline__ void shAccelPair(const StepParams& p, const ty
     double ar = second ? acc1[0] : acc0[0], aphi = second ? acc1[1] : acc0[1], alam = second ? acc1[2] : acc0[2];
     if (g.cosPhi == 0.0 && M >= 1) {
         // exact pole: the m = 1 longitudinal term's analytical limit (as shAccel)
-        const bool tides = p.env.solid || p.env.ocean;
+        const bool tides = p.env.shTides != 0;
         double an = g.alpha;
         for (int n = 1; n <= N; ++n) {
             const int ti = n * (n + 1) / 2 + 1;
@@ -922,7 +924,15 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
             }
         }
         if (fl & kShape) {
-            const double bx = fb[0], by = fb[1], bz = fb[2];
+            // body-fixed position: the Earth's frame, or the field body's
+            // own (IAU) frame about its position
+            double bx = fb[0], by = fb[1], bz = fb[2];
+            if (!isEarth) {
+                const double d0 = pos[0] - rb[0], d1 = pos[1] - rb[1], d2 = pos[2] - rb[2];
+                bx = r.SR(0) * d0 + r.SR(1) * d1 + r.SR(2) * d2;
+                by = r.SR(3) * d0 + r.SR(4) * d1 + r.SR(5) * d2;
+                bz = r.SR(6) * d0 + r.SR(7) * d1 + r.SR(8) * d2;
+            }
             double a[3];
             if constexpr (!std::is_same<T, double>::value) {
                 // split precision: objects below the split radius keep the
@@ -940,7 +950,13 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
                     shAccel<L, T>(p, tile, r, bx, by, bz, a);
             }
             double ai[3];
-            fromBody(r, a, ai);
+            if (isEarth) {
+                fromBody(r, a, ai);
+            } else {
+                ai[0] = r.SR(0) * a[0] + r.SR(3) * a[1] + r.SR(6) * a[2];
+                ai[1] = r.SR(1) * a[0] + r.SR(4) * a[1] + r.SR(7) * a[2];
+                ai[2] = r.SR(2) * a[0] + r.SR(5) * a[1] + r.SR(8) * a[2];
+            }
             ax += ai[0];
             ay += ai[1];
             az += ai[2];

@@ -347,6 +347,7 @@ class EnvSpec:
                                   # Chebyshev Euler-angle unit (3000, ECLIPJ2000-based), "both" the two, "iau"
                                   # an IAU body model (399) with barycentric nutation-precession terms
     moon_frame: bool = False      # earth.brot2 also holds an IAU body model of the Moon (301)
+    moon_field: int = 0           # degree of a synthetic lunar field written to moon.tab (0: none)
 
 
 def kaula_field(degree, seed, zonal_only=False):
@@ -640,6 +641,10 @@ def write_environment(directory, spec: EnvSpec = EnvSpec()) -> Path:
     d.mkdir(parents=True, exist_ok=True)
     C, S = kaula_field(spec.degree, spec.seed, spec.zonal_only)
     write_tab(d / "gravity.tab", C, S, spec.gm_tab, spec.r_tab, spec.degree)
+    if spec.moon_field:
+        Cm, Sm = kaula_field(spec.moon_field, spec.seed + 101)
+        Cm[2, 0] = -9.0881e-5  # the Moon's C20 (normalized), its other terms the Kaula-like draw
+        write_tab(d / "moon.tab", Cm, Sm, 4902.800192171393, 1738.0, spec.moon_field)
     if spec.ephemeris_files == 2:
         write_brie_split(d / "bodies.brie", d / "bodies2.brie", spec.start_mjd, spec.end_mjd)
     else:
@@ -667,13 +672,14 @@ def make_config(env_dir, duration, step, max_steps=1000000, threads=1, force="fu
                 relativity=True, drag=True, srp=True, start_mjd=4016.0, end_mjd=4064.0,
                 gravity="shape", atmosphere="nrlmsise00", tide_system="zero_tide",
                 occulting=("Earth",), earth_orientation=None, ephemeris=("bodies.brie",),
-                moon_gravity="point") -> dict:
+                moon_gravity="point", moon_degree=8) -> dict:
     """Run configuration in the reference schema (``example/config/envisat_full.json``).
     Paths are relative to ``env_dir`` (where the config file is written).
     ``gravity``: "shape" (the spherical-harmonic file) or "oblateness" (the
     J2 model from the constants file); ``atmosphere``: "nrlmsise00",
     "exponential" (one band) or "piecewise" (three bands); ``moon_gravity``:
-    "point" or "oblateness" (the Moon's J2 model in its IAU frame)."""
+    "point", "oblateness" (the Moon's J2 model in its IAU frame) or "shape"
+    (the lunar field of moon.tab, degree ``moon_degree``, in the same frame)."""
     earth: dict = {}
     if force == "central":
         earth = {"gravity": True}
@@ -703,6 +709,9 @@ def make_config(env_dir, duration, step, max_steps=1000000, threads=1, force="fu
                 bodies_cfg["Sun"] = {"gravity": True, "radiation": bool(srp)}
             elif b == "Moon":
                 grav_m = {"oblateness": True} if moon_gravity == "oblateness" else True
+                if moon_gravity == "shape":
+                    grav_m = {"shape": {"file": "moon.tab", "delimiter": ",", "headerLines": 0,
+                                        "degree": moon_degree, "order": moon_degree}}
                 bodies_cfg["Moon"] = ({"gravity": grav_m, "occulting": True} if "Moon" in occulting
                                       else {"gravity": grav_m})
             elif b == "JupiterBarycenter":

@@ -24,6 +24,8 @@ def env_hash(d: Path) -> str:
     h = hashlib.sha256()
     for name in ("gravity.tab", "bodies.brie", "earth.brot2", "SW-All.txt", "EOP-All.txt", "constants.json"):
         h.update((Path(d) / name).read_bytes())
+    if (Path(d) / "moon.tab").exists():  # the lunar field, where a case has one
+        h.update((Path(d) / "moon.tab").read_bytes())
     return h.hexdigest()
 
 

@@ -47,6 +47,8 @@ def env_hash(d: Path) -> str:
     h = hashlib.sha256()
     for name in ("gravity.tab", "bodies.brie", "earth.brot2", "SW-All.txt", "EOP-All.txt", "constants.json"):
         h.update((d / name).read_bytes())
+    if (d / "moon.tab").exists():  # the lunar field, where a case has one
+        h.update((d / "moon.tab").read_bytes())
     return h.hexdigest()
 
 
@@ -109,6 +111,11 @@ CASES["piecewise_drag_3h"] = (lambda: S.population_leo(24, 14, alt=(300.0, 1100.
 # Earth; the Moon's J2 moves them by 0.5-4.5 km in 2 h
 CASES["moon_j2_2h"] = (lambda: S.population_lunar(12, 17), 7200.0, 60.0, {"moon_gravity": "oblateness"},
                        {"moon_frame": True})
+# a field on a body other than the Earth: a degree-8 lunar field in the
+# Moon's IAU frame, the Earth with the J2 model (so its tides are summed on
+# their own); the lunar field moves these orbits by 0.5-5 km in 2 h
+CASES["moon_field_2h"] = (lambda: S.population_lunar(12, 18), 7200.0, 60.0,
+                          {"moon_gravity": "shape", "gravity": "oblateness"}, {"moon_frame": True, "moon_field": 8})
 
 
 def lunar_penumbra():
