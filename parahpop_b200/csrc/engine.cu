@@ -1095,7 +1095,11 @@ void Engine::uploadEnvironment() {
     // join the field's low-degree block rescaled to its GM and radius, or are
     // summed on their own (scale 1) when the Earth has no gravity field file
     for (int n = 0; n <= 6; ++n)
-        e.tideScale[n] = h.hasShape ? (tidefield::kMuEarth * 1e-9 / h.shGM) * std::pow(tidefield::kRadius * 1e-3 / h.shR, (double)n) : 1.0;
+        // in the field's units when they join the Earth's field; in the tide
+        // model's own for the tides alone (no field, or a field of another body)
+        e.tideScale[n] = h.hasShape && h.shBodyId == 399
+                             ? (tidefield::kMuEarth * 1e-9 / h.shGM) * std::pow(tidefield::kRadius * 1e-3 / h.shR, (double)n)
+                             : 1.0;
     if (h.hasShape) {
         e.shC = upload(owned_, h.shC);
         e.shS = upload(owned_, h.shS);
