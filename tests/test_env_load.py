@@ -208,3 +208,31 @@ def test_refusal_while_file_jobs_run(tmp_path):
     for _ in range(40):
         with pytest.raises(api.PhopError, match="more than one loaded high-precision orientation frame"):
             api.load_environment(d / "config.json")
+
+
+def _moon_config(d, **kw):
+    cfg = S.make_config(d, 7200.0, 60.0, **kw)
+    p = d / f"moon_{len(list(d.glob('moon_*.json')))}.json"
+    p.write_text(json.dumps(cfg))
+    return p
+
+
+def test_other_bodies_frames_and_refusals(tmp_path):
+    """The J2 model and the field of a body other than the Earth take the
+    body's IAU body model from the orientations; without it, or with a
+    second field, the load is refused with the reason."""
+    with_frame = S.write_environment(tmp_path / "a", S.EnvSpec(moon_frame=True, moon_field=8))
+    without = S.write_environment(tmp_path / "b", S.EnvSpec(moon_field=8))
+    point, _ = api.load_environment(_moon_config(with_frame))
+    j2, _ = api.load_environment(_moon_config(with_frame, moon_gravity="oblateness"))
+    field, _ = api.load_environment(_moon_config(with_frame, moon_gravity="shape", gravity="oblateness"))
+    assert len({point, j2, field}) == 3
+    for kw, what in (({"moon_gravity": "oblateness"}, "The oblateness (J2) model of Moon"),
+                     ({"moon_gravity": "shape", "gravity": "oblateness"}, "The spherical-harmonic field of Moon")):
+        with pytest.raises(api.PhopError) as e:
+            api.load_environment(_moon_config(without, **kw))
+        assert str(e.value).startswith(what + " needs its body-fixed orientation: an IAU body model unit for "
+                                       "NAIF id 301")
+    with pytest.raises(api.PhopError) as e:
+        api.load_environment(_moon_config(with_frame, moon_gravity="shape"))
+    assert "one spherical-harmonic field per configuration" in str(e.value)
