@@ -132,6 +132,7 @@ class _Env(C.Structure):
         ("iau_np_angles", C.c_int),
         ("frame_data", C.POINTER(C.c_double) * 12), ("frame_deg", (C.c_int * 3) * 12),
         ("frame_np", (C.c_int * 3) * 12), ("frame_bary_offset", C.c_int * 12), ("frame_np_deg", C.c_int * 12),
+        ("body_flattening", C.c_double * 12),
     ]
 
 
@@ -257,7 +258,7 @@ def load_environment(config_path) -> Environment:
         gm = bc.get("gm", cst.get("GM", 0.0))
         radius = cst.get("R", 0.0)
         soi = cst.get("SOIOld", cst.get("SOI", 1e20))
-        rows.append((nid, gm, radius, flags, cst.get("J2", 0.0), cst.get("GM", 0.0), soi))
+        rows.append((nid, gm, radius, flags, cst.get("J2", 0.0), cst.get("GM", 0.0), soi, bc.get("flattening", 0.0)))
     rows.sort()
     e.nbodies = len(rows)
     e.body_id = _ip(hold(np.array([r[0] for r in rows], dtype=np.int32)))
@@ -364,7 +365,8 @@ def load_environment(config_path) -> Environment:
     # bodies other than the Earth with the J2 model or the field: their IAU body models
     for bi, r in enumerate(rows):
         e.frame_bary_offset[bi] = -1
-        if r[0] == 399 or not (r[3] & (F_OBLATENESS | F_SHAPE)) or r[0] not in other_iau:
+        e.body_flattening[bi] = r[7]
+        if r[0] == 399 or not (r[3] & (F_OBLATENESS | F_SHAPE | F_ATMOSPHERE)) or r[0] not in other_iau:
             continue
         md, data = other_iau[r[0]]
         vals = list(data)

@@ -134,6 +134,7 @@ typedef struct {
     // kind 1 with its barycentric angles at frame_bary_offset (-1: none)
     const double* frame_data[12];
     int frame_deg[12][3], frame_np[12][3], frame_bary_offset[12], frame_np_deg[12];
+    double body_flattening[12];  // per body: its "flattening" (geodetic height for drag)
 } OracleEnv;
 
 }  // extern "C"
@@ -230,6 +231,38 @@ V3 position(const OracleEnv& e, double t, int body, int center) {
     for (int i = 0; i < nb && pb[i] != common; ++i) p = p + chebUnit(e, unitOf(e, pb[i]), t, nullptr);
     for (int j = 0; j < nc && pc[j] != common; ++j) p = p - chebUnit(e, unitOf(e, pc[j]), t, nullptr);
     return p;
+}
+
+// velocity of `body` relative to `center` (km/s): the chain's Chebyshev derivatives
+V3 velocity(const OracleEnv& e, double t, int body, int center) {
+    if (body == center) return {0, 0, 0};
+    int pb[16], pc[16], nb = 0, nc = 0;
+    for (int b = body; nb < 16; b = e.eph_center[unitOf(e, b)]) {
+        pb[nb++] = b;
+        if (b == 0 || unitOf(e, b) < 0) break;
+    }
+    for (int b = center; nc < 16; b = e.eph_center[unitOf(e, b)]) {
+        pc[nc++] = b;
+        if (b == 0 || unitOf(e, b) < 0) break;
+    }
+    int common = 0;
+    for (int i = 0; i < nb && !common; ++i)
+        for (int j = 0; j < nc; ++j)
+            if (pb[i] == pc[j]) {
+                common = pb[i] == 0 ? -1 : pb[i];
+                break;
+            }
+    if (common == -1) common = 0;
+    V3 v = {0, 0, 0}, dv;
+    for (int i = 0; i < nb && pb[i] != common; ++i) {
+        chebUnit(e, unitOf(e, pb[i]), t, &dv);
+        v = v + dv;
+    }
+    for (int j = 0; j < nc && pc[j] != common; ++j) {
+        chebUnit(e, unitOf(e, pc[j]), t, &dv);
+        v = v - dv;
+    }
+    return v;
 }
 
 // ---- Earth orientation ------------------------------------------------------
@@ -1006,7 +1039,26 @@ V3 acceleration(const OracleEnv& e, const ShFactors& F, V3 pos, V3 vel, double e
                 acc = acc + srp;
             }
         }
-        if ((fl & F_ATMOSPHERE) && !e.has_nrl && e.n_exp > 0) {
+        if ((fl & F_ATMOSPHERE) && body != kEarth && e.n_exp > 0) {
+            // exponential drag in another body's atmosphere (PrivateAccelerations.h:137-206):
+            // relative to the body, about its polar axis, the air moving with
+            // its rotation and its velocity
+            double Rb[9];
+            V3 wb;
+            iauRotation(e.frame_data[bi], e.frame_deg[bi], e.frame_np[bi], e.frame_bary_offset[bi], e.frame_np_deg[bi],
+                        et, Rb, &wb);
+            const V3 rrel = pos - bodyPos;
+            const V3 pole = {Rb[6], Rb[7], Rb[8]};
+            const double h = geodeticAltitude(rrel, pole, e.body_radius[bi], e.body_flattening[bi]);
+            const int band = expBand(e, h);
+            const int n = e.n_exp;
+            if (h <= e.exp_seg[3 * n + band]) {
+                const V3 vr = vel - velocity(e, et, body, kEarth) - cross(wb, rrel);
+                const double rho = e.exp_seg[band] * std::exp(-(h - e.exp_seg[n + band]) / e.exp_seg[2 * n + band]);
+                acc = acc + ((-0.5 * rho * BC * norm(vr)) * vr);
+            }
+        }
+        if ((fl & F_ATMOSPHERE) && body == kEarth && !e.has_nrl && e.n_exp > 0) {
             // exponential drag (PrivateAccelerations.h:137-206)
             if (!haveRot) {
                 earthRotation(e, et, R, &w);

@@ -28,7 +28,7 @@ namespace phop {
 
 constexpr int kMaxBodies = 12;
 constexpr int kMaxChain = 4;
-constexpr int kMaxPoles = 2;  // bodies other than the Earth with the J2 model
+constexpr int kMaxPoles = 1;  // bodies other than the Earth with the J2 model or an atmosphere
 constexpr int kTideTri = 28;  // n <= 6 triangle, index n(n+1)/2 + m
 
 constexpr int kMaxExpBands = 16;
@@ -103,6 +103,10 @@ struct DevEnv {
     int shFrame, shTides;
     int shFrameDeg[3], shFrameNp[3];
     int shFrameData, shFrameBary, shFrameNpDeg;
+    // the exponential atmosphere on a body other than the Earth: its body
+    // index (-1: none; its pole slot gives axis, rate and velocity) and flattening
+    int atmBody;
+    double atmFlattening;
 };
 
 struct EpochRecord {
@@ -113,6 +117,8 @@ struct EpochRecord {
     double dC[kTideTri];         // tide coefficient deltas, field units
     double dS[kTideTri];
     double pole[kMaxPoles][3];   // polar (body z) axes of the J2 bodies other than the Earth, inertial
+    double poleW[kMaxPoles][3];  // their angular velocities, inertial, rad/s
+    double poleV[kMaxPoles][3];  // their velocities relative to the Earth, km/s
     double fieldR[9];            // ICRF -> body rotation of a field on a body other than the Earth
     double nrlSec, nrlGast;      // UTC seconds of day, apparent sidereal time (h)
     double et;                   // the record's epoch, TDB seconds past J2000
@@ -155,6 +161,47 @@ static __device__ __forceinline__ void chebPosition(const DevEnv& e, int u, doub
             x = nx;
         }
         out[dim] = fma(s, x, c[idx] - w);
+    }
+}
+
+// velocity (km/s) of a Chebyshev unit: the derivative of its series
+static __device__ __forceinline__ void chebVelocity(const DevEnv& e, int u, double t, double out[3]) {
+    const double* d = e.ephData + e.ephOffset[u];
+    const int n = e.ephNint[u], deg = e.ephPdeg[u];
+    const double r = d[0];
+    const double* starts = d + 1;
+    const double* cf = d + 1 + n;
+    long idx = (long)((t - starts[0]) / (2 * r));
+    idx = idx < 0 ? 0 : (idx >= n ? n - 1 : idx);
+    const double s = (t - starts[idx]) / r - 1.0;
+    const double s2 = 2 * s;
+    for (int dim = 0; dim < 3; ++dim) {
+        const double* c = cf + (int64_t)dim * (deg + 1) * n;
+        double w = 0, x = 0, dw = 0, v = 0;
+        for (int i = 0; i < deg; ++i) {
+            w = c[idx + (int64_t)(deg - i) * n] - w;
+            const double nx = fma(s2, x, w);
+            w = x;
+            x = nx;
+            const double nv = fma(s2, v, fma(2.0, w, -dw));
+            dw = v;
+            v = nv;
+        }
+        out[dim] = (1.0 / r) * fma(s, v, x - dw);
+    }
+}
+
+static __device__ __forceinline__ void chainVelocity(const DevEnv& e, const int* plus, const int* minus, double t,
+                                                     double out[3]) {
+    out[0] = out[1] = out[2] = 0.0;
+    double p[3];
+    for (int k = 0; k < kMaxChain && plus[k] >= 0; ++k) {
+        chebVelocity(e, plus[k], t, p);
+        out[0] += p[0]; out[1] += p[1]; out[2] += p[2];
+    }
+    for (int k = 0; k < kMaxChain && minus[k] >= 0; ++k) {
+        chebVelocity(e, minus[k], t, p);
+        out[0] -= p[0]; out[1] -= p[1]; out[2] -= p[2];
     }
 }
 
@@ -568,15 +615,20 @@ static __device__ bool evalEpochRecordBase(const DevEnv& e, double et, EpochReco
     for (int i = 0; i < 9; ++i) r.R[i] = (i % 4 == 0) ? 1.0 : 0.0;
     r.w[0] = r.w[1] = r.w[2] = 0.0;
     if (e.hasRot) earthRotation(e, et, r.R, r.w);
-    for (int k = 0; k < kMaxPoles; ++k) {
-        r.pole[k][0] = r.pole[k][1] = r.pole[k][2] = 0.0;
-        if (k >= e.nPoles) continue;
-        // the body's z axis in inertial axes: the third row of its ICRF -> body rotation
-        double Rb[9], wb[3];
-        iauRotation(e.poleCoef + e.poleData[k], e.poleDeg[k], e.poleNp[k], e.poleBary[k], e.poleNpDeg[k], et, Rb, wb);
+    for (int k = 0; k < kMaxPoles; ++k)
+        for (int i = 0; i < 3; ++i) r.pole[k][i] = r.poleW[k][i] = r.poleV[k][i] = 0.0;
+    for (int b = 0; b < e.nbodies; ++b) {
+        const int k = e.poleSlot[b];
+        if (k < 0) continue;
+        // the body's z axis in inertial axes (the third row of its ICRF ->
+        // body rotation), its angular velocity and its velocity
+        double Rb[9];
+        iauRotation(e.poleCoef + e.poleData[k], e.poleDeg[k], e.poleNp[k], e.poleBary[k], e.poleNpDeg[k], et, Rb,
+                    r.poleW[k]);
         r.pole[k][0] = Rb[6];
         r.pole[k][1] = Rb[7];
         r.pole[k][2] = Rb[8];
+        if (b == e.atmBody) chainVelocity(e, e.chainPlus[b], e.chainMinus[b], et, r.poleV[k]);
     }
     for (int i = 0; i < 9; ++i) r.fieldR[i] = (i % 4 == 0) ? 1.0 : 0.0;
     if (e.shFrame) {

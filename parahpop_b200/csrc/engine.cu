@@ -503,7 +503,8 @@ static void selectPoleFrames(const std::vector<EarthFrameUnit>& units, HostEnvir
     for (size_t bi = 0; bi < env.bodies.size(); ++bi) {
         const auto& b = env.bodies[bi];
         const bool field = (b.flags & kShape) != 0;
-        if (b.id == 399 || !((b.flags & kOblateness) || field)) continue;
+        const bool air = (b.flags & kAtmosphere) != 0;
+        if (b.id == 399 || !((b.flags & kOblateness) || field || air)) continue;
         const EarthFrameUnit* pick = nullptr;
         for (const EarthFrameUnit& f : units)
             if (f.kind == 1 && f.target == b.id) {
@@ -511,10 +512,12 @@ static void selectPoleFrames(const std::vector<EarthFrameUnit>& units, HostEnvir
                 break;
             }
         if (!pick)
-            throw std::runtime_error(std::string(field ? "The spherical-harmonic field" : "The oblateness (J2) model")
+            throw std::runtime_error(std::string(field ? "The spherical-harmonic field"
+                                                 : air ? "The atmosphere" : "The oblateness (J2) model")
                                      + " of " + b.name + " needs its body-fixed orientation: an IAU body model unit "
                                      "for NAIF id " + std::to_string(b.id) + " among the environment's orientations.");
-        if (!field && env.poles.size() >= (size_t)kMaxPoles)
+        const bool pole = !field || air || (b.flags & kOblateness);
+        if (pole && env.poles.size() >= (size_t)kMaxPoles)
             throw std::runtime_error("This backend takes the J2 model on at most " + std::to_string(kMaxPoles)
                                      + " bodies besides the Earth.");
         HostEnvironment::PoleBody pb;
@@ -537,8 +540,8 @@ static void selectPoleFrames(const std::vector<EarthFrameUnit>& units, HostEnvir
                     pb.data.insert(pb.data.end(), u.data.begin(), u.data.end());
                     break;
                 }
-        if (field) env.shFrame = std::move(pb);
-        else env.poles.push_back(std::move(pb));
+        if (field) env.shFrame = pb;
+        if (pole) env.poles.push_back(std::move(pb));
     }
 }
 
@@ -850,15 +853,22 @@ static void loadEnvironmentFilesIn(const Value& e, HostEnvironment& env, FileJob
             } else if (k == "occulting") {
                 if (f.second.asBool()) b.flags |= kOcculting;
             } else if (k == "atmosphere") {
-                if (b.id != 399) throw std::runtime_error("Atmospheric drag is supported for the Earth only.");
-                // single-key model dispatch (interface Atmosphere.h:136-166)
+                // single-key model dispatch (interface Atmosphere.h:136-166); one
+                // atmosphere per configuration, NRLMSISE-00 on the Earth only
+                // (Environment.h:124-132)
+                for (const auto& other : env.bodies)
+                    if (other.flags & kAtmosphere)
+                        throw std::runtime_error("This backend takes one atmosphere per configuration; " + b.name
+                                                 + " would hold a second.");
                 if (!f.second.isObject() || f.second.size() != 1)
                     throw std::runtime_error("Atmosphere block must be a single-key dispatch dict naming the model.");
                 std::string mk = f.second.members()[0].first;
                 std::transform(mk.begin(), mk.end(), mk.begin(), ::tolower);
                 const Value& mv = f.second.members()[0].second;
                 b.flags |= kAtmosphere;
+                env.atmBodyId = b.id;
                 if (mk == "nrlmsise00" || mk == "nrlmsise-00") {
+                    if (b.id != 399) throw std::runtime_error("NRLMSISE-00 may only be configured on Earth.");
                     atmosphere = &mv;
                 } else if (mk == "exponential") {
                     loadExponentialAtmosphere(mv, env);
@@ -870,7 +880,8 @@ static void loadEnvironmentFilesIn(const Value& e, HostEnvironment& env, FileJob
                 if (b.id != 399) throw std::runtime_error("Body orientations are supported for the Earth only.");
                 env.earthOrientation = f.second.asString();
             } else if (k == "flattening") {
-                if (b.id == 399) env.flattening = f.second.asDouble();
+                b.flattening = f.second.asDouble();
+                if (b.id == 399) env.flattening = b.flattening;
             } else if (k == "gm") {
                 b.gm = f.second.asDouble();
             } else if (k == "oblateness" || k == "shape") {
@@ -967,7 +978,7 @@ uint64_t environmentDigest(const HostEnvironment& e) {
         }
     for (const auto& b : e.bodies) {
         mix(b.name.data(), b.name.size());
-        s(b.id), s(b.flags), s(b.gm), s(b.radius), s(b.j2), s(b.gmConst), s(b.soi);
+        s(b.id), s(b.flags), s(b.gm), s(b.radius), s(b.j2), s(b.gmConst), s(b.soi), s(b.flattening);
     }
     s(e.flattening), s(e.hasShape), s(e.shDegree), s(e.shOrder), s(e.shNormalized), s(e.shR), s(e.shGM);
     v(e.shC), v(e.shS);
@@ -986,7 +997,7 @@ uint64_t environmentDigest(const HostEnvironment& e) {
         s(pb.bodyIndex), s(pb.deg), s(pb.np), s(pb.baryOffset), s(pb.npDeg);
         v(pb.data);
     }
-    s(e.shBodyId), s(e.shFrame.bodyIndex), s(e.shFrame.deg), s(e.shFrame.np), s(e.shFrame.baryOffset);
+    s(e.atmBodyId), s(e.shBodyId), s(e.shFrame.bodyIndex), s(e.shFrame.deg), s(e.shFrame.np), s(e.shFrame.baryOffset);
     s(e.shFrame.npDeg), v(e.shFrame.data);
     return h;
 }
@@ -1146,6 +1157,13 @@ void Engine::uploadEnvironment() {
         for (int c = 0; c < 4; ++c) e.expSeg[k][c] = h.expSeg[k][c];
     e.earthRadius = h.bodies[e.earthIndex].radius;
     e.flattening = h.flattening;
+    e.atmBody = -1;
+    e.atmFlattening = 0.0;
+    for (size_t b = 0; b < h.bodies.size(); ++b)
+        if (h.bodies[b].id == h.atmBodyId && h.atmBodyId != 399 && (h.bodies[b].flags & kAtmosphere)) {
+            e.atmBody = (int)b;
+            e.atmFlattening = h.bodies[b].flattening;
+        }
     e.au = h.au;
     if (h.solid || h.ocean) {
         chainUnits(h, 10, 399, e.sunUnitsPlus, e.sunUnitsMinus);

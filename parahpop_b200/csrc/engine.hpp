@@ -38,6 +38,7 @@ struct HostEnvironment {
         int flags = 0;
         double gm = 0.0, radius = 0.0;
         double j2 = 0.0, gmConst = 0.0, soi = 1e20;  // oblateness model (constants file)
+        double flattening = 0.0;                     // the body's "flattening" (geodetic height for drag)
     };
     std::vector<Body> bodies;
     double flattening = 0.0;
@@ -90,6 +91,8 @@ struct HostEnvironment {
     // for a body other than the Earth, its IAU body model
     int shBodyId = 399;
     PoleBody shFrame;
+    // the body whose atmosphere the exponential model describes (one per configuration)
+    int atmBodyId = 399;
 };
 
 // Loads the environment of a `model` configuration object (the reference's

@@ -127,6 +127,8 @@ struct RecordRef {
     __device__ __forceinline__ double dC(int k) const { return r->dC[k]; }
     __device__ __forceinline__ double dS(int k) const { return r->dS[k]; }
     __device__ __forceinline__ double pole(int k, int i) const { return r->pole[k][i]; }
+    __device__ __forceinline__ double poleW(int k, int i) const { return r->poleW[k][i]; }
+    __device__ __forceinline__ double poleV(int k, int i) const { return r->poleV[k][i]; }
     __device__ __forceinline__ double SR(int i) const { return r->fieldR[i]; }
     // NRLMSISE-00 time inputs; valid = -1 (evaluate at the epoch in `sec`
     // when an object below the cut-off needs them) when the record has none
@@ -171,6 +173,12 @@ struct RecordInterp {
     __device__ __forceinline__ double dS(int k) const { return at((int)(offsetof(EpochRecord, dS) / 8) + k); }
     __device__ __forceinline__ double pole(int k, int i) const {
         return at((int)(offsetof(EpochRecord, pole) / 8) + 3 * k + i);
+    }
+    __device__ __forceinline__ double poleW(int k, int i) const {
+        return at((int)(offsetof(EpochRecord, poleW) / 8) + 3 * k + i);
+    }
+    __device__ __forceinline__ double poleV(int k, int i) const {
+        return at((int)(offsetof(EpochRecord, poleV) / 8) + 3 * k + i);
     }
     __device__ __forceinline__ double SR(int i) const { return at((int)(offsetof(EpochRecord, fieldR) / 8) + i); }
     // NRLMSISE-00 time inputs: evaluated exactly at the stage epoch by the
@@ -899,7 +907,7 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
         // read from the record once
         double fb[3] = {0.0, 0.0, 0.0}, rb[3] = {0.0, 0.0, 0.0};
         if (isEarth && ((fl & (kShape | kOblateness)) || ((fl & kAtmosphere) && e.hasNrl))) toBody(r, pos, fb);
-        if (((fl & kGravity) && !isEarth) || (fl & kRadiation)) {
+        if (((fl & (kGravity | kAtmosphere)) && !isEarth) || (fl & kRadiation)) {
             rb[0] = r.body(bi, 0);
             rb[1] = r.body(bi, 1);
             rb[2] = r.body(bi, 2);
@@ -1016,7 +1024,29 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
             ay += f * dp[1];
             az += f * dp[2];
         }
-        if ((fl & kAtmosphere) && !e.hasNrl && e.nExp > 0) {
+        if ((fl & kAtmosphere) && !isEarth && e.nExp > 0 && e.poleSlot[bi] >= 0) {
+            // exponential drag in another body's atmosphere (PrivateAccelerations.h:143-204):
+            // geodetic height about its polar axis, the air moving with its
+            // rotation and its velocity relative to the Earth
+            const int k = e.poleSlot[bi];
+            const double d[3] = {pos[0] - rb[0], pos[1] - rb[1], pos[2] - rb[2]};
+            const double pole[3] = {r.pole(k, 0), r.pole(k, 1), r.pole(k, 2)};
+            const double h = geodeticHeight(d, pole, e.bodyRadius[bi], e.atmFlattening);
+            int band = 0;
+            for (int sgi = 1; sgi < e.nExp; ++sgi) band += e.expSeg[sgi][1] <= h ? 1 : 0;
+            if (h <= e.expSeg[band][3]) {
+                const double rho = e.expSeg[band][0] * exp(-(h - e.expSeg[band][1]) / e.expSeg[band][2]);
+                const double w[3] = {r.poleW(k, 0), r.poleW(k, 1), r.poleW(k, 2)};
+                const double vr0 = vel[0] - r.poleV(k, 0) - (w[1] * d[2] - w[2] * d[1]);
+                const double vr1 = vel[1] - r.poleV(k, 1) - (w[2] * d[0] - w[0] * d[2]);
+                const double vr2 = vel[2] - r.poleV(k, 2) - (w[0] * d[1] - w[1] * d[0]);
+                const double f = -0.5 * rho * bc * sqrt(vr0 * vr0 + vr1 * vr1 + vr2 * vr2);
+                ax += f * vr0;
+                ay += f * vr1;
+                az += f * vr2;
+            }
+        }
+        if ((fl & kAtmosphere) && isEarth && !e.hasNrl && e.nExp > 0) {
             // piecewise exponential drag (PrivateAccelerations.h:137-206,
             // PiecewiseExponentialAtmosphere.h:40-90): band = bands above the
             // first whose base h0 <= h; no drag above the band's cut-off

@@ -672,14 +672,16 @@ def make_config(env_dir, duration, step, max_steps=1000000, threads=1, force="fu
                 relativity=True, drag=True, srp=True, start_mjd=4016.0, end_mjd=4064.0,
                 gravity="shape", atmosphere="nrlmsise00", tide_system="zero_tide",
                 occulting=("Earth",), earth_orientation=None, ephemeris=("bodies.brie",),
-                moon_gravity="point", moon_degree=8) -> dict:
+                moon_gravity="point", moon_degree=8, moon_atmosphere=False) -> dict:
     """Run configuration in the reference schema (``example/config/envisat_full.json``).
     Paths are relative to ``env_dir`` (where the config file is written).
     ``gravity``: "shape" (the spherical-harmonic file) or "oblateness" (the
     J2 model from the constants file); ``atmosphere``: "nrlmsise00",
     "exponential" (one band) or "piecewise" (three bands); ``moon_gravity``:
     "point", "oblateness" (the Moon's J2 model in its IAU frame) or "shape"
-    (the lunar field of moon.tab, degree ``moon_degree``, in the same frame)."""
+    (the lunar field of moon.tab, degree ``moon_degree``, in the same frame);
+    ``moon_atmosphere``: an exponential atmosphere on the Moon (a test of
+    drag about a body other than the Earth, not a lunar model)."""
     earth: dict = {}
     if force == "central":
         earth = {"gravity": True}
@@ -714,6 +716,10 @@ def make_config(env_dir, duration, step, max_steps=1000000, threads=1, force="fu
                                         "degree": moon_degree, "order": moon_degree}}
                 bodies_cfg["Moon"] = ({"gravity": grav_m, "occulting": True} if "Moon" in occulting
                                       else {"gravity": grav_m})
+                if moon_atmosphere:
+                    bodies_cfg["Moon"]["flattening"] = 0.0012
+                    bodies_cfg["Moon"]["atmosphere"] = {"exponential": {"rho0": 0.05, "h0": 100.0,
+                                                                        "scaleHeight": 120.0, "hCutoff": 1200.0}}
             elif b == "JupiterBarycenter":
                 bodies_cfg["JupiterBarycenter"] = {"gm": 126712764.1, "gravity": True}
     env = {"bodies": bodies_cfg, "ephemeris": list(ephemeris), "constants": "constants.json", "preferSSB": True}

@@ -116,6 +116,11 @@ CASES["moon_j2_2h"] = (lambda: S.population_lunar(12, 17), 7200.0, 60.0, {"moon_
 # their own); the lunar field moves these orbits by 0.5-5 km in 2 h
 CASES["moon_field_2h"] = (lambda: S.population_lunar(12, 18), 7200.0, 60.0,
                           {"moon_gravity": "shape", "gravity": "oblateness"}, {"moon_frame": True, "moon_field": 8})
+# drag about a body other than the Earth: an exponential atmosphere on the
+# Moon (flattening 0.0012), the air moving with the Moon's IAU rotation and
+# its velocity; it moves these orbits by 0.1-50 m in 2 h
+CASES["moon_drag_2h"] = (lambda: S.population_lunar(12, 19), 7200.0, 60.0, {"moon_atmosphere": True},
+                         {"moon_frame": True})
 
 
 def lunar_penumbra():

@@ -236,3 +236,37 @@ def test_other_bodies_frames_and_refusals(tmp_path):
     with pytest.raises(api.PhopError) as e:
         api.load_environment(_moon_config(with_frame, moon_gravity="shape"))
     assert "one spherical-harmonic field per configuration" in str(e.value)
+
+
+def test_atmosphere_of_another_body(tmp_path):
+    """An exponential atmosphere on a body other than the Earth takes the
+    body's IAU frame; NRLMSISE-00 stays on the Earth, and a configuration
+    holds one atmosphere."""
+    with_frame = S.write_environment(tmp_path / "a", S.EnvSpec(moon_frame=True))
+    without = S.write_environment(tmp_path / "b", S.EnvSpec())
+    # the Earth without drag, the Moon with an exponential atmosphere
+    cfg = S.make_config(with_frame, 7200.0, 60.0, drag=False, moon_atmosphere=True)
+    p = with_frame / "moon_air.json"
+    p.write_text(json.dumps(cfg))
+    api.load_environment(p)
+    cfg = S.make_config(without, 7200.0, 60.0, drag=False, moon_atmosphere=True)
+    p = without / "moon_air.json"
+    p.write_text(json.dumps(cfg))
+    with pytest.raises(api.PhopError) as e:
+        api.load_environment(p)
+    assert str(e.value).startswith("The atmosphere of Moon needs its body-fixed orientation")
+    # the Earth's NRLMSISE-00 and the Moon's atmosphere: two atmospheres
+    cfg = S.make_config(with_frame, 7200.0, 60.0, moon_atmosphere=True)
+    p = with_frame / "two_air.json"
+    p.write_text(json.dumps(cfg))
+    with pytest.raises(api.PhopError) as e:
+        api.load_environment(p)
+    assert "one atmosphere per configuration" in str(e.value)
+    cfg = S.make_config(with_frame, 7200.0, 60.0, drag=False)
+    cfg["model"]["environment"]["bodies"]["Moon"]["atmosphere"] = {"nrlmsise00": {
+        "spaceWeatherFile": "SW-All.txt", "coverageStartMjdUtc": 55559.0, "coverageEndMjdUtc": 55610.0}}
+    p = with_frame / "moon_nrl.json"
+    p.write_text(json.dumps(cfg))
+    with pytest.raises(api.PhopError) as e:
+        api.load_environment(p)
+    assert "NRLMSISE-00 may only be configured on Earth." in str(e.value)
