@@ -1074,7 +1074,7 @@ V3 acceleration(const OracleEnv& e, const ShFactors& F, V3 pos, V3 vel, double e
                 acc = acc + ((-0.5 * rho * BC * norm(vr)) * vr);
             }
         }
-        if ((fl & F_ATMOSPHERE) && e.has_nrl) {
+        if ((fl & F_ATMOSPHERE) && body == kEarth && e.has_nrl) {
             if (!haveRot) {
                 earthRotation(e, et, R, &w);
                 haveRot = true;

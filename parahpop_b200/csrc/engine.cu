@@ -853,24 +853,23 @@ static void loadEnvironmentFilesIn(const Value& e, HostEnvironment& env, FileJob
             } else if (k == "occulting") {
                 if (f.second.asBool()) b.flags |= kOcculting;
             } else if (k == "atmosphere") {
-                // single-key model dispatch (interface Atmosphere.h:136-166); one
-                // atmosphere per configuration, NRLMSISE-00 on the Earth only
-                // (Environment.h:124-132)
-                for (const auto& other : env.bodies)
-                    if (other.flags & kAtmosphere)
-                        throw std::runtime_error("This backend takes one atmosphere per configuration; " + b.name
-                                                 + " would hold a second.");
+                // single-key model dispatch (interface Atmosphere.h:136-166);
+                // NRLMSISE-00 on the Earth only (Environment.h:124-132), one
+                // exponential atmosphere per configuration
                 if (!f.second.isObject() || f.second.size() != 1)
                     throw std::runtime_error("Atmosphere block must be a single-key dispatch dict naming the model.");
                 std::string mk = f.second.members()[0].first;
                 std::transform(mk.begin(), mk.end(), mk.begin(), ::tolower);
                 const Value& mv = f.second.members()[0].second;
                 b.flags |= kAtmosphere;
-                env.atmBodyId = b.id;
                 if (mk == "nrlmsise00" || mk == "nrlmsise-00") {
                     if (b.id != 399) throw std::runtime_error("NRLMSISE-00 may only be configured on Earth.");
                     atmosphere = &mv;
                 } else if (mk == "exponential") {
+                    if (!env.expSeg.empty())
+                        throw std::runtime_error("This backend takes one exponential atmosphere per configuration; "
+                                                 + b.name + " would hold a second.");
+                    env.atmBodyId = b.id;
                     loadExponentialAtmosphere(mv, env);
                 } else {
                     throw std::runtime_error("Unknown atmosphere model: '" + f.second.members()[0].first

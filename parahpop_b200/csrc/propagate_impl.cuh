@@ -1066,7 +1066,7 @@ static __device__ __forceinline__ void accelerations(const StepParams& p, const 
                 az += f * vr2;
             }
         }
-        if ((fl & kAtmosphere) && e.hasNrl) {
+        if ((fl & kAtmosphere) && isEarth && e.hasNrl) {
             const double rho = nrlDensity<L>(e, r.nrlDeferred(), fb);
             const double w[3] = {r.W(0), r.W(1), r.W(2)};
             const double vr0 = vel[0] - (w[1] * pos[2] - w[2] * pos[1]);

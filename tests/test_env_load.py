@@ -255,13 +255,18 @@ def test_atmosphere_of_another_body(tmp_path):
     with pytest.raises(api.PhopError) as e:
         api.load_environment(p)
     assert str(e.value).startswith("The atmosphere of Moon needs its body-fixed orientation")
-    # the Earth's NRLMSISE-00 and the Moon's atmosphere: two atmospheres
+    # the Earth's NRLMSISE-00 beside the Moon's exponential atmosphere loads;
+    # two exponential atmospheres do not
     cfg = S.make_config(with_frame, 7200.0, 60.0, moon_atmosphere=True)
     p = with_frame / "two_air.json"
     p.write_text(json.dumps(cfg))
+    api.load_environment(p)
+    cfg = S.make_config(with_frame, 7200.0, 60.0, atmosphere="exponential", moon_atmosphere=True)
+    p = with_frame / "two_exp.json"
+    p.write_text(json.dumps(cfg))
     with pytest.raises(api.PhopError) as e:
         api.load_environment(p)
-    assert "one atmosphere per configuration" in str(e.value)
+    assert "one exponential atmosphere per configuration" in str(e.value)
     cfg = S.make_config(with_frame, 7200.0, 60.0, drag=False)
     cfg["model"]["environment"]["bodies"]["Moon"]["atmosphere"] = {"nrlmsise00": {
         "spaceWeatherFile": "SW-All.txt", "coverageStartMjdUtc": 55559.0, "coverageEndMjdUtc": 55610.0}}
