@@ -115,3 +115,30 @@ def test_kept_environment_runs_match_in_process_runs(golden, server, tmp_path):
     assert split.returncode == 0, split.stderr
     assert np.abs(_states(tmp_path / "split")[:, 2:5] - _states(tmp_path / "inproc")[:, 2:5]).max() < 1e-5
     assert server.stop() == (0, 0)
+
+
+def _exchange(sock_path, payload: bytes) -> dict:
+    import socket
+    import struct
+    s = socket.socket(socket.AF_UNIX, socket.SOCK_STREAM)
+    s.settimeout(30)
+    s.connect(sock_path)
+    s.sendall(struct.pack("<I", len(payload)) + payload)
+    n = struct.unpack("<I", s.recv(4, socket.MSG_WAITALL))[0]
+    data = b""
+    while len(data) < n:
+        data += s.recv(n - len(data))
+    s.close()
+    return json.loads(data)
+
+
+def test_malformed_requests_are_answered(server):
+    """A request that is not the protocol's JSON gets a failure answer and
+    the server keeps serving; a run request with the wrong number of paths
+    gets the driver's own message."""
+    bad = _exchange(server.sock, b"this is not json")
+    assert bad["status"] == 1 and bad["stderr"].startswith("ParaHPOP: ")
+    missing = _exchange(server.sock, json.dumps({"args": ["only-one"], "split": -1, "lanes": 0}).encode())
+    assert missing["status"] == 1
+    assert missing["stderr"].startswith("ParaHPOP: Expected CONFIG.json TARGETS.json OUTPUT_DIRECTORY")
+    assert server.stop() == (0, 0)
